@@ -1,0 +1,134 @@
+/*
+ * ppf.h -- C ABI of libppf.so, the B200 (sm_100a) particle-filter library.
+ *
+ * The library replaces the per-observation loop of pypomp's particle filter
+ * (the jitted XLA programs behind pypomp's functional API) for the built-in
+ * models LG, SV and Ricker.  Each entry point is the drop-in for one reference
+ * function; the Python host layer (pypomp_b200.functional) binds them with
+ * ctypes exactly as a maintainer would bind them from pypomp.
+ *
+ * Conventions
+ *  - Every pointer argument is DEVICE memory owned by the caller, unless the
+ *    comment says host.  The library allocates nothing on the device: all
+ *    scratch lives in the caller's workspace (size from *_workspace_bytes).
+ *  - Calls are asynchronous on the given stream and reentrant across distinct
+ *    (stream, workspace) pairs.
+ *  - Return codes: PPF_OK, PPF_EINVAL (bad sizes / null pointers / J < 1),
+ *    PPF_ECUDA (launch or runtime error), PPF_ETIMEOUT (a bounded device-side
+ *    wait gave up; results are invalid), PPF_EUNSUPPORTED.
+ *  - Arithmetic (the exact definitions every path and the C oracle share):
+ *      state and log-weights float32, model math in a fixed operation order
+ *      with the elementary functions of ppf_detmath.h;
+ *      e_j = exp(w_j - max w) rounded to the fixed-point integer
+ *      q_j = rint(e_j * 2^40) (uint64), CDF C_j = q_0 + ... + q_j exact;
+ *      systematic points with u32 = floor(U * 2^32):
+ *      parent(k) = #{ j : C_j * J * 2^32 <= (u32 + k 2^32) * C_{J-1} }
+ *      (128-bit exact; this is searchsorted(cdf, (U+k)/J, side="right"));
+ *      log-likelihood terms and their running sum in float64.
+ *    J is limited to 2^21 so that the fixed-point total fits 62 bits.
+ */
+#ifndef PPF_H
+#define PPF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPF_OK 0
+#define PPF_EINVAL 1
+#define PPF_ECUDA 2
+#define PPF_ETIMEOUT 3
+#define PPF_EUNSUPPORTED 4
+
+#define PPF_MAX_J (1 << 21)
+
+/* Built-in models (pypomp/models/linear_gaussian.py:337 LG; the SV and Ricker
+ * factories follow the same pattern, pypomp/models/spx.py:161). */
+enum { PPF_MODEL_LG = 1, PPF_MODEL_SV = 2, PPF_MODEL_RICKER = 3 };
+
+typedef struct ppf_model {
+  int32_t kind;     /* PPF_MODEL_* */
+  int32_t dx;       /* state dimension (LG 1..4, SV 2, Ricker 1) */
+  int32_t dy;       /* observation dimension (LG 1..4, SV 1, Ricker 1) */
+  int32_t n_params; /* P, the canonical parameter count */
+  float dt;         /* SV time step (1/252); ignored by the other models */
+  int32_t reserved;
+} ppf_model;
+
+/* Flags */
+#define PPF_F_CLL (1u << 0)      /* per-step conditional log-likelihood */
+#define PPF_F_ESS (1u << 1)      /* per-step effective sample size */
+#define PPF_F_FMEAN (1u << 2)    /* per-step filter mean */
+#define PPF_F_PMEAN (1u << 3)    /* per-step prediction mean */
+#define PPF_F_INJECT (1u << 4)   /* read noise from inj_* instead of Philox */
+#define PPF_F_SAVE_ANC (1u << 5) /* write resampling ancestors */
+#define PPF_F_SAVE_W (1u << 6)   /* write unnormalised log-weights */
+#define PPF_F_EST (1u << 7)      /* theta on the estimation scale */
+
+/* Execution paths; all produce bit-identical results. */
+enum {
+  PPF_PATH_AUTO = 0,     /* autotuner / size heuristic */
+  PPF_PATH_PLAIN = 1,    /* one filter at a time, textbook kernels (1x baseline) */
+  PPF_PATH_STREAM = 2,   /* batched, HBM-streaming, 2 fused kernels per step */
+  PPF_PATH_RESIDENT = 3  /* batched, one CTA per filter, swarm in shared memory */
+};
+
+/* Inputs and outputs of one batched bootstrap particle filter call over F
+ * filters.  Replaces _pfilter_internal / _pfilter_step
+ * (pypomp/core/algorithms/pfilter.py:15-182) vmapped over parameter sets and
+ * replicate keys (pfilter.py:185-207) and over panel units
+ * (_chunked_panel_pfilter_internal, pfilter.py:248-304). */
+typedef struct ppf_pfilter_desc {
+  ppf_model model;
+  int32_t J;            /* particles per filter, 1..PPF_MAX_J */
+  int32_t F;            /* filters in the batch */
+  int32_t T;            /* observations in the longest series */
+  int32_t U;            /* number of observation series (panel units) */
+  int32_t path;         /* PPF_PATH_* */
+  uint32_t flags;       /* PPF_F_* */
+  float thresh;         /* resampling threshold as in pfilter.py:159 */
+  int32_t tile;         /* particles per CTA tile (0 = autotuned) */
+  const float* theta;   /* [F][P] parameters (natural scale unless PPF_F_EST) */
+  const float* ys;      /* [U][T][dy] observations */
+  const float* ycon;    /* [U][T] per-observation constant (Ricker: lgamma(y+1)) or NULL */
+  const int32_t* unit;  /* [F] series index of each filter, or NULL (series 0) */
+  const int32_t* T_u;   /* [U] series lengths (ragged panels), or NULL (all T) */
+  const uint64_t* seeds;/* [F] Philox keys */
+  const float* inj_z0;  /* [F][J][n0] initial-state normals (PPF_F_INJECT) */
+  const float* inj_z;   /* [F][T][J][nz] process normals (PPF_F_INJECT) */
+  const float* inj_u;   /* [F][T] resampling uniforms in [0,1) (PPF_F_INJECT) */
+  double* loglik;       /* out [F] log-likelihood estimate */
+  double* cll;          /* out [F][T] (PPF_F_CLL) */
+  float* ess;           /* out [F][T] (PPF_F_ESS) */
+  float* fmean;         /* out [F][T][dx] (PPF_F_FMEAN) */
+  float* pmean;         /* out [F][T][dx] (PPF_F_PMEAN) */
+  int32_t* anc;         /* out [F][T][J] (PPF_F_SAVE_ANC) */
+  float* logw;          /* out [F][T][J] (PPF_F_SAVE_W) */
+  void* workspace;
+  size_t ws_bytes;
+} ppf_pfilter_desc;
+
+/* Workspace bytes ppf_pfilter needs for this descriptor (pointers ignored). */
+size_t ppf_pfilter_workspace_bytes(const ppf_pfilter_desc* d);
+
+/* Run the batched particle filter.  `stream` is a cudaStream_t. */
+int ppf_pfilter(const ppf_pfilter_desc* d, void* stream);
+
+/* Synchronise `stream` and report whether any bounded device-side wait of the
+ * last call that used `workspace` gave up (PPF_ETIMEOUT) -- PPF_OK otherwise. */
+int ppf_workspace_status(const void* workspace, void* stream);
+
+/* Human-readable message for a return code (static storage). */
+const char* ppf_error_string(int code);
+
+/* Library version string (static storage). */
+const char* ppf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PPF_H */

@@ -1,0 +1,154 @@
+"""ctypes wrapper of the C oracle (``oracle/_build/libppf_oracle.so``).
+
+TEST INFRASTRUCTURE ONLY.  Runs the restatement on HOST arrays with the same
+descriptor layout as the CUDA library's ``ppf_pfilter_desc`` (include/ppf.h).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+_SO = Path(__file__).resolve().parent / "_build" / "libppf_oracle.so"
+_vp = ctypes.c_void_p
+
+
+class _Model(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("dx", ctypes.c_int32), ("dy", ctypes.c_int32),
+                ("n_params", ctypes.c_int32), ("dt", ctypes.c_float), ("reserved", ctypes.c_int32)]
+
+
+class _Desc(ctypes.Structure):
+    _fields_ = [("model", _Model), ("J", ctypes.c_int32), ("F", ctypes.c_int32),
+                ("T", ctypes.c_int32), ("U", ctypes.c_int32), ("path", ctypes.c_int32),
+                ("flags", ctypes.c_uint32), ("thresh", ctypes.c_float), ("tile", ctypes.c_int32)] + [
+        (n, _vp) for n in ("theta", "ys", "ycon", "unit", "T_u", "seeds", "inj_z0", "inj_z",
+                           "inj_u", "loglik", "cll", "ess", "fmean", "pmean", "anc", "logw",
+                           "workspace")] + [("ws_bytes", ctypes.c_size_t)]
+
+
+def lib():
+    if not _SO.exists():
+        raise ImportError(f"oracle library missing: {_SO} (run `make -C oracle`)")
+    L = ctypes.CDLL(str(_SO))
+    L.ppfo_pfilter.argtypes = [ctypes.POINTER(_Desc), ctypes.c_int, ctypes.c_int]
+    L.ppfo_pfilter.restype = ctypes.c_int
+    L.ppfo_expf.argtypes = [ctypes.c_float]
+    L.ppfo_expf.restype = ctypes.c_float
+    L.ppfo_logf.argtypes = [ctypes.c_float]
+    L.ppfo_logf.restype = ctypes.c_float
+    L.ppfo_sincos2pif.argtypes = [ctypes.c_float, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+    L.ppfo_philox.argtypes = [_vp, _vp, _vp]
+    L.ppfo_normals.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                               ctypes.c_int, _vp]
+    return L
+
+
+_LIB = None
+
+
+def _L():
+    global _LIB
+    if _LIB is None:
+        _LIB = lib()
+    return _LIB
+
+
+def _p(a):
+    return 0 if a is None else a.ctypes.data
+
+
+def pfilter(kind, dx, dy, theta_f, ys, J, *, seeds=None, ycon=None, unit=None, T_u=None,
+            dt=0.0, thresh=0.0, est=False, inject=None, mop=False, CLL=False, ESS=False,
+            fmean=False, pmean=False, anc=False, logw=False, nthreads=1):
+    """Run the oracle over F filters; arrays on the host.  Returns a dict."""
+    theta_f = np.ascontiguousarray(np.atleast_2d(theta_f), dtype=np.float32)
+    F, P = theta_f.shape
+    ys = np.ascontiguousarray(ys, dtype=np.float32)
+    if ys.ndim == 2:
+        ys = ys[None]
+    U, T, _ = ys.shape
+    keep = [theta_f, ys]
+    d = _Desc()
+    d.model = _Model(kind, dx, dy, P, dt, 0)
+    d.J, d.F, d.T, d.U = J, F, T, U
+    flags = (1 if CLL else 0) | (2 if ESS else 0) | (4 if fmean else 0) | (8 if pmean else 0)
+    flags |= (32 if anc else 0) | (64 if logw else 0) | (128 if est else 0)
+    d.thresh = thresh
+    d.theta, d.ys = _p(theta_f), _p(ys)
+    if ycon is not None:
+        ycon = np.ascontiguousarray(ycon, dtype=np.float32)
+        keep.append(ycon)
+        d.ycon = _p(ycon)
+    if unit is not None:
+        unit = np.ascontiguousarray(unit, dtype=np.int32)
+        keep.append(unit)
+        d.unit = _p(unit)
+    if T_u is not None:
+        T_u = np.ascontiguousarray(T_u, dtype=np.int32)
+        keep.append(T_u)
+        d.T_u = _p(T_u)
+    if seeds is not None:
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+        keep.append(seeds)
+        d.seeds = _p(seeds)
+    if inject is not None:
+        flags |= 16
+        for k, name in (("z0", "inj_z0"), ("z", "inj_z"), ("u", "inj_u")):
+            if inject.get(k) is not None:
+                a = np.ascontiguousarray(inject[k], dtype=np.float32)
+                keep.append(a)
+                setattr(d, name, _p(a))
+    d.flags = flags
+    out = {"loglik": np.zeros(F, np.float64)}
+    if CLL:
+        out["cll"] = np.zeros((F, T), np.float64)
+    if ESS:
+        out["ess"] = np.zeros((F, T), np.float32)
+    if fmean:
+        out["fmean"] = np.zeros((F, T, dx), np.float32)
+    if pmean:
+        out["pmean"] = np.zeros((F, T, dx), np.float32)
+    if anc:
+        out["anc"] = np.zeros((F, T, J), np.int32)
+    if logw:
+        out["logw"] = np.zeros((F, T, J), np.float32)
+    d.loglik = _p(out["loglik"])
+    d.cll, d.ess = _p(out.get("cll")), _p(out.get("ess"))
+    d.fmean, d.pmean = _p(out.get("fmean")), _p(out.get("pmean"))
+    d.anc, d.logw = _p(out.get("anc")), _p(out.get("logw"))
+    rc = _L().ppfo_pfilter(ctypes.byref(d), 1 if mop else 0, int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle returned {rc}")
+    del keep
+    return out
+
+
+def expf(x):
+    return np.float32(_L().ppfo_expf(float(x)))
+
+
+def logf(x):
+    return np.float32(_L().ppfo_logf(float(x)))
+
+
+def sincos2pi(u):
+    s, c = ctypes.c_float(), ctypes.c_float()
+    _L().ppfo_sincos2pif(float(u), ctypes.byref(s), ctypes.byref(c))
+    return np.float32(s.value), np.float32(c.value)
+
+
+def philox(ctr, key):
+    ctr = np.ascontiguousarray(ctr, dtype=np.uint32)
+    key = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, np.uint32)
+    _L().ppfo_philox(_p(ctr), _p(key), _p(out))
+    return out
+
+
+def normals(seed, j, s, tag, n):
+    z = np.zeros(n, np.float32)
+    _L().ppfo_normals(int(seed), int(j), int(s), int(tag), int(n), _p(z))
+    return z

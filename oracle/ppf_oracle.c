@@ -1,0 +1,377 @@
+/*
+ * ppf_oracle.c -- C restatement of the particle-filter hot path with the CUDA
+ * library's exact arithmetic.  TEST INFRASTRUCTURE ONLY: used by tests/, by
+ * __graft_entry__.smoke() as the checker, and as bench.py's timed CPU baseline.
+ *
+ * It follows the reference's algorithm step by step --
+ *   _pfilter_internal / _pfilter_step   pypomp/core/algorithms/pfilter.py:15-182
+ *   _normalize_weights                  pypomp/core/algorithms/helpers.py:34-57
+ *   _resample (systematic, side=right)  pypomp/core/algorithms/helpers.py:14-31
+ *   _resampler (gather, -log J)         pypomp/core/algorithms/helpers.py:60-91
+ *   _mop_internal / _mop_step           pypomp/core/algorithms/mop.py:19-135
+ *   LG _rinit/_rproc/_dmeas             pypomp/models/linear_gaussian.py:139-177
+ * -- but with the arithmetic definitions of include/ppf.h: float32 model math
+ * in a fixed order, ppf_detmath.h elementary functions, the fixed-point CDF
+ * summed sequentially in uint64, and ancestors found by a sequential
+ * two-pointer merge of the systematic points with the CDF (the CUDA paths use
+ * a closed-form offset per parent and a max-scan, or a binary search).  So the
+ * CUDA results must match this file bit for bit: log-weights, ancestors,
+ * particles; the float64 log-likelihood to rounding of log().
+ *
+ * Build: see oracle/Makefile (gcc -O2 -ffp-contract=off, no fast-math).
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ppf.h"
+#include "ppf_detmath.h"
+#include "ppf_philox.h"
+
+#define LOG2PI_F 1.83787706640934548356f
+
+typedef unsigned __int128 u128;
+
+/* ------------------------------------------------------------------------ */
+/* Models (same formulas and operation order as the CUDA device code)       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int kind, dx, dy;
+  float A[16], C[16], LQ[16], L[16], Linv[4], X0[4], c0;          /* LG */
+  float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, svc0; /* SV */
+  float r, sigma, phi, N0;                                         /* Ricker */
+} consts_t;
+
+static float tanh_det(float a) {
+  const float e = pp_expf(-2.0f * fabsf(a));
+  const float t = (1.0f - e) / (1.0f + e);
+  return a < 0.0f ? -t : t;
+}
+
+static void prepare(consts_t* c, const float* th, const ppf_model* m, int est) {
+  memset(c, 0, sizeof(*c));
+  c->kind = m->kind; c->dx = m->dx; c->dy = m->dy;
+  if (m->kind == PPF_MODEL_LG) {
+    const int dx = m->dx, dy = m->dy;
+    int p = 0;
+    float LR[16] = {0};
+    for (int i = 0; i < dx; ++i)
+      for (int k = 0; k < dx; ++k) c->A[i * 4 + k] = th[p++];
+    for (int i = 0; i < dy; ++i)
+      for (int k = 0; k < dx; ++k) c->C[i * 4 + k] = th[p++];
+    for (int i = 0; i < dx; ++i)
+      for (int k = 0; k <= i; ++k) {
+        float v = th[p++];
+        if (est && i == k) v = pp_expf(v);
+        c->LQ[i * 4 + k] = v;
+      }
+    for (int i = 0; i < dy; ++i)
+      for (int k = 0; k <= i; ++k) {
+        float v = th[p++];
+        if (est && i == k) v = pp_expf(v);
+        LR[i * 4 + k] = v;
+      }
+    for (int i = 0; i < dx; ++i) c->X0[i] = th[p++];
+    float R[16] = {0};
+    for (int i = 0; i < dy; ++i)
+      for (int k = 0; k <= i; ++k) {
+        float s = 0.0f;
+        for (int l = 0; l <= k; ++l) s = s + LR[i * 4 + l] * LR[k * 4 + l];
+        R[i * 4 + k] = s;
+      }
+    for (int i = 0; i < dy; ++i)
+      for (int k = 0; k <= i; ++k) {
+        float s = R[i * 4 + k];
+        for (int l = 0; l < k; ++l) s = s - c->L[i * 4 + l] * c->L[k * 4 + l];
+        if (i == k) c->L[i * 4 + i] = sqrtf(s);
+        else c->L[i * 4 + k] = s / c->L[k * 4 + k];
+      }
+    float c0 = -0.5f * (float)dy * LOG2PI_F;
+    for (int i = 0; i < dy; ++i) {
+      c->Linv[i] = 1.0f / c->L[i * 4 + i];
+      c0 = c0 - pp_logf(c->L[i * 4 + i]);
+    }
+    c->c0 = c0;
+  } else if (m->kind == PPF_MODEL_SV) {
+    c->kappa = est ? pp_expf(th[0]) : th[0];
+    c->theta = est ? pp_expf(th[1]) : th[1];
+    c->xi = est ? pp_expf(th[2]) : th[2];
+    c->rho = est ? tanh_det(th[3]) : th[3];
+    c->mu = th[4];
+    c->v0 = th[5];
+    c->dt = m->dt;
+    c->sqdt = sqrtf(m->dt);
+    c->mudt = c->mu * c->dt;
+    c->rhoc = sqrtf(1.0f - c->rho * c->rho);
+    c->svc0 = -0.5f * LOG2PI_F - pp_logf(c->rhoc) - 0.5f * pp_logf(c->dt);
+  } else {
+    c->r = est ? pp_expf(th[0]) : th[0];
+    c->sigma = est ? pp_expf(th[1]) : th[1];
+    c->phi = est ? pp_expf(th[2]) : th[2];
+    c->N0 = est ? pp_expf(th[3]) : th[3];
+  }
+}
+
+static int n_init(const consts_t* c) { return c->kind == PPF_MODEL_LG ? c->dx : 0; }
+static int n_step(const consts_t* c) { return c->kind == PPF_MODEL_LG ? c->dx : 1; }
+
+static void rinit(const consts_t* c, const float* z, float* x) {
+  if (c->kind == PPF_MODEL_LG) {
+    for (int i = 0; i < c->dx; ++i) {
+      float s = 0.0f;
+      for (int k = 0; k <= i; ++k) s = s + c->LQ[i * 4 + k] * z[k];
+      x[i] = c->X0[i] + s;
+    }
+  } else if (c->kind == PPF_MODEL_SV) {
+    x[0] = c->v0;
+    x[1] = 0.0f;
+  } else {
+    x[0] = c->N0;
+  }
+}
+
+static void rproc(const consts_t* c, float* x, const float* z) {
+  if (c->kind == PPF_MODEL_LG) {
+    float y[4];
+    for (int i = 0; i < c->dx; ++i) {
+      float a = 0.0f;
+      for (int k = 0; k < c->dx; ++k) a = a + c->A[i * 4 + k] * x[k];
+      float s = 0.0f;
+      for (int k = 0; k <= i; ++k) s = s + c->LQ[i * 4 + k] * z[k];
+      y[i] = a + s;
+    }
+    for (int i = 0; i < c->dx; ++i) x[i] = y[i];
+  } else if (c->kind == PPF_MODEL_SV) {
+    const float v = x[0];
+    const float ev = pp_expf(v);
+    const float emv = pp_expf(-v);
+    const float emh = pp_expf(-0.5f * v);
+    const float dr = ((c->kappa * ((c->theta - ev) * emv)) * c->dt);
+    const float df = ((c->xi * emh) * c->sqdt) * z[0];
+    x[0] = (v + dr) + df;
+    x[1] = z[0];
+  } else {
+    const float N = x[0];
+    const float arg = c->sigma * z[0] - N;
+    x[0] = (c->r * N) * pp_expf(arg);
+  }
+}
+
+static float dmeas(const consts_t* c, const float* y, float ycon, const float* x) {
+  if (c->kind == PPF_MODEL_LG) {
+    float s[4];
+    float q = 0.0f;
+    for (int i = 0; i < c->dy; ++i) {
+      float a = 0.0f;
+      for (int k = 0; k < c->dx; ++k) a = a + c->C[i * 4 + k] * x[k];
+      float r = y[i] - a;
+      for (int l = 0; l < i; ++l) r = r - c->L[i * 4 + l] * s[l];
+      s[i] = r * c->Linv[i];
+      q = q + s[i] * s[i];
+    }
+    return -0.5f * q + c->c0;
+  } else if (c->kind == PPF_MODEL_SV) {
+    const float v = x[0];
+    const float sd = pp_expf(0.5f * v) * c->sqdt;
+    const float mean = c->mudt + (c->rho * sd) * x[1];
+    const float r = (y[0] - mean) / (c->rhoc * sd);
+    return -0.5f * (r * r) + (c->svc0 - 0.5f * v);
+  } else {
+    const float lam = c->phi * x[0];
+    if (y[0] == 0.0f) return -lam;
+    return (y[0] * pp_logf(lam) - lam) - ycon;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Filter loop                                                              */
+/* ------------------------------------------------------------------------ */
+
+static void noise(const ppf_pfilter_desc* d, int f, int j, int s, int n, float* z) {
+  if (d->flags & PPF_F_INJECT) {
+    if (s == 0) {
+      for (int i = 0; i < n; ++i) z[i] = d->inj_z0[((size_t)f * d->J + j) * n + i];
+    } else {
+      const size_t base = (((size_t)f * d->T + (s - 1)) * d->J + j) * n;
+      for (int i = 0; i < n; ++i) z[i] = d->inj_z[base + i];
+    }
+  } else {
+    pp_normals(d->seeds[f], (uint32_t)j, (uint32_t)s, PPF_TAG_PROCESS, n, z);
+  }
+}
+
+static uint32_t uniform32(const ppf_pfilter_desc* d, int f, int t) {
+  if (d->flags & PPF_F_INJECT) return pp_u32_from_float(d->inj_u[(size_t)f * d->T + t]);
+  return pp_resample_u32(d->seeds[f], (uint32_t)(t + 1));
+}
+
+static float propagate(const ppf_pfilter_desc* d, const consts_t* c, int f, int u, int j, int t, float* x) {
+  float z[4];
+  noise(d, f, j, t + 1, n_step(c), z);
+  rproc(c, x, z);
+  const float* y = d->ys + ((size_t)u * d->T + t) * d->model.dy;
+  const float yc = d->ycon ? d->ycon[(size_t)u * d->T + t] : 0.0f;
+  return dmeas(c, y, yc, x);
+}
+
+/* One filter.  mop != 0: resampling weights are the measurement densities
+ * alone (mop.py:120) and the log-likelihood term subtracts log J. */
+static void run_filter(const ppf_pfilter_desc* d, int f, int mop) {
+  const int J = d->J, dx = d->model.dx;
+  const int u = d->unit ? d->unit[f] : 0;
+  const int Tf = d->T_u ? d->T_u[u] : d->T;
+  consts_t c;
+  prepare(&c, d->theta + (size_t)f * d->model.n_params, &d->model, (d->flags & PPF_F_EST) != 0);
+  const float base_init = pp_logf(1.0f / (float)J);
+  const float base_rs = -pp_logf((float)J);
+  const float logthresh = d->thresh > 0.0f ? pp_logf(d->thresh) : -INFINITY;
+  float* x = (float*)malloc(sizeof(float) * dx * J);
+  float* xn = (float*)malloc(sizeof(float) * dx * J);
+  float* w = (float*)malloc(sizeof(float) * J);
+  float* wn = (float*)malloc(sizeof(float) * J);
+  uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * J);
+  int* par = (int*)malloc(sizeof(int) * J);
+  for (int j = 0; j < J; ++j) {
+    float z[4], xj[4];
+    noise(d, f, j, 0, n_init(&c), z);
+    rinit(&c, z, xj);
+    const float m = propagate(d, &c, f, u, j, 0, xj);
+    for (int k = 0; k < dx; ++k) x[k * J + j] = xj[k];
+    w[j] = (mop ? 0.0f : base_init) + m;
+  }
+  double loglik = 0.0;
+  for (int t = 0; t < Tf; ++t) {
+    if (d->logw) memcpy(d->logw + ((size_t)f * d->T + t) * J, w, sizeof(float) * J);
+    /* max / min over finite weights; NaN or +inf marks the filter */
+    int nanf = 0;
+    float Mx = -INFINITY, mn = INFINITY;
+    for (int j = 0; j < J; ++j) {
+      if (w[j] != w[j] || w[j] == INFINITY) { nanf = 1; continue; }
+      if (w[j] > Mx) Mx = w[j];
+      if (w[j] < mn) mn = w[j];
+    }
+    const int collapsed = !nanf && Mx == -INFINITY;
+    const int qc = nanf || Mx == -INFINITY;
+    uint64_t tot = 0;
+    double s2 = 0.0, fx[4] = {0, 0, 0, 0}, px[4] = {0, 0, 0, 0};
+    for (int j = 0; j < J; ++j) {
+      uint64_t q;
+      double e;
+      if (qc) { q = 1; e = 1.0; }
+      else if (w[j] != w[j]) { q = 0; e = 0.0; }
+      else {
+        const float ef = pp_expf(w[j] - Mx);
+        q = (uint64_t)llrintf(ef * 1099511627776.0f);
+        e = (double)ef;
+      }
+      tot += q;
+      C[j] = tot;
+      s2 += e * e;
+      for (int k = 0; k < dx; ++k) {
+        fx[k] += (double)x[k * J + j] * e;
+        px[k] += (double)x[k * J + j];
+      }
+    }
+    double ll;
+    if (nanf) ll = NAN;
+    else if (collapsed) ll = -INFINITY;
+    else ll = (double)Mx + log((double)tot) - 40.0 * 0.69314718055994530942 - (mop ? log((double)J) : 0.0);
+    loglik += ll;
+    if ((d->flags & PPF_F_CLL) && d->cll) d->cll[(size_t)f * d->T + t] = ll;
+    const double S1 = (double)tot * 9.094947017729282e-13;
+    if ((d->flags & PPF_F_ESS) && d->ess)
+      d->ess[(size_t)f * d->T + t] = nanf ? NAN : (collapsed ? (float)J : (float)(S1 * S1 / s2));
+    for (int k = 0; k < dx; ++k) {
+      if ((d->flags & PPF_F_FMEAN) && d->fmean)
+        d->fmean[((size_t)f * d->T + t) * dx + k] = (float)(collapsed ? px[k] / J : fx[k] / S1);
+      if ((d->flags & PPF_F_PMEAN) && d->pmean)
+        d->pmean[((size_t)f * d->T + t) * dx + k] = (float)(px[k] / J);
+    }
+    const int last = (t == Tf - 1);
+    if (last && !d->anc) break;
+    int rs;
+    if (nanf) rs = 0;
+    else if (Mx == -INFINITY) rs = 0.0f > logthresh;
+    else rs = (Mx - mn) > logthresh;
+    if (rs) {
+      /* systematic resampling: child k takes the first parent whose CDF
+       * exceeds its point, i.e. #{ j : C_j J 2^32 <= (u32 + k 2^32) tot } */
+      const uint32_t u32 = uniform32(d, f, t);
+      const u128 Jsh = (u128)((uint64_t)J << 32);
+      int j = 0;
+      for (int k = 0; k < J; ++k) {
+        const u128 R = ((u128)u32 + ((u128)k << 32)) * (u128)tot;
+        while (j < J && (u128)C[j] * Jsh <= R) ++j;
+        par[k] = j;
+      }
+    } else {
+      for (int k = 0; k < J; ++k) par[k] = k;
+    }
+    if (d->anc) memcpy(d->anc + ((size_t)f * d->T + t) * J, par, sizeof(int) * J);
+    if (last) break;
+    float lt32 = 0.0f;
+    if (!rs) {
+      if (nanf) lt32 = NAN;
+      else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
+    }
+    for (int k = 0; k < J; ++k) {
+      float xk[4];
+      for (int q = 0; q < dx; ++q) xk[q] = x[q * J + par[k]];
+      float b;
+      if (rs) b = mop ? 0.0f : base_rs;
+      else b = collapsed ? -pp_logf((float)J) : w[k] - lt32;
+      const float m = propagate(d, &c, f, u, k, t + 1, xk);
+      for (int q = 0; q < dx; ++q) xn[q * J + k] = xk[q];
+      wn[k] = b + m;
+    }
+    float* tmp = x; x = xn; xn = tmp;
+    float* tw = w; w = wn; wn = tw;
+  }
+  d->loglik[f] = loglik;
+  free(x); free(xn); free(w); free(wn); free(C); free(par);
+}
+
+typedef struct {
+  const ppf_pfilter_desc* d;
+  int mop, tid, nthreads;
+} job_t;
+
+static void* worker(void* arg) {
+  const job_t* jb = (const job_t*)arg;
+  for (int f = jb->tid; f < jb->d->F; f += jb->nthreads) run_filter(jb->d, f, jb->mop);
+  return NULL;
+}
+
+/* Runs the F filters of `d` (all pointers HOST memory); `nthreads` > 1
+ * spreads whole filters over POSIX threads. */
+int ppfo_pfilter(const ppf_pfilter_desc* d, int mop, int nthreads) {
+  if (!d || d->J < 1 || d->F < 1 || d->T < 1) return PPF_EINVAL;
+  if (nthreads <= 1 || d->F == 1) {
+    for (int f = 0; f < d->F; ++f) run_filter(d, f, mop);
+    return PPF_OK;
+  }
+  if (nthreads > 256) nthreads = 256;
+  pthread_t th[256];
+  job_t jobs[256];
+  for (int i = 0; i < nthreads; ++i) {
+    jobs[i].d = d; jobs[i].mop = mop; jobs[i].tid = i; jobs[i].nthreads = nthreads;
+    pthread_create(&th[i], NULL, worker, &jobs[i]);
+  }
+  for (int i = 0; i < nthreads; ++i) pthread_join(th[i], NULL);
+  return PPF_OK;
+}
+
+/* Elementary functions and Philox, exported for the tests that pin them. */
+float ppfo_expf(float x) { return pp_expf(x); }
+float ppfo_logf(float x) { return pp_logf(x); }
+void ppfo_sincos2pif(float u, float* s, float* c) { pp_sincos2pif(u, s, c); }
+void ppfo_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  const pp_u32x4 r = pp_philox4x32_10(ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1]);
+  for (int i = 0; i < 4; ++i) out[i] = r.v[i];
+}
+void ppfo_normals(uint64_t seed, uint32_t j, uint32_t s, uint32_t tag, int n, float* z) {
+  pp_normals(seed, j, s, tag, n, z);
+}

@@ -1,0 +1,294 @@
+"""Float32 NumPy restatement of the reference's particle-filter hot path.
+
+TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
+
+This module follows the reference's algorithms operation by operation, in
+float32 like the reference's JAX defaults, vectorised over particles:
+
+* ``pfilter``      -- ``pypomp/core/algorithms/pfilter.py:15-182``
+* ``normalize``    -- ``pypomp/core/algorithms/helpers.py:34-57``
+* ``resample``     -- ``pypomp/core/algorithms/helpers.py:14-31`` (float32
+  cumsum, ``searchsorted(..., side="right")``)
+* ``mop``          -- ``pypomp/core/algorithms/mop.py:19-135``
+* ``perfilter``    -- ``pypomp/core/algorithms/mif.py:88-258``
+* ``mif``          -- ``pypomp/core/algorithms/mif.py:16-85``
+* ``simulate``     -- ``pypomp/core/algorithms/simulate.py:15-142``
+
+Random numbers come from a *noise source*.  ``JaxKeyNoise`` replays the
+reference's own key tree (``pfilter.py:23-25,105,160``;
+``model_mechanics.py:904`` per-sub-step split and ``:586`` per-particle split;
+``mif.py:113-120,179``) through ``oracle/jaxrng.py``, which is what lets the
+oracle reproduce the reference's regression fixtures.  ``ArrayNoise`` reads
+injected arrays: it is how the same draws are fed to the CUDA kernels'
+noise-injection mode.  ``RecordingNoise`` wraps a source and records every draw
+into injection arrays.
+
+The resampling CDF here is the reference's float32 running sum.  The CUDA path
+uses an exact fixed-point CDF instead (defined in ``include/ppf.h``); the C
+oracle (``oracle/ppf_oracle.c``) restates that definition for bit-exact
+comparisons, and tests report how often the two CDFs pick different ancestors.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import jaxrng as jr
+from .models_np import MODELS
+
+f32 = np.float32
+
+
+# ---------------------------------------------------------------------------
+# Noise sources
+# ---------------------------------------------------------------------------
+
+
+class JaxKeyNoise:
+    """The reference pfilter/mop key tree, replayed with ``oracle.jaxrng``."""
+
+    def __init__(self, key: jr.Key, J: int, n_init: int, n_step: int):
+        # pfilter.py:23-25 / mop.py:30-32: split(key, J+1) -> carry key, J rinit keys
+        sk = jr.split(key, J + 1)
+        self.key = sk[0]
+        self.init_keys = sk[1:]
+        self.J = J
+        self.n_init = n_init
+        self.n_step = n_step
+
+    def init_normals(self):
+        J = self.J
+        if self.n_init == 0:
+            return np.zeros((J, 0), f32)
+        return np.stack([jr.normal(self.init_keys[j], (self.n_init,)) for j in range(J)])
+
+    def step_normals(self, t):
+        # pfilter.py:105 then model_mechanics.py:904 (one sub-step) and :586
+        s = jr.split(self.key)
+        self.key, sub = s[0], s[1]
+        s2 = jr.split(sub)
+        sub2 = s2[1]
+        pk = jr.split(sub2, self.J)
+        if self.n_step == 0:
+            return np.zeros((self.J, 0), f32)
+        return np.stack([jr.normal(pk[j], (self.n_step,)) for j in range(self.J)])
+
+    def resample_uniform(self, t):
+        # pfilter.py:160 (and mop.py:123) then helpers.py:28
+        s = jr.split(self.key)
+        self.key, sub = s[0], s[1]
+        return f32(jr.uniform(sub))
+
+
+class ArrayNoise:
+    """Injected draws: ``z0`` (J,n_init), ``z`` (T,J,n_step), ``u`` (T,)."""
+
+    def __init__(self, z0, z, u):
+        self.z0 = np.asarray(z0, f32)
+        self.z = np.asarray(z, f32)
+        self.u = np.asarray(u, f32)
+
+    def init_normals(self):
+        return self.z0
+
+    def step_normals(self, t):
+        return self.z[t]
+
+    def resample_uniform(self, t):
+        return f32(self.u[t])
+
+
+class RecordingNoise:
+    """Wraps a source and records its draws as injection arrays."""
+
+    def __init__(self, src):
+        self.src = src
+        self.z0 = None
+        self.z = []
+        self.u = []
+
+    def init_normals(self):
+        self.z0 = self.src.init_normals()
+        return self.z0
+
+    def step_normals(self, t):
+        z = self.src.step_normals(t)
+        self.z.append(z)
+        return z
+
+    def resample_uniform(self, t):
+        u = self.src.resample_uniform(t)
+        self.u.append(u)
+        return u
+
+    def arrays(self):
+        return (self.z0, np.stack(self.z), np.asarray(self.u, f32))
+
+
+# ---------------------------------------------------------------------------
+# Weight helpers (helpers.py)
+# ---------------------------------------------------------------------------
+
+
+def normalize(w: np.ndarray):
+    """``_normalize_weights`` (helpers.py:34-57)."""
+    w = w.astype(f32)
+    mw = np.max(w)
+    collapsed = mw == -np.inf
+    mw_safe = f32(0.0) if collapsed else mw
+    with np.errstate(invalid="ignore", divide="ignore", over="ignore"):
+        lt = f32(mw_safe + np.log(np.nansum(np.exp(w - mw_safe), dtype=f32)))
+    if collapsed:
+        lt = f32(-np.inf)
+        nw = np.full(w.shape, -np.log(f32(w.shape[-1])), f32)
+    else:
+        nw = (w - lt).astype(f32)
+    return nw, lt
+
+
+def resample(nw: np.ndarray, u: np.float32):
+    """``_resample`` (helpers.py:14-31): systematic, float32 CDF, side=right."""
+    J = nw.shape[-1]
+    unifs = ((u + np.arange(J, dtype=f32)) / f32(J)).astype(f32)
+    csum = np.cumsum(np.exp(nw).astype(f32), dtype=f32)
+    return np.searchsorted((csum / csum[-1]).astype(f32), unifs, side="right")
+
+
+# ---------------------------------------------------------------------------
+# pfilter
+# ---------------------------------------------------------------------------
+
+
+def pfilter(model, theta, ys, J, noise, thresh=0.0, diagnostics=False):
+    """``_pfilter_internal`` + ``_pfilter_step`` (pfilter.py:15-182).
+
+    ``model`` is a name in ``MODELS``; ``theta`` is on the natural scale.
+    Returns a dict with ``logLik`` (float32 like the reference), and when
+    ``diagnostics`` is set ``CLL``, ``ESS``, ``filter_mean``,
+    ``prediction_mean`` and the per-step ``ancestors`` and ``log_weights``
+    (unnormalised, before normalisation).
+    """
+    m = MODELS[model]
+    ys = np.asarray(ys, f32)
+    T = ys.shape[0]
+    par = m.unpack(np.asarray(theta, f32))
+    X = m.rinit(par, noise.init_normals())
+    nw = np.log(np.ones(J, f32) / f32(J)).astype(f32)
+    loglik = f32(0.0)
+    logthresh = np.log(f32(thresh)) if thresh > 0 else f32(-np.inf)
+    out = {"CLL": [], "ESS": [], "filter_mean": [], "prediction_mean": [],
+           "ancestors": [], "log_weights": []}
+    for i in range(T):
+        X = m.rproc(par, X, noise.step_normals(i), i)
+        meas = m.dmeas(par, ys[i], X)
+        w = (nw + meas).astype(f32)
+        nwn, lt = normalize(w)
+        loglik = f32(loglik + lt)
+        if diagnostics:
+            out["log_weights"].append(w)
+            out["CLL"].append(lt)
+            with np.errstate(over="ignore"):
+                out["ESS"].append(f32(1.0) / np.sum(np.exp(f32(2.0) * nwn), dtype=f32))
+            out["filter_mean"].append((X * np.exp(nwn)[:, None]).sum(axis=0, dtype=f32))
+            out["prediction_mean"].append(X.mean(axis=0, dtype=f32))
+        with np.errstate(invalid="ignore"):
+            do_resample = bool(np.max(nwn) - np.min(nwn) > logthresh)
+        u = noise.resample_uniform(i)
+        if do_resample:
+            counts = resample(nwn, u)
+            X = X[counts]
+            nw = np.full(J, -np.log(f32(J)), f32)
+        else:
+            counts = np.arange(J)
+            nw = nwn
+        if diagnostics:
+            out["ancestors"].append(counts)
+    res = {"logLik": loglik}
+    if diagnostics:
+        for k, v in out.items():
+            res[k] = np.asarray(v)
+    return res
+
+
+def mop(model, theta_est, ys, J, alpha, noise, with_ancestors=False):
+    """``_mop_internal`` + ``_mop_step`` (mop.py:19-135): value only.
+
+    ``theta_est`` is on the estimation scale (``SHOULD_TRANS = True``,
+    mop.py:16).  Returns the negative MOP log-likelihood (float32).
+    """
+    m = MODELS[model]
+    ys = np.asarray(ys, f32)
+    T = ys.shape[0]
+    par = m.unpack(m.from_est(np.asarray(theta_est, f32)))
+    X = m.rinit(par, noise.init_normals())
+    wF = np.log(np.ones(J, f32) / f32(J)).astype(f32)
+    loglik = f32(0.0)
+    anc = []
+    a = f32(alpha)
+    for i in range(T):
+        wP = (a * wF).astype(f32)
+        X = m.rproc(par, X, noise.step_normals(i), i)
+        meas = m.dmeas(par, ys[i], X)
+        loglik = f32(loglik + _lse(wP + meas) - _lse(wP))
+        nw, _ = normalize(meas)
+        u = noise.resample_uniform(i)
+        counts = resample(nw, u)
+        X = X[counts]
+        wF = wP[counts]
+        anc.append(counts)
+    if with_ancestors:
+        return f32(-loglik), np.asarray(anc)
+    return f32(-loglik)
+
+
+def _lse(v):
+    v = np.asarray(v, f32)
+    mx = np.max(v)
+    if not np.isfinite(mx):
+        mx = f32(0.0)
+    return f32(mx + np.log(np.sum(np.exp(v - mx), dtype=f32)))
+
+
+# ---------------------------------------------------------------------------
+# simulate (used to make the reference's own LG data sets)
+# ---------------------------------------------------------------------------
+
+
+def simulate(model, theta, T, key: jr.Key, nsim=1):
+    """``_simulate_internal`` (simulate.py:15-142) with nstep=1 and no covariates.
+
+    Returns ``(X (T+1, nsim, dx), Y (T, nsim, dy))`` in float32.
+    """
+    m = MODELS[model]
+    par = m.unpack(np.asarray(theta, f32))
+    sk = jr.split(key, nsim + 1)
+    key, keys = sk[0], sk[1:]
+    X = m.rinit(par, np.stack([jr.normal(keys[s], (m.n_init(par),)) for s in range(nsim)]))
+    Xs = [X]
+    Ys = []
+    for i in range(T):
+        s = jr.split(key)
+        key, sub = s[0], s[1]
+        s2 = jr.split(sub)
+        pk = jr.split(s2[1], nsim)
+        z = np.stack([jr.normal(pk[j], (m.n_step(par),)) for j in range(nsim)])
+        X = m.rproc(par, X, z, i)
+        s3 = jr.split(key, nsim + 1)
+        key, mk = s3[0], s3[1:]
+        zm = np.stack([jr.normal(mk[j], (m.n_meas(par),)) for j in range(nsim)])
+        Ys.append(m.rmeas(par, X, zm))
+        Xs.append(X)
+    return np.stack(Xs), np.stack(Ys)
+
+
+def pomp_simulate_data(model, theta, T, key: jr.Key):
+    """Data as ``Pomp.simulate(key=key, nsim=1, as_pomp=True)`` makes it.
+
+    ``estimation_mixin.py:1173-1182``: ``_update_fresh_key`` splits ``key`` and
+    uses the second half, which is split once more per parameter set
+    (``pomp.py:391-408``).
+    """
+    new_key = jr.split(key)[1]
+    k = jr.split(new_key, 1)[0]
+    X, Y = simulate(model, theta, T, k, nsim=1)
+    return X[:, 0, :], Y[:, 0, :]

@@ -1,0 +1,190 @@
+// ppf_api.cu -- the extern "C" entry points of libppf.so (declared in
+// include/ppf.h): argument validation, workspace layout and path choice.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include "ppf.h"
+#include "ppf_core.cuh"
+#include "ppf_detmath.h"
+#include "ppf_internal.h"
+
+namespace ppf {
+
+static size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+// Carve the workspace for `path`; with base == nullptr only sizes are computed.
+static size_t carve(Args& a, int path, unsigned char* base) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> unsigned char* {
+    unsigned char* p = base ? base + off : nullptr;
+    off = align_up(off + bytes);
+    return p;
+  };
+  const int dx = a.model.dx;
+  a.err = reinterpret_cast<uint32_t*>(take(64));
+  a.counter = reinterpret_cast<unsigned int*>(base ? base + 16 : nullptr);
+  if (path == PPF_PATH_STREAM) {
+    const int TILE = 2048;
+    a.tile = TILE;
+    a.ntiles = (a.J + TILE - 1) / TILE;
+    for (int i = 0; i < 2; ++i) a.acc[i] = reinterpret_cast<Acc*>(take(sizeof(Acc) * a.F));
+    for (int i = 0; i < 2; ++i) a.desc[i] = reinterpret_cast<uint64_t*>(take(8ull * a.F * a.ntiles));
+    a.excl = reinterpret_cast<uint64_t*>(take(8ull * a.F * a.ntiles));
+    a.tot = reinterpret_cast<uint64_t*>(take(8ull * a.F));
+    a.ctrl_bytes = off;
+    for (int i = 0; i < 2; ++i) a.X[i] = reinterpret_cast<float*>(take(4ull * a.F * dx * a.J));
+    for (int i = 0; i < 2; ++i) a.W[i] = reinterpret_cast<float*>(take(4ull * a.F * a.J));
+  } else if (path == PPF_PATH_PLAIN) {
+    const int nblk = (a.J + 255) / 256;
+    for (int i = 0; i < 2; ++i) a.acc[i] = reinterpret_cast<Acc*>(take(sizeof(Acc)));
+    a.tot = reinterpret_cast<uint64_t*>(take(8));
+    a.pl_carry_dev = reinterpret_cast<int*>(take(4));
+    a.ctrl_bytes = off;
+    for (int i = 0; i < 2; ++i) a.X[i] = reinterpret_cast<float*>(take(4ull * dx * a.J));
+    for (int i = 0; i < 2; ++i) a.W[i] = reinterpret_cast<float*>(take(4ull * a.J));
+    a.pl_cdf = reinterpret_cast<uint64_t*>(take(8ull * a.J));
+    a.pl_bsum = reinterpret_cast<uint64_t*>(take(8ull * nblk));
+    a.pl_boff = reinterpret_cast<uint64_t*>(take(8ull * nblk));
+    a.pl_anc = reinterpret_cast<int*>(take(4ull * a.J));
+  } else {
+    a.ctrl_bytes = off;
+  }
+  return off;
+}
+
+static int n_params_of(const ppf_model& m) {
+  switch (m.kind) {
+    case PPF_MODEL_LG:
+      return m.dx * m.dx + m.dy * m.dx + m.dx * (m.dx + 1) / 2 + m.dy * (m.dy + 1) / 2 + m.dx;
+    case PPF_MODEL_SV: return 6;
+    case PPF_MODEL_RICKER: return 4;
+    default: return -1;
+  }
+}
+
+static int check_model(const ppf_model& m) {
+  switch (m.kind) {
+    case PPF_MODEL_LG:
+      if (m.dx < 1 || m.dx > 4 || m.dy < 1 || m.dy > 4) return PPF_EUNSUPPORTED;
+      break;
+    case PPF_MODEL_SV:
+      if (m.dx != 2 || m.dy != 1 || !(m.dt > 0.0f)) return PPF_EINVAL;
+      break;
+    case PPF_MODEL_RICKER:
+      if (m.dx != 1 || m.dy != 1) return PPF_EINVAL;
+      break;
+    default: return PPF_EINVAL;
+  }
+  if (m.n_params != n_params_of(m)) return PPF_EINVAL;
+  return PPF_OK;
+}
+
+static int choose_path(const ppf_pfilter_desc* d) {
+  if (d->path != PPF_PATH_AUTO) return d->path;
+  Args a{};
+  a.J = d->J; a.model = d->model;
+  // swarm fits one CTA's shared memory: keep it on chip for the whole loop
+  if (resident_smem_bytes(a) <= kResidentSmemMax && d->J <= 16384) return PPF_PATH_RESIDENT;
+  return PPF_PATH_STREAM;
+}
+
+static int fill_args(const ppf_pfilter_desc* d, Args& a, int mode) {
+  memset(&a, 0, sizeof(a));
+  a.model = d->model;
+  a.J = d->J; a.F = d->F; a.T = d->T; a.U = d->U;
+  a.flags = d->flags;
+  a.mode = mode;
+  a.thresh = d->thresh > 0.0f ? d->thresh : 0.0f;
+  a.logthresh = a.thresh > 0.0f ? pp_logf(a.thresh) : -INFINITY;
+  a.base_init = pp_logf(1.0f / (float)d->J);
+  a.base_rs = -pp_logf((float)d->J);
+  a.theta = d->theta; a.ys = d->ys; a.ycon = d->ycon; a.unit = d->unit; a.T_u = d->T_u;
+  a.seeds = d->seeds; a.inj_z0 = d->inj_z0; a.inj_z = d->inj_z; a.inj_u = d->inj_u;
+  a.loglik = d->loglik;
+  a.cll = (d->flags & PPF_F_CLL) ? d->cll : nullptr;
+  a.ess = (d->flags & PPF_F_ESS) ? d->ess : nullptr;
+  a.fmean = (d->flags & PPF_F_FMEAN) ? d->fmean : nullptr;
+  a.pmean = (d->flags & PPF_F_PMEAN) ? d->pmean : nullptr;
+  a.anc = (d->flags & PPF_F_SAVE_ANC) ? d->anc : nullptr;
+  a.logw = (d->flags & PPF_F_SAVE_W) ? d->logw : nullptr;
+  return PPF_OK;
+}
+
+static int validate(const ppf_pfilter_desc* d) {
+  if (!d) return PPF_EINVAL;
+  if (d->J < 1 || d->J > PPF_MAX_J || d->F < 1 || d->T < 1 || d->U < 1) return PPF_EINVAL;
+  int rc = check_model(d->model);
+  if (rc) return rc;
+  if (!d->theta || !d->ys || !d->loglik) return PPF_EINVAL;
+  if (!(d->flags & PPF_F_INJECT) && !d->seeds) return PPF_EINVAL;
+  if ((d->flags & PPF_F_INJECT) && (!d->inj_z || !d->inj_u)) return PPF_EINVAL;
+  if ((d->flags & PPF_F_INJECT) && d->model.kind == PPF_MODEL_LG && !d->inj_z0) return PPF_EINVAL;
+  if (d->model.kind == PPF_MODEL_RICKER && !d->ycon) return PPF_EINVAL;
+  if ((d->flags & PPF_F_CLL) && !d->cll) return PPF_EINVAL;
+  if ((d->flags & PPF_F_ESS) && !d->ess) return PPF_EINVAL;
+  if ((d->flags & PPF_F_FMEAN) && !d->fmean) return PPF_EINVAL;
+  if ((d->flags & PPF_F_PMEAN) && !d->pmean) return PPF_EINVAL;
+  if ((d->flags & PPF_F_SAVE_ANC) && !d->anc) return PPF_EINVAL;
+  if ((d->flags & PPF_F_SAVE_W) && !d->logw) return PPF_EINVAL;
+  if (d->path < PPF_PATH_AUTO || d->path > PPF_PATH_RESIDENT) return PPF_EINVAL;
+  return PPF_OK;
+}
+
+}  // namespace ppf
+
+using namespace ppf;
+
+extern "C" {
+
+size_t ppf_pfilter_workspace_bytes(const ppf_pfilter_desc* d) {
+  if (validate(d) != PPF_OK && !(d && d->J >= 1 && d->F >= 1)) return 0;
+  Args a;
+  fill_args(d, a, MODE_PF);
+  return carve(a, choose_path(d), nullptr);
+}
+
+int ppf_pfilter(const ppf_pfilter_desc* d, void* stream) {
+  int rc = validate(d);
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  Args a;
+  fill_args(d, a, MODE_PF);
+  const int path = choose_path(d);
+  const size_t need = carve(a, path, nullptr);
+  if (!d->workspace || d->ws_bytes < need) return PPF_EINVAL;
+  carve(a, path, reinterpret_cast<unsigned char*>(d->workspace));
+  if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, s) != cudaSuccess) return PPF_ECUDA;
+  if (path == PPF_PATH_STREAM) {
+    // accumulators start at (max=-, min=+, nan=0)
+    rc = reset_accumulators(a, s);
+    if (rc) return rc;
+  }
+  rc = run_pfilter_path(a, path, s);
+  return rc;
+}
+
+int ppf_workspace_status(const void* workspace, void* stream) {
+  if (!workspace) return PPF_EINVAL;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  uint32_t err = 0;
+  if (cudaMemcpyAsync(&err, workspace, sizeof(err), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PPF_ECUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return PPF_ECUDA;
+  if (err) return PPF_ETIMEOUT;
+  return PPF_OK;
+}
+
+const char* ppf_error_string(int code) {
+  switch (code) {
+    case PPF_OK: return "ok";
+    case PPF_EINVAL: return "invalid argument";
+    case PPF_ECUDA: return "CUDA launch or runtime error";
+    case PPF_ETIMEOUT: return "a bounded device-side wait timed out";
+    case PPF_EUNSUPPORTED: return "unsupported configuration";
+    default: return "unknown error";
+  }
+}
+
+const char* ppf_version(void) { return "ppf 0.1.0 sm_100a"; }
+
+}  // extern "C"

@@ -1,0 +1,199 @@
+// ppf_core.cuh -- shared device primitives of the particle-filter kernels:
+// ordered-float keys for atomic max/min, warp/block reductions and scans,
+// the fixed-point weight, and the exact systematic-resampling offset.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "ppf.h"
+#include "ppf_detmath.h"
+#include "ppf_philox.h"
+
+namespace ppf {
+
+typedef unsigned __int128 u128;
+
+constexpr float kQScale = 1099511627776.0f;        // 2^40, fixed-point weight scale
+constexpr double kLn2 = 0.69314718055994530942;
+constexpr uint64_t kStatusAgg = 1ull << 62;
+constexpr uint64_t kStatusIncl = 2ull << 62;
+constexpr uint64_t kValueMask = (1ull << 62) - 1;
+constexpr long long kSpinCap = 1ll << 22;          // bounded waits: then PPF_ETIMEOUT
+
+// Per-filter, per-step accumulators (double-buffered by step parity).
+struct Acc {
+  unsigned int maxkey, minkey, nan, pad;
+  double s2;        // sum e^2 (ESS)
+  double fx[4];     // sum x e (filter mean)
+  double px[4];     // sum x (prediction mean)
+  double pad2;
+};
+static_assert(sizeof(Acc) == 96, "Acc layout");
+
+__device__ __forceinline__ unsigned int fkey(float f) {
+  const unsigned int b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float keyf(unsigned int k) {
+  const unsigned int b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  return __uint_as_float(b);
+}
+
+__device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// The fixed-point weight q = rint(exp(w - M) * 2^40) (collapsed filters: 1).
+__device__ __forceinline__ uint64_t qweight(float w, float M, bool collapsed) {
+  if (collapsed) return 1ull;
+  if (w != w) return 0ull;
+  const float e = pp_expf(w - M);
+  return __float2ull_rn(e * kQScale);
+}
+
+// Number of systematic points strictly below the CDF value C:
+//   nchild(C) = #{ k in [0,J) : (u32 + k 2^32) * tot < C * J * 2^32 }.
+// A double-precision estimate is corrected with exact 128-bit comparisons.
+__device__ __forceinline__ int nchild(uint64_t C, uint64_t tot, uint32_t u32, int J) {
+  const u128 L = (u128)C * (u128)((uint64_t)J << 32);
+  const u128 ut = (u128)u32 * (u128)tot;
+  if (L <= ut) return 0;
+  const double est = (double)C * (double)J / (double)tot - (double)u32 * 2.3283064365386963e-10;
+  long long k = (long long)ceil(est);
+  if (k < 0) k = 0;
+  if (k > J) k = J;
+  const u128 step = (u128)tot << 32;
+  // invariant wanted: R(k-1) < L <= R(k), R(k) = ut + k*step
+  while (k > 0 && ut + (u128)(k - 1) * step >= L) --k;
+  while (k < J && ut + (u128)k * step < L) ++k;
+  return (int)k;
+}
+
+// ------------------------------- warp / block ------------------------------
+
+__device__ __forceinline__ uint64_t warp_incl_scan_u64(uint64_t v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t n = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += n;
+  }
+  return v;
+}
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum_f64(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ unsigned int warp_max_u32(unsigned int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ unsigned int warp_min_u32(unsigned int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_incl_max_i32(int v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int n = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v = max(v, n);
+  }
+  return v;
+}
+
+// Block exclusive scan of one uint64 per thread; returns the exclusive prefix
+// and writes the block total.  `sm` needs TPB/32 + 1 entries.
+template <int TPB>
+__device__ __forceinline__ uint64_t block_excl_scan_u64(uint64_t v, uint64_t* sm, uint64_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = TPB / 32;
+  const uint64_t inc = warp_incl_scan_u64(v);
+  if (lane == 31) sm[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t wv = lane < NW ? sm[lane] : 0ull;
+    const uint64_t wi = warp_incl_scan_u64(wv);
+    if (lane < NW) sm[lane] = wi - wv;
+    if (lane == NW - 1) sm[NW] = wi;
+  }
+  __syncthreads();
+  const uint64_t res = sm[warp] + inc - v;
+  total = sm[NW];
+  __syncthreads();
+  return res;
+}
+
+// Block exclusive max-scan of one int per thread (identity -1).
+template <int TPB>
+__device__ __forceinline__ int block_excl_max_i32(int v, int* sm, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = TPB / 32;
+  const int inc = warp_incl_max_i32(v);
+  int exc = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (lane == 0) exc = -1;
+  if (lane == 31) sm[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const int wv = lane < NW ? sm[lane] : -1;
+    const int wi = warp_incl_max_i32(wv);
+    int we = __shfl_up_sync(0xffffffffu, wi, 1);
+    if (lane == 0) we = -1;
+    if (lane < NW) sm[lane] = we;
+    if (lane == NW - 1) sm[NW] = wi;
+  }
+  __syncthreads();
+  const int res = max(sm[warp], exc);
+  total = sm[NW];
+  __syncthreads();
+  return res;
+}
+
+template <int TPB>
+__device__ __forceinline__ double block_sum_f64(double v, double* sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = TPB / 32;
+  v = warp_sum_f64(v);
+  if (lane == 0) sm[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (warp == 0) {
+    r = lane < NW ? sm[lane] : 0.0;
+    r = warp_sum_f64(r);
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+template <int TPB>
+__device__ __forceinline__ void block_maxmin_u32(unsigned int& mx, unsigned int& mn, unsigned int* sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = TPB / 32;
+  mx = warp_max_u32(mx);
+  mn = warp_min_u32(mn);
+  if (lane == 0) { sm[warp] = mx; sm[NW + warp] = mn; }
+  __syncthreads();
+  if (warp == 0) {
+    unsigned int a = lane < NW ? sm[lane] : 0u;
+    unsigned int b = lane < NW ? sm[NW + lane] : 0xffffffffu;
+    a = warp_max_u32(a);
+    b = warp_min_u32(b);
+    mx = a; mn = b;
+  }
+  __syncthreads();
+}
+
+}  // namespace ppf

@@ -1,0 +1,69 @@
+// ppf_internal.h -- host/device argument block shared by the kernels of
+// libppf.so.  Not part of the public ABI (that is include/ppf.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+#include "ppf.h"
+
+namespace ppf {
+
+struct Acc;
+
+enum { MODE_PF = 0, MODE_MOP = 1, MODE_IF2 = 2 };
+
+constexpr size_t kResidentSmemMax = 220 * 1024;
+
+// Everything a kernel needs, passed by value (well under the 32 KB limit).
+struct Args {
+  ppf_model model;
+  int J, F, T, U;
+  uint32_t flags;
+  int mode;
+  float thresh, logthresh;
+  float base_init;  // log(1/J): the reference's initial log-weight (pfilter.py:35)
+  float base_rs;    // -log(J): the log-weight after resampling (helpers.py:88-90)
+  const float* theta;
+  const float* ys;
+  const float* ycon;
+  const int* unit;
+  const int* T_u;
+  const uint64_t* seeds;
+  const float* inj_z0;
+  const float* inj_z;
+  const float* inj_u;
+  double* loglik;
+  double* cll;
+  float* ess;
+  float* fmean;
+  float* pmean;
+  int* anc;
+  float* logw;
+  // workspace
+  uint32_t* err;
+  unsigned int* counter;  // [2]
+  Acc* acc[2];            // [F] each
+  uint64_t* desc[2];      // [F][ntiles] each
+  uint64_t* excl;         // [F][ntiles]
+  uint64_t* tot;          // [F]
+  float* X[2];            // [F][dx][J] each
+  float* W[2];            // [F][J] each
+  int tile, ntiles;
+  size_t ctrl_bytes;      // leading workspace bytes zeroed per call
+  // plain path
+  uint64_t* pl_cdf;       // [J]
+  uint64_t* pl_bsum;      // [nblk]
+  uint64_t* pl_boff;      // [nblk]
+  int* pl_anc;            // [J]
+  int* pl_carry_dev;      // [1]
+  // host copies for host-side loops (plain path)
+  const int* T_u_host;
+  const int* unit_host;
+};
+
+int run_pfilter_path(Args& a, int path, cudaStream_t s);
+int reset_accumulators(Args& a, cudaStream_t s);
+size_t resident_smem_bytes(const Args& a);
+
+}  // namespace ppf

@@ -1,0 +1,236 @@
+// ppf_models.cuh -- device code of the built-in models (LG, SV, Ricker).
+//
+// Each model is a struct with a per-filter constant block (`Consts`, kept in
+// shared memory by the kernels) and the three mechanics the reference's
+// plugin boundary calls per particle (pypomp/functional/structs.py:10-75):
+//   rinit  -- pypomp/models/linear_gaussian.py:139 (_rinit)
+//   rproc  -- linear_gaussian.py:151 (_rproc), one Euler step (nstep = 1)
+//   dmeas  -- linear_gaussian.py:166 (_dmeas)
+// The operation order below is the arithmetic definition that the C oracle
+// (oracle/ppf_oracle.c) restates; float32 throughout, elementary functions
+// from ppf_detmath.h, compiled with -fmad=false so no contraction happens.
+#pragma once
+
+#include <stdint.h>
+#include "ppf.h"
+#include "ppf_detmath.h"
+
+#define PPF_LOG2PI_F 1.83787706640934548356f
+
+namespace ppf {
+
+// ---------------------------------------------------------------------------
+// Linear Gaussian (dx, dy <= 4).  Parameter order as LG's canonical names:
+// A (row-major dx*dx), C (row-major dy*dx), lower triangle of chol(Q)
+// row-major, lower triangle of chol(R) row-major, X0 (dx).
+// ---------------------------------------------------------------------------
+struct LG {
+  static constexpr int kind = PPF_MODEL_LG;
+  static constexpr int MAXDX = 4;
+  static constexpr int MAXDY = 4;
+  static constexpr int MAXP = 16 + 16 + 10 + 10 + 4;
+  struct Consts {
+    int dx, dy;
+    float A[16], C[16], LQ[16], L[16], Linv[4], X0[4];
+    float c0;
+  };
+  __host__ __device__ static int n_init(const Consts& c) { return c.dx; }
+  __host__ __device__ static int n_step(const Consts& c) { return c.dx; }
+
+  __device__ static void prepare(Consts& c, const float* th, const ppf_model& m, bool est) {
+    const int dx = m.dx, dy = m.dy;
+    c.dx = dx; c.dy = dy;
+    int p = 0;
+    for (int i = 0; i < dx; ++i)
+      for (int k = 0; k < dx; ++k) c.A[i * 4 + k] = th[p++];
+    for (int i = 0; i < dy; ++i)
+      for (int k = 0; k < dx; ++k) c.C[i * 4 + k] = th[p++];
+    float LR[16];
+    for (int i = 0; i < 16; ++i) { c.LQ[i] = 0.0f; LR[i] = 0.0f; c.L[i] = 0.0f; }
+    for (int i = 0; i < dx; ++i)
+      for (int k = 0; k <= i; ++k) {
+        float v = th[p++];
+        if (est && i == k) v = pp_expf(v);
+        c.LQ[i * 4 + k] = v;
+      }
+    for (int i = 0; i < dy; ++i)
+      for (int k = 0; k <= i; ++k) {
+        float v = th[p++];
+        if (est && i == k) v = pp_expf(v);
+        LR[i * 4 + k] = v;
+      }
+    for (int i = 0; i < dx; ++i) c.X0[i] = th[p++];
+    // R = LR LR^T, then its Cholesky factor (as multivariate_normal.logpdf does).
+    float R[16];
+    for (int i = 0; i < dy; ++i)
+      for (int k = 0; k <= i; ++k) {
+        float s = 0.0f;
+        for (int l = 0; l <= k; ++l) s = s + LR[i * 4 + l] * LR[k * 4 + l];
+        R[i * 4 + k] = s;
+      }
+    for (int i = 0; i < dy; ++i)
+      for (int k = 0; k <= i; ++k) {
+        float s = R[i * 4 + k];
+        for (int l = 0; l < k; ++l) s = s - c.L[i * 4 + l] * c.L[k * 4 + l];
+        if (i == k) c.L[i * 4 + i] = sqrtf(s);
+        else c.L[i * 4 + k] = s / c.L[k * 4 + k];
+      }
+    float c0 = -0.5f * (float)dy * PPF_LOG2PI_F;
+    for (int i = 0; i < dy; ++i) {
+      c.Linv[i] = 1.0f / c.L[i * 4 + i];
+      c0 = c0 - pp_logf(c.L[i * 4 + i]);
+    }
+    c.c0 = c0;
+  }
+
+  __device__ static void rinit(const Consts& c, const float* z, float* x) {
+#pragma unroll
+    for (int i = 0; i < MAXDX; ++i) {
+      if (i < c.dx) {
+        float s = 0.0f;
+#pragma unroll
+        for (int k = 0; k <= i; ++k) s = s + c.LQ[i * 4 + k] * z[k];
+        x[i] = c.X0[i] + s;
+      }
+    }
+  }
+
+  __device__ static void rproc(const Consts& c, float* x, const float* z) {
+    float y[MAXDX];
+#pragma unroll
+    for (int i = 0; i < MAXDX; ++i) {
+      if (i < c.dx) {
+        float a = 0.0f;
+#pragma unroll
+        for (int k = 0; k < MAXDX; ++k)
+          if (k < c.dx) a = a + c.A[i * 4 + k] * x[k];
+        float s = 0.0f;
+#pragma unroll
+        for (int k = 0; k <= i; ++k) s = s + c.LQ[i * 4 + k] * z[k];
+        y[i] = a + s;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < MAXDX; ++i)
+      if (i < c.dx) x[i] = y[i];
+  }
+
+  __device__ static float dmeas(const Consts& c, const float* y, float /*ycon*/, const float* x) {
+    float s[MAXDY];
+    float q = 0.0f;
+#pragma unroll
+    for (int i = 0; i < MAXDY; ++i) {
+      if (i < c.dy) {
+        float a = 0.0f;
+#pragma unroll
+        for (int k = 0; k < MAXDX; ++k)
+          if (k < c.dx) a = a + c.C[i * 4 + k] * x[k];
+        float r = y[i] - a;
+#pragma unroll
+        for (int l = 0; l < i; ++l) r = r - c.L[i * 4 + l] * s[l];
+        s[i] = r * c.Linv[i];
+        q = q + s[i] * s[i];
+      }
+    }
+    return -0.5f * q + c.c0;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Heston-type log-variance stochastic volatility.  State (v, eps); parameters
+// (kappa, theta, xi, rho, mu, v0); estimation scale log/log/log/atanh/id/id.
+//   v' = v + kappa (theta - e^v) e^-v dt + xi e^{-v/2} sqrt(dt) eps'
+//   r  ~ N(mu dt + rho sqrt(e^{v'} dt) eps', (1 - rho^2) e^{v'} dt)
+// ---------------------------------------------------------------------------
+__host__ __device__ inline float pp_tanhf_det(float a) {
+  const float e = pp_expf(-2.0f * fabsf(a));
+  const float t = (1.0f - e) / (1.0f + e);
+  return a < 0.0f ? -t : t;
+}
+
+struct SV {
+  static constexpr int kind = PPF_MODEL_SV;
+  static constexpr int MAXDX = 2;
+  static constexpr int MAXDY = 1;
+  static constexpr int MAXP = 6;
+  struct Consts {
+    int dx, dy;
+    float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, c0;
+  };
+  __host__ __device__ static int n_init(const Consts&) { return 0; }
+  __host__ __device__ static int n_step(const Consts&) { return 1; }
+
+  __device__ static void prepare(Consts& c, const float* th, const ppf_model& m, bool est) {
+    c.dx = 2; c.dy = 1;
+    c.kappa = est ? pp_expf(th[0]) : th[0];
+    c.theta = est ? pp_expf(th[1]) : th[1];
+    c.xi = est ? pp_expf(th[2]) : th[2];
+    c.rho = est ? pp_tanhf_det(th[3]) : th[3];
+    c.mu = th[4];
+    c.v0 = th[5];
+    c.dt = m.dt;
+    c.sqdt = sqrtf(m.dt);
+    c.mudt = c.mu * c.dt;
+    c.rhoc = sqrtf(1.0f - c.rho * c.rho);
+    c.c0 = -0.5f * PPF_LOG2PI_F - pp_logf(c.rhoc) - 0.5f * pp_logf(c.dt);
+  }
+  __device__ static void rinit(const Consts& c, const float*, float* x) {
+    x[0] = c.v0;
+    x[1] = 0.0f;
+  }
+  __device__ static void rproc(const Consts& c, float* x, const float* z) {
+    const float v = x[0];
+    const float ev = pp_expf(v);
+    const float emv = pp_expf(-v);
+    const float emh = pp_expf(-0.5f * v);
+    const float dr = ((c.kappa * ((c.theta - ev) * emv)) * c.dt);
+    const float df = ((c.xi * emh) * c.sqdt) * z[0];
+    x[0] = (v + dr) + df;
+    x[1] = z[0];
+  }
+  __device__ static float dmeas(const Consts& c, const float* y, float, const float* x) {
+    const float v = x[0];
+    const float sd = pp_expf(0.5f * v) * c.sqdt;
+    const float mean = c.mudt + (c.rho * sd) * x[1];
+    const float r = (y[0] - mean) / (c.rhoc * sd);
+    return -0.5f * (r * r) + (c.c0 - 0.5f * v);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Stochastic Ricker: N' = r N exp(-N + sigma e), y ~ Poisson(phi N').
+// Parameters (r, sigma, phi, N_0); estimation scale log of each.
+// ---------------------------------------------------------------------------
+struct Ricker {
+  static constexpr int kind = PPF_MODEL_RICKER;
+  static constexpr int MAXDX = 1;
+  static constexpr int MAXDY = 1;
+  static constexpr int MAXP = 4;
+  struct Consts {
+    int dx, dy;
+    float r, sigma, phi, N0;
+  };
+  __host__ __device__ static int n_init(const Consts&) { return 0; }
+  __host__ __device__ static int n_step(const Consts&) { return 1; }
+
+  __device__ static void prepare(Consts& c, const float* th, const ppf_model&, bool est) {
+    c.dx = 1; c.dy = 1;
+    c.r = est ? pp_expf(th[0]) : th[0];
+    c.sigma = est ? pp_expf(th[1]) : th[1];
+    c.phi = est ? pp_expf(th[2]) : th[2];
+    c.N0 = est ? pp_expf(th[3]) : th[3];
+  }
+  __device__ static void rinit(const Consts& c, const float*, float* x) { x[0] = c.N0; }
+  __device__ static void rproc(const Consts& c, float* x, const float* z) {
+    const float N = x[0];
+    const float arg = c.sigma * z[0] - N;
+    x[0] = (c.r * N) * pp_expf(arg);
+  }
+  __device__ static float dmeas(const Consts& c, const float* y, float ycon, const float* x) {
+    const float lam = c.phi * x[0];
+    if (y[0] == 0.0f) return -lam;
+    return (y[0] * pp_logf(lam) - lam) - ycon;
+  }
+};
+
+}  // namespace ppf

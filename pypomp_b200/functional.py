@@ -1,0 +1,155 @@
+"""Stateless drop-ins for ``pypomp.functional`` on the CUDA library.
+
+Signatures and return layouts follow the reference
+(``pypomp/functional/pfilter.py:11-90``, ``mop.py:8-62``, ``mif.py:15-122``,
+``train.py:14-110``); the work is one call into ``libppf.so`` per batch of
+filters instead of a jitted XLA program.  Arrays come back as NumPy.
+
+``struct`` is a :class:`PompStruct` (from ``Pomp.to_struct()``), ``keys`` are
+uint64 key arrays (``pypomp_b200.random``).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi
+from .models import ModelSpec
+
+
+@dataclass
+class PompStruct:
+    """What the kernels need from a model (``pypomp/functional/structs.py:10``)."""
+
+    spec: ModelSpec
+    ys: np.ndarray            # (T, dy) float32, or (U, T, dy) for panels
+    times: np.ndarray
+    t0: float
+    T_u: np.ndarray | None = None   # (U,) lengths for ragged panels
+
+    @property
+    def param_names(self):
+        return list(self.spec.param_names)
+
+
+def _device_inputs(torch, struct: PompStruct, dev):
+    ys = np.asarray(struct.ys, dtype=np.float32)
+    if ys.ndim == 2:
+        ys = ys[None]
+    U, T, _ = ys.shape
+    ycon = struct.spec.ycon(ys)
+    ys_d = torch.from_numpy(np.ascontiguousarray(ys)).to(dev)
+    ycon_d = torch.from_numpy(np.ascontiguousarray(ycon)).to(dev) if ycon is not None else None
+    Tu_d = None
+    if struct.T_u is not None:
+        Tu_d = torch.from_numpy(np.asarray(struct.T_u, dtype=np.int32)).to(dev)
+    return ys_d, ycon_d, Tu_d, U, T
+
+
+def run_pfilter(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J: int, *,
+                thresh: float = 0.0, CLL=False, ESS=False, filter_mean=False,
+                prediction_mean=False, est=False, unit_f=None, path=None, inject=None,
+                save_ancestors=False, save_weights=False, return_torch=False):
+    """One batched call of ``ppf_pfilter`` over F filters.
+
+    ``theta_f`` (F, P) parameters, ``seeds_f`` (F,) keys.  ``inject`` is an
+    optional dict of host arrays ``z0`` (F,J,n0), ``z`` (F,T,J,nz), ``u``
+    (F,T) that replaces the Philox draws.  Returns a dict of NumPy arrays.
+    """
+    torch = _ffi.require_cuda()
+    if J < 1:
+        raise ValueError("J should be greater than 0.")
+    if J > _ffi.PPF_MAX_J:
+        raise ValueError(f"J must be at most {_ffi.PPF_MAX_J}.")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    spec = struct.spec
+    theta_f = np.ascontiguousarray(theta_f, dtype=np.float32)
+    F = theta_f.shape[0]
+    ys_d, ycon_d, Tu_d, U, T = _device_inputs(torch, struct, dev)
+    th_d = torch.from_numpy(theta_f).to(dev)
+    seeds_d = torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).copy()).to(dev)
+    unit_d = None
+    if unit_f is not None:
+        unit_d = torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
+    flags = (_ffi.F_CLL if CLL else 0) | (_ffi.F_ESS if ESS else 0)
+    flags |= (_ffi.F_FMEAN if filter_mean else 0) | (_ffi.F_PMEAN if prediction_mean else 0)
+    flags |= (_ffi.F_EST if est else 0)
+    flags |= (_ffi.F_SAVE_ANC if save_ancestors else 0) | (_ffi.F_SAVE_W if save_weights else 0)
+    out = {"loglik": torch.zeros(F, dtype=torch.float64, device=dev)}
+    f32 = dict(dtype=torch.float32, device=dev)
+    if CLL:
+        out["cll"] = torch.zeros(F, T, dtype=torch.float64, device=dev)
+    if ESS:
+        out["ess"] = torch.zeros(F, T, **f32)
+    if filter_mean:
+        out["fmean"] = torch.zeros(F, T, spec.dx, **f32)
+    if prediction_mean:
+        out["pmean"] = torch.zeros(F, T, spec.dx, **f32)
+    if save_ancestors:
+        out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=dev)
+    if save_weights:
+        out["logw"] = torch.zeros(F, T, J, **f32)
+    inj = {}
+    if inject is not None:
+        flags |= _ffi.F_INJECT
+        for k in ("z0", "z", "u"):
+            if inject.get(k) is not None:
+                inj[k] = torch.from_numpy(np.ascontiguousarray(inject[k], dtype=np.float32)).to(dev)
+    d = _ffi.PfilterDesc()
+    d.model = spec.ffi_model()
+    d.J, d.F, d.T, d.U = J, F, T, U
+    d.path = _ffi.env_path() if path is None else _ffi.PATHS[path] if isinstance(path, str) else int(path)
+    d.flags = flags
+    d.thresh = float(max(0.0, thresh))
+    d.theta, d.ys, d.ycon = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(ycon_d)
+    d.unit, d.T_u, d.seeds = _ffi.ptr(unit_d), _ffi.ptr(Tu_d), _ffi.ptr(seeds_d)
+    d.inj_z0, d.inj_z, d.inj_u = _ffi.ptr(inj.get("z0")), _ffi.ptr(inj.get("z")), _ffi.ptr(inj.get("u"))
+    d.loglik = _ffi.ptr(out["loglik"])
+    d.cll, d.ess = _ffi.ptr(out.get("cll")), _ffi.ptr(out.get("ess"))
+    d.fmean, d.pmean = _ffi.ptr(out.get("fmean")), _ffi.ptr(out.get("pmean"))
+    d.anc, d.logw = _ffi.ptr(out.get("anc")), _ffi.ptr(out.get("logw"))
+    nbytes = _ffi.LIB.ppf_pfilter_workspace_bytes(d)
+    ws = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
+    d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    _ffi.check(_ffi.LIB.ppf_pfilter(d, stream), "ppf_pfilter")
+    _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_pfilter")
+    if return_torch:
+        return out
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+def pfilter(struct: PompStruct, thetas_array, J: int, keys, thresh: float = 0.0,
+            CLL: bool = False, ESS: bool = False, filter_mean: bool = False,
+            prediction_mean: bool = False, *, path=None) -> dict:
+    """Bootstrap particle filter (``pypomp/functional/pfilter.py:11-90``).
+
+    ``thetas_array`` (n_theta, P) natural scale; ``keys`` (n_theta, reps).
+    Returns ``logLik`` (n_theta, reps) and, when requested, ``CLL``/``ESS``
+    (n_theta, reps, T) and ``filter_mean``/``prediction_mean``
+    (n_theta, reps, T, dx).
+    """
+    thetas = np.atleast_2d(np.asarray(thetas_array, dtype=np.float32))
+    keys = np.asarray(keys, dtype=np.uint64)
+    if keys.ndim == 1:
+        keys = keys.reshape(thetas.shape[0], -1)
+    n, reps = keys.shape
+    if n != thetas.shape[0]:
+        raise ValueError("keys must have shape (n_theta, reps)")
+    theta_f = np.repeat(thetas, reps, axis=0)
+    res = run_pfilter(struct, theta_f, keys.reshape(-1), J, thresh=thresh, CLL=CLL, ESS=ESS,
+                      filter_mean=filter_mean, prediction_mean=prediction_mean, path=path)
+    T = res.get("cll", res.get("ess", np.zeros((0, 0)))).shape[-1] if (CLL or ESS) else None
+    out = {"logLik": res["loglik"].reshape(n, reps)}
+    if CLL:
+        out["CLL"] = res["cll"].reshape(n, reps, -1)
+    if ESS:
+        out["ESS"] = res["ess"].reshape(n, reps, -1)
+    if filter_mean:
+        out["filter_mean"] = res["fmean"].reshape(n, reps, res["fmean"].shape[1], -1)
+    if prediction_mean:
+        out["prediction_mean"] = res["pmean"].reshape(n, reps, res["pmean"].shape[1], -1)
+    del T
+    return out

@@ -1,0 +1,227 @@
+"""``Pomp``: the object-oriented interface for the built-in CUDA models.
+
+Mirrors the reference's ``Pomp`` methods on the hot path
+(``pypomp/core/estimation_mixin.py:101`` ``pfilter``, ``:274`` ``mif``,
+``:446`` ``train``) and its result tables (``pypomp/core/analysis_mixin.py``,
+``pypomp/core/results/render.py:145-162``).  Methods keep their keyword
+arguments, return ``None``, update ``self.theta`` and append a ``Result`` to
+``self.results_history``.  ``results()`` has the columns
+``theta_idx, logLik, se, <params>``.
+"""
+
+from __future__ import annotations
+
+import time
+from copy import deepcopy
+from dataclasses import dataclass, field
+
+import numpy as np
+import pandas as pd
+
+from . import random as pprandom
+from .maths import logmeanexp, logmeanexp_se
+
+
+class PompParameters:
+    """A list of parameter dicts plus their log-likelihoods
+    (``pypomp/core/parameters/pomp.py``; pandas/numpy instead of xarray)."""
+
+    def __init__(self, theta, logLik=None):
+        if isinstance(theta, dict):
+            theta = [theta]
+        self._list = [dict(t) for t in theta]
+        self.logLik = None if logLik is None else np.asarray(logLik, dtype=float)
+
+    def num_replicates(self) -> int:
+        return len(self._list)
+
+    def get_param_names(self):
+        return list(self._list[0].keys()) if self._list else []
+
+    def params(self, as_list: bool = True):
+        return [dict(t) for t in self._list] if as_list else pd.DataFrame(self._list)
+
+    def to_array(self, names) -> np.ndarray:
+        return np.asarray([[t[n] for n in names] for t in self._list], dtype=np.float64)
+
+    @classmethod
+    def from_array(cls, arr, names):
+        arr = np.atleast_2d(np.asarray(arr, dtype=float))
+        return cls([{n: float(v) for n, v in zip(names, row)} for row in arr])
+
+    def subset(self, idx):
+        return PompParameters([self._list[i] for i in idx])
+
+    def __len__(self):
+        return len(self._list)
+
+    def __repr__(self):
+        return f"PompParameters({self._list}, logLik={self.logLik})"
+
+
+@dataclass
+class Result:
+    method: str
+    theta: PompParameters
+    payload: dict
+    config: dict = field(default_factory=dict)
+    execution_time: float | None = None
+    key: object = None
+
+    def to_dataframe(self, ignore_nan: bool = False) -> pd.DataFrame:
+        if self.method == "pfilter":
+            arr = np.asarray(self.payload["logLiks"])
+            logLik = np.atleast_1d(logmeanexp(arr, axis=-1, ignore_nan=ignore_nan))
+            se = (logmeanexp_se(arr, axis=-1, ignore_nan=ignore_nan)
+                  if arr.shape[-1] > 1 else np.full_like(logLik, np.nan))
+            df = pd.DataFrame({"theta_idx": np.arange(len(self.theta)), "logLik": logLik,
+                               "se": np.atleast_1d(se)})
+            return pd.concat([df, pd.DataFrame(self.theta.params(as_list=True))], axis=1)
+        # mif / train: final iteration of the trace
+        tr = self.traces()
+        last = tr[tr["iteration"] == tr["iteration"].max()].drop(columns=["iteration", "method"])
+        return last.reset_index(drop=True)
+
+    def traces(self) -> pd.DataFrame:
+        if self.method == "pfilter":
+            df = self.to_dataframe()
+            df.insert(1, "iteration", 0)
+            df.insert(2, "method", "pfilter")
+            return df
+        logliks = np.asarray(self.payload["logLiks"])      # (n, M+1)
+        traces = np.asarray(self.payload["traces"])        # (n, M+1, P)
+        names = self.payload["param_names"]
+        rows = []
+        n, M1 = logliks.shape
+        for i in range(n):
+            for m in range(M1):
+                r = {"theta_idx": i, "iteration": m, "method": self.method,
+                     "logLik": logliks[i, m], "se": np.nan}
+                r.update({nm: traces[i, m, p] for p, nm in enumerate(names)})
+                rows.append(r)
+        return pd.DataFrame(rows)
+
+
+class ResultsHistory:
+    def __init__(self):
+        self._results: list[Result] = []
+
+    def add(self, r: Result):
+        self._results.append(r)
+
+    def __getitem__(self, i):
+        return self._results[i]
+
+    def __len__(self):
+        return len(self._results)
+
+    def results(self, index: int = -1, ignore_nan: bool = False) -> pd.DataFrame:
+        return self._results[index].to_dataframe(ignore_nan=ignore_nan)
+
+    def traces(self) -> pd.DataFrame:
+        frames = []
+        offset = 0
+        for r in self._results:
+            tr = r.traces().copy()
+            tr["iteration"] = tr["iteration"] + offset
+            offset = int(tr["iteration"].max()) + (1 if r.method == "pfilter" else 0)
+            frames.append(tr)
+        return pd.concat(frames, ignore_index=True) if frames else pd.DataFrame()
+
+    def time(self):
+        return [r.execution_time for r in self._results]
+
+
+class Pomp:
+    """A partially observed Markov process on one of the built-in CUDA models."""
+
+    def __init__(self, spec, ys: pd.DataFrame, theta, t0: float = 0.0, fresh_key=None):
+        self.spec = spec
+        if not isinstance(ys, pd.DataFrame):
+            ys = pd.DataFrame(np.asarray(ys, dtype=float),
+                              index=np.arange(1, len(ys) + 1, dtype=float),
+                              columns=list(spec.obsnames))
+        self.ys = ys
+        self.t0 = float(t0)
+        self.theta = theta if isinstance(theta, PompParameters) else PompParameters(theta)
+        self.fresh_key = None if fresh_key is None else pprandom.as_key(fresh_key)
+        self.results_history = ResultsHistory()
+
+    # -- reference-facing attributes --------------------------------------
+    @property
+    def canonical_param_names(self):
+        return list(self.spec.param_names)
+
+    @property
+    def statenames(self):
+        return list(self.spec.statenames)
+
+    def to_struct(self):
+        from .functional import PompStruct
+
+        return PompStruct(spec=self.spec, ys=self.ys.to_numpy(dtype=np.float32),
+                          times=self.ys.index.to_numpy(dtype=float), t0=self.t0)
+
+    def _update_fresh_key(self, key=None):
+        """``pypomp/core/pomp.py:391-408``: split the key, keep one half."""
+        old_key = self.fresh_key if key is None else pprandom.as_key(key)
+        if old_key is None:
+            raise ValueError(
+                "Both the key argument and the fresh_key attribute are None. "
+                "At least one key must be given.")
+        self.fresh_key, new_key = pprandom.split(old_key)
+        return new_key, old_key
+
+    def _prepare_theta_input(self, theta):
+        if theta is None:
+            return self.theta
+        if isinstance(theta, dict) or isinstance(theta, list):
+            theta = PompParameters(theta)
+        if not isinstance(theta, PompParameters):
+            raise TypeError("theta must be a PompParameters object or None")
+        if set(theta.get_param_names()) != set(self.canonical_param_names):
+            raise ValueError("theta parameter names must match canonical_param_names up to reordering")
+        return theta
+
+    # -- estimation ----------------------------------------------------------
+    def pfilter(self, J: int, key=None, theta=None, thresh: float = 0.0, reps: int = 1,
+                CLL: bool = False, ESS: bool = False, filter_mean: bool = False,
+                prediction_mean: bool = False, track_time: bool = True) -> None:
+        """Bootstrap particle filter (``pypomp/core/estimation_mixin.py:101-272``)."""
+        from . import functional as F
+
+        start = time.time()
+        thresh = float(max(0.0, thresh))
+        theta_in = deepcopy(self._prepare_theta_input(theta))
+        theta_for_results = deepcopy(theta_in)
+        new_key, old_key = self._update_fresh_key(key)
+        if J < 1:
+            raise ValueError("J should be greater than 0.")
+        n = theta_in.num_replicates()
+        thetas = theta_in.to_array(self.canonical_param_names)
+        keys = pprandom.split(new_key, n * reps).reshape(n, reps)
+        res = F.pfilter(self.to_struct(), thetas, J, keys, thresh, CLL, ESS, filter_mean, prediction_mean)
+        logliks = res["logLik"]
+        theta_in.logLik = logmeanexp(logliks, axis=-1)
+        self.theta = theta_in
+        payload = {"logLiks": logliks}
+        for k in ("CLL", "ESS", "filter_mean", "prediction_mean"):
+            if k in res:
+                payload[k] = res[k]
+        self.results_history.add(Result(
+            method="pfilter", theta=theta_for_results, payload=payload,
+            config={"J": J, "reps": reps, "thresh": thresh},
+            execution_time=(time.time() - start) if track_time else None, key=old_key))
+
+    # -- analysis ------------------------------------------------------------
+    def results(self, index: int = -1, ignore_nan: bool = False) -> pd.DataFrame:
+        return self.results_history.results(index=index, ignore_nan=ignore_nan)
+
+    def traces(self) -> pd.DataFrame:
+        return self.results_history.traces()
+
+    def CLL(self, index: int = -1) -> np.ndarray:
+        return self.results_history[index].payload["CLL"]
+
+    def ESS(self, index: int = -1) -> np.ndarray:
+        return self.results_history[index].payload["ESS"]
