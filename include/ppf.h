@@ -15,7 +15,8 @@
  *    (stream, workspace) pairs.
  *  - Return codes: PPF_OK, PPF_EINVAL (bad sizes / null pointers / J < 1),
  *    PPF_ECUDA (launch or runtime error), PPF_ETIMEOUT (a bounded device-side
- *    wait gave up; results are invalid), PPF_EUNSUPPORTED.
+ *    wait gave up; results are invalid), PPF_EUNSUPPORTED, PPF_EINTERNAL (a
+ *    device-side consistency check failed and the access was skipped).
  *  - Arithmetic (the exact definitions every path and the C oracle share):
  *      state and log-weights float32, model math in a fixed operation order
  *      with the elementary functions of ppf_detmath.h;
@@ -42,6 +43,7 @@ extern "C" {
 #define PPF_ECUDA 2
 #define PPF_ETIMEOUT 3
 #define PPF_EUNSUPPORTED 4
+#define PPF_EINTERNAL 5
 
 #define PPF_MAX_J (1 << 21)
 
@@ -117,9 +119,20 @@ size_t ppf_pfilter_workspace_bytes(const ppf_pfilter_desc* d);
 /* Run the batched particle filter.  `stream` is a cudaStream_t. */
 int ppf_pfilter(const ppf_pfilter_desc* d, void* stream);
 
-/* Synchronise `stream` and report whether any bounded device-side wait of the
- * last call that used `workspace` gave up (PPF_ETIMEOUT) -- PPF_OK otherwise. */
+/* Synchronise `stream` and report the device-side status of the last call
+ * that used `workspace`: PPF_ETIMEOUT if a bounded wait gave up,
+ * PPF_EINTERNAL if an index check failed, PPF_OK otherwise. */
 int ppf_workspace_status(const void* workspace, void* stream);
+
+/* Per-kernel timing of the calls made between begin and end: CUDA events are
+ * recorded on the launch stream around each kernel (host-side bookkeeping
+ * only).  ppf_profile_end synchronises and writes, for each kernel kind k < n,
+ * the summed milliseconds ms[k] and launch count count[k].  Kinds: 0 init,
+ * 1 weight-sum + lookback, 2 resample + propagate, 3 resident filter,
+ * 4 plain-path step (four kernels), 5..8 MOP forward / recompute / adjoint /
+ * IF2.  Not reentrant. */
+int ppf_profile_begin(void);
+int ppf_profile_end(double* ms, int* count, int n);
 
 /* Human-readable message for a return code (static storage). */
 const char* ppf_error_string(int code);

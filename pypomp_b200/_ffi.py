@@ -16,7 +16,7 @@ from pathlib import Path
 
 _LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libppf.so"
 
-PPF_OK, PPF_EINVAL, PPF_ECUDA, PPF_ETIMEOUT, PPF_EUNSUPPORTED = 0, 1, 2, 3, 4
+PPF_OK, PPF_EINVAL, PPF_ECUDA, PPF_ETIMEOUT, PPF_EUNSUPPORTED, PPF_EINTERNAL = 0, 1, 2, 3, 4, 5
 PPF_MAX_J = 1 << 21
 MODEL_LG, MODEL_SV, MODEL_RICKER = 1, 2, 3
 
@@ -37,6 +37,8 @@ EXPORTED = (
     "ppf_pfilter_workspace_bytes",
     "ppf_pfilter",
     "ppf_workspace_status",
+    "ppf_profile_begin",
+    "ppf_profile_end",
     "ppf_error_string",
     "ppf_version",
 )
@@ -109,6 +111,10 @@ def _load():
     lib.ppf_pfilter.restype = ctypes.c_int
     lib.ppf_workspace_status.argtypes = [_vp, _vp]
     lib.ppf_workspace_status.restype = ctypes.c_int
+    lib.ppf_profile_begin.argtypes = []
+    lib.ppf_profile_begin.restype = ctypes.c_int
+    lib.ppf_profile_end.argtypes = [_vp, _vp, ctypes.c_int]
+    lib.ppf_profile_end.restype = ctypes.c_int
     lib.ppf_error_string.argtypes = [ctypes.c_int]
     lib.ppf_error_string.restype = ctypes.c_char_p
     lib.ppf_version.argtypes = []
@@ -118,6 +124,24 @@ def _load():
 
 LIB = _load()
 LIB_PATH = str(_LIB_PATH)
+
+
+KIND_NAMES = ("init", "sum_lookback", "resample_propagate", "resident", "plain_step",
+              "mop_forward", "mop_recompute", "mop_adjoint", "if2")
+
+
+def profile_begin() -> None:
+    check(LIB.ppf_profile_begin(), "ppf_profile_begin")
+
+
+def profile_end() -> dict:
+    """{kind name: (total ms, launches)} for the calls since profile_begin()."""
+    import numpy as np
+
+    ms = np.zeros(16, np.float64)
+    cnt = np.zeros(16, np.int32)
+    check(LIB.ppf_profile_end(ms.ctypes.data, cnt.ctypes.data, 16), "ppf_profile_end")
+    return {KIND_NAMES[i]: (float(ms[i]), int(cnt[i])) for i in range(len(KIND_NAMES)) if cnt[i]}
 
 
 def error_string(code: int) -> str:

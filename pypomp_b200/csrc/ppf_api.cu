@@ -170,7 +170,29 @@ int ppf_workspace_status(const void* workspace, void* stream) {
   uint32_t err = 0;
   if (cudaMemcpyAsync(&err, workspace, sizeof(err), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PPF_ECUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return PPF_ECUDA;
-  if (err) return PPF_ETIMEOUT;
+  if (err & 1u) return PPF_ETIMEOUT;
+  if (err) return PPF_EINTERNAL;
+  return PPF_OK;
+}
+
+int ppf_profile_begin(void) {
+  g_prof.enabled = true;
+  g_prof.used = 0;
+  return PPF_OK;
+}
+
+int ppf_profile_end(double* ms, int* count, int n) {
+  if (!ms || !count || n < 1) return PPF_EINVAL;
+  for (int i = 0; i < n; ++i) { ms[i] = 0.0; count[i] = 0; }
+  for (int i = 0; i < g_prof.used; ++i) {
+    if (cudaEventSynchronize(g_prof.evs[i].b) != cudaSuccess) return PPF_ECUDA;
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, g_prof.evs[i].a, g_prof.evs[i].b);
+    const int k = g_prof.evs[i].kind;
+    if (k >= 0 && k < n) { ms[k] += t; count[k] += 1; }
+  }
+  g_prof.enabled = false;
+  g_prof.used = 0;
   return PPF_OK;
 }
 
@@ -181,6 +203,7 @@ const char* ppf_error_string(int code) {
     case PPF_ECUDA: return "CUDA launch or runtime error";
     case PPF_ETIMEOUT: return "a bounded device-side wait timed out";
     case PPF_EUNSUPPORTED: return "unsupported configuration";
+    case PPF_EINTERNAL: return "a device-side consistency check failed";
     default: return "unknown error";
   }
 }

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <vector>
 #include "ppf.h"
 
 namespace ppf {
@@ -61,6 +62,18 @@ struct Args {
   const int* T_u_host;
   const int* unit_host;
 };
+
+enum { KIND_INIT = 0, KIND_SUM = 1, KIND_RESPROP = 2, KIND_RESIDENT = 3, KIND_PLAIN = 4,
+       KIND_MOP_FWD = 5, KIND_MOP_RECOMP = 6, KIND_MOP_BWD = 7, KIND_IF2 = 8, KIND_COUNT = 16 };
+
+struct Profiler {
+  struct Ev { cudaEvent_t a, b; int kind; };
+  bool enabled = false;
+  int used = 0;
+  std::vector<Ev> evs;
+  void mark(int kind, cudaStream_t s, bool start);
+};
+extern Profiler g_prof;
 
 int run_pfilter_path(Args& a, int path, cudaStream_t s);
 int reset_accumulators(Args& a, cudaStream_t s);

@@ -173,6 +173,10 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
   if (threadIdx.x == 0) s_v = atomicAdd(a.counter + (t & 1), 1);
   __syncthreads();
   const int v = s_v;
+  if (v >= a.ntiles * a.F) {  // defensive: a stale counter must not index past the batch
+    if (threadIdx.x == 0) atomicOr(a.err, 4u);
+    return;
+  }
   const int f = v / a.ntiles, b = v % a.ntiles;
   const int u = filter_unit(a, f);
   if (t >= filter_len(a, u)) return;
@@ -283,13 +287,14 @@ __global__ void __launch_bounds__(TPB) k_resprop(Args a, int t) {
   const int f = blockIdx.y, b = blockIdx.x;
   const int u = filter_unit(a, f);
   const int Tf = filter_len(a, u);
-  if (t >= Tf) return;
   const int p = t & 1;
-  // reset the next step's lookback descriptors and tile counter
+  // reset the next step's lookback descriptors and tile counter (before any
+  // early exit: finished filters of a ragged panel still own these slots)
   if (threadIdx.x == 0) {
     a.desc[p ^ 1][(size_t)f * a.ntiles + b] = 0ull;
     if (b == 0 && f == 0) a.counter[p ^ 1] = 0;
   }
+  if (t >= Tf) return;
   const Acc acc = a.acc[p][f];
   const uint64_t tot = a.tot[f];
   if (b == 0 && threadIdx.x == 0) finalize_step(a, f, t, acc, tot, a.loglik + f);
@@ -393,6 +398,7 @@ __global__ void __launch_bounds__(TPB) k_resprop(Args a, int t) {
       for (int i = threadIdx.x; i < wn; i += TPB) {
         const int l = mk[i];
         const int k = w0 + i;
+        if (l < 0 || l >= ntile) { atomicOr(a.err, 2u); continue; }  // defensive: never index out of the tile
         if (a.anc) a.anc[((size_t)f * a.T + t) * a.J + k] = jt + l;
         if (last) continue;
         float x[M::MAXDX];
@@ -583,7 +589,8 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
       const int k = threadIdx.x + it * TPB;
       if (k < J) {
         float x[M::MAXDX];
-        const int l = mk[k];
+        int l = mk[k];
+        if (l < 0 || l >= J) { atomicOr(a.err, 2u); l = 0; }  // defensive: never index outside the swarm
         for (int d = 0; d < dx; ++d) x[d] = xs[d * J + l];
         const float m = propagate<M>(a, c, f, u, k, t + 1, x);
 #pragma unroll
@@ -762,6 +769,30 @@ __global__ void __launch_bounds__(TPB) kp_anc(Args a, int f, int t) {
 // Host dispatch
 // ============================================================================
 
+// Optional per-kernel timing (ppf_profile_begin / ppf_profile_end): CUDA
+// events recorded on the launch stream around each kernel of the next calls.
+Profiler g_prof;
+
+void Profiler::mark(int kind, cudaStream_t s, bool start) {
+  if (!enabled) return;
+  if (start) {
+    if (used >= (int)evs.size()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      evs.push_back({a, b, 0});
+    }
+    evs[used].kind = kind;
+    cudaEventRecord(evs[used].a, s);
+  } else {
+    cudaEventRecord(evs[used].b, s);
+    ++used;
+  }
+}
+
+#define PROF_BEGIN(kind) g_prof.mark(kind, s, true)
+#define PROF_END(kind) g_prof.mark(kind, s, false)
+
 template <class M>
 int run_stream(Args& a, cudaStream_t s) {
   constexpr int TPB = 256, IT = 8, TILE = TPB * IT;
@@ -774,10 +805,16 @@ int run_stream(Args& a, cudaStream_t s) {
     attr_set = true;
   }
   dim3 grid(a.ntiles, a.F);
+  PROF_BEGIN(KIND_INIT);
   k_init<M, TPB><<<grid, TPB, 0, s>>>(a);
+  PROF_END(KIND_INIT);
   for (int t = 0; t < a.T; ++t) {
+    PROF_BEGIN(KIND_SUM);
     k_sum<M, TPB, IT><<<a.ntiles * a.F, TPB, 0, s>>>(a, t);
+    PROF_END(KIND_SUM);
+    PROF_BEGIN(KIND_RESPROP);
     k_resprop<M, TPB, IT><<<grid, TPB, smem, s>>>(a, t);
+    PROF_END(KIND_RESPROP);
   }
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
@@ -791,7 +828,9 @@ template <class M, int MAXIT>
 int launch_resident(Args& a, size_t smem, cudaStream_t s) {
   constexpr int TPB = 512;
   cudaFuncSetAttribute(k_resident<M, TPB, MAXIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  PROF_BEGIN(KIND_RESIDENT);
   k_resident<M, TPB, MAXIT><<<a.F, TPB, smem, s>>>(a);
+  PROF_END(KIND_RESIDENT);
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
 
@@ -813,10 +852,12 @@ int run_plain(Args& a, cudaStream_t s) {
   for (int f = 0; f < a.F; ++f) {
     k_reset_acc<<<1, 1, 0, s>>>(a.acc[0]);
     for (int t = 0; t < a.T; ++t) {
+      PROF_BEGIN(KIND_PLAIN);
       kp_prop<M, TPB><<<nblk, TPB, 0, s>>>(a, f, t);
       kp_scan1<TPB><<<nblk, TPB, 0, s>>>(a, f, t);
       kp_scan2<1024><<<1, 1024, 0, s>>>(a, f, t, nblk);
       kp_anc<TPB><<<nblk, TPB, 0, s>>>(a, f, t);
+      PROF_END(KIND_PLAIN);
     }
   }
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;

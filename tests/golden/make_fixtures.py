@@ -1,0 +1,101 @@
+"""Generate the committed golden fixtures under tests/golden/.
+
+Run from the repository root (needs the reference checkout only to read its
+regression CSVs; the GPU tests read only the files written here):
+
+    python tests/golden/make_fixtures.py [/path/to/reference]
+
+Writes
+  ref_values.json  the reference's locked regression values, read from
+                   tests/test_regression/*/*.csv of the reference checkout
+                   (pfilter logLik, per-step diagnostics, MOP value, simulate)
+  ref_lg1d.npz     the reference's 1-D LG data set (``LG(A=[[0.9]], T=4,
+                   key=jax.random.key(0))``, tests/test_regression/conftest.py:23)
+                   regenerated through oracle/jaxrng.py, plus the exact
+                   normals and uniforms the reference draws for each locked
+                   filter run (replayed key trees), for noise-injection runs
+"""
+
+from __future__ import annotations
+
+import csv
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle import jaxrng as jr  # noqa: E402
+from oracle import refpath as rp  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+f32 = np.float32
+
+# LG(A=[[0.9]]) natural-scale theta in canonical order A11, C11, Q11, R11, X0_1
+# (default Q = 1/100 -> chol 0.1; default R = 1/10 -> chol sqrt(0.1)).
+THETA_LG1D = np.array([0.9, 1.0, 0.1, np.sqrt(0.1), 0.0], dtype=f32)
+
+
+def _read_csv(path: Path) -> dict:
+    with open(path) as fh:
+        rows = list(csv.reader(fh))
+    header = rows[0][1:]
+    cols = {h: [] for h in header}
+    for r in rows[1:]:
+        for h, v in zip(header, r[1:]):
+            if v != "":
+                cols[h].append(float(v))
+    return cols
+
+
+def main(ref_root: Path):
+    reg = ref_root / "tests" / "test_regression"
+    values = {
+        "pfilter": _read_csv(reg / "test_pfilter_regression" / "test_pfilter_regression.csv"),
+        "pfilter_diagnostics": _read_csv(reg / "test_pfilter_regression" / "test_pfilter_diagnostics_regression.csv"),
+        "mop": _read_csv(reg / "test_mop_regression" / "test_mop_regression.csv"),
+        "simulate": _read_csv(reg / "test_simulate_regression" / "test_simulate_regression.csv"),
+        "mif": _read_csv(reg / "test_mif_regression" / "test_mif_regression.csv"),
+        "mif_full_trace": _read_csv(reg / "test_mif_regression" / "test_mif_full_trace_regression.csv"),
+        "train": _read_csv(reg / "test_train_regression" / "test_train_regression.csv"),
+        "tolerance": {"atol": 1e-6, "rtol": 1e-4},
+        "source": "pypomp 0.4.10.2 tests/test_regression (tolerance: tests/test_regression/conftest.py:118-125)",
+    }
+    (OUT / "ref_values.json").write_text(json.dumps(values, indent=1))
+
+    # Data: Pomp.simulate(key=key(0)) inside LG(...)
+    X, Y = rp.pomp_simulate_data("LG", THETA_LG1D, 4, jr.key(0))
+    ys = Y.astype(f32)
+    J = 12
+    arrays = {"theta": THETA_LG1D, "ys": ys}
+    # pfilter regression: keys = split(key(20260811), 1)
+    k = jr.split(jr.key(20260811), 1)[0]
+    rec = rp.RecordingNoise(rp.JaxKeyNoise(k, J, 1, 1))
+    rp.pfilter("LG", THETA_LG1D, ys, J, rec)
+    z0, z, u = rec.arrays()
+    arrays.update(pf_z0=z0, pf_z=z, pf_u=u)
+    # diagnostics: thetas (theta0, 1.05 theta0), keys = split(key(20260812), 2)
+    ks = jr.split(jr.key(20260812), 2)
+    thetas = np.stack([THETA_LG1D, (THETA_LG1D * f32(1.05)).astype(f32)])
+    zz0, zz, uu = [], [], []
+    for r in range(2):
+        rec = rp.RecordingNoise(rp.JaxKeyNoise(ks[r], J, 1, 1))
+        rp.pfilter("LG", thetas[r], ys, J, rec, diagnostics=True)
+        a, b, c = rec.arrays()
+        zz0.append(a); zz.append(b); uu.append(c)
+    arrays.update(diag_theta=thetas, diag_z0=np.stack(zz0), diag_z=np.stack(zz), diag_u=np.stack(uu))
+    # mop regression: keys = split(key(20260811), 1), alpha 0.5, theta0 read as estimation scale
+    k = jr.split(jr.key(20260811), 1)[0]
+    rec = rp.RecordingNoise(rp.JaxKeyNoise(k, J, 1, 1))
+    rp.mop("LG", THETA_LG1D, ys, J, 0.5, rec)
+    z0, z, u = rec.arrays()
+    arrays.update(mop_z0=z0, mop_z=z, mop_u=u)
+    np.savez(OUT / "ref_lg1d.npz", **arrays)
+
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))

@@ -1,0 +1,65 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares (CPU)."""
+
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared_symbols():
+    syms = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        # only extern "C" function declarations of the public ABI (ppf_*)
+        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(ppf_\w+)\s*\(", text, re.M):
+            syms.add(m.group(1))
+    return syms
+
+
+def test_library_exports_declared_symbols():
+    from pypomp_b200 import _ffi
+
+    out = subprocess.run(["nm", "-D", "--defined-only", _ffi.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\sT\s(ppf_\w+)", out))
+    declared = _declared_symbols()
+    assert declared, "no declarations parsed"
+    missing = declared - exported
+    assert not missing, f"declared but not exported: {missing}"
+    assert set(_ffi.EXPORTED) <= exported
+
+
+def test_error_strings_and_version():
+    from pypomp_b200 import _ffi
+
+    assert _ffi.error_string(_ffi.PPF_OK) == "ok"
+    assert "timed out" in _ffi.error_string(_ffi.PPF_ETIMEOUT)
+    assert "sm_100a" in _ffi.version()
+
+
+def test_workspace_size_is_host_only():
+    from pypomp_b200 import _ffi
+
+    d = _ffi.PfilterDesc()
+    d.model = _ffi.PpfModel(_ffi.MODEL_LG, 2, 2, 16, 0.0, 0)
+    d.J, d.F, d.T, d.U = 262144, 64, 1000, 1
+    d.path = _ffi.PATH_STREAM
+    n = _ffi.LIB.ppf_pfilter_workspace_bytes(d)
+    # X and W double-buffered: 2 * 64 * 262144 * (2 + 1) * 4 bytes, plus control
+    assert n >= 2 * 64 * 262144 * 12
+    assert n < 2 * 64 * 262144 * 12 + (1 << 24)
+
+
+def test_validation_messages_without_gpu(lg2d):
+    from pypomp_b200 import functional as F
+
+    with pytest.raises(ValueError, match="J should be greater than 0"):
+        lg2d.pfilter(J=0, key=1)
+    st = lg2d.to_struct()
+    th = lg2d.theta.to_array(lg2d.canonical_param_names)
+    with pytest.raises((ValueError, RuntimeError)):
+        F.run_pfilter(st, th, np.array([1], np.uint64), 0)

@@ -1,0 +1,211 @@
+"""Parity of the CUDA particle filter with the oracle (GPU).
+
+Every execution path (plain, stream, resident) is compared with the C oracle
+bit for bit on log-weights and resampling ancestors, in both noise-injection
+and Philox modes; log-likelihoods agree to float64 rounding of log().  The
+reference's own locked fixtures are reproduced by feeding the reference's
+draws through the injection mode.  Edge cases: J=1, T=1, partial tiles,
+thresh > 1 (steps without resampling), ragged panels, collapsed weights,
+non-finite parameters.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import cora, kalman
+
+pytestmark = pytest.mark.gpu
+
+PATHS = ["plain", "stream", "resident"]
+f32 = np.float32
+
+
+def _F():
+    from pypomp_b200 import functional as F
+
+    return F
+
+
+def _bits_equal(a, b):
+    a = np.asarray(a, f32)
+    b = np.asarray(b, f32)
+    same = (a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))
+    return bool(np.all(same))
+
+
+def _compare(got, want, what):
+    assert np.array_equal(got["anc"], want["anc"]), f"{what}: ancestors differ"
+    assert _bits_equal(got["logw"], want["logw"]), f"{what}: log-weights differ"
+    np.testing.assert_allclose(got["loglik"], want["loglik"], rtol=1e-12, atol=1e-12, err_msg=what)
+    if "cll" in want:
+        np.testing.assert_allclose(got["cll"], want["cll"], rtol=1e-12, atol=1e-12, err_msg=what)
+    if "ess" in want:
+        np.testing.assert_allclose(got["ess"], want["ess"], rtol=1e-5, err_msg=what)
+    for k in ("fmean", "pmean"):
+        if k in want:
+            np.testing.assert_allclose(got[k], want[k], rtol=1e-5, atol=1e-6, err_msg=what)
+
+
+def _models():
+    import pypomp_b200 as pp
+
+    from tests.conftest import LG2_Q, LG2_R
+
+    lg = pp.LG(T=12, Q=LG2_Q, R=LG2_R, key=3)
+    sv = pp.SV(T=12, key=1)
+    rk = pp.Ricker(T=12, key=2)
+    return {"LG": lg, "SV": sv, "Ricker": rk}
+
+
+def _thetas(m, F):
+    th = np.repeat(m.theta.to_array(m.canonical_param_names), F, axis=0).astype(f32)
+    for f in range(1, F):
+        th[f, 0] *= f32(1.0 - 0.03 * f)
+    return th
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("model", ["LG", "SV", "Ricker"])
+@pytest.mark.parametrize("J", [1, 777, 5000])
+def test_philox_mode_bit_exact(path, model, J):
+    F = _F()
+    m = _models()[model]
+    st = m.to_struct()
+    th = _thetas(m, 3)
+    seeds = np.array([3, 1000, 77], np.uint64)
+    spec = m.spec
+    ycon = spec.ycon(st.ys)
+    want = cora.pfilter(spec.kind, spec.dx, spec.dy, th, st.ys, J, seeds=seeds, ycon=ycon,
+                        dt=spec.dt, anc=True, logw=True, CLL=True, ESS=True, fmean=True, pmean=True)
+    got = F.run_pfilter(st, th, seeds, J, path=path, save_ancestors=True, save_weights=True,
+                        CLL=True, ESS=True, filter_mean=True, prediction_mean=True)
+    _compare(got, want, f"{model}/{path}/J={J}")
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_injection_mode_bit_exact_lg2d(path, lg2d):
+    F = _F()
+    st = lg2d.to_struct()
+    th = lg2d.theta.to_array(lg2d.canonical_param_names).astype(f32)
+    J, T = 4096, 50
+    rng = np.random.default_rng(1234)
+    inj = dict(z0=rng.standard_normal((1, J, 2)).astype(f32),
+               z=rng.standard_normal((1, T, J, 2)).astype(f32), u=rng.random((1, T)).astype(f32))
+    want = cora.pfilter(1, 2, 2, th, st.ys, J, inject=inj, anc=True, logw=True, CLL=True, ESS=True)
+    got = F.run_pfilter(st, th, np.zeros(1, np.uint64), J, path=path, inject=inj,
+                        save_ancestors=True, save_weights=True, CLL=True, ESS=True)
+    _compare(got, want, f"inject/{path}")
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_reference_fixtures_through_injection(path, ref_values, ref_lg1d):
+    """The reference's own normals and uniforms reproduce its locked values."""
+    F = _F()
+    from pypomp_b200.models import lg_spec
+    from pypomp_b200.functional import PompStruct
+
+    tol = ref_values["tolerance"]
+    st = PompStruct(spec=lg_spec(1, 1), ys=ref_lg1d["ys"], times=np.arange(1, 5.0), t0=0.0)
+    inj = dict(z0=ref_lg1d["diag_z0"], z=ref_lg1d["diag_z"], u=ref_lg1d["diag_u"])
+    got = F.run_pfilter(st, ref_lg1d["diag_theta"], np.zeros(2, np.uint64), 12, path=path,
+                        inject=inj, CLL=True, ESS=True, filter_mean=True, prediction_mean=True)
+    gold = ref_values["pfilter_diagnostics"]
+    for r in range(2):
+        np.testing.assert_allclose(got["loglik"][r], gold["logLik"][r], **tol)
+        for t in range(4):
+            np.testing.assert_allclose(got["cll"][r, t], gold[f"CLL_rep{r}_t{t}"][0], **tol)
+            np.testing.assert_allclose(got["ess"][r, t], gold[f"ESS_rep{r}_t{t}"][0], **tol)
+            np.testing.assert_allclose(got["fmean"][r, t, 0], gold[f"filter_mean_rep{r}_t{t}"][0], **tol)
+            np.testing.assert_allclose(got["pmean"][r, t, 0], gold[f"prediction_mean_rep{r}_t{t}"][0], **tol)
+    inj = dict(z0=ref_lg1d["pf_z0"][None], z=ref_lg1d["pf_z"][None], u=ref_lg1d["pf_u"][None])
+    got = F.run_pfilter(st, ref_lg1d["theta"][None], np.zeros(1, np.uint64), 12, path=path, inject=inj)
+    np.testing.assert_allclose(got["loglik"][0], ref_values["pfilter"]["logLik"][0], **tol)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_thresh_ragged_panel_and_T1(path):
+    F = _F()
+    import pypomp_b200 as pp
+    from pypomp_b200.functional import PompStruct
+
+    units = [pp.Ricker(T=9, key=k) for k in range(3)]
+    ys = np.stack([u.ys.to_numpy(dtype=f32) for u in units])
+    T_u = np.array([5, 9, 1], np.int32)
+    st = PompStruct(spec=units[0].spec, ys=ys, times=np.arange(1, 10.0), t0=0.0, T_u=T_u)
+    th = _thetas(units[0], 6)
+    unit = np.array([0, 1, 2, 0, 1, 2], np.int32)
+    seeds = np.arange(6, dtype=np.uint64) * 7 + 1
+    spec = units[0].spec
+    for thresh in (0.0, 20.0):
+        want = cora.pfilter(spec.kind, 1, 1, th, ys, 3000, seeds=seeds, ycon=spec.ycon(ys), unit=unit,
+                            T_u=T_u, thresh=thresh, anc=True, logw=True, CLL=True)
+        got = F.run_pfilter(st, th, seeds, 3000, thresh=thresh, unit_f=unit, path=path,
+                            save_ancestors=True, save_weights=True, CLL=True)
+        for f in range(6):
+            Tf = T_u[unit[f]]
+            assert np.array_equal(got["anc"][f, :Tf], want["anc"][f, :Tf]), (path, thresh, f)
+            assert _bits_equal(got["logw"][f, :Tf], want["logw"][f, :Tf]), (path, thresh, f)
+        np.testing.assert_allclose(got["loglik"], want["loglik"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_collapsed_and_nonfinite(path):
+    F = _F()
+    import pypomp_b200 as pp
+
+    m = pp.Ricker(T=6, key=5)
+    st = m.to_struct()
+    th = np.repeat(m.theta.to_array(m.canonical_param_names), 3, axis=0).astype(f32)
+    th[1, 2] = 0.0          # phi = 0: every particle has zero likelihood for y > 0
+    th[2, 0] = np.nan       # r = NaN: NaN weights
+    seeds = np.array([1, 2, 3], np.uint64)
+    want = cora.pfilter(3, 1, 1, th, st.ys, 700, seeds=seeds, ycon=m.spec.ycon(st.ys), anc=True, CLL=True)
+    got = F.run_pfilter(st, th, seeds, 700, path=path, save_ancestors=True, CLL=True)
+    assert np.array_equal(got["anc"], want["anc"])
+    assert np.isneginf(want["loglik"][1]) and np.isnan(want["loglik"][2])
+    assert np.isneginf(got["loglik"][1]) and np.isnan(got["loglik"][2])
+    np.testing.assert_allclose(got["loglik"][0], want["loglik"][0], rtol=1e-12)
+
+
+def test_lg_c1_against_kalman(lg2d):
+    """Config 1 through the public Pomp API: logLik within MC error of FP64 Kalman."""
+    th = lg2d.theta.to_array(lg2d.canonical_param_names)
+    A, C, Q, R, X0 = kalman.lg_matrices(th[0], 2, 2)
+    exact = kalman.kalman_loglik(lg2d.to_struct().ys, A, C, Q, R, X0)
+    lg2d.pfilter(J=1000, key=2024, reps=32, CLL=True, ESS=True)
+    df = lg2d.results()
+    assert list(df.columns[:3]) == ["theta_idx", "logLik", "se"]
+    lls = lg2d.results_history[-1].payload["logLiks"][0]
+    assert abs(np.mean(lls) - exact) < 4 * np.std(lls) / np.sqrt(lls.size) + 0.05
+    cll = lg2d.CLL()
+    np.testing.assert_allclose(cll.sum(axis=-1), lg2d.results_history[-1].payload["logLiks"], rtol=1e-10)
+    ess = lg2d.ESS()
+    assert np.all(ess >= 1) and np.all(ess <= 1000)
+
+
+def test_lg_c2_full_width_properties(lg2d):
+    """Config 2 width (J=262144) on a short horizon: bit-exact vs oracle, sorted ancestors."""
+    F = _F()
+    st = lg2d.to_struct()
+    st.ys = st.ys[:6]
+    th = np.repeat(lg2d.theta.to_array(lg2d.canonical_param_names), 2, axis=0).astype(f32)
+    seeds = np.array([0, 1], np.uint64)
+    J = 262144
+    want = cora.pfilter(1, 2, 2, th, st.ys, J, seeds=seeds, anc=True, CLL=True, nthreads=2)
+    got = F.run_pfilter(st, th, seeds, J, path="stream", save_ancestors=True, CLL=True)
+    assert np.array_equal(got["anc"], want["anc"])
+    np.testing.assert_allclose(got["loglik"], want["loglik"], rtol=1e-12)
+    assert np.all(np.diff(got["anc"], axis=-1) >= 0)
+    np.testing.assert_allclose(got["cll"].sum(-1), got["loglik"], rtol=1e-12)
+
+
+def test_j_validation():
+    F = _F()
+    import pypomp_b200 as pp
+
+    m = pp.Ricker(T=3)
+    th = m.theta.to_array(m.canonical_param_names)
+    with pytest.raises(ValueError, match="J should be greater than 0"):
+        F.run_pfilter(m.to_struct(), th, np.array([1], np.uint64), 0)
+    with pytest.raises(ValueError):
+        F.run_pfilter(m.to_struct(), th, np.array([1], np.uint64), (1 << 21) + 1)
