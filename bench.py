@@ -179,7 +179,7 @@ def run_ours(args):
     seeds = (np.arange(NSEED, dtype=np.uint64) + np.uint64(1000 * rank))
 
     # ---- device-resident inputs, one descriptor, C-ABI calls -------------
-    ys_d = torch.from_numpy(st.ys).to(dev)
+    ys_d = torch.from_numpy(np.ascontiguousarray(st.ys)).to(dev)
     th_d = torch.from_numpy(th).to(dev)
     seeds_d = torch.from_numpy(seeds.view(np.int64).copy()).to(dev)
     ll_d = torch.zeros(NSEED, dtype=torch.float64, device=dev)
@@ -323,6 +323,22 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile_case(args):
+    """A small case of the same kernels for ncu captures: the headline model
+    and J, 8 seeds, the first 12 observations, one call."""
+    import torch
+
+    from pypomp_b200 import functional as F
+
+    m = workload()
+    st = m.to_struct()
+    st.ys = st.ys[:12]
+    th = np.repeat(m.theta.to_array(m.canonical_param_names), 8, axis=0).astype(np.float32)
+    out = F.run_pfilter(st, th, np.arange(8, dtype=np.uint64), J, path=args.path)
+    torch.cuda.synchronize()
+    print("profile case logLik", out["loglik"][:2])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,8 +348,13 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-t", type=int, default=40)
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run one small call of the same kernels (for ncu) and exit")
+    ap.add_argument("--path", default="stream")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

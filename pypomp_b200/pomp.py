@@ -159,7 +159,9 @@ class Pomp:
     def to_struct(self):
         from .functional import PompStruct
 
-        return PompStruct(spec=self.spec, ys=self.ys.to_numpy(dtype=np.float32),
+        # C-contiguous (row-major [T][dy]): pandas hands out column-major views
+        ys = np.ascontiguousarray(self.ys.to_numpy(dtype=np.float32, copy=True))
+        return PompStruct(spec=self.spec, ys=ys,
                           times=self.ys.index.to_numpy(dtype=float), t0=self.t0)
 
     def _update_fresh_key(self, key=None):
