@@ -8,10 +8,10 @@
  * ten rounds.  Tests check it against the paper's known-answer vectors.
  *
  * Counter layout used by every kernel (one 64-bit key per filter):
- *   c0 = particle index j
+ *   c0 = normal-stream block (normal i of a step comes from block i / 4)
  *   c1 = step s (0 = initial draw, i+1 = the step into observation i)
- *   c2 = purpose tag | (block << 8); tags: 0 process noise, 1 resampling
- *        uniform (c0 = 0), 2 IF2 parameter perturbation
+ *   c2 = purpose tag: 0 process noise, 1 resampling uniform (c0 = 0),
+ *        2 IF2 parameter perturbation
  *   c3 = 0
  * Each call yields four 32-bit words; normals come in pairs by Box-Muller:
  *   u1 = ((w0 >> 8) + 1) 2^-24 in (0, 1],  u2 = (w1 >> 8) 2^-24 in [0, 1)
@@ -71,18 +71,29 @@ PPF_HD void pp_boxmuller(uint32_t wa, uint32_t wb, float* z0, float* z1) {
   *z1 = rr * s;
 }
 
-/* n standard normals (n <= 4*nblk) for (particle j, step s, tag). */
-PPF_HD void pp_normals(uint64_t seed, uint32_t j, uint32_t s, uint32_t tag, int n, float* z) {
-  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  for (int b = 0; 4 * b < n; ++b) {
-    const pp_u32x4 w = pp_philox4x32_10(j, s, tag | ((uint32_t)b << 8), 0u, k0, k1);
-    float a0, a1, a2, a3;
-    pp_boxmuller(w.v[0], w.v[1], &a0, &a1);
-    pp_boxmuller(w.v[2], w.v[3], &a2, &a3);
-    if (4 * b + 0 < n) z[4 * b + 0] = a0;
-    if (4 * b + 1 < n) z[4 * b + 1] = a1;
-    if (4 * b + 2 < n) z[4 * b + 2] = a2;
-    if (4 * b + 3 < n) z[4 * b + 3] = a3;
+/* Normal number i of the stream (step s, tag) of one filter:
+ * element i % 4 of the four normals made from Philox(c0 = i / 4, s, tag, 0).
+ * Particle k draws the n consecutive normals i = k n ... k n + n - 1, so a
+ * group of 4 consecutive particles consumes exactly n Philox calls and 2n
+ * Box-Muller pairs -- every word is used. */
+PPF_HD void pp_normal4(uint64_t seed, uint32_t call, uint32_t s, uint32_t tag, float* z4) {
+  const pp_u32x4 w = pp_philox4x32_10(call, s, tag, 0u, (uint32_t)seed, (uint32_t)(seed >> 32));
+  pp_boxmuller(w.v[0], w.v[1], &z4[0], &z4[1]);
+  pp_boxmuller(w.v[2], w.v[3], &z4[2], &z4[3]);
+}
+
+/* The n normals of particle k (n <= 16), computed one at a time; bit-identical
+ * to the grouped computation the kernels use. */
+PPF_HD void pp_normals(uint64_t seed, uint32_t k, uint32_t s, uint32_t tag, int n, float* z) {
+  uint32_t cached = 0xffffffffu;
+  float z4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  for (int r = 0; r < n; ++r) {
+    const uint32_t i = k * (uint32_t)n + (uint32_t)r;
+    if ((i >> 2) != cached) {
+      cached = i >> 2;
+      pp_normal4(seed, cached, s, tag, z4);
+    }
+    z[r] = z4[i & 3u];
   }
 }
 

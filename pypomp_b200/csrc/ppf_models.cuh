@@ -24,9 +24,12 @@ namespace ppf {
 // A (row-major dx*dx), C (row-major dy*dx), lower triangle of chol(Q)
 // row-major, lower triangle of chol(R) row-major, X0 (dx).
 // ---------------------------------------------------------------------------
+template <int DX>
 struct LG {
   static constexpr int kind = PPF_MODEL_LG;
-  static constexpr int MAXDX = 4;
+  static constexpr int MAXDX = DX;     // state dimension, fixed per instantiation
+  static constexpr int NZ = DX;        // process normals per particle-step
+  static constexpr int NZ0 = DX;       // initial-state normals per particle
   static constexpr int MAXDY = 4;
   static constexpr int MAXP = 16 + 16 + 10 + 10 + 4;
   struct Consts {
@@ -34,11 +37,8 @@ struct LG {
     float A[16], C[16], LQ[16], L[16], Linv[4], X0[4];
     float c0;
   };
-  __host__ __device__ static int n_init(const Consts& c) { return c.dx; }
-  __host__ __device__ static int n_step(const Consts& c) { return c.dx; }
-
   __device__ static void prepare(Consts& c, const float* th, const ppf_model& m, bool est) {
-    const int dx = m.dx, dy = m.dy;
+    const int dx = DX, dy = m.dy;
     c.dx = dx; c.dy = dy;
     int p = 0;
     for (int i = 0; i < dx; ++i)
@@ -85,34 +85,28 @@ struct LG {
 
   __device__ static void rinit(const Consts& c, const float* z, float* x) {
 #pragma unroll
-    for (int i = 0; i < MAXDX; ++i) {
-      if (i < c.dx) {
-        float s = 0.0f;
+    for (int i = 0; i < DX; ++i) {
+      float s = 0.0f;
 #pragma unroll
-        for (int k = 0; k <= i; ++k) s = s + c.LQ[i * 4 + k] * z[k];
-        x[i] = c.X0[i] + s;
-      }
+      for (int k = 0; k <= i; ++k) s = s + c.LQ[i * 4 + k] * z[k];
+      x[i] = c.X0[i] + s;
     }
   }
 
   __device__ static void rproc(const Consts& c, float* x, const float* z) {
-    float y[MAXDX];
+    float y[DX];
 #pragma unroll
-    for (int i = 0; i < MAXDX; ++i) {
-      if (i < c.dx) {
-        float a = 0.0f;
+    for (int i = 0; i < DX; ++i) {
+      float a = 0.0f;
 #pragma unroll
-        for (int k = 0; k < MAXDX; ++k)
-          if (k < c.dx) a = a + c.A[i * 4 + k] * x[k];
-        float s = 0.0f;
+      for (int k = 0; k < DX; ++k) a = a + c.A[i * 4 + k] * x[k];
+      float s = 0.0f;
 #pragma unroll
-        for (int k = 0; k <= i; ++k) s = s + c.LQ[i * 4 + k] * z[k];
-        y[i] = a + s;
-      }
+      for (int k = 0; k <= i; ++k) s = s + c.LQ[i * 4 + k] * z[k];
+      y[i] = a + s;
     }
 #pragma unroll
-    for (int i = 0; i < MAXDX; ++i)
-      if (i < c.dx) x[i] = y[i];
+    for (int i = 0; i < DX; ++i) x[i] = y[i];
   }
 
   __device__ static float dmeas(const Consts& c, const float* y, float /*ycon*/, const float* x) {
@@ -123,8 +117,7 @@ struct LG {
       if (i < c.dy) {
         float a = 0.0f;
 #pragma unroll
-        for (int k = 0; k < MAXDX; ++k)
-          if (k < c.dx) a = a + c.C[i * 4 + k] * x[k];
+        for (int k = 0; k < DX; ++k) a = a + c.C[i * 4 + k] * x[k];
         float r = y[i] - a;
 #pragma unroll
         for (int l = 0; l < i; ++l) r = r - c.L[i * 4 + l] * s[l];
@@ -151,14 +144,14 @@ __host__ __device__ inline float pp_tanhf_det(float a) {
 struct SV {
   static constexpr int kind = PPF_MODEL_SV;
   static constexpr int MAXDX = 2;
+  static constexpr int NZ = 1;
+  static constexpr int NZ0 = 0;
   static constexpr int MAXDY = 1;
   static constexpr int MAXP = 6;
   struct Consts {
     int dx, dy;
     float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, c0;
   };
-  __host__ __device__ static int n_init(const Consts&) { return 0; }
-  __host__ __device__ static int n_step(const Consts&) { return 1; }
 
   __device__ static void prepare(Consts& c, const float* th, const ppf_model& m, bool est) {
     c.dx = 2; c.dy = 1;
@@ -204,14 +197,14 @@ struct SV {
 struct Ricker {
   static constexpr int kind = PPF_MODEL_RICKER;
   static constexpr int MAXDX = 1;
+  static constexpr int NZ = 1;
+  static constexpr int NZ0 = 0;
   static constexpr int MAXDY = 1;
   static constexpr int MAXP = 4;
   struct Consts {
     int dx, dy;
     float r, sigma, phi, N0;
   };
-  __host__ __device__ static int n_init(const Consts&) { return 0; }
-  __host__ __device__ static int n_step(const Consts&) { return 1; }
 
   __device__ static void prepare(Consts& c, const float* th, const ppf_model&, bool est) {
     c.dx = 1; c.dy = 1;

@@ -34,8 +34,13 @@ namespace ppf {
 
 // ------------------------------ shared helpers ------------------------------
 
+__device__ __forceinline__ int filter_len(const Args& a, int u) { return a.T_u ? a.T_u[u] : a.T; }
+__device__ __forceinline__ int filter_unit(const Args& a, int f) { return a.unit ? a.unit[f] : 0; }
+
+// Normals of one particle (used by the plain path and by single particles).
 template <class M>
 __device__ __forceinline__ void step_noise(const Args& a, int f, int j, int s, int n, float* z) {
+  if (n <= 0) return;
   if (a.flags & PPF_F_INJECT) {
     if (s == 0) {
       for (int i = 0; i < n; ++i) z[i] = a.inj_z0[((size_t)f * a.J + j) * n + i];
@@ -48,25 +53,49 @@ __device__ __forceinline__ void step_noise(const Args& a, int f, int j, int s, i
   }
 }
 
+// Normals of the group of 4 consecutive particles k0..k0+3 (k0 % 4 == 0) at
+// step s, N per particle: z[e*N + r].  Philox calls (k0 N)/4 ... + N-1 cover
+// the group exactly; positions past J read zeros in injection mode.
+template <int N>
+__device__ __forceinline__ void group_noise(const Args& a, int f, int s, int k0, float* z) {
+  if (N == 0) return;
+  if (a.flags & PPF_F_INJECT) {
+    const float* src = (s == 0) ? a.inj_z0 + (size_t)f * a.J * N
+                                : a.inj_z + (((size_t)f * a.T + (s - 1)) * a.J) * N;
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+#pragma unroll
+      for (int r = 0; r < N; ++r) z[e * N + r] = (k0 + e < a.J) ? src[(size_t)(k0 + e) * N + r] : 0.0f;
+  } else {
+    const uint64_t seed = a.seeds[f];
+    const uint32_t c0 = (uint32_t)(k0 / 4) * N;
+#pragma unroll
+    for (int c = 0; c < N; ++c) pp_normal4(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
+  }
+}
+
 __device__ __forceinline__ uint32_t resample_u32(const Args& a, int f, int t) {
   if (a.flags & PPF_F_INJECT) return pp_u32_from_float(a.inj_u[(size_t)f * a.T + t]);
   return pp_resample_u32(a.seeds[f], (uint32_t)(t + 1));
 }
 
-__device__ __forceinline__ int filter_len(const Args& a, int u) { return a.T_u ? a.T_u[u] : a.T; }
-__device__ __forceinline__ int filter_unit(const Args& a, int f) { return a.unit ? a.unit[f] : 0; }
-
-// rproc into observation t (step s = t+1) and dmeas at observation t.
+// rproc with the given normals, then dmeas at observation t.
 template <class M>
-__device__ __forceinline__ float propagate(const Args& a, const typename M::Consts& c, int f, int u,
-                                           int j, int t, float* x) {
-  float z[M::MAXDX > 0 ? M::MAXDX : 1];
-  const int nz = M::n_step(c);
-  step_noise<M>(a, f, j, t + 1, nz, z);
+__device__ __forceinline__ float prop1(const Args& a, const typename M::Consts& c, int u, int t,
+                                       float* x, const float* z) {
   M::rproc(c, x, z);
   const float* y = a.ys + ((size_t)u * a.T + t) * a.model.dy;
   const float yc = a.ycon ? a.ycon[(size_t)u * a.T + t] : 0.0f;
   return M::dmeas(c, y, yc, x);
+}
+
+// Single-particle propagate into observation t (plain path).
+template <class M>
+__device__ __forceinline__ float propagate(const Args& a, const typename M::Consts& c, int f, int u,
+                                           int j, int t, float* x) {
+  float z[M::NZ > 0 ? M::NZ : 1];
+  step_noise<M>(a, f, j, t + 1, M::NZ, z);
+  return prop1<M>(a, c, u, t, x, z);
 }
 
 // Finalise one observation of one filter: log-likelihood term and outputs.
@@ -111,6 +140,63 @@ __device__ __forceinline__ void accum_maxmin(float w, unsigned int& mx, unsigned
   mn = min(mn, k);
 }
 
+// Constants of the exact systematic-offset test for one filter and step:
+//   child k lies below CDF value C  <=>  k tot + chi < C J,
+// chi = floor(u32 tot / 2^32) (derivation in ppf_core.cuh, nchild).
+struct Offsets {
+  uint64_t tot, chi;
+  double inv, chi_d;   // J / tot and chi / tot, for the first guess
+  int J;
+};
+
+__device__ __forceinline__ Offsets make_offsets(uint64_t tot, uint32_t u32, int J) {
+  Offsets o;
+  o.tot = tot;
+  o.chi = __umul64hi((uint64_t)u32 << 32, tot);   // (u32 * tot) >> 32
+  o.inv = (double)J / (double)tot;
+  o.chi_d = (double)o.chi / (double)tot;
+  o.J = J;
+  return o;
+}
+
+// 128-bit a*b for 64-bit a, b as (hi, lo).
+__device__ __forceinline__ void mul64(uint64_t a, uint64_t b, uint64_t& hi, uint64_t& lo) {
+  lo = a * b;
+  hi = __umul64hi(a, b);
+}
+
+// k tot + chi < C J ?
+__device__ __forceinline__ bool below(const Offsets& o, long long k, uint64_t CJhi, uint64_t CJlo) {
+  uint64_t h, l;
+  mul64((uint64_t)k, o.tot, h, l);
+  l += o.chi;
+  h += (l < o.chi);
+  return (h < CJhi) || (h == CJhi && l < CJlo);
+}
+
+// nchild(C) = #{ k in [0,J) : k tot + chi < C J }.
+__device__ __forceinline__ int nchild_fast(const Offsets& o, uint64_t C) {
+  uint64_t CJhi, CJlo;
+  mul64(C, (uint64_t)o.J, CJhi, CJlo);
+  long long k = (long long)ceil((double)C * o.inv - o.chi_d);
+  if (k < 0) k = 0;
+  if (k > o.J) k = o.J;
+  while (k > 0 && !below(o, k - 1, CJhi, CJlo)) --k;
+  while (k < o.J && below(o, k, CJhi, CJlo)) ++k;
+  return (int)k;
+}
+
+// Parent (tile-local index) of child k: the last l in [0, n) with st[l] <= k.
+__device__ __forceinline__ int find_parent(const int* st, int n, int k) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (st[mid] <= k) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // ============================================================================
 // STREAM path
 // ============================================================================
@@ -120,29 +206,38 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
   __shared__ typename M::Consts c;
   __shared__ unsigned int smk[2 * (TPB / 32)];
   __shared__ double sd[TPB / 32];
+  constexpr int DX = M::MAXDX;
   const int f = blockIdx.y;
   const int u = filter_unit(a, f);
   if (threadIdx.x == 0) M::prepare(c, a.theta + (size_t)f * a.model.n_params, a.model, (a.flags & PPF_F_EST) != 0);
   __syncthreads();
-  const int dx = a.model.dx;
-  float* X = a.X[0] + (size_t)f * dx * a.J;
+  float* X = a.X[0] + (size_t)f * DX * a.J;
   float* W = a.W[0] + (size_t)f * a.J;
   unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
-  double px[M::MAXDX];
-  for (int d = 0; d < M::MAXDX; ++d) px[d] = 0.0;
+  double px[DX];
+#pragma unroll
+  for (int d = 0; d < DX; ++d) px[d] = 0.0;
   const int j0 = blockIdx.x * a.tile;
   const int j1 = min(j0 + a.tile, a.J);
-  for (int j = j0 + threadIdx.x; j < j1; j += TPB) {
-    float z[M::MAXDX > 0 ? M::MAXDX : 1];
-    float x[M::MAXDX];
-    step_noise<M>(a, f, j, 0, M::n_init(c), z);
-    M::rinit(c, z, x);
-    const float m = propagate<M>(a, c, f, u, j, 0, x);
-    const float w = (a.mode == MODE_MOP ? 0.0f : a.base_init) + m;
-    for (int d = 0; d < dx; ++d) { X[(size_t)d * a.J + j] = x[d]; px[d] += (double)x[d]; }
-    W[j] = w;
-    if (a.logw) a.logw[((size_t)f * a.T) * a.J + j] = w;
-    accum_maxmin(w, mx, mn, nn);
+  const float base = (a.mode == MODE_MOP ? 0.0f : a.base_init);
+  for (int k0 = j0 + 4 * threadIdx.x; k0 < j1; k0 += 4 * TPB) {
+    float z0[4 * (M::NZ0 > 0 ? M::NZ0 : 1)];
+    float z[4 * M::NZ];
+    group_noise<M::NZ0>(a, f, 0, k0, z0);
+    group_noise<M::NZ>(a, f, 1, k0, z);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = k0 + e;
+      if (k >= j1) break;
+      float x[DX];
+      M::rinit(c, z0 + e * M::NZ0, x);
+      const float w = base + prop1<M>(a, c, u, 0, x, z + e * M::NZ);
+#pragma unroll
+      for (int d = 0; d < DX; ++d) { X[(size_t)d * a.J + k] = x[d]; px[d] += (double)x[d]; }
+      W[k] = w;
+      if (a.logw) a.logw[((size_t)f * a.T) * a.J + k] = w;
+      accum_maxmin(w, mx, mn, nn);
+    }
   }
   block_maxmin_u32<TPB>(mx, mn, smk);
   nn = __syncthreads_or(nn);
@@ -154,7 +249,8 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
     if (blockIdx.x == 0) a.loglik[f] = 0.0;
   }
   if (a.flags & PPF_F_PMEAN) {
-    for (int d = 0; d < dx; ++d) {
+#pragma unroll
+    for (int d = 0; d < DX; ++d) {
       const double s = block_sum_f64<TPB>(px[d], sd);
       if (threadIdx.x == 0) atomicAdd(&acc->px[d], s);
     }
@@ -166,10 +262,10 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
 template <class M, int TPB, int IT>
 __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
   constexpr int TILE = TPB * IT;
+  constexpr int DX = M::MAXDX;
   __shared__ int s_v;
   __shared__ uint64_t s_scan[TPB / 32 + 1];
   __shared__ double sd[TPB / 32];
-  __shared__ uint64_t s_excl;
   if (threadIdx.x == 0) s_v = atomicAdd(a.counter + (t & 1), 1);
   __syncthreads();
   const int v = s_v;
@@ -196,13 +292,21 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
   uint64_t qs = 0;
   double s2 = 0.0;
   float wv[IT];
+  // float4 loads only when every filter's row starts 16-byte aligned (J % 4 == 0)
+  if (jb + IT <= a.J && (IT % 4) == 0 && (a.J & 3) == 0) {
 #pragma unroll
-  for (int i = 0; i < IT; ++i) wv[i] = (jb + i < a.J) ? W[jb + i] : -INFINITY;
+    for (int i = 0; i < IT; i += 4) {
+      const float4 v4 = *reinterpret_cast<const float4*>(W + jb + i);
+      wv[i] = v4.x; wv[i + 1] = v4.y; wv[i + 2] = v4.z; wv[i + 3] = v4.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < IT; ++i) wv[i] = (jb + i < a.J) ? W[jb + i] : -INFINITY;
+  }
 #pragma unroll
   for (int i = 0; i < IT; ++i) {
     if (jb + i < a.J) {
-      const uint64_t q = qweight(wv[i], Mx, collapsed);
-      qs += q;
+      qs += qweight(wv[i], Mx, collapsed);
       if (a.flags & PPF_F_ESS) {
         const double e = collapsed ? 1.0 : (double)pp_expf(wv[i] - Mx);
         s2 += e * e;
@@ -243,7 +347,6 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
       if (lane == 0) st_release_u64(desc + b, kStatusIncl | (excl + btot));
     }
     if (lane == 0) {
-      s_excl = excl;
       a.excl[(size_t)f * a.ntiles + b] = excl;
       if (b == a.ntiles - 1) a.tot[f] = excl + btot;
     }
@@ -253,8 +356,9 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
     if (threadIdx.x == 0) atomicAdd(&a.acc[p][f].s2, s);
   }
   if (a.flags & PPF_F_FMEAN) {
-    const float* X = a.X[p] + (size_t)f * a.model.dx * a.J;
-    for (int d = 0; d < a.model.dx; ++d) {
+    const float* X = a.X[p] + (size_t)f * DX * a.J;
+#pragma unroll
+    for (int d = 0; d < DX; ++d) {
       double s = 0.0;
 #pragma unroll
       for (int i = 0; i < IT; ++i)
@@ -270,19 +374,24 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
 
 // Resample the parents of one tile and propagate their children to the next
 // observation (rproc + dmeas fused), writing the next step's X, W.
+//   1. fixed-point weights of the tile's parents, block scan, plus the tile's
+//      exclusive prefix from k_sum: the exact CDF C_l of every parent;
+//   2. closed-form first-child offset st[l] = nchild(C_{l-1}) per parent into
+//      shared memory, parent states staged in shared memory;
+//   3. the tile's children [st[0], st[n]) in groups of 4: binary search of the
+//      first child's parent, gather from shared memory, one Philox call per
+//      4 normals, rproc + dmeas, coalesced stores.
 template <class M, int TPB, int IT>
-__global__ void __launch_bounds__(TPB) k_resprop(Args a, int t) {
+__global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
   constexpr int TILE = TPB * IT;
-  constexpr int CH = TILE;
+  constexpr int DX = M::MAXDX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float* xs = reinterpret_cast<float*>(smem_raw);                       // [dx][TILE]
-  int* mk = reinterpret_cast<int*>(smem_raw + sizeof(float) * M::MAXDX * TILE);  // [CH]
+  float* xs = reinterpret_cast<float*>(smem_raw);                              // [DX][TILE]
+  int* st = reinterpret_cast<int*>(smem_raw + sizeof(float) * DX * TILE);      // [TILE + 1]
   __shared__ typename M::Consts c;
   __shared__ uint64_t s_scan[TPB / 32 + 1];
-  __shared__ int s_mx[TPB / 32 + 1];
   __shared__ unsigned int smk[2 * (TPB / 32)];
   __shared__ double sd[TPB / 32];
-  __shared__ int s_klo, s_khi;
 
   const int f = blockIdx.y, b = blockIdx.x;
   const int u = filter_unit(a, f);
@@ -298,21 +407,23 @@ __global__ void __launch_bounds__(TPB) k_resprop(Args a, int t) {
   const Acc acc = a.acc[p][f];
   const uint64_t tot = a.tot[f];
   if (b == 0 && threadIdx.x == 0) finalize_step(a, f, t, acc, tot, a.loglik + f);
-  if (t == Tf - 1 && !(a.flags & PPF_F_SAVE_ANC)) return;
+  const bool last = (t == Tf - 1);
+  if (last && !a.anc) return;
   if (threadIdx.x == 0) M::prepare(c, a.theta + (size_t)f * a.model.n_params, a.model, (a.flags & PPF_F_EST) != 0);
   const bool nanf = acc.nan != 0;
   const float Mx = keyf(acc.maxkey);
   const bool collapsed = !nanf && Mx == -INFINITY;
   const bool rs = decide_resample(a, acc);
-  const int dx = a.model.dx;
-  const float* Xc = a.X[p] + (size_t)f * dx * a.J;
+  const float* Xc = a.X[p] + (size_t)f * DX * a.J;
   const float* Wc = a.W[p] + (size_t)f * a.J;
-  float* Xn = a.X[p ^ 1] + (size_t)f * dx * a.J;
+  float* Xn = a.X[p ^ 1] + (size_t)f * DX * a.J;
   float* Wn = a.W[p ^ 1] + (size_t)f * a.J;
-  const bool last = (t == Tf - 1);
+  int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * a.J : nullptr;
+  float* logw = a.logw ? a.logw + ((size_t)f * a.T + t + 1) * a.J : nullptr;
   unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
-  double px[M::MAXDX];
-  for (int d = 0; d < M::MAXDX; ++d) px[d] = 0.0;
+  double px[DX];
+#pragma unroll
+  for (int d = 0; d < DX; ++d) px[d] = 0.0;
   const float base = (a.mode == MODE_MOP) ? 0.0f : a.base_rs;
   const int jt = b * TILE;
   const int ntile = min(TILE, a.J - jt);
@@ -323,94 +434,98 @@ __global__ void __launch_bounds__(TPB) k_resprop(Args a, int t) {
     float lt32 = 0.0f;
     if (nanf) lt32 = __int_as_float(0x7fc00000);
     else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
-    for (int l = threadIdx.x; l < ntile; l += TPB) {
-      const int j = jt + l;
-      if (a.anc) a.anc[((size_t)f * a.T + t) * a.J + j] = j;
-      if (last) continue;
-      float x[M::MAXDX];
-      for (int d = 0; d < dx; ++d) x[d] = Xc[(size_t)d * a.J + j];
-      const float nw = collapsed ? -pp_logf((float)a.J) : Wc[j] - lt32;
-      const float m = propagate<M>(a, c, f, u, j, t + 1, x);
-      const float w = nw + m;
-      for (int d = 0; d < dx; ++d) { Xn[(size_t)d * a.J + j] = x[d]; px[d] += (double)x[d]; }
-      Wn[j] = w;
-      if (a.logw) a.logw[((size_t)f * a.T + t + 1) * a.J + j] = w;
-      accum_maxmin(w, mx, mn, nn);
+    const float nwc = -pp_logf((float)a.J);
+    for (int k0 = jt + 4 * threadIdx.x; k0 < jt + ntile; k0 += 4 * TPB) {
+      float z[4 * M::NZ];
+      if (!last) group_noise<M::NZ>(a, f, t + 2, k0, z);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int k = k0 + e;
+        if (k >= jt + ntile) break;
+        if (anc) anc[k] = k;
+        if (last) continue;
+        float x[DX];
+#pragma unroll
+        for (int d = 0; d < DX; ++d) x[d] = Xc[(size_t)d * a.J + k];
+        const float nw = collapsed ? nwc : Wc[k] - lt32;
+        const float w = nw + prop1<M>(a, c, u, t + 1, x, z + e * M::NZ);
+#pragma unroll
+        for (int d = 0; d < DX; ++d) { Xn[(size_t)d * a.J + k] = x[d]; px[d] += (double)x[d]; }
+        Wn[k] = w;
+        if (logw) logw[k] = w;
+        accum_maxmin(w, mx, mn, nn);
+      }
     }
   } else {
-    const uint32_t u32 = resample_u32(a, f, t);
+    const Offsets o = make_offsets(tot, resample_u32(a, f, t), a.J);
     const uint64_t E = a.excl[(size_t)f * a.ntiles + b];
-    // 1. fixed-point weights and their tile-local exclusive scan
+    // 1. fixed-point weights of this thread's parents and the tile scan
     const int l0 = threadIdx.x * IT;
     uint64_t q[IT];
     uint64_t qs = 0;
+    {
+      float wv[IT];
+      if (l0 + IT <= ntile && (a.J & 3) == 0) {
 #pragma unroll
-    for (int i = 0; i < IT; ++i) {
-      q[i] = (l0 + i < ntile) ? qweight(Wc[jt + l0 + i], Mx, collapsed) : 0ull;
-      qs += q[i];
+        for (int i = 0; i < IT; i += 4) {
+          const float4 v4 = *reinterpret_cast<const float4*>(Wc + jt + l0 + i);
+          wv[i] = v4.x; wv[i + 1] = v4.y; wv[i + 2] = v4.z; wv[i + 3] = v4.w;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < IT; ++i) wv[i] = (l0 + i < ntile) ? Wc[jt + l0 + i] : 0.0f;
+      }
+#pragma unroll
+      for (int i = 0; i < IT; ++i) {
+        q[i] = (l0 + i < ntile) ? qweight(wv[i], Mx, collapsed) : 0ull;
+        qs += q[i];
+      }
     }
     uint64_t btot;
     const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
-    // 2. closed-form first-child offsets of each parent; stage parent states
-    int st[IT], en[IT];
+    // 2. first-child offsets and staged parent states
     {
       uint64_t C = E + tex;
-      int prev = nchild(C, tot, u32, a.J);
-      if (threadIdx.x == 0) s_klo = prev;
 #pragma unroll
       for (int i = 0; i < IT; ++i) {
+        if (l0 + i < ntile) st[l0 + i] = nchild_fast(o, C);
         C += q[i];
-        const int e = (l0 + i < ntile) ? nchild(C, tot, u32, a.J) : prev;
-        st[i] = prev; en[i] = e; prev = e;
       }
-      if (l0 < ntile && l0 + IT >= ntile) s_khi = prev;
-      if (ntile <= 0 && threadIdx.x == 0) s_khi = s_klo;
+      if (l0 < ntile && l0 + IT >= ntile) st[ntile] = nchild_fast(o, E + btot);
     }
     for (int l = threadIdx.x; l < ntile; l += TPB)
-      for (int d = 0; d < dx; ++d) xs[d * TILE + l] = Xc[(size_t)d * a.J + jt + l];
+#pragma unroll
+      for (int d = 0; d < DX; ++d) xs[d * TILE + l] = Xc[(size_t)d * a.J + jt + l];
     __syncthreads();
-    const int klo = s_klo, khi = s_khi;
-    // 3. expand children window by window: mark each parent's first child,
-    //    max-scan the marks, then process the children in order.
-    int carry = -1;
-    for (int w0 = klo; w0 < khi; w0 += CH) {
-      const int wn = min(CH, khi - w0);
-      for (int i = threadIdx.x; i < CH; i += TPB) mk[i] = -1;
-      __syncthreads();
+    const int klo = st[0], khi = st[ntile];
+    // 3. children in groups of 4
+    const int kA = klo & ~3;
+    for (int k0 = kA + 4 * threadIdx.x; k0 < khi; k0 += 4 * TPB) {
+      float z[4 * M::NZ];
+      if (!last) group_noise<M::NZ>(a, f, t + 2, k0, z);
+      int l = find_parent(st, ntile, max(k0, klo));
 #pragma unroll
-      for (int i = 0; i < IT; ++i)
-        if (en[i] > st[i] && st[i] >= w0 && st[i] < w0 + CH) mk[st[i] - w0] = l0 + i;
-      __syncthreads();
-      {
-        constexpr int PER = CH / TPB;
-        int loc[PER];
-        int run = -1;
-#pragma unroll
-        for (int i = 0; i < PER; ++i) { run = max(run, mk[threadIdx.x * PER + i]); loc[i] = run; }
-        int tmax;
-        const int ex = block_excl_max_i32<TPB>(run, s_mx, tmax);
-        const int base_c = max(ex, carry);
-#pragma unroll
-        for (int i = 0; i < PER; ++i) mk[threadIdx.x * PER + i] = max(base_c, loc[i]);
-        carry = max(carry, tmax);
-      }
-      __syncthreads();
-      for (int i = threadIdx.x; i < wn; i += TPB) {
-        const int l = mk[i];
-        const int k = w0 + i;
-        if (l < 0 || l >= ntile) { atomicOr(a.err, 2u); continue; }  // defensive: never index out of the tile
-        if (a.anc) a.anc[((size_t)f * a.T + t) * a.J + k] = jt + l;
+      for (int e = 0; e < 4; ++e) {
+        const int k = k0 + e;
+        if (k < klo) continue;
+        if (k >= khi) break;
+        int adv = 0;
+        while (l + 1 < ntile && st[l + 1] <= k) {
+          ++l;
+          if (++adv > 8) { l = find_parent(st, ntile, k); break; }
+        }
+        if (anc) anc[k] = jt + l;
         if (last) continue;
-        float x[M::MAXDX];
-        for (int d = 0; d < dx; ++d) x[d] = xs[d * TILE + l];
-        const float m = propagate<M>(a, c, f, u, k, t + 1, x);
-        const float w = base + m;
-        for (int d = 0; d < dx; ++d) { Xn[(size_t)d * a.J + k] = x[d]; px[d] += (double)x[d]; }
+        float x[DX];
+#pragma unroll
+        for (int d = 0; d < DX; ++d) x[d] = xs[d * TILE + l];
+        const float w = base + prop1<M>(a, c, u, t + 1, x, z + e * M::NZ);
+#pragma unroll
+        for (int d = 0; d < DX; ++d) { Xn[(size_t)d * a.J + k] = x[d]; px[d] += (double)x[d]; }
         Wn[k] = w;
-        if (a.logw) a.logw[((size_t)f * a.T + t + 1) * a.J + k] = w;
+        if (logw) logw[k] = w;
         accum_maxmin(w, mx, mn, nn);
       }
-      __syncthreads();
     }
   }
   if (last) return;
@@ -423,7 +538,8 @@ __global__ void __launch_bounds__(TPB) k_resprop(Args a, int t) {
     if (nn) atomicOr(&an->nan, 1u);
   }
   if (a.flags & PPF_F_PMEAN) {
-    for (int d = 0; d < dx; ++d) {
+#pragma unroll
+    for (int d = 0; d < DX; ++d) {
       const double s = block_sum_f64<TPB>(px[d], sd);
       if (threadIdx.x == 0) atomicAdd(&an->px[d], s);
     }
@@ -432,24 +548,22 @@ __global__ void __launch_bounds__(TPB) k_resprop(Args a, int t) {
 
 // ============================================================================
 // RESIDENT path: one CTA per filter, the whole time loop in one launch.
-// Shared memory: xs[dx][J] float, ws[J] float, mk[J] int.
+// Shared memory: xs[DX][J] float, ws[J] float, st[J+1] int.
 // ============================================================================
 
-template <class M, int TPB, int MAXIT>
+template <class M, int TPB, int MAXG>
 __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int DX = M::MAXDX;
   const int J = a.J;
-  const int dx = a.model.dx;
   float* xs = reinterpret_cast<float*>(smem_raw);
-  float* ws = xs + (size_t)dx * J;
-  int* mk = reinterpret_cast<int*>(ws + J);
+  float* ws = xs + (size_t)DX * J;
+  int* st = reinterpret_cast<int*>(ws + J);
   __shared__ typename M::Consts c;
   __shared__ uint64_t s_scan[TPB / 32 + 1];
-  __shared__ int s_mx[TPB / 32 + 1];
   __shared__ unsigned int smk[2 * (TPB / 32)];
   __shared__ double sd[TPB / 32];
   __shared__ Acc s_acc;
-  __shared__ uint64_t s_tot;
   __shared__ double s_ll;
 
   const int f = blockIdx.x;
@@ -460,28 +574,36 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     s_ll = 0.0;
   }
   __syncthreads();
-  // blocked ownership for the scan: thread owns [l0, l0+per)
+  // blocked ownership for the scan: thread owns [l0, l1)
   const int per = (J + TPB - 1) / TPB;
   const int l0 = min(J, threadIdx.x * per);
   const int l1 = min(J, l0 + per);
 
-  // step 0: rinit + rproc + dmeas for every particle
-  for (int j = threadIdx.x; j < J; j += TPB) {
-    float z[M::MAXDX > 0 ? M::MAXDX : 1];
-    float x[M::MAXDX];
-    step_noise<M>(a, f, j, 0, M::n_init(c), z);
-    M::rinit(c, z, x);
-    const float m = propagate<M>(a, c, f, u, j, 0, x);
-    const float w = (a.mode == MODE_MOP ? 0.0f : a.base_init) + m;
-    for (int d = 0; d < dx; ++d) xs[d * J + j] = x[d];
-    ws[j] = w;
-    if (a.logw) a.logw[((size_t)f * a.T) * J + j] = w;
+  // step 0: rinit + rproc + dmeas, groups of 4
+  for (int g = threadIdx.x; 4 * g < J; g += TPB) {
+    const int k0 = 4 * g;
+    float z0[4 * (M::NZ0 > 0 ? M::NZ0 : 1)];
+    float z[4 * M::NZ];
+    group_noise<M::NZ0>(a, f, 0, k0, z0);
+    group_noise<M::NZ>(a, f, 1, k0, z);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = k0 + e;
+      if (k >= J) break;
+      float x[DX];
+      M::rinit(c, z0 + e * M::NZ0, x);
+      const float w = (a.mode == MODE_MOP ? 0.0f : a.base_init) + prop1<M>(a, c, u, 0, x, z + e * M::NZ);
+#pragma unroll
+      for (int d = 0; d < DX; ++d) xs[d * J + k] = x[d];
+      ws[k] = w;
+      if (a.logw) a.logw[((size_t)f * a.T) * J + k] = w;
+    }
   }
   __syncthreads();
   const float base = (a.mode == MODE_MOP) ? 0.0f : a.base_rs;
 
   for (int t = 0; t < Tf; ++t) {
-    // (a) max / min / nan and prediction-mean sums
+    // (a) max / min / nan
     unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
     for (int j = l0; j < l1; ++j) accum_maxmin(ws[j], mx, mn, nn);
     block_maxmin_u32<TPB>(mx, mn, smk);
@@ -494,30 +616,29 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     const bool nanf = s_acc.nan != 0;
     const float Mx = keyf(s_acc.maxkey);
     const bool collapsed = !nanf && Mx == -INFINITY;
-    const bool qcollapsed = nanf || Mx == -INFINITY;
+    const bool qc = nanf || Mx == -INFINITY;
     // (b) fixed-point weights, scan, total
     uint64_t qs = 0;
-    double s2 = 0.0;
-    for (int j = l0; j < l1; ++j) {
-      qs += qweight(ws[j], Mx, qcollapsed);
-      if (a.flags & (PPF_F_ESS)) {
-        const double e = qcollapsed ? 1.0 : (double)pp_expf(ws[j] - Mx);
-        s2 += e * e;
-      }
-    }
+    for (int j = l0; j < l1; ++j) qs += qweight(ws[j], Mx, qc);
     uint64_t tot;
     const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, tot);
     if (a.flags & PPF_F_ESS) {
+      double s2 = 0.0;
+      for (int j = l0; j < l1; ++j) {
+        const double e = qc ? 1.0 : (double)pp_expf(ws[j] - Mx);
+        s2 += e * e;
+      }
       const double s = block_sum_f64<TPB>(s2, sd);
       if (threadIdx.x == 0) s_acc.s2 = s;
     }
     if (a.flags & (PPF_F_FMEAN | PPF_F_PMEAN)) {
-      for (int d = 0; d < dx; ++d) {
+#pragma unroll
+      for (int d = 0; d < DX; ++d) {
         double sf = 0.0, sp = 0.0;
         for (int j = l0; j < l1; ++j) {
           const double xv = (double)xs[d * J + j];
           sp += xv;
-          sf += xv * (qcollapsed ? 1.0 : (double)pp_expf(ws[j] - Mx));
+          sf += xv * (qc ? 1.0 : (double)pp_expf(ws[j] - Mx));
         }
         sf = block_sum_f64<TPB>(sf, sd);
         sp = block_sum_f64<TPB>(sp, sd);
@@ -526,86 +647,102 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      s_tot = tot;
       double ll = s_ll;
       finalize_step(a, f, t, s_acc, tot, &ll);
       s_ll = ll;
     }
-    __syncthreads();
     const bool last = (t == Tf - 1);
     if (last && !a.anc) break;
     const bool rs = decide_resample(a, s_acc);
+    int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
+    float* logw = a.logw ? a.logw + ((size_t)f * a.T + t + 1) * J : nullptr;
     if (!rs) {
       float lt32 = 0.0f;
       if (nanf) lt32 = __int_as_float(0x7fc00000);
       else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
-      if (a.anc)
-        for (int j = threadIdx.x; j < J; j += TPB) a.anc[((size_t)f * a.T + t) * J + j] = j;
-      if (last) break;
-      for (int j = threadIdx.x; j < J; j += TPB) {
-        float x[M::MAXDX];
-        for (int d = 0; d < dx; ++d) x[d] = xs[d * J + j];
-        const float nw = collapsed ? -pp_logf((float)J) : ws[j] - lt32;
-        const float m = propagate<M>(a, c, f, u, j, t + 1, x);
-        const float w = nw + m;
-        for (int d = 0; d < dx; ++d) xs[d * J + j] = x[d];
-        ws[j] = w;
-        if (a.logw) a.logw[((size_t)f * a.T + t + 1) * J + j] = w;
+      const float nwc = -pp_logf((float)J);
+      __syncthreads();
+      for (int g = threadIdx.x; 4 * g < J; g += TPB) {
+        const int k0 = 4 * g;
+        float z[4 * M::NZ];
+        if (!last) group_noise<M::NZ>(a, f, t + 2, k0, z);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int k = k0 + e;
+          if (k >= J) break;
+          if (anc) anc[k] = k;
+          if (last) continue;
+          float x[DX];
+#pragma unroll
+          for (int d = 0; d < DX; ++d) x[d] = xs[d * J + k];
+          const float nw = collapsed ? nwc : ws[k] - lt32;
+          const float w = nw + prop1<M>(a, c, u, t + 1, x, z + e * M::NZ);
+#pragma unroll
+          for (int d = 0; d < DX; ++d) xs[d * J + k] = x[d];
+          ws[k] = w;
+          if (logw) logw[k] = w;
+        }
       }
       __syncthreads();
+      if (last) break;
       continue;
     }
-    // (c) offsets and marks
-    const uint32_t u32 = resample_u32(a, f, t);
-    for (int j = threadIdx.x; j < J; j += TPB) mk[j] = -1;
-    __syncthreads();
+    // (c) first-child offsets of every parent
+    const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
     {
       uint64_t C = tex;
-      int prev = nchild(C, tot, u32, J);
       for (int j = l0; j < l1; ++j) {
-        C += qweight(ws[j], Mx, qcollapsed);
-        const int e = nchild(C, tot, u32, J);
-        if (e > prev) mk[prev] = j;
-        prev = e;
+        st[j] = nchild_fast(o, C);
+        C += qweight(ws[j], Mx, qc);
+      }
+      if (threadIdx.x == TPB - 1) st[J] = J;
+    }
+    __syncthreads();
+    // (d) children: parent from shared memory, propagate, keep in registers
+    float nx[MAXG][4][DX];
+    float nw[MAXG][4];
+#pragma unroll
+    for (int gi = 0; gi < MAXG; ++gi) {
+      const int k0 = 4 * (threadIdx.x + gi * TPB);
+      if (k0 < J) {
+        float z[4 * M::NZ];
+        if (!last) group_noise<M::NZ>(a, f, t + 2, k0, z);
+        int l = find_parent(st, J, k0);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int k = k0 + e;
+          if (k >= J) break;
+          int adv = 0;
+          while (l + 1 < J && st[l + 1] <= k) {
+            ++l;
+            if (++adv > 8) { l = find_parent(st, J, k); break; }
+          }
+          if (anc) anc[k] = l;
+          if (last) continue;
+          float x[DX];
+#pragma unroll
+          for (int d = 0; d < DX; ++d) x[d] = xs[d * J + l];
+          nw[gi][e] = base + prop1<M>(a, c, u, t + 1, x, z + e * M::NZ);
+#pragma unroll
+          for (int d = 0; d < DX; ++d) nx[gi][e][d] = x[d];
+        }
       }
     }
     __syncthreads();
-    {
-      int run = -1;
-      for (int j = l0; j < l1; ++j) { run = max(run, mk[j]); mk[j] = run; }
-      int tmax;
-      const int ex = block_excl_max_i32<TPB>(run, s_mx, tmax);
-      for (int j = l0; j < l1; ++j) mk[j] = max(mk[j], ex);
-    }
-    __syncthreads();
-    if (a.anc)
-      for (int k = threadIdx.x; k < J; k += TPB) a.anc[((size_t)f * a.T + t) * J + k] = mk[k];
     if (last) break;
-    // (d) children: gather parent from shared memory, propagate, then store
-    float nx[MAXIT][M::MAXDX];
-    float nw[MAXIT];
 #pragma unroll
-    for (int it = 0; it < MAXIT; ++it) {
-      const int k = threadIdx.x + it * TPB;
-      if (k < J) {
-        float x[M::MAXDX];
-        int l = mk[k];
-        if (l < 0 || l >= J) { atomicOr(a.err, 2u); l = 0; }  // defensive: never index outside the swarm
-        for (int d = 0; d < dx; ++d) x[d] = xs[d * J + l];
-        const float m = propagate<M>(a, c, f, u, k, t + 1, x);
+    for (int gi = 0; gi < MAXG; ++gi) {
+      const int k0 = 4 * (threadIdx.x + gi * TPB);
+      if (k0 < J) {
 #pragma unroll
-        for (int d = 0; d < M::MAXDX; ++d) nx[it][d] = x[d];
-        nw[it] = base + m;
-      }
-    }
-    __syncthreads();
+        for (int e = 0; e < 4; ++e) {
+          const int k = k0 + e;
+          if (k >= J) break;
 #pragma unroll
-    for (int it = 0; it < MAXIT; ++it) {
-      const int k = threadIdx.x + it * TPB;
-      if (k < J) {
-        for (int d = 0; d < dx; ++d) xs[d * J + k] = nx[it][d];
-        ws[k] = nw[it];
-        if (a.logw) a.logw[((size_t)f * a.T + t + 1) * J + k] = nw[it];
+          for (int d = 0; d < DX; ++d) xs[d * J + k] = nx[gi][e][d];
+          ws[k] = nw[gi][e];
+          if (logw) logw[k] = nw[gi][e];
+        }
       }
     }
     __syncthreads();
@@ -643,8 +780,8 @@ __global__ void __launch_bounds__(TPB) kp_prop(Args a, int f, int t) {
     float x[M::MAXDX];
     float w0;
     if (t == 0) {
-      float z[M::MAXDX > 0 ? M::MAXDX : 1];
-      step_noise<M>(a, f, j, 0, M::n_init(c), z);
+      float z[M::NZ0 > 0 ? M::NZ0 : 1];
+      step_noise<M>(a, f, j, 0, M::NZ0, z);
       M::rinit(c, z, x);
       w0 = (a.mode == MODE_MOP ? 0.0f : a.base_init);
     } else {
@@ -798,12 +935,10 @@ int run_stream(Args& a, cudaStream_t s) {
   constexpr int TPB = 256, IT = 8, TILE = TPB * IT;
   a.tile = TILE;
   a.ntiles = (a.J + TILE - 1) / TILE;
-  const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * TILE;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_resprop<M, TPB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set = true;
-  }
+  const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4);
+  if (cudaFuncSetAttribute(k_resprop<M, TPB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return PPF_ECUDA;
   dim3 grid(a.ntiles, a.F);
   PROF_BEGIN(KIND_INIT);
   k_init<M, TPB><<<grid, TPB, 0, s>>>(a);
@@ -821,15 +956,17 @@ int run_stream(Args& a, cudaStream_t s) {
 
 template <class M>
 size_t resident_smem(const Args& a) {
-  return (size_t)a.J * sizeof(float) * (a.model.dx + 1) + (size_t)a.J * sizeof(int);
+  return (size_t)a.J * sizeof(float) * (M::MAXDX + 1) + (size_t)(a.J + 4) * sizeof(int);
 }
 
-template <class M, int MAXIT>
+template <class M, int MAXG>
 int launch_resident(Args& a, size_t smem, cudaStream_t s) {
   constexpr int TPB = 512;
-  cudaFuncSetAttribute(k_resident<M, TPB, MAXIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaFuncSetAttribute(k_resident<M, TPB, MAXG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return PPF_ECUDA;
   PROF_BEGIN(KIND_RESIDENT);
-  k_resident<M, TPB, MAXIT><<<a.F, TPB, smem, s>>>(a);
+  k_resident<M, TPB, MAXG><<<a.F, TPB, smem, s>>>(a);
   PROF_END(KIND_RESIDENT);
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
@@ -838,11 +975,12 @@ template <class M>
 int run_resident(Args& a, cudaStream_t s) {
   constexpr int TPB = 512;
   const size_t smem = resident_smem<M>(a);
-  const int per = (a.J + TPB - 1) / TPB;
-  if (smem > kResidentSmemMax || per > 32) return PPF_EUNSUPPORTED;
-  if (per <= 2) return launch_resident<M, 2>(a, smem, s);
-  if (per <= 8) return launch_resident<M, 8>(a, smem, s);
-  return launch_resident<M, 32>(a, smem, s);
+  const int groups = (a.J + 4 * TPB - 1) / (4 * TPB);   // groups of 4 children per thread
+  if (smem > kResidentSmemMax || groups > 8) return PPF_EUNSUPPORTED;
+  if (groups <= 1) return launch_resident<M, 1>(a, smem, s);
+  if (groups <= 2) return launch_resident<M, 2>(a, smem, s);
+  if (groups <= 4) return launch_resident<M, 4>(a, smem, s);
+  return launch_resident<M, 8>(a, smem, s);
 }
 
 template <class M>
@@ -885,7 +1023,14 @@ int dispatch_model(Args& a, int path, cudaStream_t s) {
 
 int run_pfilter_path(Args& a, int path, cudaStream_t s) {
   switch (a.model.kind) {
-    case PPF_MODEL_LG: return dispatch_model<LG>(a, path, s);
+    case PPF_MODEL_LG:
+      switch (a.model.dx) {
+        case 1: return dispatch_model<LG<1>>(a, path, s);
+        case 2: return dispatch_model<LG<2>>(a, path, s);
+        case 3: return dispatch_model<LG<3>>(a, path, s);
+        case 4: return dispatch_model<LG<4>>(a, path, s);
+        default: return PPF_EUNSUPPORTED;
+      }
     case PPF_MODEL_SV: return dispatch_model<SV>(a, path, s);
     case PPF_MODEL_RICKER: return dispatch_model<Ricker>(a, path, s);
     default: return PPF_EINVAL;
@@ -893,7 +1038,7 @@ int run_pfilter_path(Args& a, int path, cudaStream_t s) {
 }
 
 size_t resident_smem_bytes(const Args& a) {
-  return (size_t)a.J * sizeof(float) * (a.model.dx + 1) + (size_t)a.J * sizeof(int);
+  return (size_t)a.J * sizeof(float) * (a.model.dx + 1) + (size_t)(a.J + 4) * sizeof(int);
 }
 
 }  // namespace ppf
