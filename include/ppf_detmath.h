@@ -114,6 +114,27 @@ PPF_HD float pp_logf(float x) {
   return pp_fma(ef, 0.693145751953125f, lo);
 }
 
+/* log(x) for x in [2^-24, 1]: pp_logf without the special-case tests (same
+ * arithmetic, so equal results on that domain). */
+PPF_HD float pp_log_unit(float x) {
+  const uint32_t b = pp_f2u(x);
+  int e = (int)((b >> 23) & 0xffu) - 127;
+  float m = pp_u2f((b & 0x007fffffu) | 0x3f800000u);
+  if (m > 1.41421353816986083984375f) { m = m * 0.5f; e += 1; }
+  const float f = m - 1.0f;
+  const float s = f / (2.0f + f);
+  const float z = s * s;
+  float R = 0.2222222238779068f;
+  R = pp_fma(R, z, 0.2857142984867096f);
+  R = pp_fma(R, z, 0.4000000059604645f);
+  R = pp_fma(R, z, 0.6666666865348816f);
+  R = R * z;
+  const float lm = f - s * (f - R);
+  const float ef = (float)e;
+  const float lo = pp_fma(ef, 1.428606765330187045e-06f, lm);
+  return pp_fma(ef, 0.693145751953125f, lo);
+}
+
 /* sin(2 pi u), cos(2 pi u) for u in [0, 1). */
 PPF_HD void pp_sincos2pif(float u, float* sn, float* cs) {
   const float v = u * 4.0f;                 /* exact */

@@ -64,7 +64,7 @@ PPF_HD pp_u32x4 pp_philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t
 PPF_HD void pp_boxmuller(uint32_t wa, uint32_t wb, float* z0, float* z1) {
   const float u1 = (float)((wa >> 8) + 1u) * 5.9604644775390625e-08f;  /* 2^-24 */
   const float u2 = (float)(wb >> 8) * 5.9604644775390625e-08f;
-  const float rr = sqrtf(-2.0f * pp_logf(u1));
+  const float rr = sqrtf(-2.0f * pp_log_unit(u1));
   float s, c;
   pp_sincos2pif(u2, &s, &c);
   *z0 = rr * c;

@@ -41,7 +41,7 @@ typedef unsigned __int128 u128;
 typedef struct {
   int kind, dx, dy;
   float A[16], C[16], LQ[16], L[16], Linv[4], X0[4], c0;          /* LG */
-  float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, svc0; /* SV */
+  float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, svc0, kdt, xsq; /* SV */
   float r, sigma, phi, N0;                                         /* Ricker */
 } consts_t;
 
@@ -107,6 +107,8 @@ static void prepare(consts_t* c, const float* th, const ppf_model* m, int est) {
     c->mudt = c->mu * c->dt;
     c->rhoc = sqrtf(1.0f - c->rho * c->rho);
     c->svc0 = -0.5f * LOG2PI_F - pp_logf(c->rhoc) - 0.5f * pp_logf(c->dt);
+    c->kdt = c->kappa * c->dt;
+    c->xsq = c->xi * c->sqdt;
   } else {
     c->r = est ? pp_expf(th[0]) : th[0];
     c->sigma = est ? pp_expf(th[1]) : th[1];
@@ -121,9 +123,9 @@ static int n_step(const consts_t* c) { return c->kind == PPF_MODEL_LG ? c->dx : 
 static void rinit(const consts_t* c, const float* z, float* x) {
   if (c->kind == PPF_MODEL_LG) {
     for (int i = 0; i < c->dx; ++i) {
-      float s = 0.0f;
-      for (int k = 0; k <= i; ++k) s = s + c->LQ[i * 4 + k] * z[k];
-      x[i] = c->X0[i] + s;
+      float acc = c->X0[i];
+      for (int k = 0; k <= i; ++k) acc = fmaf(c->LQ[i * 4 + k], z[k], acc);
+      x[i] = acc;
     }
   } else if (c->kind == PPF_MODEL_SV) {
     x[0] = c->v0;
@@ -137,26 +139,23 @@ static void rproc(const consts_t* c, float* x, const float* z) {
   if (c->kind == PPF_MODEL_LG) {
     float y[4];
     for (int i = 0; i < c->dx; ++i) {
-      float a = 0.0f;
-      for (int k = 0; k < c->dx; ++k) a = a + c->A[i * 4 + k] * x[k];
-      float s = 0.0f;
-      for (int k = 0; k <= i; ++k) s = s + c->LQ[i * 4 + k] * z[k];
-      y[i] = a + s;
+      float acc = 0.0f;
+      for (int k = 0; k < c->dx; ++k) acc = fmaf(c->A[i * 4 + k], x[k], acc);
+      for (int k = 0; k <= i; ++k) acc = fmaf(c->LQ[i * 4 + k], z[k], acc);
+      y[i] = acc;
     }
     for (int i = 0; i < c->dx; ++i) x[i] = y[i];
   } else if (c->kind == PPF_MODEL_SV) {
     const float v = x[0];
-    const float ev = pp_expf(v);
-    const float emv = pp_expf(-v);
     const float emh = pp_expf(-0.5f * v);
-    const float dr = ((c->kappa * ((c->theta - ev) * emv)) * c->dt);
-    const float df = ((c->xi * emh) * c->sqdt) * z[0];
-    x[0] = (v + dr) + df;
+    const float emv = emh * emh;
+    const float a1 = fmaf(c->theta, emv, -1.0f);
+    const float v1 = fmaf(c->kdt, a1, v);
+    x[0] = fmaf(c->xsq * emh, z[0], v1);
     x[1] = z[0];
   } else {
     const float N = x[0];
-    const float arg = c->sigma * z[0] - N;
-    x[0] = (c->r * N) * pp_expf(arg);
+    x[0] = (c->r * N) * pp_expf(fmaf(c->sigma, z[0], -N));
   }
 }
 
@@ -166,23 +165,23 @@ static float dmeas(const consts_t* c, const float* y, float ycon, const float* x
     float q = 0.0f;
     for (int i = 0; i < c->dy; ++i) {
       float a = 0.0f;
-      for (int k = 0; k < c->dx; ++k) a = a + c->C[i * 4 + k] * x[k];
+      for (int k = 0; k < c->dx; ++k) a = fmaf(c->C[i * 4 + k], x[k], a);
       float r = y[i] - a;
-      for (int l = 0; l < i; ++l) r = r - c->L[i * 4 + l] * s[l];
+      for (int l = 0; l < i; ++l) r = fmaf(-c->L[i * 4 + l], s[l], r);
       s[i] = r * c->Linv[i];
-      q = q + s[i] * s[i];
+      q = fmaf(s[i], s[i], q);
     }
-    return -0.5f * q + c->c0;
+    return fmaf(-0.5f, q, c->c0);
   } else if (c->kind == PPF_MODEL_SV) {
     const float v = x[0];
     const float sd = pp_expf(0.5f * v) * c->sqdt;
-    const float mean = c->mudt + (c->rho * sd) * x[1];
+    const float mean = fmaf(c->rho * sd, x[1], c->mudt);
     const float r = (y[0] - mean) / (c->rhoc * sd);
-    return -0.5f * (r * r) + (c->svc0 - 0.5f * v);
+    return fmaf(-0.5f * r, r, fmaf(-0.5f, v, c->svc0));
   } else {
     const float lam = c->phi * x[0];
     if (y[0] == 0.0f) return -lam;
-    return (y[0] * pp_logf(lam) - lam) - ycon;
+    return fmaf(y[0], pp_logf(lam), -lam) - ycon;
   }
 }
 

@@ -86,10 +86,10 @@ struct LG {
   __device__ static void rinit(const Consts& c, const float* z, float* x) {
 #pragma unroll
     for (int i = 0; i < DX; ++i) {
-      float s = 0.0f;
+      float acc = c.X0[i];
 #pragma unroll
-      for (int k = 0; k <= i; ++k) s = s + c.LQ[i * 4 + k] * z[k];
-      x[i] = c.X0[i] + s;
+      for (int k = 0; k <= i; ++k) acc = pp_fma(c.LQ[i * 4 + k], z[k], acc);
+      x[i] = acc;
     }
   }
 
@@ -97,13 +97,12 @@ struct LG {
     float y[DX];
 #pragma unroll
     for (int i = 0; i < DX; ++i) {
-      float a = 0.0f;
+      float acc = 0.0f;
 #pragma unroll
-      for (int k = 0; k < DX; ++k) a = a + c.A[i * 4 + k] * x[k];
-      float s = 0.0f;
+      for (int k = 0; k < DX; ++k) acc = pp_fma(c.A[i * 4 + k], x[k], acc);
 #pragma unroll
-      for (int k = 0; k <= i; ++k) s = s + c.LQ[i * 4 + k] * z[k];
-      y[i] = a + s;
+      for (int k = 0; k <= i; ++k) acc = pp_fma(c.LQ[i * 4 + k], z[k], acc);
+      y[i] = acc;
     }
 #pragma unroll
     for (int i = 0; i < DX; ++i) x[i] = y[i];
@@ -117,15 +116,15 @@ struct LG {
       if (i < c.dy) {
         float a = 0.0f;
 #pragma unroll
-        for (int k = 0; k < DX; ++k) a = a + c.C[i * 4 + k] * x[k];
+        for (int k = 0; k < DX; ++k) a = pp_fma(c.C[i * 4 + k], x[k], a);
         float r = y[i] - a;
 #pragma unroll
-        for (int l = 0; l < i; ++l) r = r - c.L[i * 4 + l] * s[l];
+        for (int l = 0; l < i; ++l) r = pp_fma(-c.L[i * 4 + l], s[l], r);
         s[i] = r * c.Linv[i];
-        q = q + s[i] * s[i];
+        q = pp_fma(s[i], s[i], q);
       }
     }
-    return -0.5f * q + c.c0;
+    return pp_fma(-0.5f, q, c.c0);
   }
 };
 
@@ -150,7 +149,7 @@ struct SV {
   static constexpr int MAXP = 6;
   struct Consts {
     int dx, dy;
-    float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, c0;
+    float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, c0, kdt, xsq;
   };
 
   __device__ static void prepare(Consts& c, const float* th, const ppf_model& m, bool est) {
@@ -166,27 +165,29 @@ struct SV {
     c.mudt = c.mu * c.dt;
     c.rhoc = sqrtf(1.0f - c.rho * c.rho);
     c.c0 = -0.5f * PPF_LOG2PI_F - pp_logf(c.rhoc) - 0.5f * pp_logf(c.dt);
+    c.kdt = c.kappa * c.dt;
+    c.xsq = c.xi * c.sqdt;
   }
   __device__ static void rinit(const Consts& c, const float*, float* x) {
     x[0] = c.v0;
     x[1] = 0.0f;
   }
+  // (theta - e^v) e^-v = theta e^-v - 1;  e^-v = (e^{-v/2})^2
   __device__ static void rproc(const Consts& c, float* x, const float* z) {
     const float v = x[0];
-    const float ev = pp_expf(v);
-    const float emv = pp_expf(-v);
     const float emh = pp_expf(-0.5f * v);
-    const float dr = ((c.kappa * ((c.theta - ev) * emv)) * c.dt);
-    const float df = ((c.xi * emh) * c.sqdt) * z[0];
-    x[0] = (v + dr) + df;
+    const float emv = emh * emh;
+    const float a1 = pp_fma(c.theta, emv, -1.0f);
+    const float v1 = pp_fma(c.kdt, a1, v);
+    x[0] = pp_fma(c.xsq * emh, z[0], v1);
     x[1] = z[0];
   }
   __device__ static float dmeas(const Consts& c, const float* y, float, const float* x) {
     const float v = x[0];
     const float sd = pp_expf(0.5f * v) * c.sqdt;
-    const float mean = c.mudt + (c.rho * sd) * x[1];
+    const float mean = pp_fma(c.rho * sd, x[1], c.mudt);
     const float r = (y[0] - mean) / (c.rhoc * sd);
-    return -0.5f * (r * r) + (c.c0 - 0.5f * v);
+    return pp_fma(-0.5f * r, r, pp_fma(-0.5f, v, c.c0));
   }
 };
 
@@ -216,13 +217,12 @@ struct Ricker {
   __device__ static void rinit(const Consts& c, const float*, float* x) { x[0] = c.N0; }
   __device__ static void rproc(const Consts& c, float* x, const float* z) {
     const float N = x[0];
-    const float arg = c.sigma * z[0] - N;
-    x[0] = (c.r * N) * pp_expf(arg);
+    x[0] = (c.r * N) * pp_expf(pp_fma(c.sigma, z[0], -N));
   }
   __device__ static float dmeas(const Consts& c, const float* y, float ycon, const float* x) {
     const float lam = c.phi * x[0];
     if (y[0] == 0.0f) return -lam;
-    return (y[0] * pp_logf(lam) - lam) - ycon;
+    return pp_fma(y[0], pp_logf(lam), -lam) - ycon;
   }
 };
 

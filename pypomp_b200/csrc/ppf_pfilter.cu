@@ -79,14 +79,34 @@ __device__ __forceinline__ uint32_t resample_u32(const Args& a, int f, int t) {
   return pp_resample_u32(a.seeds[f], (uint32_t)(t + 1));
 }
 
+// Observation t of series u into registers.
+template <class M>
+struct Obs {
+  float y[M::MAXDY];
+  float yc;
+  __device__ __forceinline__ void load(const Args& a, int u, int t) {
+    const float* p = a.ys + ((size_t)u * a.T + t) * a.model.dy;
+#pragma unroll
+    for (int i = 0; i < M::MAXDY; ++i) y[i] = (i < a.model.dy) ? p[i] : 0.0f;
+    yc = a.ycon ? a.ycon[(size_t)u * a.T + t] : 0.0f;
+  }
+};
+
+// rproc with the given normals, then dmeas at the loaded observation.
+template <class M>
+__device__ __forceinline__ float step1(const typename M::Consts& c, const Obs<M>& ob, float* x,
+                                       const float* z) {
+  M::rproc(c, x, z);
+  return M::dmeas(c, ob.y, ob.yc, x);
+}
+
 // rproc with the given normals, then dmeas at observation t.
 template <class M>
 __device__ __forceinline__ float prop1(const Args& a, const typename M::Consts& c, int u, int t,
                                        float* x, const float* z) {
-  M::rproc(c, x, z);
-  const float* y = a.ys + ((size_t)u * a.T + t) * a.model.dy;
-  const float yc = a.ycon ? a.ycon[(size_t)u * a.T + t] : 0.0f;
-  return M::dmeas(c, y, yc, x);
+  Obs<M> ob;
+  ob.load(a, u, t);
+  return step1<M>(c, ob, x, z);
 }
 
 // Single-particle propagate into observation t (plain path).
@@ -165,24 +185,33 @@ __device__ __forceinline__ void mul64(uint64_t a, uint64_t b, uint64_t& hi, uint
   hi = __umul64hi(a, b);
 }
 
-// k tot + chi < C J ?
-__device__ __forceinline__ bool below(const Offsets& o, long long k, uint64_t CJhi, uint64_t CJlo) {
-  uint64_t h, l;
-  mul64((uint64_t)k, o.tot, h, l);
-  l += o.chi;
-  h += (l < o.chi);
-  return (h < CJhi) || (h == CJhi && l < CJlo);
-}
-
-// nchild(C) = #{ k in [0,J) : k tot + chi < C J }.
+// nchild(C) = #{ k in [0,J) : k tot + chi < C J } = #{ k : k tot < D },
+// D = C J - chi.  A double-precision guess k is corrected with the exact
+// 128-bit comparisons  k tot < D  (one product, then add or subtract tot).
 __device__ __forceinline__ int nchild_fast(const Offsets& o, uint64_t C) {
-  uint64_t CJhi, CJlo;
-  mul64(C, (uint64_t)o.J, CJhi, CJlo);
+  uint64_t Dh, Dl;
+  mul64(C, (uint64_t)o.J, Dh, Dl);
+  Dh -= (Dl < o.chi);
+  Dl -= o.chi;                                  // D = C J - chi (may be negative)
+  if ((long long)Dh < 0 || (Dh == 0 && Dl == 0)) return 0;
   long long k = (long long)ceil((double)C * o.inv - o.chi_d);
   if (k < 0) k = 0;
   if (k > o.J) k = o.J;
-  while (k > 0 && !below(o, k - 1, CJhi, CJlo)) --k;
-  while (k < o.J && below(o, k, CJhi, CJlo)) ++k;
+  uint64_t Ph, Pl;
+  mul64((uint64_t)k, o.tot, Ph, Pl);            // P = k tot
+  // while (k > 0 && (k-1) tot >= D): k--
+  while (k > 0) {
+    const uint64_t ql = Pl - o.tot, qh = Ph - (Pl < o.tot);
+    if ((qh < Dh) || (qh == Dh && ql < Dl)) break;
+    Ph = qh; Pl = ql; --k;
+  }
+  // while (k < J && k tot < D): k++
+  while (k < o.J && ((Ph < Dh) || (Ph == Dh && Pl < Dl))) {
+    const uint64_t nl = Pl + o.tot;
+    Ph += (nl < Pl);
+    Pl = nl;
+    ++k;
+  }
   return (int)k;
 }
 
@@ -211,14 +240,20 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
   const int u = filter_unit(a, f);
   if (threadIdx.x == 0) M::prepare(c, a.theta + (size_t)f * a.model.n_params, a.model, (a.flags & PPF_F_EST) != 0);
   __syncthreads();
-  float* X = a.X[0] + (size_t)f * DX * a.J;
-  float* W = a.W[0] + (size_t)f * a.J;
+  const typename M::Consts cr = c;
+  Obs<M> ob;
+  ob.load(a, u, 0);
+  const int J = a.J;
+  float* X = a.X[0] + (size_t)f * DX * J;
+  float* W = a.W[0] + (size_t)f * J;
+  float* logw = a.logw ? a.logw + ((size_t)f * a.T) * J : nullptr;
+  const bool pm = (a.flags & PPF_F_PMEAN) != 0;
   unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
   double px[DX];
 #pragma unroll
   for (int d = 0; d < DX; ++d) px[d] = 0.0;
   const int j0 = blockIdx.x * a.tile;
-  const int j1 = min(j0 + a.tile, a.J);
+  const int j1 = min(j0 + a.tile, J);
   const float base = (a.mode == MODE_MOP ? 0.0f : a.base_init);
   for (int k0 = j0 + 4 * threadIdx.x; k0 < j1; k0 += 4 * TPB) {
     float z0[4 * (M::NZ0 > 0 ? M::NZ0 : 1)];
@@ -230,12 +265,15 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
       const int k = k0 + e;
       if (k >= j1) break;
       float x[DX];
-      M::rinit(c, z0 + e * M::NZ0, x);
-      const float w = base + prop1<M>(a, c, u, 0, x, z + e * M::NZ);
+      M::rinit(cr, z0 + e * M::NZ0, x);
+      const float w = base + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
-      for (int d = 0; d < DX; ++d) { X[(size_t)d * a.J + k] = x[d]; px[d] += (double)x[d]; }
+      for (int d = 0; d < DX; ++d) {
+        X[d * J + k] = x[d];
+        if (pm) px[d] += (double)x[d];
+      }
       W[k] = w;
-      if (a.logw) a.logw[((size_t)f * a.T) * a.J + k] = w;
+      if (logw) logw[k] = w;
       accum_maxmin(w, mx, mn, nn);
     }
   }
@@ -248,7 +286,7 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
     if (nn) atomicOr(&acc->nan, 1u);
     if (blockIdx.x == 0) a.loglik[f] = 0.0;
   }
-  if (a.flags & PPF_F_PMEAN) {
+  if (pm) {
 #pragma unroll
     for (int d = 0; d < DX; ++d) {
       const double s = block_sum_f64<TPB>(px[d], sd);
@@ -414,20 +452,25 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
   const float Mx = keyf(acc.maxkey);
   const bool collapsed = !nanf && Mx == -INFINITY;
   const bool rs = decide_resample(a, acc);
-  const float* Xc = a.X[p] + (size_t)f * DX * a.J;
-  const float* Wc = a.W[p] + (size_t)f * a.J;
-  float* Xn = a.X[p ^ 1] + (size_t)f * DX * a.J;
-  float* Wn = a.W[p ^ 1] + (size_t)f * a.J;
-  int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * a.J : nullptr;
-  float* logw = a.logw ? a.logw + ((size_t)f * a.T + t + 1) * a.J : nullptr;
+  const int J = a.J;
+  const float* Xc = a.X[p] + (size_t)f * DX * J;
+  const float* Wc = a.W[p] + (size_t)f * J;
+  float* Xn = a.X[p ^ 1] + (size_t)f * DX * J;
+  float* Wn = a.W[p ^ 1] + (size_t)f * J;
+  int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
+  float* logw = a.logw ? a.logw + ((size_t)f * a.T + t + 1) * J : nullptr;
+  const bool pm = (a.flags & PPF_F_PMEAN) != 0;
+  Obs<M> ob;
+  if (!last) ob.load(a, u, t + 1);
   unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
   double px[DX];
 #pragma unroll
   for (int d = 0; d < DX; ++d) px[d] = 0.0;
   const float base = (a.mode == MODE_MOP) ? 0.0f : a.base_rs;
   const int jt = b * TILE;
-  const int ntile = min(TILE, a.J - jt);
+  const int ntile = min(TILE, J - jt);
   __syncthreads();
+  const typename M::Consts cr = c;
 
   if (!rs) {
     // No resampling: every particle is its own child; weights carry over.
@@ -446,18 +489,21 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
         if (last) continue;
         float x[DX];
 #pragma unroll
-        for (int d = 0; d < DX; ++d) x[d] = Xc[(size_t)d * a.J + k];
+        for (int d = 0; d < DX; ++d) x[d] = Xc[d * J + k];
         const float nw = collapsed ? nwc : Wc[k] - lt32;
-        const float w = nw + prop1<M>(a, c, u, t + 1, x, z + e * M::NZ);
+        const float w = nw + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
-        for (int d = 0; d < DX; ++d) { Xn[(size_t)d * a.J + k] = x[d]; px[d] += (double)x[d]; }
+        for (int d = 0; d < DX; ++d) {
+          Xn[d * J + k] = x[d];
+          if (pm) px[d] += (double)x[d];
+        }
         Wn[k] = w;
         if (logw) logw[k] = w;
         accum_maxmin(w, mx, mn, nn);
       }
     }
   } else {
-    const Offsets o = make_offsets(tot, resample_u32(a, f, t), a.J);
+    const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
     const uint64_t E = a.excl[(size_t)f * a.ntiles + b];
     // 1. fixed-point weights of this thread's parents and the tile scan
     const int l0 = threadIdx.x * IT;
@@ -495,7 +541,7 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
     }
     for (int l = threadIdx.x; l < ntile; l += TPB)
 #pragma unroll
-      for (int d = 0; d < DX; ++d) xs[d * TILE + l] = Xc[(size_t)d * a.J + jt + l];
+      for (int d = 0; d < DX; ++d) xs[d * TILE + l] = Xc[d * J + jt + l];
     __syncthreads();
     const int klo = st[0], khi = st[ntile];
     // 3. children in groups of 4
@@ -519,9 +565,12 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
         float x[DX];
 #pragma unroll
         for (int d = 0; d < DX; ++d) x[d] = xs[d * TILE + l];
-        const float w = base + prop1<M>(a, c, u, t + 1, x, z + e * M::NZ);
+        const float w = base + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
-        for (int d = 0; d < DX; ++d) { Xn[(size_t)d * a.J + k] = x[d]; px[d] += (double)x[d]; }
+        for (int d = 0; d < DX; ++d) {
+          Xn[d * J + k] = x[d];
+          if (pm) px[d] += (double)x[d];
+        }
         Wn[k] = w;
         if (logw) logw[k] = w;
         accum_maxmin(w, mx, mn, nn);
@@ -537,7 +586,7 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
     if (mn != 0xffffffffu) atomicMin(&an->minkey, mn);
     if (nn) atomicOr(&an->nan, 1u);
   }
-  if (a.flags & PPF_F_PMEAN) {
+  if (pm) {
 #pragma unroll
     for (int d = 0; d < DX; ++d) {
       const double s = block_sum_f64<TPB>(px[d], sd);
@@ -574,12 +623,15 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     s_ll = 0.0;
   }
   __syncthreads();
+  const typename M::Consts cr = c;
   // blocked ownership for the scan: thread owns [l0, l1)
   const int per = (J + TPB - 1) / TPB;
   const int l0 = min(J, threadIdx.x * per);
   const int l1 = min(J, l0 + per);
 
   // step 0: rinit + rproc + dmeas, groups of 4
+  Obs<M> ob;
+  ob.load(a, u, 0);
   for (int g = threadIdx.x; 4 * g < J; g += TPB) {
     const int k0 = 4 * g;
     float z0[4 * (M::NZ0 > 0 ? M::NZ0 : 1)];
@@ -591,8 +643,8 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
       const int k = k0 + e;
       if (k >= J) break;
       float x[DX];
-      M::rinit(c, z0 + e * M::NZ0, x);
-      const float w = (a.mode == MODE_MOP ? 0.0f : a.base_init) + prop1<M>(a, c, u, 0, x, z + e * M::NZ);
+      M::rinit(cr, z0 + e * M::NZ0, x);
+      const float w = (a.mode == MODE_MOP ? 0.0f : a.base_init) + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
       for (int d = 0; d < DX; ++d) xs[d * J + k] = x[d];
       ws[k] = w;
@@ -656,6 +708,7 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     const bool rs = decide_resample(a, s_acc);
     int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
     float* logw = a.logw ? a.logw + ((size_t)f * a.T + t + 1) * J : nullptr;
+    if (!last) ob.load(a, u, t + 1);
     if (!rs) {
       float lt32 = 0.0f;
       if (nanf) lt32 = __int_as_float(0x7fc00000);
@@ -676,7 +729,7 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
 #pragma unroll
           for (int d = 0; d < DX; ++d) x[d] = xs[d * J + k];
           const float nw = collapsed ? nwc : ws[k] - lt32;
-          const float w = nw + prop1<M>(a, c, u, t + 1, x, z + e * M::NZ);
+          const float w = nw + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
           for (int d = 0; d < DX; ++d) xs[d * J + k] = x[d];
           ws[k] = w;
@@ -722,7 +775,7 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
           float x[DX];
 #pragma unroll
           for (int d = 0; d < DX; ++d) x[d] = xs[d * J + l];
-          nw[gi][e] = base + prop1<M>(a, c, u, t + 1, x, z + e * M::NZ);
+          nw[gi][e] = base + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
           for (int d = 0; d < DX; ++d) nx[gi][e][d] = x[d];
         }
