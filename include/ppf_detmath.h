@@ -69,11 +69,10 @@ PPF_HD float pp_rint(float x) {
 PPF_HD float pp_pow2i(int n) { return pp_u2f((uint32_t)(n + 127) << 23); }
 
 PPF_HD float pp_expf(float x) {
-  if (x != x) return x;
-  if (x > 88.72283935546875f) return pp_u2f(0x7f800000u);
-  if (x < -103.97208404541016f) return 0.0f;
-  const float k = pp_rint(x * 1.44269502162933349609375f);        /* x / ln2 */
-  float r = pp_fma(-k, 0.693145751953125f, x);                      /* ln2 hi (16 bits) */
+  /* special cases are selected at the end so the main path has no branches */
+  const float xc = fminf(fmaxf(x, -103.97208404541016f), 88.72283935546875f);
+  const float k = pp_rint(xc * 1.44269502162933349609375f);       /* x / ln2 */
+  float r = pp_fma(-k, 0.693145751953125f, xc);                     /* ln2 hi (16 bits) */
   r = pp_fma(-k, 1.428606765330187045e-06f, r);                      /* ln2 - hi */
   float p = 1.98412698412698413e-04f;                                /* 1/7! */
   p = pp_fma(p, r, 1.38888888888888889e-03f);                        /* 1/6! */
@@ -84,22 +83,24 @@ PPF_HD float pp_expf(float x) {
   p = pp_fma(p, r, 1.0f);
   p = pp_fma(p, r, 1.0f);
   const int ki = (int)k;
-  const int k1 = ki / 2;
+  const int k1 = ki >> 1;                                            /* floor(k/2) */
   const int k2 = ki - k1;
-  return (p * pp_pow2i(k1)) * pp_pow2i(k2);
+  float y = (p * pp_pow2i(k1)) * pp_pow2i(k2);
+  y = (x > 88.72283935546875f) ? pp_u2f(0x7f800000u) : y;
+  y = (x < -103.97208404541016f) ? 0.0f : y;
+  return (x != x) ? x : y;
 }
 
 PPF_HD float pp_logf(float x) {
-  if (x != x) return x;
-  if (x < 0.0f) return pp_u2f(0x7fc00000u);
-  if (x == 0.0f) return pp_u2f(0xff800000u);
-  if (x == pp_u2f(0x7f800000u)) return x;
-  int adj = 0;
-  if (x < 1.17549435082228750797e-38f) { x = x * 8388608.0f; adj = -23; }
-  const uint32_t b = pp_f2u(x);
-  int e = (int)((b >> 23) & 0xffu) - 127 + adj;
+  /* main path on a safe input; special cases selected at the end */
+  const int sub = x < 1.17549435082228750797e-38f;
+  const float xs = sub ? x * 8388608.0f : x;
+  const uint32_t b = pp_f2u(xs);
+  int e = (int)((b >> 23) & 0xffu) - 127 - (sub ? 23 : 0);
   float m = pp_u2f((b & 0x007fffffu) | 0x3f800000u);               /* [1, 2) */
-  if (m > 1.41421353816986083984375f) { m = m * 0.5f; e += 1; }     /* [0.707, 1.414] */
+  const int hi = m > 1.41421353816986083984375f;
+  m = hi ? m * 0.5f : m;                                            /* [0.707, 1.414] */
+  e += hi;
   const float f = m - 1.0f;
   const float s = f / (2.0f + f);
   const float z = s * s;
@@ -111,7 +112,11 @@ PPF_HD float pp_logf(float x) {
   const float lm = f - s * (f - R);
   const float ef = (float)e;
   const float lo = pp_fma(ef, 1.428606765330187045e-06f, lm);
-  return pp_fma(ef, 0.693145751953125f, lo);
+  float y = pp_fma(ef, 0.693145751953125f, lo);
+  y = (x == pp_u2f(0x7f800000u)) ? x : y;
+  y = (x == 0.0f) ? pp_u2f(0xff800000u) : y;
+  y = (x < 0.0f) ? pp_u2f(0x7fc00000u) : y;
+  return (x != x) ? x : y;
 }
 
 /* log(x) for x in [2^-24, 1]: pp_logf without the special-case tests (same
@@ -160,12 +165,11 @@ PPF_HD void pp_sincos2pif(float u, float* sn, float* cs) {
   const float c = pp_fma(pc, t2, 1.0f);
   const float a = swap ? c : s;             /* sin of the in-quadrant angle */
   const float bb = swap ? s : c;            /* cos of the in-quadrant angle */
-  switch (q) {
-    case 0: *sn = a; *cs = bb; break;
-    case 1: *sn = bb; *cs = -a; break;
-    case 2: *sn = -a; *cs = -bb; break;
-    default: *sn = -bb; *cs = a; break;
-  }
+  /* rotate by q quarter turns: (a, bb) -> (bb, -a) -> (-a, -bb) -> (-bb, a) */
+  const float s1 = (q & 1) ? bb : a;
+  const float c1 = (q & 1) ? a : bb;
+  *sn = (q >= 2) ? -s1 : s1;
+  *cs = ((q == 1) | (q == 2)) ? -c1 : c1;
 }
 
 #endif /* PPF_DETMATH_H */

@@ -56,10 +56,10 @@ __device__ __forceinline__ void step_noise(const Args& a, int f, int j, int s, i
 // Normals of the group of 4 consecutive particles k0..k0+3 (k0 % 4 == 0) at
 // step s, N per particle: z[e*N + r].  Philox calls (k0 N)/4 ... + N-1 cover
 // the group exactly; positions past J read zeros in injection mode.
-template <int N>
+template <int N, bool INJ>
 __device__ __forceinline__ void group_noise(const Args& a, int f, int s, int k0, float* z) {
   if (N == 0) return;
-  if (a.flags & PPF_F_INJECT) {
+  if (INJ) {
     const float* src = (s == 0) ? a.inj_z0 + (size_t)f * a.J * N
                                 : a.inj_z + (((size_t)f * a.T + (s - 1)) * a.J) * N;
 #pragma unroll
@@ -154,10 +154,11 @@ __device__ __forceinline__ bool decide_resample(const Args& a, const Acc& acc) {
 }
 
 __device__ __forceinline__ void accum_maxmin(float w, unsigned int& mx, unsigned int& mn, unsigned int& nn) {
-  if (w != w || w == INFINITY) { nn = 1u; return; }
+  const bool bad = (w != w) | (w == INFINITY);
   const unsigned int k = fkey(w);
-  mx = max(mx, k);
-  mn = min(mn, k);
+  nn |= bad ? 1u : 0u;
+  mx = bad ? mx : max(mx, k);
+  mn = bad ? mn : min(mn, k);
 }
 
 // Constants of the exact systematic-offset test for one filter and step:
@@ -186,33 +187,33 @@ __device__ __forceinline__ void mul64(uint64_t a, uint64_t b, uint64_t& hi, uint
 }
 
 // nchild(C) = #{ k in [0,J) : k tot + chi < C J } = #{ k : k tot < D },
-// D = C J - chi.  A double-precision guess k is corrected with the exact
-// 128-bit comparisons  k tot < D  (one product, then add or subtract tot).
+// D = C J - chi.  The double-precision guess ceil(D / tot) is within one of
+// the answer (its relative error is ~1e-16 on a value below 2^21), so one
+// exact 128-bit comparison on each side settles it; a bounded loop covers the
+// impossible case defensively.
+__device__ __forceinline__ bool lt128(uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl) {
+  return (ah < bh) | ((ah == bh) & (al < bl));
+}
+
 __device__ __forceinline__ int nchild_fast(const Offsets& o, uint64_t C) {
   uint64_t Dh, Dl;
   mul64(C, (uint64_t)o.J, Dh, Dl);
   Dh -= (Dl < o.chi);
   Dl -= o.chi;                                  // D = C J - chi (may be negative)
-  if ((long long)Dh < 0 || (Dh == 0 && Dl == 0)) return 0;
+  const bool nonpos = ((long long)Dh < 0) | ((Dh == 0) & (Dl == 0));
   long long k = (long long)ceil((double)C * o.inv - o.chi_d);
-  if (k < 0) k = 0;
-  if (k > o.J) k = o.J;
+  k = k < 0 ? 0 : (k > o.J ? o.J : k);
   uint64_t Ph, Pl;
   mul64((uint64_t)k, o.tot, Ph, Pl);            // P = k tot
-  // while (k > 0 && (k-1) tot >= D): k--
-  while (k > 0) {
-    const uint64_t ql = Pl - o.tot, qh = Ph - (Pl < o.tot);
-    if ((qh < Dh) || (qh == Dh && ql < Dl)) break;
-    Ph = qh; Pl = ql; --k;
+  for (int it = 0; it < 4; ++it) {
+    const uint64_t ql = Pl - o.tot, qh = Ph - (Pl < o.tot);     // (k-1) tot
+    const bool down = (k > 0) & !lt128(qh, ql, Dh, Dl);        // (k-1) tot >= D
+    const bool up = (k < o.J) & lt128(Ph, Pl, Dh, Dl);          // k tot < D
+    if (!(down | up)) break;
+    if (down) { Ph = qh; Pl = ql; --k; }
+    else { const uint64_t nl = Pl + o.tot; Ph += (nl < Pl); Pl = nl; ++k; }
   }
-  // while (k < J && k tot < D): k++
-  while (k < o.J && ((Ph < Dh) || (Ph == Dh && Pl < Dl))) {
-    const uint64_t nl = Pl + o.tot;
-    Ph += (nl < Pl);
-    Pl = nl;
-    ++k;
-  }
-  return (int)k;
+  return nonpos ? 0 : (int)k;
 }
 
 // Parent (tile-local index) of child k: the last l in [0, n) with st[l] <= k.
@@ -230,7 +231,32 @@ __device__ __forceinline__ int find_parent(const int* st, int n, int k) {
 // STREAM path
 // ============================================================================
 
-template <class M, int TPB>
+// Store the 4 children k0..k0+3 (valid[e]) of one group: float4 stores when
+// the whole group is valid and rows are 16-byte aligned (J % 4 == 0).
+template <int DX>
+__device__ __forceinline__ void store_group(float* Xn, float* Wn, float* logw, int J, int k0,
+                                            const float (&xo)[4][DX], const float (&wo)[4],
+                                            int nvalid_lo, int nvalid_hi) {
+  const bool full = (nvalid_lo == 0) & (nvalid_hi == 4) & ((J & 3) == 0);
+  if (full) {
+#pragma unroll
+    for (int d = 0; d < DX; ++d)
+      *reinterpret_cast<float4*>(Xn + d * J + k0) = make_float4(xo[0][d], xo[1][d], xo[2][d], xo[3][d]);
+    *reinterpret_cast<float4*>(Wn + k0) = make_float4(wo[0], wo[1], wo[2], wo[3]);
+    if (logw) *reinterpret_cast<float4*>(logw + k0) = make_float4(wo[0], wo[1], wo[2], wo[3]);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (e < nvalid_lo || e >= nvalid_hi) continue;
+#pragma unroll
+      for (int d = 0; d < DX; ++d) Xn[d * J + k0 + e] = xo[e][d];
+      Wn[k0 + e] = wo[e];
+      if (logw) logw[k0 + e] = wo[e];
+    }
+  }
+}
+
+template <class M, int TPB, bool INJ>
 __global__ void __launch_bounds__(TPB) k_init(Args a) {
   __shared__ typename M::Consts c;
   __shared__ unsigned int smk[2 * (TPB / 32)];
@@ -258,24 +284,25 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
   for (int k0 = j0 + 4 * threadIdx.x; k0 < j1; k0 += 4 * TPB) {
     float z0[4 * (M::NZ0 > 0 ? M::NZ0 : 1)];
     float z[4 * M::NZ];
-    group_noise<M::NZ0>(a, f, 0, k0, z0);
-    group_noise<M::NZ>(a, f, 1, k0, z);
+    group_noise<M::NZ0, INJ>(a, f, 0, k0, z0);
+    group_noise<M::NZ, INJ>(a, f, 1, k0, z);
+    float xo[4][DX];
+    float wo[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      const int k = k0 + e;
-      if (k >= j1) break;
       float x[DX];
       M::rinit(cr, z0 + e * M::NZ0, x);
-      const float w = base + step1<M>(cr, ob, x, z + e * M::NZ);
+      wo[e] = base + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
-      for (int d = 0; d < DX; ++d) {
-        X[d * J + k] = x[d];
-        if (pm) px[d] += (double)x[d];
+      for (int d = 0; d < DX; ++d) xo[e][d] = x[d];
+      if (k0 + e < j1) {
+        accum_maxmin(wo[e], mx, mn, nn);
+        if (pm)
+#pragma unroll
+          for (int d = 0; d < DX; ++d) px[d] += (double)x[d];
       }
-      W[k] = w;
-      if (logw) logw[k] = w;
-      accum_maxmin(w, mx, mn, nn);
     }
+    store_group<DX>(X, W, logw, J, k0, xo, wo, 0, min(4, j1 - k0));
   }
   block_maxmin_u32<TPB>(mx, mn, smk);
   nn = __syncthreads_or(nn);
@@ -302,7 +329,7 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
   __shared__ int s_v;
-  __shared__ uint64_t s_scan[TPB / 32 + 1];
+  __shared__ uint64_t s_red[TPB / 32];
   __shared__ double sd[TPB / 32];
   if (threadIdx.x == 0) s_v = atomicAdd(a.counter + (t & 1), 1);
   __syncthreads();
@@ -325,13 +352,13 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
   const bool nanf = acc.nan != 0;
   const float Mx = keyf(acc.maxkey);
   const bool collapsed = nanf || Mx == -INFINITY;
-  const float* W = a.W[p] + (size_t)f * a.J;
+  const int J = a.J;
+  const float* W = a.W[p] + (size_t)f * J;
   const int jb = b * TILE + threadIdx.x * IT;
   uint64_t qs = 0;
-  double s2 = 0.0;
   float wv[IT];
   // float4 loads only when every filter's row starts 16-byte aligned (J % 4 == 0)
-  if (jb + IT <= a.J && (IT % 4) == 0 && (a.J & 3) == 0) {
+  if (jb + IT <= J && (IT % 4) == 0 && (J & 3) == 0) {
 #pragma unroll
     for (int i = 0; i < IT; i += 4) {
       const float4 v4 = *reinterpret_cast<const float4*>(W + jb + i);
@@ -339,23 +366,22 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < IT; ++i) wv[i] = (jb + i < a.J) ? W[jb + i] : -INFINITY;
+    for (int i = 0; i < IT; ++i) wv[i] = (jb + i < J) ? W[jb + i] : -INFINITY;
   }
 #pragma unroll
-  for (int i = 0; i < IT; ++i) {
-    if (jb + i < a.J) {
-      qs += qweight(wv[i], Mx, collapsed);
-      if (a.flags & PPF_F_ESS) {
-        const double e = collapsed ? 1.0 : (double)pp_expf(wv[i] - Mx);
-        s2 += e * e;
-      }
-    }
+  for (int i = 0; i < IT; ++i) qs += (jb + i < J) ? qweight(wv[i], Mx, collapsed) : 0ull;
+  // block total
+  {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t wsum = warp_sum_u64(qs);
+    if (lane == 0) s_red[warp] = wsum;
+    __syncthreads();
   }
-  uint64_t btot;
-  block_excl_scan_u64<TPB>(qs, s_scan, btot);
   uint64_t* desc = a.desc[p] + (size_t)f * a.ntiles;
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
+    uint64_t btot = lane < TPB / 32 ? s_red[lane] : 0ull;
+    btot = warp_sum_u64(btot);
     uint64_t excl = 0;
     if (b == 0) {
       if (lane == 0) st_release_u64(desc, kStatusIncl | btot);
@@ -390,19 +416,26 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
     }
   }
   if (a.flags & PPF_F_ESS) {
+    double s2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < IT; ++i)
+      if (jb + i < J) {
+        const double e = collapsed ? 1.0 : (double)pp_expf(wv[i] - Mx);
+        s2 += e * e;
+      }
     const double s = block_sum_f64<TPB>(s2, sd);
     if (threadIdx.x == 0) atomicAdd(&a.acc[p][f].s2, s);
   }
   if (a.flags & PPF_F_FMEAN) {
-    const float* X = a.X[p] + (size_t)f * DX * a.J;
+    const float* X = a.X[p] + (size_t)f * DX * J;
 #pragma unroll
     for (int d = 0; d < DX; ++d) {
       double s = 0.0;
 #pragma unroll
       for (int i = 0; i < IT; ++i)
-        if (jb + i < a.J) {
+        if (jb + i < J) {
           const double e = collapsed ? 1.0 : (double)pp_expf(wv[i] - Mx);
-          s += (double)X[(size_t)d * a.J + jb + i] * e;
+          s += (double)X[d * J + jb + i] * e;
         }
       s = block_sum_f64<TPB>(s, sd);
       if (threadIdx.x == 0) atomicAdd(&a.acc[p][f].fx[d], s);
@@ -413,19 +446,23 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
 // Resample the parents of one tile and propagate their children to the next
 // observation (rproc + dmeas fused), writing the next step's X, W.
 //   1. fixed-point weights of the tile's parents, block scan, plus the tile's
-//      exclusive prefix from k_sum: the exact CDF C_l of every parent;
+//      exclusive prefix from k_sum: the exact CDF of every parent;
 //   2. closed-form first-child offset st[l] = nchild(C_{l-1}) per parent into
-//      shared memory, parent states staged in shared memory;
-//   3. the tile's children [st[0], st[n]) in groups of 4: binary search of the
-//      first child's parent, gather from shared memory, one Philox call per
-//      4 normals, rproc + dmeas, coalesced stores.
-template <class M, int TPB, int IT>
-__global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
+//      shared memory (st[l] = l on steps without resampling), parent states
+//      staged in shared memory;
+//   3. merge-path partition of the tile's children [st[0], st[n]) into equal
+//      runs of RUN children per thread: one binary search for the run's first
+//      parent, then a linear walk; per group of 4 children one set of Philox
+//      calls (every word used), rproc + dmeas, float4 stores.
+template <class M, int TPB, int IT, bool INJ>
+__global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a, int t) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
+  constexpr int RUN = 8;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* xs = reinterpret_cast<float*>(smem_raw);                              // [DX][TILE]
   int* st = reinterpret_cast<int*>(smem_raw + sizeof(float) * DX * TILE);      // [TILE + 1]
+  float* wcar = reinterpret_cast<float*>(st + TILE + 4);                      // [TILE] (no-resample steps)
   __shared__ typename M::Consts c;
   __shared__ uint64_t s_scan[TPB / 32 + 1];
   __shared__ unsigned int smk[2 * (TPB / 32)];
@@ -451,6 +488,7 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
   const bool nanf = acc.nan != 0;
   const float Mx = keyf(acc.maxkey);
   const bool collapsed = !nanf && Mx == -INFINITY;
+  const bool qc = nanf || Mx == -INFINITY;
   const bool rs = decide_resample(a, acc);
   const int J = a.J;
   const float* Xc = a.X[p] + (size_t)f * DX * J;
@@ -469,68 +507,33 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
   const float base = (a.mode == MODE_MOP) ? 0.0f : a.base_rs;
   const int jt = b * TILE;
   const int ntile = min(TILE, J - jt);
-  __syncthreads();
-  const typename M::Consts cr = c;
+  const int l0 = threadIdx.x * IT;
 
-  if (!rs) {
-    // No resampling: every particle is its own child; weights carry over.
-    float lt32 = 0.0f;
-    if (nanf) lt32 = __int_as_float(0x7fc00000);
-    else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
-    const float nwc = -pp_logf((float)a.J);
-    for (int k0 = jt + 4 * threadIdx.x; k0 < jt + ntile; k0 += 4 * TPB) {
-      float z[4 * M::NZ];
-      if (!last) group_noise<M::NZ>(a, f, t + 2, k0, z);
+  // 1-2. parents: CDF and first-child offsets (or identity), staged states
+  {
+    float wv[IT];
+    if (l0 + IT <= ntile && (J & 3) == 0) {
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int k = k0 + e;
-        if (k >= jt + ntile) break;
-        if (anc) anc[k] = k;
-        if (last) continue;
-        float x[DX];
-#pragma unroll
-        for (int d = 0; d < DX; ++d) x[d] = Xc[d * J + k];
-        const float nw = collapsed ? nwc : Wc[k] - lt32;
-        const float w = nw + step1<M>(cr, ob, x, z + e * M::NZ);
-#pragma unroll
-        for (int d = 0; d < DX; ++d) {
-          Xn[d * J + k] = x[d];
-          if (pm) px[d] += (double)x[d];
-        }
-        Wn[k] = w;
-        if (logw) logw[k] = w;
-        accum_maxmin(w, mx, mn, nn);
+      for (int i = 0; i < IT; i += 4) {
+        const float4 v4 = *reinterpret_cast<const float4*>(Wc + jt + l0 + i);
+        wv[i] = v4.x; wv[i + 1] = v4.y; wv[i + 2] = v4.z; wv[i + 3] = v4.w;
       }
+    } else {
+#pragma unroll
+      for (int i = 0; i < IT; ++i) wv[i] = (l0 + i < ntile) ? Wc[jt + l0 + i] : 0.0f;
     }
-  } else {
-    const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
-    const uint64_t E = a.excl[(size_t)f * a.ntiles + b];
-    // 1. fixed-point weights of this thread's parents and the tile scan
-    const int l0 = threadIdx.x * IT;
-    uint64_t q[IT];
-    uint64_t qs = 0;
-    {
-      float wv[IT];
-      if (l0 + IT <= ntile && (a.J & 3) == 0) {
-#pragma unroll
-        for (int i = 0; i < IT; i += 4) {
-          const float4 v4 = *reinterpret_cast<const float4*>(Wc + jt + l0 + i);
-          wv[i] = v4.x; wv[i + 1] = v4.y; wv[i + 2] = v4.z; wv[i + 3] = v4.w;
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < IT; ++i) wv[i] = (l0 + i < ntile) ? Wc[jt + l0 + i] : 0.0f;
-      }
+    if (rs) {
+      const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
+      const uint64_t E = a.excl[(size_t)f * a.ntiles + b];
+      uint64_t q[IT];
+      uint64_t qs = 0;
 #pragma unroll
       for (int i = 0; i < IT; ++i) {
-        q[i] = (l0 + i < ntile) ? qweight(wv[i], Mx, collapsed) : 0ull;
+        q[i] = (l0 + i < ntile) ? qweight(wv[i], Mx, qc) : 0ull;
         qs += q[i];
       }
-    }
-    uint64_t btot;
-    const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
-    // 2. first-child offsets and staged parent states
-    {
+      uint64_t btot;
+      const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
       uint64_t C = E + tex;
 #pragma unroll
       for (int i = 0; i < IT; ++i) {
@@ -538,43 +541,69 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
         C += q[i];
       }
       if (l0 < ntile && l0 + IT >= ntile) st[ntile] = nchild_fast(o, E + btot);
-    }
-    for (int l = threadIdx.x; l < ntile; l += TPB)
+    } else {
+      float lt32 = 0.0f;
+      if (nanf) lt32 = __int_as_float(0x7fc00000);
+      else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
+      const float nwc = -pp_logf((float)J);
 #pragma unroll
-      for (int d = 0; d < DX; ++d) xs[d * TILE + l] = Xc[d * J + jt + l];
-    __syncthreads();
-    const int klo = st[0], khi = st[ntile];
-    // 3. children in groups of 4
-    const int kA = klo & ~3;
-    for (int k0 = kA + 4 * threadIdx.x; k0 < khi; k0 += 4 * TPB) {
+      for (int i = 0; i < IT; ++i)
+        if (l0 + i < ntile) {
+          st[l0 + i] = jt + l0 + i;
+          wcar[l0 + i] = collapsed ? nwc : wv[i] - lt32;
+        }
+      if (l0 < ntile && l0 + IT >= ntile) st[ntile] = jt + ntile;
+    }
+  }
+  for (int l = threadIdx.x; l < ntile; l += TPB)
+#pragma unroll
+    for (int d = 0; d < DX; ++d) xs[d * TILE + l] = Xc[d * J + jt + l];
+  __syncthreads();
+  const typename M::Consts cr = c;
+  const int klo = st[0], khi = st[ntile];
+
+  // 3. children, in runs of RUN per thread
+  const int kA = klo & ~3;
+  const int nrun = (khi - kA + RUN - 1) / RUN;
+  for (int r = threadIdx.x; r < nrun; r += TPB) {
+    const int ka = kA + r * RUN;
+    int l = find_parent(st, ntile, max(ka, klo));
+#pragma unroll
+    for (int g = 0; g < RUN / 4; ++g) {
+      const int k0 = ka + 4 * g;
+      if (k0 >= khi) break;
+      const int lo = max(0, klo - k0), hi = min(4, khi - k0);   // valid e in [lo, hi)
       float z[4 * M::NZ];
-      if (!last) group_noise<M::NZ>(a, f, t + 2, k0, z);
-      int l = find_parent(st, ntile, max(k0, klo));
+      if (!last) group_noise<M::NZ, INJ>(a, f, t + 2, k0, z);
+      float xo[4][DX];
+      float wo[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int k = k0 + e;
-        if (k < klo) continue;
-        if (k >= khi) break;
-        int adv = 0;
-        while (l + 1 < ntile && st[l + 1] <= k) {
-          ++l;
-          if (++adv > 8) { l = find_parent(st, ntile, k); break; }
+        const bool valid = (e >= lo) & (e < hi);
+        if (valid) {
+          int adv = 0;
+          while (l + 1 < ntile && st[l + 1] <= k) {
+            ++l;
+            if (++adv > 8) { l = find_parent(st, ntile, k); break; }
+          }
+          if (anc) anc[k] = jt + l;
         }
-        if (anc) anc[k] = jt + l;
-        if (last) continue;
         float x[DX];
 #pragma unroll
         for (int d = 0; d < DX; ++d) x[d] = xs[d * TILE + l];
-        const float w = base + step1<M>(cr, ob, x, z + e * M::NZ);
+        const float wb = rs ? base : wcar[l];
+        wo[e] = wb + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
-        for (int d = 0; d < DX; ++d) {
-          Xn[d * J + k] = x[d];
-          if (pm) px[d] += (double)x[d];
+        for (int d = 0; d < DX; ++d) xo[e][d] = x[d];
+        if (valid) {
+          accum_maxmin(wo[e], mx, mn, nn);
+          if (pm)
+#pragma unroll
+            for (int d = 0; d < DX; ++d) px[d] += (double)x[d];
         }
-        Wn[k] = w;
-        if (logw) logw[k] = w;
-        accum_maxmin(w, mx, mn, nn);
       }
+      if (!last) store_group<DX>(Xn, Wn, logw, J, k0, xo, wo, lo, hi);
     }
   }
   if (last) return;
@@ -597,13 +626,16 @@ __global__ void __launch_bounds__(TPB, 3) k_resprop(Args a, int t) {
 
 // ============================================================================
 // RESIDENT path: one CTA per filter, the whole time loop in one launch.
-// Shared memory: xs[DX][J] float, ws[J] float, st[J+1] int.
+// Shared memory: xs[DX][J] float, ws[J] float, st[J+1] int.  Children are
+// processed in runs of 8 per thread and buffered in registers until every
+// parent has been read.
 // ============================================================================
 
-template <class M, int TPB, int MAXG>
+template <class M, int TPB, int MAXR, bool INJ>
 __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int DX = M::MAXDX;
+  constexpr int RUN = 8;
   const int J = a.J;
   float* xs = reinterpret_cast<float*>(smem_raw);
   float* ws = xs + (size_t)DX * J;
@@ -636,8 +668,8 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     const int k0 = 4 * g;
     float z0[4 * (M::NZ0 > 0 ? M::NZ0 : 1)];
     float z[4 * M::NZ];
-    group_noise<M::NZ0>(a, f, 0, k0, z0);
-    group_noise<M::NZ>(a, f, 1, k0, z);
+    group_noise<M::NZ0, INJ>(a, f, 0, k0, z0);
+    group_noise<M::NZ, INJ>(a, f, 1, k0, z);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int k = k0 + e;
@@ -709,92 +741,75 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
     float* logw = a.logw ? a.logw + ((size_t)f * a.T + t + 1) * J : nullptr;
     if (!last) ob.load(a, u, t + 1);
-    if (!rs) {
-      float lt32 = 0.0f;
-      if (nanf) lt32 = __int_as_float(0x7fc00000);
-      else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
-      const float nwc = -pp_logf((float)J);
-      __syncthreads();
-      for (int g = threadIdx.x; 4 * g < J; g += TPB) {
-        const int k0 = 4 * g;
-        float z[4 * M::NZ];
-        if (!last) group_noise<M::NZ>(a, f, t + 2, k0, z);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int k = k0 + e;
-          if (k >= J) break;
-          if (anc) anc[k] = k;
-          if (last) continue;
-          float x[DX];
-#pragma unroll
-          for (int d = 0; d < DX; ++d) x[d] = xs[d * J + k];
-          const float nw = collapsed ? nwc : ws[k] - lt32;
-          const float w = nw + step1<M>(cr, ob, x, z + e * M::NZ);
-#pragma unroll
-          for (int d = 0; d < DX; ++d) xs[d * J + k] = x[d];
-          ws[k] = w;
-          if (logw) logw[k] = w;
-        }
-      }
-      __syncthreads();
-      if (last) break;
-      continue;
-    }
-    // (c) first-child offsets of every parent
-    const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
-    {
+    // (c) first-child offsets of every parent (identity without resampling);
+    //     without resampling the carried weight replaces ws in place
+    if (rs) {
+      const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
       uint64_t C = tex;
       for (int j = l0; j < l1; ++j) {
         st[j] = nchild_fast(o, C);
         C += qweight(ws[j], Mx, qc);
       }
-      if (threadIdx.x == TPB - 1) st[J] = J;
+    } else {
+      float lt32 = 0.0f;
+      if (nanf) lt32 = __int_as_float(0x7fc00000);
+      else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
+      const float nwc = -pp_logf((float)J);
+      for (int j = l0; j < l1; ++j) {
+        st[j] = j;
+        ws[j] = collapsed ? nwc : ws[j] - lt32;
+      }
     }
+    if (threadIdx.x == TPB - 1) st[J] = J;
     __syncthreads();
-    // (d) children: parent from shared memory, propagate, keep in registers
-    float nx[MAXG][4][DX];
-    float nw[MAXG][4];
+    // (d) children: runs of 8, kept in registers until all parents are read
+    float nx[MAXR][RUN][DX];
+    float nw[MAXR][RUN];
 #pragma unroll
-    for (int gi = 0; gi < MAXG; ++gi) {
-      const int k0 = 4 * (threadIdx.x + gi * TPB);
-      if (k0 < J) {
-        float z[4 * M::NZ];
-        if (!last) group_noise<M::NZ>(a, f, t + 2, k0, z);
-        int l = find_parent(st, J, k0);
+    for (int ri = 0; ri < MAXR; ++ri) {
+      const int ka = RUN * (threadIdx.x + ri * TPB);
+      if (ka < J) {
+        int l = find_parent(st, J, ka);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int k = k0 + e;
-          if (k >= J) break;
-          int adv = 0;
-          while (l + 1 < J && st[l + 1] <= k) {
-            ++l;
-            if (++adv > 8) { l = find_parent(st, J, k); break; }
+        for (int g = 0; g < RUN / 4; ++g) {
+          const int k0 = ka + 4 * g;
+          if (k0 >= J) break;
+          float z[4 * M::NZ];
+          if (!last) group_noise<M::NZ, INJ>(a, f, t + 2, k0, z);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int k = k0 + e;
+            if (k >= J) break;
+            int adv = 0;
+            while (l + 1 < J && st[l + 1] <= k) {
+              ++l;
+              if (++adv > 8) { l = find_parent(st, J, k); break; }
+            }
+            if (anc) anc[k] = l;
+            float x[DX];
+#pragma unroll
+            for (int d = 0; d < DX; ++d) x[d] = xs[d * J + l];
+            const float wb = rs ? base : ws[l];
+            nw[ri][4 * g + e] = last ? 0.0f : wb + step1<M>(cr, ob, x, z + e * M::NZ);
+#pragma unroll
+            for (int d = 0; d < DX; ++d) nx[ri][4 * g + e][d] = x[d];
           }
-          if (anc) anc[k] = l;
-          if (last) continue;
-          float x[DX];
-#pragma unroll
-          for (int d = 0; d < DX; ++d) x[d] = xs[d * J + l];
-          nw[gi][e] = base + step1<M>(cr, ob, x, z + e * M::NZ);
-#pragma unroll
-          for (int d = 0; d < DX; ++d) nx[gi][e][d] = x[d];
         }
       }
     }
     __syncthreads();
     if (last) break;
 #pragma unroll
-    for (int gi = 0; gi < MAXG; ++gi) {
-      const int k0 = 4 * (threadIdx.x + gi * TPB);
-      if (k0 < J) {
+    for (int ri = 0; ri < MAXR; ++ri) {
+      const int ka = RUN * (threadIdx.x + ri * TPB);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int k = k0 + e;
-          if (k >= J) break;
+      for (int e = 0; e < RUN; ++e) {
+        const int k = ka + e;
+        if (k < J) {
 #pragma unroll
-          for (int d = 0; d < DX; ++d) xs[d * J + k] = nx[gi][e][d];
-          ws[k] = nw[gi][e];
-          if (logw) logw[k] = nw[gi][e];
+          for (int d = 0; d < DX; ++d) xs[d * J + k] = nx[ri][e][d];
+          ws[k] = nw[ri][e];
+          if (logw) logw[k] = nw[ri][e];
         }
       }
     }
@@ -983,28 +998,33 @@ void Profiler::mark(int kind, cudaStream_t s, bool start) {
 #define PROF_BEGIN(kind) g_prof.mark(kind, s, true)
 #define PROF_END(kind) g_prof.mark(kind, s, false)
 
-template <class M>
-int run_stream(Args& a, cudaStream_t s) {
+template <class M, bool INJ>
+int run_stream_t(Args& a, cudaStream_t s) {
   constexpr int TPB = 256, IT = 8, TILE = TPB * IT;
   a.tile = TILE;
   a.ntiles = (a.J + TILE - 1) / TILE;
-  const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4);
-  if (cudaFuncSetAttribute(k_resprop<M, TPB, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4) + sizeof(float) * TILE;
+  if (cudaFuncSetAttribute(k_resprop<M, TPB, IT, INJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return PPF_ECUDA;
   dim3 grid(a.ntiles, a.F);
   PROF_BEGIN(KIND_INIT);
-  k_init<M, TPB><<<grid, TPB, 0, s>>>(a);
+  k_init<M, TPB, INJ><<<grid, TPB, 0, s>>>(a);
   PROF_END(KIND_INIT);
   for (int t = 0; t < a.T; ++t) {
     PROF_BEGIN(KIND_SUM);
     k_sum<M, TPB, IT><<<a.ntiles * a.F, TPB, 0, s>>>(a, t);
     PROF_END(KIND_SUM);
     PROF_BEGIN(KIND_RESPROP);
-    k_resprop<M, TPB, IT><<<grid, TPB, smem, s>>>(a, t);
+    k_resprop<M, TPB, IT, INJ><<<grid, TPB, smem, s>>>(a, t);
     PROF_END(KIND_RESPROP);
   }
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
+template <class M>
+int run_stream(Args& a, cudaStream_t s) {
+  return (a.flags & PPF_F_INJECT) ? run_stream_t<M, true>(a, s) : run_stream_t<M, false>(a, s);
 }
 
 template <class M>
@@ -1012,28 +1032,32 @@ size_t resident_smem(const Args& a) {
   return (size_t)a.J * sizeof(float) * (M::MAXDX + 1) + (size_t)(a.J + 4) * sizeof(int);
 }
 
-template <class M, int MAXG>
+template <class M, int MAXR, bool INJ>
 int launch_resident(Args& a, size_t smem, cudaStream_t s) {
   constexpr int TPB = 512;
-  if (cudaFuncSetAttribute(k_resident<M, TPB, MAXG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(k_resident<M, TPB, MAXR, INJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return PPF_ECUDA;
   PROF_BEGIN(KIND_RESIDENT);
-  k_resident<M, TPB, MAXG><<<a.F, TPB, smem, s>>>(a);
+  k_resident<M, TPB, MAXR, INJ><<<a.F, TPB, smem, s>>>(a);
   PROF_END(KIND_RESIDENT);
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
 
+template <class M, bool INJ>
+int run_resident_t(Args& a, cudaStream_t s) {
+  constexpr int TPB = 512, RUN = 8;
+  const size_t smem = resident_smem<M>(a);
+  const int runs = (a.J + RUN * TPB - 1) / (RUN * TPB);   // runs of 8 children per thread
+  if (smem > kResidentSmemMax || runs > 4) return PPF_EUNSUPPORTED;
+  if (runs <= 1) return launch_resident<M, 1, INJ>(a, smem, s);
+  if (runs <= 2) return launch_resident<M, 2, INJ>(a, smem, s);
+  return launch_resident<M, 4, INJ>(a, smem, s);
+}
+
 template <class M>
 int run_resident(Args& a, cudaStream_t s) {
-  constexpr int TPB = 512;
-  const size_t smem = resident_smem<M>(a);
-  const int groups = (a.J + 4 * TPB - 1) / (4 * TPB);   // groups of 4 children per thread
-  if (smem > kResidentSmemMax || groups > 8) return PPF_EUNSUPPORTED;
-  if (groups <= 1) return launch_resident<M, 1>(a, smem, s);
-  if (groups <= 2) return launch_resident<M, 2>(a, smem, s);
-  if (groups <= 4) return launch_resident<M, 4>(a, smem, s);
-  return launch_resident<M, 8>(a, smem, s);
+  return (a.flags & PPF_F_INJECT) ? run_resident_t<M, true>(a, s) : run_resident_t<M, false>(a, s);
 }
 
 template <class M>
