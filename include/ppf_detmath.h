@@ -13,9 +13,10 @@
  *   pp_expf   Cody & Waite (1980) argument reduction x = k ln2 + r with a
  *             two-part ln2, then the Taylor series of e^r to degree 7
  *             (|r| <= ln2/2, truncation < 6e-9 relative), scaled by 2^k.
- *   pp_logf   x = m 2^e with m in [sqrt(1/2), sqrt(2)); log(m) = 2 atanh(s),
- *             s = (m-1)/(m+1), written as f - s (f - R) with f = m-1 and
- *             R = 2s^2/3 + 2s^4/5 + 2s^6/7 + 2s^8/9 (|s| <= 0.1716).
+ *   pp_logf   x = m 2^e with m in [sqrt(1/2), sqrt(2)); log(m) = log(1+f),
+ *             f = m - 1, by the division-free polynomial pp_log1p_red
+ *             (least-squares fit on Chebyshev nodes, see there), plus e ln2
+ *             with the two-part ln2.
  *   pp_sincos2pif  sin/cos of 2 pi u for u in [0,1): exact octant reduction
  *             of u, then Taylor series of sin and cos on [0, pi/4].
  * Accuracy (checked against double-precision libm in tests): <= 2 ulp.
@@ -91,6 +92,24 @@ PPF_HD float pp_expf(float x) {
   return (x != x) ? x : y;
 }
 
+/* log(1+f) for f in [sqrt(1/2)-1, sqrt(2)-1] as f - f^2/2 + f^3 R(f), R a
+ * degree-8 polynomial fitted by least squares on Chebyshev nodes of the
+ * interval (float64 fit, coefficients rounded to float32); < 0.75 ulp. */
+PPF_HD float pp_log1p_red(float f) {
+  float p = 0.07148932665586472f;
+  p = pp_fma(p, f, -0.1157151460647583f);
+  p = pp_fma(p, f, 0.1166200265288353f);
+  p = pp_fma(p, f, -0.12411021441221237f);
+  p = pp_fma(p, f, 0.14249871671199799f);
+  p = pp_fma(p, f, -0.1666848063468933f);
+  p = pp_fma(p, f, 0.2000070959329605f);
+  p = pp_fma(p, f, -0.24999989569187164f);
+  p = pp_fma(p, f, 0.3333333134651184f);
+  const float f2 = f * f;
+  const float f3 = f2 * f;
+  return f + pp_fma(f3, p, -0.5f * f2);
+}
+
 PPF_HD float pp_logf(float x) {
   /* main path on a safe input; special cases selected at the end */
   const int sub = x < 1.17549435082228750797e-38f;
@@ -101,15 +120,7 @@ PPF_HD float pp_logf(float x) {
   const int hi = m > 1.41421353816986083984375f;
   m = hi ? m * 0.5f : m;                                            /* [0.707, 1.414] */
   e += hi;
-  const float f = m - 1.0f;
-  const float s = f / (2.0f + f);
-  const float z = s * s;
-  float R = 0.2222222238779068f;                                     /* 2/9 */
-  R = pp_fma(R, z, 0.2857142984867096f);                             /* 2/7 */
-  R = pp_fma(R, z, 0.4000000059604645f);                             /* 2/5 */
-  R = pp_fma(R, z, 0.6666666865348816f);                             /* 2/3 */
-  R = R * z;
-  const float lm = f - s * (f - R);
+  const float lm = pp_log1p_red(m - 1.0f);
   const float ef = (float)e;
   const float lo = pp_fma(ef, 1.428606765330187045e-06f, lm);
   float y = pp_fma(ef, 0.693145751953125f, lo);
@@ -126,15 +137,7 @@ PPF_HD float pp_log_unit(float x) {
   int e = (int)((b >> 23) & 0xffu) - 127;
   float m = pp_u2f((b & 0x007fffffu) | 0x3f800000u);
   if (m > 1.41421353816986083984375f) { m = m * 0.5f; e += 1; }
-  const float f = m - 1.0f;
-  const float s = f / (2.0f + f);
-  const float z = s * s;
-  float R = 0.2222222238779068f;
-  R = pp_fma(R, z, 0.2857142984867096f);
-  R = pp_fma(R, z, 0.4000000059604645f);
-  R = pp_fma(R, z, 0.6666666865348816f);
-  R = R * z;
-  const float lm = f - s * (f - R);
+  const float lm = pp_log1p_red(m - 1.0f);
   const float ef = (float)e;
   const float lo = pp_fma(ef, 1.428606765330187045e-06f, lm);
   return pp_fma(ef, 0.693145751953125f, lo);

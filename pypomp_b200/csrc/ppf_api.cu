@@ -33,6 +33,7 @@ static size_t carve(Args& a, int path, unsigned char* base) {
     a.excl = reinterpret_cast<uint64_t*>(take(8ull * a.F * a.ntiles));
     a.tot = reinterpret_cast<uint64_t*>(take(8ull * a.F));
     a.ctrl_bytes = off;
+    a.consts = take(512ull * a.F);
     for (int i = 0; i < 2; ++i) a.X[i] = reinterpret_cast<float*>(take(4ull * a.F * dx * a.J));
     for (int i = 0; i < 2; ++i) a.W[i] = reinterpret_cast<float*>(take(4ull * a.F * a.J));
   } else if (path == PPF_PATH_PLAIN) {

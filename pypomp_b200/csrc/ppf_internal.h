@@ -50,6 +50,7 @@ struct Args {
   uint64_t* tot;          // [F]
   float* X[2];            // [F][dx][J] each
   float* W[2];            // [F][J] each
+  unsigned char* consts;  // [F][512 B] per-filter model constants
   int tile, ntiles;
   size_t ctrl_bytes;      // leading workspace bytes zeroed per call
   // plain path

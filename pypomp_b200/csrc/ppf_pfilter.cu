@@ -216,6 +216,37 @@ __device__ __forceinline__ int nchild_fast(const Offsets& o, uint64_t C) {
   return nonpos ? 0 : (int)k;
 }
 
+// Incremental form for consecutive parents: with P = k tot + chi and
+// D = C J, a parent of weight q moves D by q J (< 2^62) and its children are
+// the points P < D passed while advancing k.  No floating point, no division.
+struct OffWalk {
+  uint64_t Dh, Dl, Ph, Pl;
+  int k;
+};
+
+__device__ __forceinline__ OffWalk offwalk_init(const Offsets& o, uint64_t C) {
+  OffWalk w;
+  w.k = nchild_fast(o, C);
+  mul64(C, (uint64_t)o.J, w.Dh, w.Dl);
+  mul64((uint64_t)w.k, o.tot, w.Ph, w.Pl);
+  w.Pl += o.chi;
+  w.Ph += (w.Pl < o.chi);
+  return w;
+}
+
+// Add a parent of weight q; returns nchild of the new cumulative weight.
+__device__ __forceinline__ int offwalk_add(const Offsets& o, OffWalk& w, uint64_t q) {
+  const uint64_t add = q * (uint64_t)o.J;
+  w.Dl += add;
+  w.Dh += (w.Dl < add);
+  while (w.k < o.J && lt128(w.Ph, w.Pl, w.Dh, w.Dl)) {
+    w.Pl += o.tot;
+    w.Ph += (w.Pl < o.tot);
+    ++w.k;
+  }
+  return w.k;
+}
+
 // Parent (tile-local index) of child k: the last l in [0, n) with st[l] <= k.
 __device__ __forceinline__ int find_parent(const int* st, int n, int k) {
   int lo = 0, hi = n;
@@ -230,6 +261,28 @@ __device__ __forceinline__ int find_parent(const int* st, int n, int k) {
 // ============================================================================
 // STREAM path
 // ============================================================================
+
+// Per-filter model constants, computed once per call (Cholesky factors, log
+// determinants, transformed parameters) and copied by every block.
+constexpr int kConstStride = 512;   // bytes per filter in the workspace
+
+template <class M>
+__global__ void k_prep(Args a) {
+  static_assert(sizeof(typename M::Consts) <= kConstStride, "Consts stride");
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= a.F) return;
+  typename M::Consts c;
+  M::prepare(c, a.theta + (size_t)f * a.model.n_params, a.model, (a.flags & PPF_F_EST) != 0);
+  *reinterpret_cast<typename M::Consts*>(a.consts + (size_t)f * kConstStride) = c;
+}
+
+template <class M>
+__device__ __forceinline__ void load_consts(const Args& a, int f, typename M::Consts& c) {
+  constexpr int NW = (sizeof(typename M::Consts) + 3) / 4;
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(a.consts + (size_t)f * kConstStride);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&c);
+  for (int i = threadIdx.x; i < NW; i += blockDim.x) dst[i] = src[i];
+}
 
 // Store the 4 children k0..k0+3 (valid[e]) of one group: float4 stores when
 // the whole group is valid and rows are 16-byte aligned (J % 4 == 0).
@@ -264,7 +317,7 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
   constexpr int DX = M::MAXDX;
   const int f = blockIdx.y;
   const int u = filter_unit(a, f);
-  if (threadIdx.x == 0) M::prepare(c, a.theta + (size_t)f * a.model.n_params, a.model, (a.flags & PPF_F_EST) != 0);
+  load_consts<M>(a, f, c);
   __syncthreads();
   const typename M::Consts cr = c;
   Obs<M> ob;
@@ -463,6 +516,8 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a
   float* xs = reinterpret_cast<float*>(smem_raw);                              // [DX][TILE]
   int* st = reinterpret_cast<int*>(smem_raw + sizeof(float) * DX * TILE);      // [TILE + 1]
   float* wcar = reinterpret_cast<float*>(st + TILE + 4);                      // [TILE] (no-resample steps)
+  float* wsm = wcar;                                                           // W row lands here first
+  __shared__ __align__(8) uint64_t bar[2];                                     // [0]: W row, [1]: X rows
   __shared__ typename M::Consts c;
   __shared__ uint64_t s_scan[TPB / 32 + 1];
   __shared__ unsigned int smk[2 * (TPB / 32)];
@@ -484,15 +539,34 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a
   if (b == 0 && threadIdx.x == 0) finalize_step(a, f, t, acc, tot, a.loglik + f);
   const bool last = (t == Tf - 1);
   if (last && !a.anc) return;
-  if (threadIdx.x == 0) M::prepare(c, a.theta + (size_t)f * a.model.n_params, a.model, (a.flags & PPF_F_EST) != 0);
+  const int J = a.J;
+  const int jt = b * TILE;
+  const int ntile = min(TILE, J - jt);
+  // Rows of this tile are contiguous: with J % 4 == 0 every row starts
+  // 16-byte aligned and ntile is a multiple of 4, so one thread issues TMA
+  // bulk copies of the W row and the DX state rows into shared memory; the
+  // parent-phase arithmetic below overlaps the state copies.
+  const bool bulk = (J & 3) == 0;
+  const float* Wc = a.W[p] + (size_t)f * J;
+  const float* Xc = a.X[p] + (size_t)f * DX * J;
+  if (bulk) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      fence_mbar_init();
+      mbar_expect_tx(&bar[0], (uint32_t)(ntile * 4));
+      bulk_g2s(wsm, Wc + jt, (uint32_t)(ntile * 4), &bar[0]);
+      mbar_expect_tx(&bar[1], (uint32_t)(ntile * 4 * DX));
+#pragma unroll
+      for (int d = 0; d < DX; ++d) bulk_g2s(xs + d * TILE, Xc + (size_t)d * J + jt, (uint32_t)(ntile * 4), &bar[1]);
+    }
+  }
+  load_consts<M>(a, f, c);
   const bool nanf = acc.nan != 0;
   const float Mx = keyf(acc.maxkey);
   const bool collapsed = !nanf && Mx == -INFINITY;
   const bool qc = nanf || Mx == -INFINITY;
   const bool rs = decide_resample(a, acc);
-  const int J = a.J;
-  const float* Xc = a.X[p] + (size_t)f * DX * J;
-  const float* Wc = a.W[p] + (size_t)f * J;
   float* Xn = a.X[p ^ 1] + (size_t)f * DX * J;
   float* Wn = a.W[p ^ 1] + (size_t)f * J;
   int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
@@ -505,19 +579,23 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a
 #pragma unroll
   for (int d = 0; d < DX; ++d) px[d] = 0.0;
   const float base = (a.mode == MODE_MOP) ? 0.0f : a.base_rs;
-  const int jt = b * TILE;
-  const int ntile = min(TILE, J - jt);
   const int l0 = threadIdx.x * IT;
+  __syncthreads();   // barrier init visible to all threads
+  bool ok = true;
+  if (bulk) ok = mbar_wait(&bar[0], 0);
 
   // 1-2. parents: CDF and first-child offsets (or identity), staged states
   {
     float wv[IT];
-    if (l0 + IT <= ntile && (J & 3) == 0) {
+    if (bulk && l0 + IT <= ntile) {
 #pragma unroll
       for (int i = 0; i < IT; i += 4) {
-        const float4 v4 = *reinterpret_cast<const float4*>(Wc + jt + l0 + i);
+        const float4 v4 = *reinterpret_cast<const float4*>(wsm + l0 + i);
         wv[i] = v4.x; wv[i + 1] = v4.y; wv[i + 2] = v4.z; wv[i + 3] = v4.w;
       }
+    } else if (bulk) {
+#pragma unroll
+      for (int i = 0; i < IT; ++i) wv[i] = (l0 + i < ntile) ? wsm[l0 + i] : 0.0f;
     } else {
 #pragma unroll
       for (int i = 0; i < IT; ++i) wv[i] = (l0 + i < ntile) ? Wc[jt + l0 + i] : 0.0f;
@@ -534,13 +612,16 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a
       }
       uint64_t btot;
       const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
-      uint64_t C = E + tex;
+      if (l0 < ntile) {
+        OffWalk wk = offwalk_init(o, E + tex);
+        st[l0] = wk.k;
 #pragma unroll
-      for (int i = 0; i < IT; ++i) {
-        if (l0 + i < ntile) st[l0 + i] = nchild_fast(o, C);
-        C += q[i];
+        for (int i = 0; i < IT; ++i) {
+          if (l0 + i >= ntile) break;
+          const int kn = offwalk_add(o, wk, q[i]);
+          if (i + 1 < IT || l0 + i + 1 == ntile) st[l0 + i + 1] = kn;
+        }
       }
-      if (l0 < ntile && l0 + IT >= ntile) st[ntile] = nchild_fast(o, E + btot);
     } else {
       float lt32 = 0.0f;
       if (nanf) lt32 = __int_as_float(0x7fc00000);
@@ -555,9 +636,14 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a
       if (l0 < ntile && l0 + IT >= ntile) st[ntile] = jt + ntile;
     }
   }
-  for (int l = threadIdx.x; l < ntile; l += TPB)
+  if (bulk) {
+    if (!mbar_wait(&bar[1], 0)) ok = false;
+  } else {
+    for (int l = threadIdx.x; l < ntile; l += TPB)
 #pragma unroll
-    for (int d = 0; d < DX; ++d) xs[d * TILE + l] = Xc[d * J + jt + l];
+      for (int d = 0; d < DX; ++d) xs[d * TILE + l] = Xc[d * J + jt + l];
+  }
+  if (!ok && threadIdx.x == 0) atomicOr(a.err, 1u);
   __syncthreads();
   const typename M::Consts cr = c;
   const int klo = st[0], khi = st[ntile];
@@ -745,10 +831,12 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     //     without resampling the carried weight replaces ws in place
     if (rs) {
       const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
-      uint64_t C = tex;
-      for (int j = l0; j < l1; ++j) {
-        st[j] = nchild_fast(o, C);
-        C += qweight(ws[j], Mx, qc);
+      if (l0 < l1) {
+        OffWalk wk = offwalk_init(o, tex);
+        for (int j = l0; j < l1; ++j) {
+          st[j] = wk.k;
+          offwalk_add(o, wk, qweight(ws[j], Mx, qc));
+        }
       }
     } else {
       float lt32 = 0.0f;
@@ -1008,6 +1096,7 @@ int run_stream_t(Args& a, cudaStream_t s) {
                            (int)smem) != cudaSuccess)
     return PPF_ECUDA;
   dim3 grid(a.ntiles, a.F);
+  k_prep<M><<<(a.F + 127) / 128, 128, 0, s>>>(a);
   PROF_BEGIN(KIND_INIT);
   k_init<M, TPB, INJ><<<grid, TPB, 0, s>>>(a);
   PROF_END(KIND_INIT);
