@@ -325,7 +325,8 @@ def run_ours(args):
 
 def run_profile_case(args):
     """A small case of the same kernels for ncu captures: the headline model
-    and J, 8 seeds, the first 12 observations, one call."""
+    and J, 24 seeds (state 2 x 24 x 262144 x 12 B = 151 MB, larger than L2),
+    the first 12 observations, one call."""
     import torch
 
     from pypomp_b200 import functional as F
@@ -333,8 +334,8 @@ def run_profile_case(args):
     m = workload()
     st = m.to_struct()
     st.ys = st.ys[:12]
-    th = np.repeat(m.theta.to_array(m.canonical_param_names), 8, axis=0).astype(np.float32)
-    out = F.run_pfilter(st, th, np.arange(8, dtype=np.uint64), J, path=args.path)
+    th = np.repeat(m.theta.to_array(m.canonical_param_names), 24, axis=0).astype(np.float32)
+    out = F.run_pfilter(st, th, np.arange(24, dtype=np.uint64), J, path=args.path)
     torch.cuda.synchronize()
     print("profile case logLik", out["loglik"][:2])
 
