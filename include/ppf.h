@@ -113,6 +113,39 @@ typedef struct ppf_pfilter_desc {
   size_t ws_bytes;
 } ppf_pfilter_desc;
 
+/* MOP-alpha objective and gradient over F filters.  Replaces _mop_internal /
+ * _mop_step (pypomp/core/algorithms/mop.py:19-135) vmapped over parameter
+ * sets (mop.py:138) and its jax.value_and_grad (ad_helpers.py:32-54).
+ * theta is on the ESTIMATION scale (the model's from_est is applied on the
+ * device, mop.py:16).  value[f] = -sum_t ll_t (the negative MOP
+ * log-likelihood); grad[f][p] = d value[f] / d theta[f][p] on the estimation
+ * scale, from the adjoint sweep over stored ancestors with state checkpoints
+ * every ckpt_every steps (0: ceil(sqrt(T))). */
+typedef struct ppf_mop_desc {
+  ppf_model model;
+  int32_t J, F, T, U;
+  uint32_t flags;         /* PPF_F_INJECT only */
+  float alpha;            /* MOP discount in [0, 1] */
+  int32_t ckpt_every;     /* 0 = ceil(sqrt(T)) */
+  const float* theta;     /* [F][P] estimation scale */
+  const float* ys;        /* [U][T][dy] */
+  const float* ycon;      /* [U][T] or NULL */
+  const int32_t* unit;    /* [F] or NULL */
+  const int32_t* T_u;     /* [U] or NULL */
+  const uint64_t* seeds;  /* [F] */
+  const float* inj_z0;
+  const float* inj_z;
+  const float* inj_u;
+  double* value;          /* out [F] */
+  double* grad;           /* out [F][P] or NULL (value only) */
+  int32_t* anc;           /* optional out [F][T][J] resampling ancestors */
+  void* workspace;
+  size_t ws_bytes;
+} ppf_mop_desc;
+
+size_t ppf_mop_workspace_bytes(const ppf_mop_desc* d);
+int ppf_mop(const ppf_mop_desc* d, void* stream);
+
 /* Workspace bytes ppf_pfilter needs for this descriptor (pointers ignored). */
 size_t ppf_pfilter_workspace_bytes(const ppf_pfilter_desc* d);
 

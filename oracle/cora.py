@@ -35,6 +35,8 @@ def lib():
     L = ctypes.CDLL(str(_SO))
     L.ppfo_pfilter.argtypes = [ctypes.POINTER(_Desc), ctypes.c_int, ctypes.c_int]
     L.ppfo_pfilter.restype = ctypes.c_int
+    L.ppfo_mop_surrogate.argtypes = [ctypes.POINTER(_Desc), ctypes.c_float, _vp, _vp, _vp, _vp]
+    L.ppfo_mop_surrogate.restype = ctypes.c_int
     L.ppfo_expf.argtypes = [ctypes.c_float]
     L.ppfo_expf.restype = ctypes.c_float
     L.ppfo_logf.argtypes = [ctypes.c_float]
@@ -124,6 +126,51 @@ def pfilter(kind, dx, dy, theta_f, ys, J, *, seeds=None, ycon=None, unit=None, T
         raise RuntimeError(f"oracle returned {rc}")
     del keep
     return out
+
+
+def mop_surrogate(kind, dx, dy, theta_est, ys, J, alpha, anc, m0=None, *, seeds=None,
+                  ycon=None, dt=0.0, inject=None):
+    """MOP-alpha surrogate value (frozen ancestry, frozen stop_gradient(m)).
+
+    ``anc`` (F,T,J) ancestors; ``m0`` (F,T,J) or None to record it.  Returns
+    ``(value (F,), m0 (F,T,J))``."""
+    theta_est = np.ascontiguousarray(np.atleast_2d(theta_est), dtype=np.float32)
+    F, P = theta_est.shape
+    ys = np.ascontiguousarray(ys, dtype=np.float32)
+    if ys.ndim == 2:
+        ys = ys[None]
+    U, T, _ = ys.shape
+    keep = [theta_est, ys]
+    d = _Desc()
+    d.model = _Model(kind, dx, dy, P, dt, 0)
+    d.J, d.F, d.T, d.U = J, F, T, U
+    flags = 128
+    d.theta, d.ys = _p(theta_est), _p(ys)
+    if ycon is not None:
+        ycon = np.ascontiguousarray(ycon, dtype=np.float32)
+        keep.append(ycon)
+        d.ycon = _p(ycon)
+    if seeds is not None:
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+        keep.append(seeds)
+        d.seeds = _p(seeds)
+    if inject is not None:
+        flags |= 16
+        for k, name in (("z0", "inj_z0"), ("z", "inj_z"), ("u", "inj_u")):
+            if inject.get(k) is not None:
+                a = np.ascontiguousarray(inject[k], dtype=np.float32)
+                keep.append(a)
+                setattr(d, name, _p(a))
+    d.flags = flags
+    anc = np.ascontiguousarray(anc, dtype=np.int32)
+    m0_out = np.zeros((F, T, J), np.float32)
+    m0_in = None if m0 is None else np.ascontiguousarray(m0, dtype=np.float32)
+    value = np.zeros(F, np.float64)
+    rc = _L().ppfo_mop_surrogate(ctypes.byref(d), float(alpha), _p(anc), _p(m0_in), _p(m0_out), _p(value))
+    if rc != 0:
+        raise RuntimeError(f"oracle returned {rc}")
+    del keep
+    return value, (m0_out if m0 is None else m0_in)
 
 
 def expf(x):

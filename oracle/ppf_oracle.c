@@ -363,6 +363,70 @@ int ppfo_pfilter(const ppf_pfilter_desc* d, int mop, int nthreads) {
   return PPF_OK;
 }
 
+/* MOP-alpha surrogate for gradient checks (mop.py:69-135 as a function of
+ * theta with the discrete choices frozen): ancestors anc[F][T][J] are given,
+ * and stop_gradient(m) is the constant m0[F][T][J] recorded at the base
+ * parameters (pass m0_in = NULL to record it into m0_out).  In float64:
+ *   wP = alpha wF;  ll_t = LSE(wP + m) - LSE(wP);  wF = (wP + m - m0)[anc]
+ * value[f] = -sum_t ll_t.  At the base parameters it equals the MOP value; its
+ * derivative there is the MOP-alpha gradient. */
+static double lse(const double* v, int n) {
+  double mx = -INFINITY;
+  for (int i = 0; i < n; ++i) mx = v[i] > mx ? v[i] : mx;
+  if (!(mx > -INFINITY)) return mx;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += exp(v[i] - mx);
+  return mx + log(s);
+}
+
+int ppfo_mop_surrogate(const ppf_pfilter_desc* d, float alpha, const int* anc, const float* m0_in,
+                       float* m0_out, double* value) {
+  const int J = d->J, dx = d->model.dx, T = d->T;
+  for (int f = 0; f < d->F; ++f) {
+    const int u = d->unit ? d->unit[f] : 0;
+    consts_t c;
+    prepare(&c, d->theta + (size_t)f * d->model.n_params, &d->model, (d->flags & PPF_F_EST) != 0);
+    float* x = (float*)malloc(sizeof(float) * dx * J);
+    float* xp = (float*)malloc(sizeof(float) * dx * J);
+    double* wF = (double*)malloc(sizeof(double) * J);
+    double* wP = (double*)malloc(sizeof(double) * J);
+    double* v = (double*)malloc(sizeof(double) * J);
+    float* m = (float*)malloc(sizeof(float) * J);
+    for (int j = 0; j < J; ++j) {
+      float z[4], xj[4];
+      noise(d, f, j, 0, n_init(&c), z);
+      rinit(&c, z, xj);
+      for (int k = 0; k < dx; ++k) x[k * J + j] = xj[k];
+      wF[j] = -log((double)J);
+    }
+    double ll = 0.0;
+    for (int t = 0; t < T; ++t) {
+      for (int j = 0; j < J; ++j) {
+        wP[j] = (double)alpha * wF[j];
+        float xj[4];
+        for (int k = 0; k < dx; ++k) xj[k] = x[k * J + j];
+        m[j] = propagate(d, &c, f, u, j, t, xj);
+        for (int k = 0; k < dx; ++k) xp[k * J + j] = xj[k];
+        v[j] = wP[j] + (double)m[j];
+      }
+      const double a1 = lse(v, J), a2 = lse(wP, J);
+      ll += a1 - a2;
+      const float* m0 = m0_in ? m0_in + ((size_t)f * T + t) * J : m;
+      if (!m0_in && m0_out) memcpy(m0_out + ((size_t)f * T + t) * J, m, sizeof(float) * J);
+      const int* at = anc + ((size_t)f * T + t) * J;
+      for (int k = 0; k < J; ++k) {
+        const int j = at[k];
+        for (int q = 0; q < dx; ++q) x[q * J + k] = xp[q * J + j];
+        v[k] = wP[j] + (double)m[j] - (double)m0[j];
+      }
+      memcpy(wF, v, sizeof(double) * J);
+    }
+    value[f] = -ll;
+    free(x); free(xp); free(wF); free(wP); free(v); free(m);
+  }
+  return PPF_OK;
+}
+
 /* Elementary functions and Philox, exported for the tests that pin them. */
 float ppfo_expf(float x) { return pp_expf(x); }
 float ppfo_logf(float x) { return pp_logf(x); }

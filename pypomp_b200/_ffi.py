@@ -36,6 +36,8 @@ PATHS = {"auto": PATH_AUTO, "plain": PATH_PLAIN, "stream": PATH_STREAM, "residen
 EXPORTED = (
     "ppf_pfilter_workspace_bytes",
     "ppf_pfilter",
+    "ppf_mop_workspace_bytes",
+    "ppf_mop",
     "ppf_workspace_status",
     "ppf_profile_begin",
     "ppf_profile_end",
@@ -89,6 +91,33 @@ class PfilterDesc(ctypes.Structure):
     ]
 
 
+class MopDesc(ctypes.Structure):
+    _fields_ = [
+        ("model", PpfModel),
+        ("J", ctypes.c_int32),
+        ("F", ctypes.c_int32),
+        ("T", ctypes.c_int32),
+        ("U", ctypes.c_int32),
+        ("flags", ctypes.c_uint32),
+        ("alpha", ctypes.c_float),
+        ("ckpt_every", ctypes.c_int32),
+        ("theta", _vp),
+        ("ys", _vp),
+        ("ycon", _vp),
+        ("unit", _vp),
+        ("T_u", _vp),
+        ("seeds", _vp),
+        ("inj_z0", _vp),
+        ("inj_z", _vp),
+        ("inj_u", _vp),
+        ("value", _vp),
+        ("grad", _vp),
+        ("anc", _vp),
+        ("workspace", _vp),
+        ("ws_bytes", ctypes.c_size_t),
+    ]
+
+
 class PpfError(RuntimeError):
     """A non-zero return code from libppf.so."""
 
@@ -109,6 +138,10 @@ def _load():
     lib.ppf_pfilter_workspace_bytes.restype = ctypes.c_size_t
     lib.ppf_pfilter.argtypes = [ctypes.POINTER(PfilterDesc), _vp]
     lib.ppf_pfilter.restype = ctypes.c_int
+    lib.ppf_mop_workspace_bytes.argtypes = [ctypes.POINTER(MopDesc)]
+    lib.ppf_mop_workspace_bytes.restype = ctypes.c_size_t
+    lib.ppf_mop.argtypes = [ctypes.POINTER(MopDesc), _vp]
+    lib.ppf_mop.restype = ctypes.c_int
     lib.ppf_workspace_status.argtypes = [_vp, _vp]
     lib.ppf_workspace_status.restype = ctypes.c_int
     lib.ppf_profile_begin.argtypes = []

@@ -132,6 +132,62 @@ static int validate(const ppf_pfilter_desc* d) {
   return PPF_OK;
 }
 
+// MOP: stream-path carve plus the adjoint working set.
+static size_t carve_mop(Args& a, MopWork& w, const ppf_mop_desc* d, unsigned char* base) {
+  size_t off = carve(a, PPF_PATH_STREAM, base);
+  auto take = [&](size_t bytes) -> unsigned char* {
+    unsigned char* p = base ? base + off : nullptr;
+    off = align_up(off + bytes);
+    return p;
+  };
+  const int dx = a.model.dx;
+  const size_t F = a.F, T = a.T, J = a.J;
+  int L = d->ckpt_every;
+  if (L <= 0) {
+    L = 1;
+    while ((size_t)L * L < T) ++L;
+  }
+  a.ckpt_every = L;
+  a.nseg = (int)((T + L - 1) / L);
+  int32_t* anc = reinterpret_cast<int32_t*>(take(d->anc ? 0 : 4 * F * T * J));
+  a.anc = d->anc ? d->anc : anc;
+  a.mop_off = reinterpret_cast<int*>(take(4 * F * T * (J + 1)));
+  a.mop_ckpt = reinterpret_cast<float*>(take(4 * F * a.nseg * dx * J));
+  a.mop_M = reinterpret_cast<float*>(take(4 * F * T));
+  a.mop_S = reinterpret_cast<double*>(take(8 * F * T));
+  w.sb = reinterpret_cast<float*>(take(4 * F * L * dx * J));
+  w.lx = reinterpret_cast<float*>(take(4 * 2 * F * dx * J));
+  w.lw = reinterpret_cast<float*>(take(4 * 2 * F * J));
+  w.gnat = reinterpret_cast<double*>(take(8 * F * 64));
+  return off;
+}
+
+static int validate_mop(const ppf_mop_desc* d) {
+  if (!d) return PPF_EINVAL;
+  if (d->J < 1 || d->J > PPF_MAX_J || d->F < 1 || d->T < 1 || d->U < 1) return PPF_EINVAL;
+  int rc = check_model(d->model);
+  if (rc) return rc;
+  if (!d->theta || !d->ys || !d->value) return PPF_EINVAL;
+  if (!(d->flags & PPF_F_INJECT) && !d->seeds) return PPF_EINVAL;
+  if ((d->flags & PPF_F_INJECT) && (!d->inj_z || !d->inj_u)) return PPF_EINVAL;
+  if ((d->flags & PPF_F_INJECT) && d->model.kind == PPF_MODEL_LG && !d->inj_z0) return PPF_EINVAL;
+  if (d->model.kind == PPF_MODEL_RICKER && !d->ycon) return PPF_EINVAL;
+  if (!(d->alpha >= 0.0f && d->alpha <= 1.0f)) return PPF_EINVAL;
+  return PPF_OK;
+}
+
+static void mop_to_pfilter(const ppf_mop_desc* d, ppf_pfilter_desc* p) {
+  memset(p, 0, sizeof(*p));
+  p->model = d->model;
+  p->J = d->J; p->F = d->F; p->T = d->T; p->U = d->U;
+  p->path = PPF_PATH_STREAM;
+  p->flags = (d->flags & PPF_F_INJECT) | PPF_F_EST;
+  p->thresh = 0.0f;
+  p->theta = d->theta; p->ys = d->ys; p->ycon = d->ycon; p->unit = d->unit; p->T_u = d->T_u;
+  p->seeds = d->seeds; p->inj_z0 = d->inj_z0; p->inj_z = d->inj_z; p->inj_u = d->inj_u;
+  p->loglik = d->value;
+}
+
 }  // namespace ppf
 
 using namespace ppf;
@@ -163,6 +219,49 @@ int ppf_pfilter(const ppf_pfilter_desc* d, void* stream) {
   }
   rc = run_pfilter_path(a, path, s);
   return rc;
+}
+
+size_t ppf_mop_workspace_bytes(const ppf_mop_desc* d) {
+  if (!d || d->J < 1 || d->F < 1 || d->T < 1) return 0;
+  ppf_pfilter_desc p;
+  mop_to_pfilter(d, &p);
+  Args a;
+  fill_args(&p, a, MODE_MOP);
+  MopWork w;
+  memset(&w, 0, sizeof(w));
+  return carve_mop(a, w, d, nullptr);
+}
+
+// value = -sum_t ll_t: the forward accumulates +ll into `value`, then a tiny
+// kernel negates it (same stream).
+__global__ void k_negate(double* v, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = -v[i];
+}
+
+int ppf_mop(const ppf_mop_desc* d, void* stream) {
+  int rc = validate_mop(d);
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  ppf_pfilter_desc p;
+  mop_to_pfilter(d, &p);
+  Args a;
+  fill_args(&p, a, MODE_MOP);
+  a.flags |= PPF_F_SAVE_ANC;
+  MopWork w;
+  memset(&w, 0, sizeof(w));
+  const size_t need = carve_mop(a, w, d, nullptr);
+  if (!d->workspace || d->ws_bytes < need) return PPF_EINVAL;
+  carve_mop(a, w, d, reinterpret_cast<unsigned char*>(d->workspace));
+  w.grad = d->grad;
+  w.alpha = d->alpha;
+  if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, s) != cudaSuccess) return PPF_ECUDA;
+  rc = reset_accumulators(a, s);
+  if (rc) return rc;
+  rc = run_mop(a, w, s);
+  if (rc) return rc;
+  k_negate<<<(d->F + 127) / 128, 128, 0, s>>>(d->value, d->F);
+  return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
 
 int ppf_workspace_status(const void* workspace, void* stream) {

@@ -59,6 +59,13 @@ struct Args {
   uint64_t* pl_boff;      // [nblk]
   int* pl_anc;            // [J]
   int* pl_carry_dev;      // [1]
+  // MOP forward saves (stream path, MODE_MOP): first-child offsets, state
+  // checkpoints every ckpt_every steps, per-step max and weight sum of m.
+  int* mop_off;           // [F][T][J+1]
+  float* mop_ckpt;        // [F][nseg][DX][J]
+  int ckpt_every, nseg;
+  float* mop_M;           // [F][T]
+  double* mop_S;          // [F][T]
   // host copies for host-side loops (plain path)
   const int* T_u_host;
   const int* unit_host;
@@ -75,8 +82,22 @@ struct Profiler {
   void mark(int kind, cudaStream_t s, bool start);
 };
 extern Profiler g_prof;
+#define PROF_BEGIN(kind) ::ppf::g_prof.mark(kind, s, true)
+#define PROF_END(kind) ::ppf::g_prof.mark(kind, s, false)
+
+// MOP adjoint working set (workspace carve-outs) and outputs.
+struct MopWork {
+  float* lx;      // [2][F][DX][J]
+  float* lw;      // [2][F][J]
+  float* sb;      // [F][ckpt_every][DX][J] recomputed states of one segment
+  double* gnat;   // [F][64] natural-scale gradient sums
+  double* grad;   // out [F][P] estimation-scale gradient, or nullptr
+  float alpha;
+};
 
 int run_pfilter_path(Args& a, int path, cudaStream_t s);
+int run_stream_any(Args& a, cudaStream_t s);   // stream path, any model
+int run_mop(Args& a, const MopWork& w, cudaStream_t s);
 int reset_accumulators(Args& a, cudaStream_t s);
 size_t resident_smem_bytes(const Args& a);
 

@@ -126,6 +126,96 @@ struct LG {
     }
     return pp_fma(-0.5f, q, c.c0);
   }
+
+  // ---- adjoint (MOP-alpha gradient).  Natural-scale gradient in a padded
+  // layout with static indices: A[DX*DX] | C[4*DX] | LQ tril(DX) | LR tril(4)
+  // | X0[DX]; the host maps it to the canonical order.
+  static constexpr int NQ = DX * (DX + 1) / 2;
+  static constexpr int GA = 0, GC = DX * DX, GQ = GC + 4 * DX, GR = GQ + NQ, GX0 = GR + 10;
+  static constexpr int NG = GX0 + DX;
+  struct Keep {
+    float xP[DX];
+    float s[MAXDY];
+  };
+  __device__ static float fwd_keep(const Consts& c, const float* y, float, const float* xin,
+                                   const float* z, Keep& k) {
+#pragma unroll
+    for (int i = 0; i < DX; ++i) k.xP[i] = xin[i];
+    rproc(c, k.xP, z);
+    float q = 0.0f;
+#pragma unroll
+    for (int i = 0; i < MAXDY; ++i) {
+      k.s[i] = 0.0f;
+      if (i < c.dy) {
+        float a = 0.0f;
+#pragma unroll
+        for (int kk = 0; kk < DX; ++kk) a = pp_fma(c.C[i * 4 + kk], k.xP[kk], a);
+        float r = y[i] - a;
+#pragma unroll
+        for (int l = 0; l < i; ++l) r = pp_fma(-c.L[i * 4 + l], k.s[l], r);
+        k.s[i] = r * c.Linv[i];
+        q = pp_fma(k.s[i], k.s[i], q);
+      }
+    }
+    return pp_fma(-0.5f, q, c.c0);
+  }
+  // lx: in = adjoint of x^P from the children, out = adjoint of xin.
+  __device__ static void bwd(const Consts& c, const float* xin, const float* z, const Keep& k,
+                             float lm, float* lx, float* g) {
+    // v = L^-T s
+    float v[MAXDY];
+#pragma unroll
+    for (int i = MAXDY - 1; i >= 0; --i) {
+      v[i] = 0.0f;
+      if (i < c.dy) {
+        float r = k.s[i];
+#pragma unroll
+        for (int l = i + 1; l < MAXDY; ++l)
+          if (l < c.dy) r = r - c.L[l * 4 + i] * v[l];
+        v[i] = r * c.Linv[i];
+      }
+    }
+    float lxP[DX];
+#pragma unroll
+    for (int kk = 0; kk < DX; ++kk) {
+      float a = lx[kk];
+#pragma unroll
+      for (int i = 0; i < MAXDY; ++i)
+        if (i < c.dy) a = a + lm * c.C[i * 4 + kk] * v[i];
+      lxP[kk] = a;
+    }
+#pragma unroll
+    for (int i = 0; i < MAXDY; ++i)
+      if (i < c.dy) {
+#pragma unroll
+        for (int kk = 0; kk < DX; ++kk) g[GC + i * DX + kk] += lm * v[i] * k.xP[kk];
+#pragma unroll
+        for (int l = 0; l <= i; ++l) g[GR + i * (i + 1) / 2 + l] += lm * v[i] * k.s[l];
+        g[GR + i * (i + 1) / 2 + i] -= lm * c.Linv[i];
+      }
+#pragma unroll
+    for (int i = 0; i < DX; ++i) {
+#pragma unroll
+      for (int kk = 0; kk < DX; ++kk) g[GA + i * DX + kk] += lxP[i] * xin[kk];
+#pragma unroll
+      for (int kk = 0; kk <= i; ++kk) g[GQ + i * (i + 1) / 2 + kk] += lxP[i] * z[kk];
+    }
+#pragma unroll
+    for (int kk = 0; kk < DX; ++kk) {
+      float a = 0.0f;
+#pragma unroll
+      for (int i = 0; i < DX; ++i) a = a + c.A[i * 4 + kk] * lxP[i];
+      lx[kk] = a;
+    }
+  }
+  __device__ static void bwd_init(const Consts&, const float* z0, const float* lx0, float* g) {
+#pragma unroll
+    for (int i = 0; i < DX; ++i) {
+      g[GX0 + i] += lx0[i];
+#pragma unroll
+      for (int kk = 0; kk <= i; ++kk) g[GQ + i * (i + 1) / 2 + kk] += lx0[i] * z0[kk];
+    }
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -189,6 +279,53 @@ struct SV {
     const float r = (y[0] - mean) / (c.rhoc * sd);
     return pp_fma(-0.5f * r, r, pp_fma(-0.5f, v, c.c0));
   }
+
+  // ---- adjoint: natural-scale gradient in canonical order
+  // (kappa, theta, xi, rho, mu, v0).
+  static constexpr int NG = 6;
+  struct Keep {
+    float xP[2];
+    float emh, sd, r, A;
+  };
+  __device__ static float fwd_keep(const Consts& c, const float* y, float, const float* xin,
+                                   const float* z, Keep& k) {
+    k.xP[0] = xin[0];
+    k.xP[1] = xin[1];
+    k.emh = pp_expf(-0.5f * xin[0]);
+    rproc(c, k.xP, z);
+    const float v = k.xP[0];
+    k.sd = pp_expf(0.5f * v) * c.sqdt;
+    const float mean = pp_fma(c.rho * k.sd, k.xP[1], c.mudt);
+    k.r = (y[0] - mean) / (c.rhoc * k.sd);
+    k.A = (y[0] - c.mudt) / k.sd;
+    return pp_fma(-0.5f * k.r, k.r, pp_fma(-0.5f, v, c.c0));
+  }
+  __device__ static void bwd(const Consts& c, const float* xin, const float* z, const Keep& k,
+                             float lm, float* lx, float* g) {
+    const float rc = c.rhoc;
+    const float eps = k.xP[1];
+    // dmeas: d/dv' = r A/(2 rc) - 1/2 ; d/deps = r rho / rc
+    const float dgv = 0.5f * k.r * k.A / rc - 0.5f;
+    const float dge = k.r * c.rho / rc;
+    const float rc3 = rc * rc * rc;
+    g[3] += lm * (-k.r * (k.A * c.rho - eps) / rc3 + c.rho / (rc * rc));
+    g[4] += lm * (k.r * c.dt / (rc * k.sd));
+    const float lv = lx[0] + lm * dgv;          // adjoint of v'
+    // (eps' = z has no parameter or state dependence; its adjoint lx[1] + lm dge stops here)
+    (void)dge;
+    // rproc: v' = v + kappa dt (theta e^-v - 1) + xi sqrt(dt) e^{-v/2} z
+    const float emv = k.emh * k.emh;
+    g[0] += lv * c.dt * (c.theta * emv - 1.0f);
+    g[1] += lv * c.kappa * c.dt * emv;
+    g[2] += lv * c.sqdt * k.emh * z[0];
+    const float dvv = 1.0f - c.kdt * c.theta * emv - 0.5f * c.xsq * k.emh * z[0];
+    lx[0] = lv * dvv;
+    lx[1] = 0.0f;
+    (void)xin;
+  }
+  __device__ static void bwd_init(const Consts&, const float*, const float* lx0, float* g) {
+    g[5] += lx0[0];
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -223,6 +360,36 @@ struct Ricker {
     const float lam = c.phi * x[0];
     if (y[0] == 0.0f) return -lam;
     return pp_fma(y[0], pp_logf(lam), -lam) - ycon;
+  }
+
+  // ---- adjoint: natural-scale gradient in canonical order (r, sigma, phi, N_0).
+  static constexpr int NG = 4;
+  struct Keep {
+    float xP[1];
+    float y;
+  };
+  __device__ static float fwd_keep(const Consts& c, const float* y, float ycon, const float* xin,
+                                   const float* z, Keep& k) {
+    k.xP[0] = xin[0];
+    rproc(c, k.xP, z);
+    k.y = y[0];
+    return dmeas(c, y, ycon, k.xP);
+  }
+  __device__ static void bwd(const Consts& c, const float* xin, const float* z, const Keep& k,
+                             float lm, float* lx, float* g) {
+    const float Np = k.xP[0];
+    const float N = xin[0];
+    // dmeas: y log(phi N') - phi N' - log y!
+    const float dgN = k.y / Np - c.phi;
+    g[2] += lm * (k.y / c.phi - Np);
+    const float lN = lx[0] + lm * dgN;
+    // rproc: N' = r N exp(-N + sigma z)
+    g[0] += lN * Np / c.r;
+    g[1] += lN * Np * z[0];
+    lx[0] = lN * Np * (1.0f / N - 1.0f);
+  }
+  __device__ static void bwd_init(const Consts&, const float*, const float* lx0, float* g) {
+    g[3] += lx0[0];
   }
 };
 

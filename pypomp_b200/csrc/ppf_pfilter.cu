@@ -29,285 +29,9 @@
 #include "ppf_core.cuh"
 #include "ppf_models.cuh"
 #include "ppf_internal.h"
+#include "ppf_kernels.cuh"
 
 namespace ppf {
-
-// ------------------------------ shared helpers ------------------------------
-
-__device__ __forceinline__ int filter_len(const Args& a, int u) { return a.T_u ? a.T_u[u] : a.T; }
-__device__ __forceinline__ int filter_unit(const Args& a, int f) { return a.unit ? a.unit[f] : 0; }
-
-// Normals of one particle (used by the plain path and by single particles).
-template <class M>
-__device__ __forceinline__ void step_noise(const Args& a, int f, int j, int s, int n, float* z) {
-  if (n <= 0) return;
-  if (a.flags & PPF_F_INJECT) {
-    if (s == 0) {
-      for (int i = 0; i < n; ++i) z[i] = a.inj_z0[((size_t)f * a.J + j) * n + i];
-    } else {
-      const size_t base = (((size_t)f * a.T + (s - 1)) * a.J + j) * n;
-      for (int i = 0; i < n; ++i) z[i] = a.inj_z[base + i];
-    }
-  } else {
-    pp_normals(a.seeds[f], (uint32_t)j, (uint32_t)s, PPF_TAG_PROCESS, n, z);
-  }
-}
-
-// Normals of the group of 4 consecutive particles k0..k0+3 (k0 % 4 == 0) at
-// step s, N per particle: z[e*N + r].  Philox calls (k0 N)/4 ... + N-1 cover
-// the group exactly; positions past J read zeros in injection mode.
-template <int N, bool INJ>
-__device__ __forceinline__ void group_noise(const Args& a, int f, int s, int k0, float* z) {
-  if (N == 0) return;
-  if (INJ) {
-    const float* src = (s == 0) ? a.inj_z0 + (size_t)f * a.J * N
-                                : a.inj_z + (((size_t)f * a.T + (s - 1)) * a.J) * N;
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-#pragma unroll
-      for (int r = 0; r < N; ++r) z[e * N + r] = (k0 + e < a.J) ? src[(size_t)(k0 + e) * N + r] : 0.0f;
-  } else {
-    const uint64_t seed = a.seeds[f];
-    const uint32_t c0 = (uint32_t)(k0 / 4) * N;
-#pragma unroll
-    for (int c = 0; c < N; ++c) pp_normal4(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
-  }
-}
-
-__device__ __forceinline__ uint32_t resample_u32(const Args& a, int f, int t) {
-  if (a.flags & PPF_F_INJECT) return pp_u32_from_float(a.inj_u[(size_t)f * a.T + t]);
-  return pp_resample_u32(a.seeds[f], (uint32_t)(t + 1));
-}
-
-// Observation t of series u into registers.
-template <class M>
-struct Obs {
-  float y[M::MAXDY];
-  float yc;
-  __device__ __forceinline__ void load(const Args& a, int u, int t) {
-    const float* p = a.ys + ((size_t)u * a.T + t) * a.model.dy;
-#pragma unroll
-    for (int i = 0; i < M::MAXDY; ++i) y[i] = (i < a.model.dy) ? p[i] : 0.0f;
-    yc = a.ycon ? a.ycon[(size_t)u * a.T + t] : 0.0f;
-  }
-};
-
-// rproc with the given normals, then dmeas at the loaded observation.
-template <class M>
-__device__ __forceinline__ float step1(const typename M::Consts& c, const Obs<M>& ob, float* x,
-                                       const float* z) {
-  M::rproc(c, x, z);
-  return M::dmeas(c, ob.y, ob.yc, x);
-}
-
-// rproc with the given normals, then dmeas at observation t.
-template <class M>
-__device__ __forceinline__ float prop1(const Args& a, const typename M::Consts& c, int u, int t,
-                                       float* x, const float* z) {
-  Obs<M> ob;
-  ob.load(a, u, t);
-  return step1<M>(c, ob, x, z);
-}
-
-// Single-particle propagate into observation t (plain path).
-template <class M>
-__device__ __forceinline__ float propagate(const Args& a, const typename M::Consts& c, int f, int u,
-                                           int j, int t, float* x) {
-  float z[M::NZ > 0 ? M::NZ : 1];
-  step_noise<M>(a, f, j, t + 1, M::NZ, z);
-  return prop1<M>(a, c, u, t, x, z);
-}
-
-// Finalise one observation of one filter: log-likelihood term and outputs.
-__device__ void finalize_step(const Args& a, int f, int t, const Acc& acc, uint64_t tot, double* loglik) {
-  const bool nanf = acc.nan != 0;
-  const float Mx = keyf(acc.maxkey);
-  const bool collapsed = !nanf && Mx == -INFINITY;
-  double ll;
-  if (nanf) ll = __longlong_as_double(0x7ff8000000000000ll);
-  else if (collapsed) ll = -INFINITY;
-  else ll = (double)Mx + log((double)tot) - 40.0 * kLn2 - (a.mode == MODE_MOP ? log((double)a.J) : 0.0);
-  *loglik += ll;
-  if ((a.flags & PPF_F_CLL) && a.cll) a.cll[(size_t)f * a.T + t] = ll;
-  const double S1 = (double)tot * 9.094947017729282e-13;  // 2^-40
-  if ((a.flags & PPF_F_ESS) && a.ess) {
-    float e;
-    if (nanf) e = __int_as_float(0x7fc00000);
-    else if (collapsed) e = (float)a.J;
-    else e = (float)(S1 * S1 / acc.s2);
-    a.ess[(size_t)f * a.T + t] = e;
-  }
-  const int dx = a.model.dx;
-  if ((a.flags & PPF_F_FMEAN) && a.fmean)
-    for (int d = 0; d < dx; ++d)
-      a.fmean[((size_t)f * a.T + t) * dx + d] = (float)(collapsed ? acc.px[d] / a.J : acc.fx[d] / S1);
-  if ((a.flags & PPF_F_PMEAN) && a.pmean)
-    for (int d = 0; d < dx; ++d) a.pmean[((size_t)f * a.T + t) * dx + d] = (float)(acc.px[d] / a.J);
-}
-
-__device__ __forceinline__ bool decide_resample(const Args& a, const Acc& acc) {
-  if (acc.nan) return false;
-  const float Mx = keyf(acc.maxkey);
-  if (Mx == -INFINITY) return 0.0f > a.logthresh;
-  const float mn = keyf(acc.minkey);
-  return (Mx - mn) > a.logthresh;
-}
-
-__device__ __forceinline__ void accum_maxmin(float w, unsigned int& mx, unsigned int& mn, unsigned int& nn) {
-  const bool bad = (w != w) | (w == INFINITY);
-  const unsigned int k = fkey(w);
-  nn |= bad ? 1u : 0u;
-  mx = bad ? mx : max(mx, k);
-  mn = bad ? mn : min(mn, k);
-}
-
-// Constants of the exact systematic-offset test for one filter and step:
-//   child k lies below CDF value C  <=>  k tot + chi < C J,
-// chi = floor(u32 tot / 2^32) (derivation in ppf_core.cuh, nchild).
-struct Offsets {
-  uint64_t tot, chi;
-  double inv, chi_d;   // J / tot and chi / tot, for the first guess
-  int J;
-};
-
-__device__ __forceinline__ Offsets make_offsets(uint64_t tot, uint32_t u32, int J) {
-  Offsets o;
-  o.tot = tot;
-  o.chi = __umul64hi((uint64_t)u32 << 32, tot);   // (u32 * tot) >> 32
-  o.inv = (double)J / (double)tot;
-  o.chi_d = (double)o.chi / (double)tot;
-  o.J = J;
-  return o;
-}
-
-// 128-bit a*b for 64-bit a, b as (hi, lo).
-__device__ __forceinline__ void mul64(uint64_t a, uint64_t b, uint64_t& hi, uint64_t& lo) {
-  lo = a * b;
-  hi = __umul64hi(a, b);
-}
-
-// nchild(C) = #{ k in [0,J) : k tot + chi < C J } = #{ k : k tot < D },
-// D = C J - chi.  The double-precision guess ceil(D / tot) is within one of
-// the answer (its relative error is ~1e-16 on a value below 2^21), so one
-// exact 128-bit comparison on each side settles it; a bounded loop covers the
-// impossible case defensively.
-__device__ __forceinline__ bool lt128(uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl) {
-  return (ah < bh) | ((ah == bh) & (al < bl));
-}
-
-__device__ __forceinline__ int nchild_fast(const Offsets& o, uint64_t C) {
-  uint64_t Dh, Dl;
-  mul64(C, (uint64_t)o.J, Dh, Dl);
-  Dh -= (Dl < o.chi);
-  Dl -= o.chi;                                  // D = C J - chi (may be negative)
-  const bool nonpos = ((long long)Dh < 0) | ((Dh == 0) & (Dl == 0));
-  long long k = (long long)ceil((double)C * o.inv - o.chi_d);
-  k = k < 0 ? 0 : (k > o.J ? o.J : k);
-  uint64_t Ph, Pl;
-  mul64((uint64_t)k, o.tot, Ph, Pl);            // P = k tot
-  for (int it = 0; it < 4; ++it) {
-    const uint64_t ql = Pl - o.tot, qh = Ph - (Pl < o.tot);     // (k-1) tot
-    const bool down = (k > 0) & !lt128(qh, ql, Dh, Dl);        // (k-1) tot >= D
-    const bool up = (k < o.J) & lt128(Ph, Pl, Dh, Dl);          // k tot < D
-    if (!(down | up)) break;
-    if (down) { Ph = qh; Pl = ql; --k; }
-    else { const uint64_t nl = Pl + o.tot; Ph += (nl < Pl); Pl = nl; ++k; }
-  }
-  return nonpos ? 0 : (int)k;
-}
-
-// Incremental form for consecutive parents: with P = k tot + chi and
-// D = C J, a parent of weight q moves D by q J (< 2^62) and its children are
-// the points P < D passed while advancing k.  No floating point, no division.
-struct OffWalk {
-  uint64_t Dh, Dl, Ph, Pl;
-  int k;
-};
-
-__device__ __forceinline__ OffWalk offwalk_init(const Offsets& o, uint64_t C) {
-  OffWalk w;
-  w.k = nchild_fast(o, C);
-  mul64(C, (uint64_t)o.J, w.Dh, w.Dl);
-  mul64((uint64_t)w.k, o.tot, w.Ph, w.Pl);
-  w.Pl += o.chi;
-  w.Ph += (w.Pl < o.chi);
-  return w;
-}
-
-// Add a parent of weight q; returns nchild of the new cumulative weight.
-__device__ __forceinline__ int offwalk_add(const Offsets& o, OffWalk& w, uint64_t q) {
-  const uint64_t add = q * (uint64_t)o.J;
-  w.Dl += add;
-  w.Dh += (w.Dl < add);
-  while (w.k < o.J && lt128(w.Ph, w.Pl, w.Dh, w.Dl)) {
-    w.Pl += o.tot;
-    w.Ph += (w.Pl < o.tot);
-    ++w.k;
-  }
-  return w.k;
-}
-
-// Parent (tile-local index) of child k: the last l in [0, n) with st[l] <= k.
-__device__ __forceinline__ int find_parent(const int* st, int n, int k) {
-  int lo = 0, hi = n;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (st[mid] <= k) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
-// ============================================================================
-// STREAM path
-// ============================================================================
-
-// Per-filter model constants, computed once per call (Cholesky factors, log
-// determinants, transformed parameters) and copied by every block.
-constexpr int kConstStride = 512;   // bytes per filter in the workspace
-
-template <class M>
-__global__ void k_prep(Args a) {
-  static_assert(sizeof(typename M::Consts) <= kConstStride, "Consts stride");
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= a.F) return;
-  typename M::Consts c;
-  M::prepare(c, a.theta + (size_t)f * a.model.n_params, a.model, (a.flags & PPF_F_EST) != 0);
-  *reinterpret_cast<typename M::Consts*>(a.consts + (size_t)f * kConstStride) = c;
-}
-
-template <class M>
-__device__ __forceinline__ void load_consts(const Args& a, int f, typename M::Consts& c) {
-  constexpr int NW = (sizeof(typename M::Consts) + 3) / 4;
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(a.consts + (size_t)f * kConstStride);
-  uint32_t* dst = reinterpret_cast<uint32_t*>(&c);
-  for (int i = threadIdx.x; i < NW; i += blockDim.x) dst[i] = src[i];
-}
-
-// Store the 4 children k0..k0+3 (valid[e]) of one group: float4 stores when
-// the whole group is valid and rows are 16-byte aligned (J % 4 == 0).
-template <int DX>
-__device__ __forceinline__ void store_group(float* Xn, float* Wn, float* logw, int J, int k0,
-                                            const float (&xo)[4][DX], const float (&wo)[4],
-                                            int nvalid_lo, int nvalid_hi) {
-  const bool full = (nvalid_lo == 0) & (nvalid_hi == 4) & ((J & 3) == 0);
-  if (full) {
-#pragma unroll
-    for (int d = 0; d < DX; ++d)
-      *reinterpret_cast<float4*>(Xn + d * J + k0) = make_float4(xo[0][d], xo[1][d], xo[2][d], xo[3][d]);
-    *reinterpret_cast<float4*>(Wn + k0) = make_float4(wo[0], wo[1], wo[2], wo[3]);
-    if (logw) *reinterpret_cast<float4*>(logw + k0) = make_float4(wo[0], wo[1], wo[2], wo[3]);
-  } else {
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      if (e < nvalid_lo || e >= nvalid_hi) continue;
-#pragma unroll
-      for (int d = 0; d < DX; ++d) Xn[d * J + k0 + e] = xo[e][d];
-      Wn[k0 + e] = wo[e];
-      if (logw) logw[k0 + e] = wo[e];
-    }
-  }
-}
 
 template <class M, int TPB, bool INJ>
 __global__ void __launch_bounds__(TPB) k_init(Args a) {
@@ -345,6 +69,9 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
     for (int e = 0; e < 4; ++e) {
       float x[DX];
       M::rinit(cr, z0 + e * M::NZ0, x);
+      if (a.mop_ckpt && k0 + e < j1)
+#pragma unroll
+        for (int d = 0; d < DX; ++d) a.mop_ckpt[((size_t)f * a.nseg * DX + d) * J + k0 + e] = x[d];
       wo[e] = base + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
       for (int d = 0; d < DX; ++d) xo[e][d] = x[d];
@@ -647,6 +374,16 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a
   __syncthreads();
   const typename M::Consts cr = c;
   const int klo = st[0], khi = st[ntile];
+  // MOP: keep the first-child offsets of every parent for the adjoint sweep
+  if (a.mop_off) {
+    int* off = a.mop_off + ((size_t)f * a.T + t) * (J + 1) + jt;
+    for (int l = threadIdx.x; l <= ntile; l += TPB)
+      if (l < ntile || jt + ntile == J) off[l] = st[l];
+  }
+  // MOP: checkpoint the resampled states x^F_t when step t+1 opens a segment
+  float* ckpt = nullptr;
+  if (a.mop_ckpt && (t + 1) % a.ckpt_every == 0 && (t + 1) / a.ckpt_every < a.nseg)
+    ckpt = a.mop_ckpt + ((size_t)f * a.nseg + (t + 1) / a.ckpt_every) * DX * J;
 
   // 3. children, in runs of RUN per thread
   const int kA = klo & ~3;
@@ -678,6 +415,9 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a
         float x[DX];
 #pragma unroll
         for (int d = 0; d < DX; ++d) x[d] = xs[d * TILE + l];
+        if (ckpt && valid)
+#pragma unroll
+          for (int d = 0; d < DX; ++d) ckpt[d * J + k] = x[d];
         const float wb = rs ? base : wcar[l];
         wo[e] = wb + step1<M>(cr, ob, x, z + e * M::NZ);
 #pragma unroll
@@ -1083,8 +823,6 @@ void Profiler::mark(int kind, cudaStream_t s, bool start) {
   }
 }
 
-#define PROF_BEGIN(kind) g_prof.mark(kind, s, true)
-#define PROF_END(kind) g_prof.mark(kind, s, false)
 
 template <class M, bool INJ>
 int run_stream_t(Args& a, cudaStream_t s) {
@@ -1202,6 +940,8 @@ int run_pfilter_path(Args& a, int path, cudaStream_t s) {
     default: return PPF_EINVAL;
   }
 }
+
+int run_stream_any(Args& a, cudaStream_t s) { return run_pfilter_path(a, PPF_PATH_STREAM, s); }
 
 size_t resident_smem_bytes(const Args& a) {
   return (size_t)a.J * sizeof(float) * (a.model.dx + 1) + (size_t)(a.J + 4) * sizeof(int);

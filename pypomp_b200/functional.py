@@ -153,3 +153,83 @@ def pfilter(struct: PompStruct, thetas_array, J: int, keys, thresh: float = 0.0,
         out["prediction_mean"] = res["pmean"].reshape(n, reps, res["pmean"].shape[1], -1)
     del T
     return out
+
+
+def run_mop(struct: PompStruct, theta_est_f: np.ndarray, seeds_f: np.ndarray, J: int, alpha: float,
+            *, grad: bool = True, unit_f=None, inject=None, ckpt_every: int = 0,
+            save_ancestors: bool = False, return_torch: bool = False):
+    """One batched call of ``ppf_mop``: MOP-alpha value (negative log-likelihood,
+    summed over time) and, when ``grad``, its gradient on the estimation scale."""
+    torch = _ffi.require_cuda()
+    if J < 1:
+        raise ValueError("J should be greater than 0.")
+    if J > _ffi.PPF_MAX_J:
+        raise ValueError(f"J must be at most {_ffi.PPF_MAX_J}.")
+    if not 0.0 <= float(alpha) <= 1.0:
+        raise ValueError("alpha must be in [0, 1]")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    spec = struct.spec
+    theta_est_f = np.ascontiguousarray(np.atleast_2d(theta_est_f), dtype=np.float32)
+    F = theta_est_f.shape[0]
+    ys_d, ycon_d, Tu_d, U, T = _device_inputs(torch, struct, dev)
+    th_d = torch.from_numpy(theta_est_f).to(dev)
+    seeds_d = torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).copy()).to(dev)
+    unit_d = None
+    if unit_f is not None:
+        unit_d = torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
+    out = {"value": torch.zeros(F, dtype=torch.float64, device=dev)}
+    if grad:
+        out["grad"] = torch.zeros(F, spec.n_params, dtype=torch.float64, device=dev)
+    if save_ancestors:
+        out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=dev)
+    inj = {}
+    flags = 0
+    if inject is not None:
+        flags |= _ffi.F_INJECT
+        for k in ("z0", "z", "u"):
+            if inject.get(k) is not None:
+                inj[k] = torch.from_numpy(np.ascontiguousarray(inject[k], dtype=np.float32)).to(dev)
+    d = _ffi.MopDesc()
+    d.model = spec.ffi_model()
+    d.J, d.F, d.T, d.U = J, F, T, U
+    d.flags = flags
+    d.alpha = float(alpha)
+    d.ckpt_every = int(ckpt_every)
+    d.theta, d.ys, d.ycon = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(ycon_d)
+    d.unit, d.T_u, d.seeds = _ffi.ptr(unit_d), _ffi.ptr(Tu_d), _ffi.ptr(seeds_d)
+    d.inj_z0, d.inj_z, d.inj_u = _ffi.ptr(inj.get("z0")), _ffi.ptr(inj.get("z")), _ffi.ptr(inj.get("u"))
+    d.value, d.grad, d.anc = _ffi.ptr(out["value"]), _ffi.ptr(out.get("grad")), _ffi.ptr(out.get("anc"))
+    nbytes = _ffi.LIB.ppf_mop_workspace_bytes(d)
+    ws = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
+    d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    _ffi.check(_ffi.LIB.ppf_mop(d, stream), "ppf_mop")
+    _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_mop")
+    if return_torch:
+        return out
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+def mop(struct: PompStruct, thetas_array, J: int, alpha: float, keys) -> np.ndarray:
+    """MOP-alpha negative log-likelihood (``pypomp/functional/mop.py:8-62``).
+
+    ``thetas_array`` (n, P) on the estimation scale, ``keys`` (n,).
+    """
+    th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float32))
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    if keys.shape[0] != th.shape[0]:
+        raise ValueError("keys must have one key per parameter set")
+    return run_mop(struct, th, keys, J, alpha, grad=False)["value"]
+
+
+def mop_value_and_grad(struct: PompStruct, thetas_array, J: int, alpha: float, keys, mean: bool = True):
+    """Value and gradient of the (mean) MOP objective
+    (``pypomp/core/algorithms/ad_helpers.py:32-54`` ``_jvg_mop``): with
+    ``mean`` both are divided by the series length as ``_mop_internal_mean``
+    does (``mop.py:148-158``)."""
+    th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float32))
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    res = run_mop(struct, th, keys, J, alpha, grad=True)
+    T = np.asarray(struct.ys).shape[-2]
+    scale = 1.0 / T if mean else 1.0
+    return res["value"] * scale, res["grad"] * scale

@@ -1,0 +1,117 @@
+"""MOP-alpha value and adjoint gradient on the GPU against the oracle.
+
+* the reference's locked MOP value (``test_mop_regression.csv``) is reproduced
+  by feeding the reference's own draws through the injection mode;
+* forward ancestors are bit-identical to the C oracle's MOP run;
+* the adjoint gradient matches central finite differences (h = 1e-3) of the
+  MOP-alpha surrogate with frozen ancestry and frozen stop_gradient(m)
+  (``oracle/ppf_oracle.c``, ``ppfo_mop_surrogate``) to relative error <= 1e-3;
+* the gradient does not depend on the checkpoint spacing (bit-identical).
+"""
+
+import numpy as np
+import pytest
+
+from oracle import cora
+
+pytestmark = pytest.mark.gpu
+f32 = np.float32
+
+
+def _F():
+    from pypomp_b200 import functional as F
+
+    return F
+
+
+def test_mop_reference_fixture_through_injection(ref_values, ref_lg1d):
+    F = _F()
+    from pypomp_b200.functional import PompStruct
+    from pypomp_b200.models import lg_spec
+
+    st = PompStruct(spec=lg_spec(1, 1), ys=ref_lg1d["ys"], times=np.arange(1, 5.0), t0=0.0)
+    inj = dict(z0=ref_lg1d["mop_z0"][None], z=ref_lg1d["mop_z"][None], u=ref_lg1d["mop_u"][None])
+    # test_mop_regression.py passes theta0 (natural values) as estimation-scale input
+    res = F.run_mop(st, ref_lg1d["theta"][None], np.zeros(1, np.uint64), 12, 0.5, inject=inj, grad=True)
+    np.testing.assert_allclose(res["value"][0], ref_values["mop"]["mop"][0], **ref_values["tolerance"])
+    assert np.all(np.isfinite(res["grad"]))
+
+
+def _case(model):
+    import pypomp_b200 as pp
+
+    from tests.conftest import LG2_Q, LG2_R
+
+    if model == "LG":
+        m = pp.LG(T=15, Q=LG2_Q, R=LG2_R, key=3)
+        J = 1500
+    elif model == "SV":
+        m = pp.SV(T=30, key=1)
+        J = 2048
+    else:
+        m = pp.Ricker(T=20, key=2)
+        J = 1600
+    st = m.to_struct()
+    th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(f32)
+    return m, st, th, J
+
+
+def _oracle_kw(m, st):
+    spec = m.spec
+    return dict(ycon=spec.ycon(st.ys), dt=spec.dt)
+
+
+@pytest.mark.parametrize("model", ["LG", "SV", "Ricker"])
+def test_mop_forward_ancestors_bit_exact(model):
+    F = _F()
+    m, st, th, J = _case(model)
+    spec = m.spec
+    seeds = np.array([5, 6], np.uint64)
+    th2 = np.repeat(th, 2, axis=0)
+    th2[1, 0] += f32(0.01)
+    want = cora.pfilter(spec.kind, spec.dx, spec.dy, th2, st.ys, J, seeds=seeds, est=True, mop=True,
+                        anc=True, **_oracle_kw(m, st))
+    got = F.run_mop(st, th2, seeds, J, 0.97, grad=False, save_ancestors=True)
+    assert np.array_equal(got["anc"], want["anc"])
+    np.testing.assert_allclose(got["value"], -want["loglik"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("alpha", [0.0, 0.5, 0.97, 1.0])
+@pytest.mark.parametrize("model", ["LG", "SV", "Ricker"])
+def test_mop_gradient_vs_finite_differences(model, alpha):
+    F = _F()
+    m, st, th, J = _case(model)
+    spec = m.spec
+    seeds = np.array([11], np.uint64)
+    kw = _oracle_kw(m, st)
+    got = F.run_mop(st, th, seeds, J, alpha, grad=True, save_ancestors=True)
+    anc = got["anc"]
+    base, m0 = cora.mop_surrogate(spec.kind, spec.dx, spec.dy, th, st.ys, J, alpha, anc, seeds=seeds, **kw)
+    np.testing.assert_allclose(base[0], got["value"][0], rtol=1e-9)
+    h = 1e-3
+    P = th.shape[1]
+    fd = np.zeros(P)
+    for p in range(P):
+        tp = th.copy()
+        tm = th.copy()
+        tp[0, p] += f32(h)
+        tm[0, p] -= f32(h)
+        hp = float(tp[0, p]) - float(th[0, p])
+        hm = float(th[0, p]) - float(tm[0, p])
+        vp, _ = cora.mop_surrogate(spec.kind, spec.dx, spec.dy, tp, st.ys, J, alpha, anc, m0, seeds=seeds, **kw)
+        vm, _ = cora.mop_surrogate(spec.kind, spec.dx, spec.dy, tm, st.ys, J, alpha, anc, m0, seeds=seeds, **kw)
+        fd[p] = (vp[0] - vm[0]) / (hp + hm)
+    g = got["grad"][0]
+    err = np.linalg.norm(g - fd) / np.linalg.norm(fd)
+    assert err <= 1e-3, (model, alpha, err, g, fd)
+
+
+def test_mop_gradient_independent_of_checkpoint_spacing():
+    F = _F()
+    m, st, th, J = _case("SV")
+    seeds = np.array([3], np.uint64)
+    ref = F.run_mop(st, th, seeds, J, 0.97, grad=True, ckpt_every=1)
+    for ck in (2, 7, 0, 30):
+        got = F.run_mop(st, th, seeds, J, 0.97, grad=True, ckpt_every=ck)
+        assert np.array_equal(got["grad"], ref["grad"]), ck
+        assert np.array_equal(got["value"], ref["value"])
