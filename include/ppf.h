@@ -44,6 +44,7 @@ extern "C" {
 #define PPF_ETIMEOUT 3
 #define PPF_EUNSUPPORTED 4
 #define PPF_EINTERNAL 5
+#define PPF_ESCRATCH 6
 
 #define PPF_MAX_J (1 << 21)
 
@@ -166,6 +167,21 @@ int ppf_workspace_status(const void* workspace, void* stream);
  * IF2.  Not reentrant. */
 int ppf_profile_begin(void);
 int ppf_profile_end(double* ms, int* count, int n);
+
+/* ppf_pfilter for callers that cannot allocate device memory.  No counterpart
+ * in the reference: pypomp runs on JAX, whose runtime owns device memory.
+ * Some callers of this library cannot hand it a workspace -- a host runtime
+ * that owns the whole device pool and forbids other allocations, or plugin
+ * code not allowed to call the CUDA allocator.  This entry point runs the same
+ * filter as ppf_pfilter (descriptor fields `workspace` and `ws_bytes` are
+ * ignored) on a scratch array of PPF_NOALLOC_SCRATCH_BYTES compiled into the
+ * library, and allocates nothing.  A request whose workspace
+ * (ppf_pfilter_workspace_bytes) exceeds that size returns PPF_ESCRATCH.  All
+ * calls on a device share the array, so calls that overlap on the GPU race;
+ * the first call on a device looks up the array's address and should come
+ * before any stream capture; the call synchronises the stream. */
+#define PPF_NOALLOC_SCRATCH_BYTES (16u << 20)
+int ppf_pfilter_noalloc(const ppf_pfilter_desc* d, void* stream);
 
 /* Human-readable message for a return code (static storage). */
 const char* ppf_error_string(int code);

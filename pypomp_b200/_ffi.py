@@ -16,7 +16,8 @@ from pathlib import Path
 
 _LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libppf.so"
 
-PPF_OK, PPF_EINVAL, PPF_ECUDA, PPF_ETIMEOUT, PPF_EUNSUPPORTED, PPF_EINTERNAL = 0, 1, 2, 3, 4, 5
+PPF_OK, PPF_EINVAL, PPF_ECUDA, PPF_ETIMEOUT, PPF_EUNSUPPORTED, PPF_EINTERNAL, PPF_ESCRATCH = 0, 1, 2, 3, 4, 5, 6
+NOALLOC_SCRATCH_BYTES = 16 << 20
 PPF_MAX_J = 1 << 21
 MODEL_LG, MODEL_SV, MODEL_RICKER = 1, 2, 3
 
@@ -39,6 +40,7 @@ EXPORTED = (
     "ppf_mop_workspace_bytes",
     "ppf_mop",
     "ppf_workspace_status",
+    "ppf_pfilter_noalloc",
     "ppf_profile_begin",
     "ppf_profile_end",
     "ppf_error_string",
@@ -142,6 +144,8 @@ def _load():
     lib.ppf_mop_workspace_bytes.restype = ctypes.c_size_t
     lib.ppf_mop.argtypes = [ctypes.POINTER(MopDesc), _vp]
     lib.ppf_mop.restype = ctypes.c_int
+    lib.ppf_pfilter_noalloc.argtypes = [ctypes.POINTER(PfilterDesc), _vp]
+    lib.ppf_pfilter_noalloc.restype = ctypes.c_int
     lib.ppf_workspace_status.argtypes = [_vp, _vp]
     lib.ppf_workspace_status.restype = ctypes.c_int
     lib.ppf_profile_begin.argtypes = []

@@ -304,6 +304,7 @@ const char* ppf_error_string(int code) {
     case PPF_ETIMEOUT: return "a bounded device-side wait timed out";
     case PPF_EUNSUPPORTED: return "unsupported configuration";
     case PPF_EINTERNAL: return "a device-side consistency check failed";
+    case PPF_ESCRATCH: return "the request needs more scratch than the no-allocation entry point holds";
     default: return "unknown error";
   }
 }
