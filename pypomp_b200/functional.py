@@ -233,3 +233,66 @@ def mop_value_and_grad(struct: PompStruct, thetas_array, J: int, alpha: float, k
     T = np.asarray(struct.ys).shape[-2]
     scale = 1.0 / T if mean else 1.0
     return res["value"] * scale, res["grad"] * scale
+
+
+def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alpha: float, keys,
+          alpha_cooling: float = 1.0, thresh: float = 0.0, n_monitors: int = 1):
+    """MOP-alpha gradient training (``pypomp/functional/train.py:14-110`` /
+    ``_train_internal``, ``train.py:38-180``).
+
+    ``thetas_array`` (n, P) on the estimation scale, ``keys`` (n,).  Each
+    iteration: cosine-cooled alpha (``train.py:82-85``), one batched MOP value
+    and gradient for all n parameter sets (the gradient of the mean objective,
+    ``_mop_internal_mean``), optional clipping, the optimiser step and
+    ``theta += eta[m] * direction``.  The recorded negative log-likelihood is
+    the MOP value at the current parameters (n_monitors == 1) or the mean of
+    ``n_monitors`` particle filters (n_monitors > 1; NaN for 0).  Returns
+    ``(neg_logliks (n, M+1), thetas (n, M+1, P))`` with a NaN first entry.
+    """
+    from . import random as pprandom
+    from .optim import LearningRate, cosine_alpha
+
+    if optimizer.ls:
+        raise NotImplementedError("line search is not supported by the CUDA train loop")
+    th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float64)).copy()
+    n, P = th.shape
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    if keys.shape[0] != n:
+        raise ValueError("keys must have one key per parameter set")
+    names = list(struct.spec.param_names)
+    eta_arr = eta.to_array(names, M) if isinstance(eta, LearningRate) else np.broadcast_to(
+        np.asarray(eta, dtype=np.float64), (max(M, 1), P))
+    T = np.asarray(struct.ys).shape[-2]
+    state = optimizer.init_state(th)
+    nll = np.full((n, M + 1), np.nan)
+    traces = np.zeros((n, M + 1, P))
+    traces[:, 0] = th
+    chain = [int(k) for k in keys]
+    for m in range(M):
+        alpha_m = 1.0 - (1.0 - alpha) * cosine_alpha(m, M, alpha_cooling)
+        subs = np.zeros(n, np.uint64)
+        for i in range(n):
+            chain[i], subs[i] = (int(v) for v in pprandom.split(chain[i]))
+        res = run_mop(struct, th.astype(np.float32), subs, J, alpha_m, grad=True)
+        grad = res["grad"] / T
+        if n_monitors == 1:
+            nll[:, m + 1] = res["value"]
+        elif n_monitors > 1:
+            mon = np.zeros((n, n_monitors), np.uint64)
+            for i in range(n):
+                ks = pprandom.split(chain[i], n_monitors + 1)
+                chain[i] = int(ks[0])
+                mon[i] = ks[1:]
+            pf = run_pfilter(struct, np.repeat(th.astype(np.float32), n_monitors, axis=0),
+                             mon.reshape(-1), J, thresh=thresh, est=True)
+            nll[:, m + 1] = -pf["loglik"].reshape(n, n_monitors).mean(axis=1)
+        for i in range(n):
+            chain[i] = int(pprandom.split(chain[i])[0])
+        if optimizer.clip_norm is not None:
+            grad = np.clip(grad, -optimizer.clip_norm, optimizer.clip_norm)
+        direction, state = optimizer.step(grad, state, m)
+        if optimizer.scale:
+            direction = direction / np.linalg.norm(direction, axis=-1, keepdims=True)
+        th = th + eta_arr[m] * direction
+        traces[:, m + 1] = th
+    return nll, traces
