@@ -147,6 +147,50 @@ typedef struct ppf_mop_desc {
 size_t ppf_mop_workspace_bytes(const ppf_mop_desc* d);
 int ppf_mop(const ppf_mop_desc* d, void* stream);
 
+/* One IF2 iteration: the perturbed particle filter over F independent
+ * parameter swarms.  Replaces _perfilter_internal / _perfilter_scan_body
+ * (pypomp/core/algorithms/mif.py:88-258) with _resampler_thetas
+ * (pypomp/core/algorithms/helpers.py:103-141); Pomp.mif / functional mif
+ * (pypomp/functional/mif.py:15, pypomp/core/estimation_mixin.py:274) call it
+ * once per iteration.  Each particle carries a parameter vector on the
+ * estimation scale: perturbed by rw_sig0[p] * cool0[u] * N(0,1) before the
+ * initial state is drawn, by rw_sig[p] * cool[u][t] * N(0,1) before step t;
+ * state and vector are resampled together; measurement log-densities that
+ * are NaN become log(1e-18) (mif.py:205-210).  Outputs: loglik[f] (sum of the
+ * conditional log-likelihoods of the perturbed filter) and swarm_out, the
+ * vectors after the last step's resampling.  The swarm layout is
+ * parameter-major [F][P][J] (the reference holds (J, P) per replicate). */
+typedef struct ppf_perfilter_desc {
+  ppf_model model;
+  int32_t J, F, T, U;
+  uint32_t flags;          /* PPF_F_INJECT, PPF_F_CLL, PPF_F_SAVE_ANC */
+  float thresh;            /* resample when max(nw) - min(nw) > log(thresh) */
+  const float* swarm_in;   /* [F][P][J] estimation scale */
+  float* swarm_out;        /* out [F][P][J]; may not alias swarm_in */
+  const float* rw_sig;     /* [P] per-step random-walk sds (estimation scale) */
+  const float* rw_sig0;    /* [P] sds of the t0-only perturbation */
+  const float* cool;       /* [U][T] cooling factor of the step-t perturbation */
+  const float* cool0;      /* [U] cooling factor of the t0 perturbation */
+  const float* ys;         /* [U][T][dy] */
+  const float* ycon;       /* [U][T] or NULL */
+  const int32_t* unit;     /* [F] or NULL */
+  const int32_t* T_u;      /* [U] or NULL */
+  const uint64_t* seeds;   /* [F] */
+  const float* inj_zp0;    /* [F][J][P] t0 perturbation normals (PPF_F_INJECT) */
+  const float* inj_zp;     /* [F][T][J][P] per-step perturbation normals */
+  const float* inj_z0;     /* [F][J][n_init] */
+  const float* inj_z;      /* [F][T][J][n_step] */
+  const float* inj_u;      /* [F][T] */
+  double* loglik;          /* out [F] */
+  double* cll;             /* out [F][T] (PPF_F_CLL) */
+  int32_t* anc;            /* out [F][T][J] (PPF_F_SAVE_ANC) */
+  void* workspace;
+  size_t ws_bytes;
+} ppf_perfilter_desc;
+
+size_t ppf_perfilter_workspace_bytes(const ppf_perfilter_desc* d);
+int ppf_perfilter(const ppf_perfilter_desc* d, void* stream);
+
 /* Workspace bytes ppf_pfilter needs for this descriptor (pointers ignored). */
 size_t ppf_pfilter_workspace_bytes(const ppf_pfilter_desc* d);
 

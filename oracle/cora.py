@@ -29,6 +29,15 @@ class _Desc(ctypes.Structure):
                            "workspace")] + [("ws_bytes", ctypes.c_size_t)]
 
 
+class _IF2Desc(ctypes.Structure):
+    _fields_ = [("model", _Model), ("J", ctypes.c_int32), ("F", ctypes.c_int32),
+                ("T", ctypes.c_int32), ("U", ctypes.c_int32), ("flags", ctypes.c_uint32),
+                ("thresh", ctypes.c_float)] + [
+        (n, _vp) for n in ("swarm_in", "swarm_out", "rw_sig", "rw_sig0", "cool", "cool0", "ys",
+                           "ycon", "unit", "T_u", "seeds", "inj_zp0", "inj_zp", "inj_z0", "inj_z",
+                           "inj_u", "loglik", "cll", "anc", "workspace")] + [("ws_bytes", ctypes.c_size_t)]
+
+
 def lib():
     if not _SO.exists():
         raise ImportError(f"oracle library missing: {_SO} (run `make -C oracle`)")
@@ -37,6 +46,8 @@ def lib():
     L.ppfo_pfilter.restype = ctypes.c_int
     L.ppfo_mop_surrogate.argtypes = [ctypes.POINTER(_Desc), ctypes.c_float, _vp, _vp, _vp, _vp]
     L.ppfo_mop_surrogate.restype = ctypes.c_int
+    L.ppfo_perfilter.argtypes = [ctypes.POINTER(_IF2Desc), ctypes.c_int]
+    L.ppfo_perfilter.restype = ctypes.c_int
     L.ppfo_expf.argtypes = [ctypes.c_float]
     L.ppfo_expf.restype = ctypes.c_float
     L.ppfo_logf.argtypes = [ctypes.c_float]
@@ -171,6 +182,61 @@ def mop_surrogate(kind, dx, dy, theta_est, ys, J, alpha, anc, m0=None, *, seeds=
         raise RuntimeError(f"oracle returned {rc}")
     del keep
     return value, (m0_out if m0 is None else m0_in)
+
+
+def perfilter(kind, dx, dy, swarm, ys, J, rw_sig, rw_sig0, cool, cool0, *, seeds=None,
+              ycon=None, unit=None, T_u=None, dt=0.0, thresh=0.0, inject=None, CLL=False,
+              anc=False, nthreads=1):
+    """One IF2 iteration over F swarms (``swarm`` (F, P, J), estimation scale).
+
+    ``cool`` (U, T) and ``cool0`` (U,) are the cooling factors; ``inject`` may
+    hold ``zp0`` (F,J,P), ``zp`` (F,T,J,P), ``z0``, ``z``, ``u``.  Returns a
+    dict with ``loglik`` (F,), ``swarm`` (F, P, J) and optional ``cll``/``anc``."""
+    swarm = np.ascontiguousarray(swarm, dtype=np.float32)
+    F, P, Jc = swarm.shape
+    assert Jc == J
+    ys = np.ascontiguousarray(ys, dtype=np.float32)
+    if ys.ndim == 2:
+        ys = ys[None]
+    U, T, _ = ys.shape
+    rw_sig = np.ascontiguousarray(rw_sig, dtype=np.float32)
+    rw_sig0 = np.ascontiguousarray(rw_sig0, dtype=np.float32)
+    cool = np.ascontiguousarray(np.broadcast_to(np.asarray(cool, np.float32), (U, T)))
+    cool0 = np.ascontiguousarray(np.broadcast_to(np.asarray(cool0, np.float32), (U,)))
+    keep = [swarm, ys, rw_sig, rw_sig0, cool, cool0]
+    d = _IF2Desc()
+    d.model = _Model(kind, dx, dy, P, dt, 0)
+    d.J, d.F, d.T, d.U = J, F, T, U
+    d.thresh = thresh
+    flags = (1 if CLL else 0) | (32 if anc else 0)
+    d.swarm_in, d.ys = _p(swarm), _p(ys)
+    d.rw_sig, d.rw_sig0, d.cool, d.cool0 = _p(rw_sig), _p(rw_sig0), _p(cool), _p(cool0)
+    for name, a, dt_ in (("ycon", ycon, np.float32), ("unit", unit, np.int32), ("T_u", T_u, np.int32),
+                         ("seeds", seeds, np.uint64)):
+        if a is not None:
+            a = np.ascontiguousarray(a, dtype=dt_)
+            keep.append(a)
+            setattr(d, name, _p(a))
+    if inject is not None:
+        flags |= 16
+        for k in ("zp0", "zp", "z0", "z", "u"):
+            if inject.get(k) is not None:
+                a = np.ascontiguousarray(inject[k], dtype=np.float32)
+                keep.append(a)
+                setattr(d, "inj_" + k, _p(a))
+    d.flags = flags
+    out = {"loglik": np.zeros(F, np.float64), "swarm": np.zeros((F, P, J), np.float32)}
+    if CLL:
+        out["cll"] = np.zeros((F, T), np.float64)
+    if anc:
+        out["anc"] = np.zeros((F, T, J), np.int32)
+    d.loglik, d.swarm_out = _p(out["loglik"]), _p(out["swarm"])
+    d.cll, d.anc = _p(out.get("cll")), _p(out.get("anc"))
+    rc = _L().ppfo_perfilter(ctypes.byref(d), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle returned {rc}")
+    del keep
+    return out
 
 
 def expf(x):

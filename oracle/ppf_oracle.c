@@ -9,6 +9,8 @@
  *   _resample (systematic, side=right)  pypomp/core/algorithms/helpers.py:14-31
  *   _resampler (gather, -log J)         pypomp/core/algorithms/helpers.py:60-91
  *   _mop_internal / _mop_step           pypomp/core/algorithms/mop.py:19-135
+ *   _perfilter_internal / scan body     pypomp/core/algorithms/mif.py:88-258
+ *   _resampler_thetas                   pypomp/core/algorithms/helpers.py:103-141
  *   LG _rinit/_rproc/_dmeas             pypomp/models/linear_gaussian.py:139-177
  * -- but with the arithmetic definitions of include/ppf.h: float32 model math
  * in a fixed order, ppf_detmath.h elementary functions, the fixed-point CDF
@@ -424,6 +426,196 @@ int ppfo_mop_surrogate(const ppf_pfilter_desc* d, float alpha, const int* anc, c
     value[f] = -ll;
     free(x); free(xp); free(wF); free(wP); free(v); free(m);
   }
+  return PPF_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* IF2 perturbed filter (mif.py:88-258)                                     */
+/* ------------------------------------------------------------------------ */
+
+static void if2_noise(const ppf_perfilter_desc* d, int f, int j, int s, int n, float* z) {
+  if (n <= 0) return;
+  if (d->flags & PPF_F_INJECT) {
+    if (s == 0) {
+      for (int i = 0; i < n; ++i) z[i] = d->inj_z0[((size_t)f * d->J + j) * n + i];
+    } else {
+      const size_t base = (((size_t)f * d->T + (s - 1)) * d->J + j) * n;
+      for (int i = 0; i < n; ++i) z[i] = d->inj_z[base + i];
+    }
+  } else {
+    pp_normals(d->seeds[f], (uint32_t)j, (uint32_t)s, PPF_TAG_PROCESS, n, z);
+  }
+}
+
+/* P perturbation normals of particle j: s = 0 before rinit, s = t + 1 before step t. */
+static void if2_perturb_noise(const ppf_perfilter_desc* d, int f, int j, int s, int P, float* z) {
+  if (d->flags & PPF_F_INJECT) {
+    const float* src = (s == 0) ? d->inj_zp0 + ((size_t)f * d->J + j) * P
+                                : d->inj_zp + (((size_t)f * d->T + (s - 1)) * d->J + j) * P;
+    for (int i = 0; i < P; ++i) z[i] = src[i];
+  } else {
+    pp_normals(d->seeds[f], (uint32_t)j, (uint32_t)s, PPF_TAG_PERTURB, P, z);
+  }
+}
+
+/* jnp.nan_to_num(m, nan=log(1e-18)) (mif.py:205-210) */
+static float if2_measure(float m) {
+  if (m != m) return pp_logf(1e-18f);
+  if (m == INFINITY) return 3.4028234663852886e38f;
+  if (m == -INFINITY) return -3.4028234663852886e38f;
+  return m;
+}
+
+/* Perturb th (P values) with sds sig * cool, then step the particle:
+ * rproc with process normals of counter s, dmeas at observation t. */
+static float if2_step(const ppf_perfilter_desc* d, int f, int u, int j, int t, int s, float cool,
+                      float* th, float* x) {
+  const int P = d->model.n_params;
+  float zp[64];
+  if2_perturb_noise(d, f, j, s, P, zp);
+  for (int p = 0; p < P; ++p) th[p] = th[p] + (cool * d->rw_sig[p]) * zp[p];
+  consts_t c;
+  prepare(&c, th, &d->model, 1);
+  float z[4];
+  if2_noise(d, f, j, s, n_step(&c), z);
+  rproc(&c, x, z);
+  const float* y = d->ys + ((size_t)u * d->T + t) * d->model.dy;
+  const float yc = d->ycon ? d->ycon[(size_t)u * d->T + t] : 0.0f;
+  return if2_measure(dmeas(&c, y, yc, x));
+}
+
+static void run_perfilter(const ppf_perfilter_desc* d, int f) {
+  const int J = d->J, dx = d->model.dx, P = d->model.n_params;
+  const int u = d->unit ? d->unit[f] : 0;
+  const int Tf = d->T_u ? d->T_u[u] : d->T;
+  const float base_init = pp_logf(1.0f / (float)J);
+  const float base_rs = -pp_logf((float)J);
+  const float logthresh = d->thresh > 0.0f ? pp_logf(d->thresh) : -INFINITY;
+  const float* cool = d->cool + (size_t)u * d->T;
+  float* x = (float*)malloc(sizeof(float) * dx * J);
+  float* xn = (float*)malloc(sizeof(float) * dx * J);
+  float* th = (float*)malloc(sizeof(float) * P * J);
+  float* thn = (float*)malloc(sizeof(float) * P * J);
+  float* w = (float*)malloc(sizeof(float) * J);
+  float* wn = (float*)malloc(sizeof(float) * J);
+  uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * J);
+  int* par = (int*)malloc(sizeof(int) * J);
+  const float* S = d->swarm_in + (size_t)f * P * J;
+  for (int j = 0; j < J; ++j) {
+    float tj[64], zp[64], z[4], xj[4];
+    for (int p = 0; p < P; ++p) tj[p] = S[(size_t)p * J + j];
+    if2_perturb_noise(d, f, j, 0, P, zp);
+    for (int p = 0; p < P; ++p) tj[p] = tj[p] + (d->cool0[u] * d->rw_sig0[p]) * zp[p];
+    consts_t c;
+    prepare(&c, tj, &d->model, 1);
+    if2_noise(d, f, j, 0, n_init(&c), z);
+    rinit(&c, z, xj);
+    const float m = if2_step(d, f, u, j, 0, 1, cool[0], tj, xj);
+    for (int k = 0; k < dx; ++k) x[k * J + j] = xj[k];
+    for (int p = 0; p < P; ++p) th[(size_t)p * J + j] = tj[p];
+    w[j] = base_init + m;
+  }
+  double loglik = 0.0;
+  for (int t = 0; t < Tf; ++t) {
+    int nanf = 0;
+    float Mx = -INFINITY, mn = INFINITY;
+    for (int j = 0; j < J; ++j) {
+      if (w[j] != w[j] || w[j] == INFINITY) { nanf = 1; continue; }
+      if (w[j] > Mx) Mx = w[j];
+      if (w[j] < mn) mn = w[j];
+    }
+    const int collapsed = !nanf && Mx == -INFINITY;
+    const int qc = nanf || Mx == -INFINITY;
+    uint64_t tot = 0;
+    for (int j = 0; j < J; ++j) {
+      uint64_t q;
+      if (qc) q = 1;
+      else if (w[j] != w[j]) q = 0;
+      else q = (uint64_t)llrintf(pp_expf(w[j] - Mx) * 1099511627776.0f);
+      tot += q;
+      C[j] = tot;
+    }
+    double ll;
+    if (nanf) ll = NAN;
+    else if (collapsed) ll = -INFINITY;
+    else ll = (double)Mx + log((double)tot) - 40.0 * 0.69314718055994530942;
+    loglik += ll;
+    if ((d->flags & PPF_F_CLL) && d->cll) d->cll[(size_t)f * d->T + t] = ll;
+    int rs;
+    if (nanf) rs = 0;
+    else if (Mx == -INFINITY) rs = 0.0f > logthresh;
+    else rs = (Mx - mn) > logthresh;
+    if (rs) {
+      const uint32_t u32 = (d->flags & PPF_F_INJECT) ? pp_u32_from_float(d->inj_u[(size_t)f * d->T + t])
+                                                     : pp_resample_u32(d->seeds[f], (uint32_t)(t + 1));
+      const u128 Jsh = (u128)((uint64_t)J << 32);
+      int j = 0;
+      for (int k = 0; k < J; ++k) {
+        const u128 R = ((u128)u32 + ((u128)k << 32)) * (u128)tot;
+        while (j < J && (u128)C[j] * Jsh <= R) ++j;
+        par[k] = j;
+      }
+    } else {
+      for (int k = 0; k < J; ++k) par[k] = k;
+    }
+    if ((d->flags & PPF_F_SAVE_ANC) && d->anc) memcpy(d->anc + ((size_t)f * d->T + t) * J, par, sizeof(int) * J);
+    if (t == Tf - 1) {
+      float* out = d->swarm_out + (size_t)f * P * J;
+      for (int k = 0; k < J; ++k)
+        for (int p = 0; p < P; ++p) out[(size_t)p * J + k] = th[(size_t)p * J + par[k]];
+      break;
+    }
+    float lt32 = 0.0f;
+    if (!rs) {
+      if (nanf) lt32 = NAN;
+      else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
+    }
+    for (int k = 0; k < J; ++k) {
+      float xk[4], tk[64];
+      for (int q = 0; q < dx; ++q) xk[q] = x[q * J + par[k]];
+      for (int p = 0; p < P; ++p) tk[p] = th[(size_t)p * J + par[k]];
+      float b;
+      if (rs) b = base_rs;
+      else b = collapsed ? -pp_logf((float)J) : w[k] - lt32;
+      const float m = if2_step(d, f, u, k, t + 1, t + 2, cool[t + 1], tk, xk);
+      for (int q = 0; q < dx; ++q) xn[q * J + k] = xk[q];
+      for (int p = 0; p < P; ++p) thn[(size_t)p * J + k] = tk[p];
+      wn[k] = b + m;
+    }
+    float* tmp = x; x = xn; xn = tmp;
+    float* tt = th; th = thn; thn = tt;
+    float* tw = w; w = wn; wn = tw;
+  }
+  d->loglik[f] = loglik;
+  free(x); free(xn); free(th); free(thn); free(w); free(wn); free(C); free(par);
+}
+
+typedef struct {
+  const ppf_perfilter_desc* d;
+  int tid, nthreads;
+} if2_job_t;
+
+static void* if2_worker(void* arg) {
+  const if2_job_t* jb = (const if2_job_t*)arg;
+  for (int f = jb->tid; f < jb->d->F; f += jb->nthreads) run_perfilter(jb->d, f);
+  return NULL;
+}
+
+/* Runs the F perturbed filters of `d` (all pointers HOST memory). */
+int ppfo_perfilter(const ppf_perfilter_desc* d, int nthreads) {
+  if (!d || d->J < 1 || d->F < 1 || d->T < 1 || d->model.n_params > 64) return PPF_EINVAL;
+  if (nthreads <= 1 || d->F == 1) {
+    for (int f = 0; f < d->F; ++f) run_perfilter(d, f);
+    return PPF_OK;
+  }
+  if (nthreads > 256) nthreads = 256;
+  pthread_t th[256];
+  if2_job_t jobs[256];
+  for (int i = 0; i < nthreads; ++i) {
+    jobs[i].d = d; jobs[i].tid = i; jobs[i].nthreads = nthreads;
+    pthread_create(&th[i], NULL, if2_worker, &jobs[i]);
+  }
+  for (int i = 0; i < nthreads; ++i) pthread_join(th[i], NULL);
   return PPF_OK;
 }
 

@@ -292,3 +292,205 @@ def pomp_simulate_data(model, theta, T, key: jr.Key):
     k = jr.split(new_key, 1)[0]
     X, Y = simulate(model, theta, T, k, nsim=1)
     return X[:, 0, :], Y[:, 0, :]
+
+
+# ---------------------------------------------------------------------------
+# IF2: perturbed filter and the mif loop
+# ---------------------------------------------------------------------------
+
+
+class JaxPerfilterNoise:
+    """The key tree of one IF2 iteration (``mif.py:112-140`` and ``:171-181``).
+
+    ``split(key)`` -> carry key, t0-perturbation key (normal (J, P)); then
+    ``split(key, J+1)`` -> carry key, J rinit keys; then
+    ``split(key, T+1)[1:]`` are the step keys, each split in 3 (perturbation
+    normal (J, P), process key, resampling key).  Inside ``rprocess_interp``
+    the process key is split once per sub-step and then per particle
+    (``model_mechanics.py:904`` and ``:586``), as in the bootstrap filter.
+    """
+
+    def __init__(self, key: jr.Key, J: int, P: int, n_init: int, n_step: int, T: int):
+        s = jr.split(key)
+        key, sub = s[0], s[1]
+        self.zp0 = jr.normal(sub, (J, P))
+        sk = jr.split(key, J + 1)
+        key, self.init_keys = sk[0], sk[1:]
+        self.step_keys = jr.split(key, T + 1)[1:]
+        self.J, self.P, self.n_init, self.n_step = J, P, n_init, n_step
+
+    def perturb0(self):
+        return self.zp0
+
+    def init_normals(self):
+        if self.n_init == 0:
+            return np.zeros((self.J, 0), f32)
+        return np.stack([jr.normal(self.init_keys[j], (self.n_init,)) for j in range(self.J)])
+
+    def _keys(self, t):
+        k3 = jr.split(self.step_keys[t], 3)
+        return k3[0], k3[1], k3[2]
+
+    def perturb(self, t):
+        return jr.normal(self._keys(t)[0], (self.J, self.P))
+
+    def step_normals(self, t):
+        if self.n_step == 0:
+            return np.zeros((self.J, 0), f32)
+        sub2 = jr.split(self._keys(t)[1])[1]
+        pk = jr.split(sub2, self.J)
+        return np.stack([jr.normal(pk[j], (self.n_step,)) for j in range(self.J)])
+
+    def resample_uniform(self, t):
+        return f32(jr.uniform(self._keys(t)[2]))
+
+
+class ArrayPerfilterNoise:
+    """Injected IF2 draws: ``zp0`` (J,P), ``zp`` (T,J,P), ``z0``, ``z``, ``u``."""
+
+    def __init__(self, zp0, zp, z0, z, u):
+        self.zp0, self.zp = np.asarray(zp0, f32), np.asarray(zp, f32)
+        self.z0, self.z, self.u = np.asarray(z0, f32), np.asarray(z, f32), np.asarray(u, f32)
+
+    def perturb0(self):
+        return self.zp0
+
+    def init_normals(self):
+        return self.z0
+
+    def perturb(self, t):
+        return self.zp[t]
+
+    def step_normals(self, t):
+        return self.z[t]
+
+    def resample_uniform(self, t):
+        return f32(self.u[t])
+
+
+class RecordingPerfilterNoise:
+    """Wraps an IF2 noise source and records its draws as injection arrays."""
+
+    def __init__(self, src):
+        self.src = src
+        self.rec = {"zp0": None, "z0": None, "zp": [], "z": [], "u": []}
+
+    def perturb0(self):
+        self.rec["zp0"] = self.src.perturb0()
+        return self.rec["zp0"]
+
+    def init_normals(self):
+        self.rec["z0"] = self.src.init_normals()
+        return self.rec["z0"]
+
+    def perturb(self, t):
+        v = self.src.perturb(t)
+        self.rec["zp"].append(v)
+        return v
+
+    def step_normals(self, t):
+        v = self.src.step_normals(t)
+        self.rec["z"].append(v)
+        return v
+
+    def resample_uniform(self, t):
+        v = self.src.resample_uniform(t)
+        self.rec["u"].append(v)
+        return v
+
+    def arrays(self):
+        r = self.rec
+        return {"zp0": r["zp0"], "zp": np.stack(r["zp"]), "z0": r["z0"], "z": np.stack(r["z"]),
+                "u": np.asarray(r["u"], f32)}
+
+
+def _per_particle(m, th_est, fn):
+    """Apply ``fn(par, j)`` for each particle's natural-scale parameters."""
+    nat = m.from_est(th_est)
+    return [fn(m.unpack(nat[j]), j) for j in range(th_est.shape[0])]
+
+
+def perfilter(model, swarm_est, ys, J, rw_sig, rw_sig0, cool, cool0, noise, thresh=0.0):
+    """``_perfilter_internal`` + ``_perfilter_scan_body`` (mif.py:88-258).
+
+    ``swarm_est`` (J, P) on the estimation scale; ``cool`` (T,) and ``cool0``
+    are the cooling factors.  Returns ``(swarm (J, P) after the last
+    resampling, loglik float32)``.
+    """
+    m = MODELS[model]
+    ys = np.asarray(ys, f32)
+    T = ys.shape[0]
+    rw_sig = np.asarray(rw_sig, f32)
+    rw_sig0 = np.asarray(rw_sig0, f32)
+    th = np.asarray(swarm_est, f32)
+    th = (th + (f32(cool0) * rw_sig0)[None, :] * noise.perturb0()).astype(f32)
+    z0 = noise.init_normals()
+    X = np.concatenate(_per_particle(m, th, lambda p, j: m.rinit(p, z0[j:j + 1])), axis=0).astype(f32)
+    nw = np.full(J, -np.log(f32(J)), f32)
+    loglik = f32(0.0)
+    logthresh = np.log(f32(thresh)) if thresh > 0 else f32(-np.inf)
+    log1e18 = np.log(f32(1e-18))
+    for t in range(T):
+        thp = (th + (f32(cool[t]) * rw_sig)[None, :] * noise.perturb(t)).astype(f32)
+        z = noise.step_normals(t)
+        X = np.concatenate(_per_particle(m, thp, lambda p, j: m.rproc(p, X[j:j + 1], z[j:j + 1], t)),
+                           axis=0).astype(f32)
+        meas = np.concatenate(_per_particle(m, thp, lambda p, j: m.dmeas(p, ys[t], X[j:j + 1]))).astype(f32)
+        meas = np.nan_to_num(meas, nan=log1e18).astype(f32)
+        w = (nw + meas).astype(f32)
+        nwn, lt = normalize(w)
+        loglik = f32(loglik + lt)
+        with np.errstate(invalid="ignore"):
+            do_resample = bool(np.max(nwn) - np.min(nwn) > logthresh)
+        u = noise.resample_uniform(t)
+        if do_resample:
+            counts = resample(nwn, u)
+            X = X[counts]
+            th = thp[counts]
+            nw = (nwn[counts] - nwn[counts] - np.log(f32(J))).astype(f32)
+        else:
+            th = thp
+            nw = nwn
+    return th, loglik
+
+
+def mif(model, theta, ys, J, M, rw_sig, rw_sig0, cooling, key: jr.Key, n_monitors=0, thresh=0.0):
+    """``_mif_internal`` + ``_mif_scan_body`` (mif.py:16-85) for one replicate.
+
+    ``theta`` (P,) natural scale; ``cooling(nt, m, ntimes)`` the schedule.
+    Returns ``(logliks (M,), traces (M+1, P) natural, final swarm (J, P)
+    natural, draws)`` where ``draws`` lists, per iteration, the recorded
+    perturbed-filter draws and the monitors' draws.
+    """
+    m = MODELS[model]
+    ys = np.asarray(ys, f32)
+    T = ys.shape[0]
+    th_est = m.to_est(np.asarray(theta, f32))
+    P = th_est.shape[0]
+    par0 = m.unpack(np.asarray(theta, f32))
+    n_init, n_step = m.n_init(par0), m.n_step(par0)
+    swarm = np.repeat(th_est[None, :], J, axis=0).astype(f32)
+    m_keys = jr.split(key, M + 1)[1:]
+    means = [swarm.mean(axis=0, dtype=f32)]
+    logliks, draws = [], []
+    for it in range(M):
+        cool = np.array([cooling(i, it, T) for i in range(T)], f32)
+        rec = RecordingPerfilterNoise(JaxPerfilterNoise(m_keys[it], J, P, n_init, n_step, T))
+        new_swarm, ll = perfilter(model, swarm, ys, J, rw_sig, rw_sig0, cool, cool[0], rec, thresh)
+        mon = []
+        if n_monitors >= 1:
+            mean = swarm.mean(axis=0, dtype=f32)
+            mon_keys = jr.split(m_keys[it], n_monitors)
+            nll = []
+            for i in range(n_monitors):
+                r = RecordingNoise(JaxKeyNoise(mon_keys[i], J, n_init, n_step))
+                nll.append(-pfilter(model, m.from_est(mean), ys, J, r, thresh)["logLik"])
+                z0, z, u = r.arrays()
+                mon.append({"z0": z0, "z": z, "u": u})
+            ll = -np.mean(np.asarray(nll, f32), dtype=f32)
+        logliks.append(f32(ll))
+        draws.append({"perfilter": rec.arrays(), "monitors": mon})
+        swarm = new_swarm
+        means.append(swarm.mean(axis=0, dtype=f32))
+    traces = m.from_est(np.stack(means))
+    return np.asarray(logliks, f32), traces, m.from_est(swarm), draws

@@ -39,6 +39,8 @@ EXPORTED = (
     "ppf_pfilter",
     "ppf_mop_workspace_bytes",
     "ppf_mop",
+    "ppf_perfilter_workspace_bytes",
+    "ppf_perfilter",
     "ppf_workspace_status",
     "ppf_pfilter_noalloc",
     "ppf_profile_begin",
@@ -120,6 +122,39 @@ class MopDesc(ctypes.Structure):
     ]
 
 
+class PerfilterDesc(ctypes.Structure):
+    _fields_ = [
+        ("model", PpfModel),
+        ("J", ctypes.c_int32),
+        ("F", ctypes.c_int32),
+        ("T", ctypes.c_int32),
+        ("U", ctypes.c_int32),
+        ("flags", ctypes.c_uint32),
+        ("thresh", ctypes.c_float),
+        ("swarm_in", _vp),
+        ("swarm_out", _vp),
+        ("rw_sig", _vp),
+        ("rw_sig0", _vp),
+        ("cool", _vp),
+        ("cool0", _vp),
+        ("ys", _vp),
+        ("ycon", _vp),
+        ("unit", _vp),
+        ("T_u", _vp),
+        ("seeds", _vp),
+        ("inj_zp0", _vp),
+        ("inj_zp", _vp),
+        ("inj_z0", _vp),
+        ("inj_z", _vp),
+        ("inj_u", _vp),
+        ("loglik", _vp),
+        ("cll", _vp),
+        ("anc", _vp),
+        ("workspace", _vp),
+        ("ws_bytes", ctypes.c_size_t),
+    ]
+
+
 class PpfError(RuntimeError):
     """A non-zero return code from libppf.so."""
 
@@ -144,6 +179,10 @@ def _load():
     lib.ppf_mop_workspace_bytes.restype = ctypes.c_size_t
     lib.ppf_mop.argtypes = [ctypes.POINTER(MopDesc), _vp]
     lib.ppf_mop.restype = ctypes.c_int
+    lib.ppf_perfilter_workspace_bytes.argtypes = [ctypes.POINTER(PerfilterDesc)]
+    lib.ppf_perfilter_workspace_bytes.restype = ctypes.c_size_t
+    lib.ppf_perfilter.argtypes = [ctypes.POINTER(PerfilterDesc), _vp]
+    lib.ppf_perfilter.restype = ctypes.c_int
     lib.ppf_pfilter_noalloc.argtypes = [ctypes.POINTER(PfilterDesc), _vp]
     lib.ppf_pfilter_noalloc.restype = ctypes.c_int
     lib.ppf_workspace_status.argtypes = [_vp, _vp]

@@ -188,6 +188,49 @@ static void mop_to_pfilter(const ppf_mop_desc* d, ppf_pfilter_desc* p) {
   p->loglik = d->value;
 }
 
+// IF2: stream-path carve plus the two parameter-swarm buffers.
+static size_t carve_if2(Args& a, unsigned char* base) {
+  size_t off = carve(a, PPF_PATH_STREAM, base);
+  for (int i = 0; i < 2; ++i) {
+    a.TH[i] = reinterpret_cast<float*>(base ? base + off : nullptr);
+    off = align_up(off + 4ull * a.F * a.model.n_params * a.J);
+  }
+  return off;
+}
+
+static int validate_if2(const ppf_perfilter_desc* d) {
+  if (!d) return PPF_EINVAL;
+  if (d->J < 1 || d->J > PPF_MAX_J || d->F < 1 || d->T < 1 || d->U < 1) return PPF_EINVAL;
+  int rc = check_model(d->model);
+  if (rc) return rc;
+  if (!d->swarm_in || !d->swarm_out || !d->rw_sig || !d->rw_sig0 || !d->cool || !d->cool0) return PPF_EINVAL;
+  if (d->swarm_in == d->swarm_out) return PPF_EINVAL;
+  if (!d->ys || !d->loglik) return PPF_EINVAL;
+  if (!(d->flags & PPF_F_INJECT) && !d->seeds) return PPF_EINVAL;
+  if ((d->flags & PPF_F_INJECT) && (!d->inj_z || !d->inj_u || !d->inj_zp0 || !d->inj_zp)) return PPF_EINVAL;
+  if ((d->flags & PPF_F_INJECT) && d->model.kind == PPF_MODEL_LG && !d->inj_z0) return PPF_EINVAL;
+  if (d->model.kind == PPF_MODEL_RICKER && !d->ycon) return PPF_EINVAL;
+  if ((d->flags & PPF_F_CLL) && !d->cll) return PPF_EINVAL;
+  if ((d->flags & PPF_F_SAVE_ANC) && !d->anc) return PPF_EINVAL;
+  return PPF_OK;
+}
+
+static void fill_if2(const ppf_perfilter_desc* d, Args& a) {
+  ppf_pfilter_desc p;
+  memset(&p, 0, sizeof(p));
+  p.model = d->model;
+  p.J = d->J; p.F = d->F; p.T = d->T; p.U = d->U;
+  p.flags = (d->flags & (PPF_F_INJECT | PPF_F_CLL | PPF_F_SAVE_ANC)) | PPF_F_EST;
+  p.thresh = d->thresh;
+  p.ys = d->ys; p.ycon = d->ycon; p.unit = d->unit; p.T_u = d->T_u;
+  p.seeds = d->seeds; p.inj_z0 = d->inj_z0; p.inj_z = d->inj_z; p.inj_u = d->inj_u;
+  p.loglik = d->loglik; p.cll = d->cll; p.anc = d->anc;
+  fill_args(&p, a, MODE_IF2);
+  a.swarm_in = d->swarm_in; a.swarm_out = d->swarm_out;
+  a.rw_sig = d->rw_sig; a.rw_sig0 = d->rw_sig0; a.cool = d->cool; a.cool0 = d->cool0;
+  a.inj_zp0 = d->inj_zp0; a.inj_zp = d->inj_zp;
+}
+
 }  // namespace ppf
 
 using namespace ppf;
@@ -262,6 +305,29 @@ int ppf_mop(const ppf_mop_desc* d, void* stream) {
   if (rc) return rc;
   k_negate<<<(d->F + 127) / 128, 128, 0, s>>>(d->value, d->F);
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
+size_t ppf_perfilter_workspace_bytes(const ppf_perfilter_desc* d) {
+  if (!d || d->J < 1 || d->F < 1 || d->T < 1 || n_params_of(d->model) < 1) return 0;
+  Args a;
+  fill_if2(d, a);
+  a.model.n_params = n_params_of(d->model);
+  return carve_if2(a, nullptr);
+}
+
+int ppf_perfilter(const ppf_perfilter_desc* d, void* stream) {
+  int rc = validate_if2(d);
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  Args a;
+  fill_if2(d, a);
+  const size_t need = carve_if2(a, nullptr);
+  if (!d->workspace || d->ws_bytes < need) return PPF_EINVAL;
+  carve_if2(a, reinterpret_cast<unsigned char*>(d->workspace));
+  if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, s) != cudaSuccess) return PPF_ECUDA;
+  rc = reset_accumulators(a, s);
+  if (rc) return rc;
+  return run_if2(a, s);
 }
 
 int ppf_workspace_status(const void* workspace, void* stream) {

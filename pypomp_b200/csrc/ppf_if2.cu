@@ -1,0 +1,294 @@
+// ppf_if2.cu -- one iteration of IF2's perturbed particle filter.
+//
+// Replaces _perfilter_internal / _perfilter_scan_body
+// (pypomp/core/algorithms/mif.py:88-258) and _resampler_thetas
+// (helpers.py:103-141): every particle carries its own parameter vector on
+// the estimation scale.  Before the first step the vector is perturbed with
+// sds rw_sig0 * cool0 (mif.py:113-120) and the initial state is drawn with it;
+// before every step it is perturbed with sds rw_sig * cool[t] (mif.py:178-181),
+// then rproc and dmeas run with the perturbed vector, non-finite measurement
+// densities are mapped as jnp.nan_to_num(..., nan=log(1e-18)) does
+// (mif.py:205-210), and resampling moves state and vector together.  The
+// output is the swarm after the final resampling and the log-likelihood.
+// Weights, the exact CDF and the systematic offsets are those of the bootstrap
+// filter (the same k_sum, the same offset walk).
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include "ppf.h"
+#include "ppf_core.cuh"
+#include "ppf_internal.h"
+#include "ppf_kernels.cuh"
+#include "ppf_models.cuh"
+
+namespace ppf {
+
+// jnp.nan_to_num(m, nan=log(1e-18)): NaN -> log(1e-18), +inf -> FLT_MAX,
+// -inf -> -FLT_MAX.
+__device__ __forceinline__ float if2_measure(float m, float log1e18) {
+  if (m != m) return log1e18;
+  if (m == INFINITY) return FLT_MAX;
+  if (m == -INFINITY) return -FLT_MAX;
+  return m;
+}
+
+// Normals of particle k for IF2 perturbations (P per particle, tag PERTURB).
+template <bool INJ>
+__device__ __forceinline__ void perturb_noise(const Args& a, int f, int k, int s, int P, float* z) {
+  if (INJ) {
+    const float* src = (s == 0) ? a.inj_zp0 + ((size_t)f * a.J + k) * P
+                                : a.inj_zp + (((size_t)f * a.T + (s - 1)) * a.J + k) * P;
+    for (int i = 0; i < P; ++i) z[i] = src[i];
+  } else {
+    pp_normals(a.seeds[f], (uint32_t)k, (uint32_t)s, PPF_TAG_PERTURB, P, z);
+  }
+}
+
+template <class M, int TPB, bool INJ>
+__global__ void __launch_bounds__(TPB) k_if2_init(Args a) {
+  __shared__ unsigned int smk[2 * (TPB / 32)];
+  constexpr int DX = M::MAXDX;
+  constexpr int MP = M::MAXP;
+  const int f = blockIdx.y;
+  const int u = filter_unit(a, f);
+  const int J = a.J, P = a.model.n_params;
+  const float log1e18 = pp_logf(1e-18f);
+  Obs<M> ob;
+  ob.load(a, u, 0);
+  const float c0 = a.cool0[u], c1 = a.cool[(size_t)u * a.T];
+  float* X = a.X[0] + (size_t)f * DX * J;
+  float* W = a.W[0] + (size_t)f * J;
+  float* TH = a.TH[0] + (size_t)f * P * J;
+  const float* S = a.swarm_in + (size_t)f * P * J;
+  unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
+  const int k = blockIdx.x * TPB + threadIdx.x;
+  if (k < J) {
+    float th[MP];
+    float zp[MP];
+#pragma unroll
+    for (int p = 0; p < MP; ++p) th[p] = (p < P) ? S[(size_t)p * J + k] : 0.0f;
+    perturb_noise<INJ>(a, f, k, 0, P, zp);
+#pragma unroll
+    for (int p = 0; p < MP; ++p)
+      if (p < P) th[p] = th[p] + (c0 * a.rw_sig0[p]) * zp[p];
+    typename M::Consts c;
+    M::prepare(c, th, a.model, true);
+    float x[DX];
+    float z0[M::NZ0 > 0 ? M::NZ0 : 1];
+    step_noise<M>(a, f, k, 0, M::NZ0, z0);
+    M::rinit(c, z0, x);
+    perturb_noise<INJ>(a, f, k, 1, P, zp);
+#pragma unroll
+    for (int p = 0; p < MP; ++p)
+      if (p < P) th[p] = th[p] + (c1 * a.rw_sig[p]) * zp[p];
+    M::prepare(c, th, a.model, true);
+    float z[M::NZ];
+    step_noise<M>(a, f, k, 1, M::NZ, z);
+    const float m = if2_measure(step1<M>(c, ob, x, z), log1e18);
+    const float w = a.base_init + m;
+#pragma unroll
+    for (int d = 0; d < DX; ++d) X[d * J + k] = x[d];
+    W[k] = w;
+#pragma unroll
+    for (int p = 0; p < MP; ++p)
+      if (p < P) TH[(size_t)p * J + k] = th[p];
+    accum_maxmin(w, mx, mn, nn);
+  }
+  block_maxmin_u32<TPB>(mx, mn, smk);
+  nn = __syncthreads_or(nn);
+  Acc* acc = a.acc[0] + f;
+  if (threadIdx.x == 0) {
+    atomicMax(&acc->maxkey, mx);
+    atomicMin(&acc->minkey, mn);
+    if (nn) atomicOr(&acc->nan, 1u);
+    if (blockIdx.x == 0) a.loglik[f] = 0.0;
+  }
+}
+
+// Resample the tile's parents (state + parameter vector) and, unless this is
+// the filter's last step, perturb each child's vector and propagate it.
+// Parent states are staged in shared memory; a child reads its parent's
+// parameter vector straight from global memory (children of consecutive
+// parents are consecutive, so a warp's reads stay nearly coalesced).
+template <class M, int TPB, int IT, bool INJ>
+__global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
+  constexpr int TILE = TPB * IT;
+  constexpr int DX = M::MAXDX;
+  constexpr int MP = M::MAXP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int P = a.model.n_params;
+  float* xs = reinterpret_cast<float*>(smem_raw);                 // [DX][TILE]
+  int* st = reinterpret_cast<int*>(xs + DX * TILE);               // [TILE + 1]
+  float* wcar = reinterpret_cast<float*>(st + TILE + 4);          // [TILE]
+  __shared__ uint64_t s_scan[TPB / 32 + 1];
+  __shared__ unsigned int smk[2 * (TPB / 32)];
+
+  const int f = blockIdx.y, b = blockIdx.x;
+  const int u = filter_unit(a, f);
+  const int Tf = filter_len(a, u);
+  const int p2 = t & 1;
+  if (threadIdx.x == 0) {
+    a.desc[p2 ^ 1][(size_t)f * a.ntiles + b] = 0ull;
+    if (b == 0 && f == 0) a.counter[p2 ^ 1] = 0;
+  }
+  if (t >= Tf) return;
+  const Acc acc = a.acc[p2][f];
+  const uint64_t tot = a.tot[f];
+  if (b == 0 && threadIdx.x == 0) finalize_step(a, f, t, acc, tot, a.loglik + f);
+  const bool last = (t == Tf - 1);
+  const bool nanf = acc.nan != 0;
+  const float Mx = keyf(acc.maxkey);
+  const bool collapsed = !nanf && Mx == -INFINITY;
+  const bool qc = nanf || Mx == -INFINITY;
+  const bool rs = decide_resample(a, acc);
+  const int J = a.J;
+  const int jt = b * TILE;
+  const int ntile = min(TILE, J - jt);
+  const float* Xc = a.X[p2] + (size_t)f * DX * J;
+  const float* Wc = a.W[p2] + (size_t)f * J;
+  const float* THc = a.TH[p2] + (size_t)f * P * J;
+  float* Xn = a.X[p2 ^ 1] + (size_t)f * DX * J;
+  float* Wn = a.W[p2 ^ 1] + (size_t)f * J;
+  float* THn = a.TH[p2 ^ 1] + (size_t)f * P * J;
+  float* Sout = a.swarm_out + (size_t)f * P * J;
+  int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
+  const float log1e18 = pp_logf(1e-18f);
+  Obs<M> ob;
+  if (!last) ob.load(a, u, t + 1);
+  const float cl = last ? 0.0f : a.cool[(size_t)u * a.T + t + 1];
+  const int l0 = threadIdx.x * IT;
+  {
+    float wv[IT];
+#pragma unroll
+    for (int i = 0; i < IT; ++i) wv[i] = (l0 + i < ntile) ? Wc[jt + l0 + i] : 0.0f;
+    if (rs) {
+      const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
+      const uint64_t E = a.excl[(size_t)f * a.ntiles + b];
+      uint64_t q[IT];
+      uint64_t qs = 0;
+#pragma unroll
+      for (int i = 0; i < IT; ++i) {
+        q[i] = (l0 + i < ntile) ? qweight(wv[i], Mx, qc) : 0ull;
+        qs += q[i];
+      }
+      uint64_t btot;
+      const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
+      if (l0 < ntile) {
+        OffWalk wk = offwalk_init(o, E + tex);
+        st[l0] = wk.k;
+#pragma unroll
+        for (int i = 0; i < IT; ++i) {
+          if (l0 + i >= ntile) break;
+          const int kn = offwalk_add(o, wk, q[i]);
+          if (i + 1 < IT || l0 + i + 1 == ntile) st[l0 + i + 1] = kn;
+        }
+      }
+    } else {
+      float lt32 = 0.0f;
+      if (nanf) lt32 = __int_as_float(0x7fc00000);
+      else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
+      const float nwc = -pp_logf((float)J);
+#pragma unroll
+      for (int i = 0; i < IT; ++i)
+        if (l0 + i < ntile) {
+          st[l0 + i] = jt + l0 + i;
+          wcar[l0 + i] = collapsed ? nwc : wv[i] - lt32;
+        }
+      if (l0 < ntile && l0 + IT >= ntile) st[ntile] = jt + ntile;
+    }
+  }
+  for (int l = threadIdx.x; l < ntile; l += TPB) {
+#pragma unroll
+    for (int d = 0; d < DX; ++d) xs[d * TILE + l] = Xc[d * J + jt + l];
+  }
+  __syncthreads();
+  const int klo = st[0], khi = st[ntile];
+  unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
+  for (int k = klo + threadIdx.x; k < khi; k += TPB) {
+    const int l = find_parent(st, ntile, k);
+    if (anc) anc[k] = jt + l;
+    float th[MP];
+#pragma unroll
+    for (int p = 0; p < MP; ++p) th[p] = (p < P) ? THc[(size_t)p * J + jt + l] : 0.0f;
+    if (last) {
+#pragma unroll
+      for (int p = 0; p < MP; ++p)
+        if (p < P) Sout[(size_t)p * J + k] = th[p];
+      continue;
+    }
+    float zp[MP];
+    perturb_noise<INJ>(a, f, k, t + 2, P, zp);
+#pragma unroll
+    for (int p = 0; p < MP; ++p)
+      if (p < P) th[p] = th[p] + (cl * a.rw_sig[p]) * zp[p];
+    typename M::Consts c;
+    M::prepare(c, th, a.model, true);
+    float x[DX];
+#pragma unroll
+    for (int d = 0; d < DX; ++d) x[d] = xs[d * TILE + l];
+    float z[M::NZ];
+    step_noise<M>(a, f, k, t + 2, M::NZ, z);
+    const float m = if2_measure(step1<M>(c, ob, x, z), log1e18);
+    const float w = (rs ? a.base_rs : wcar[l]) + m;
+#pragma unroll
+    for (int d = 0; d < DX; ++d) Xn[d * J + k] = x[d];
+    Wn[k] = w;
+#pragma unroll
+    for (int p = 0; p < MP; ++p)
+      if (p < P) THn[(size_t)p * J + k] = th[p];
+    accum_maxmin(w, mx, mn, nn);
+  }
+  if (last) return;
+  block_maxmin_u32<TPB>(mx, mn, smk);
+  nn = __syncthreads_or(nn);
+  Acc* an = a.acc[p2 ^ 1] + f;
+  if (threadIdx.x == 0) {
+    if (mx) atomicMax(&an->maxkey, mx);
+    if (mn != 0xffffffffu) atomicMin(&an->minkey, mn);
+    if (nn) atomicOr(&an->nan, 1u);
+  }
+}
+
+template <class M, bool INJ>
+int run_if2_t(Args& a, cudaStream_t s) {
+  constexpr int TPB = 256, IT = 8, TILE = TPB * IT;
+  if (a.tile != TILE) return PPF_EINVAL;   // the workspace was carved for this tile
+  const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4) + sizeof(float) * TILE;
+  if (cudaFuncSetAttribute(k_if2_resprop<M, TPB, IT, INJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return PPF_ECUDA;
+  dim3 grid_init((a.J + TPB - 1) / TPB, a.F);
+  dim3 grid(a.ntiles, a.F);
+  PROF_BEGIN(KIND_IF2);
+  k_if2_init<M, TPB, INJ><<<grid_init, TPB, 0, s>>>(a);
+  for (int t = 0; t < a.T; ++t) {
+    k_sum<M, TPB, IT><<<a.ntiles * a.F, TPB, 0, s>>>(a, t);
+    k_if2_resprop<M, TPB, IT, INJ><<<grid, TPB, smem, s>>>(a, t);
+  }
+  PROF_END(KIND_IF2);
+  return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
+template <class M>
+int run_if2_m(Args& a, cudaStream_t s) {
+  return (a.flags & PPF_F_INJECT) ? run_if2_t<M, true>(a, s) : run_if2_t<M, false>(a, s);
+}
+
+int run_if2(Args& a, cudaStream_t s) {
+  switch (a.model.kind) {
+    case PPF_MODEL_LG:
+      switch (a.model.dx) {
+        case 1: return run_if2_m<LG<1>>(a, s);
+        case 2: return run_if2_m<LG<2>>(a, s);
+        case 3: return run_if2_m<LG<3>>(a, s);
+        case 4: return run_if2_m<LG<4>>(a, s);
+        default: return PPF_EUNSUPPORTED;
+      }
+    case PPF_MODEL_SV: return run_if2_m<SV>(a, s);
+    case PPF_MODEL_RICKER: return run_if2_m<Ricker>(a, s);
+    default: return PPF_EINVAL;
+  }
+}
+
+}  // namespace ppf

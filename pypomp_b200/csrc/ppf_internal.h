@@ -66,6 +66,16 @@ struct Args {
   int ckpt_every, nseg;
   float* mop_M;           // [F][T]
   double* mop_S;          // [F][T]
+  // IF2 perturbed filter (MODE_IF2): per-particle parameter swarm
+  const float* swarm_in;  // [F][P][J] estimation scale
+  float* swarm_out;       // [F][P][J] after the final resampling
+  float* TH[2];           // [F][P][J] each, perturbed parameters of the live swarm
+  const float* rw_sig;    // [P] per-step sds
+  const float* rw_sig0;   // [P] t0 sds
+  const float* cool;      // [U][T] cooling factor of the perturbation before step t
+  const float* cool0;     // [U] cooling factor of the t0 perturbation
+  const float* inj_zp0;   // [F][J][P] t0 perturbation normals (PPF_F_INJECT)
+  const float* inj_zp;    // [F][T][J][P] per-step perturbation normals (PPF_F_INJECT)
   // host copies for host-side loops (plain path)
   const int* T_u_host;
   const int* unit_host;
@@ -98,6 +108,7 @@ struct MopWork {
 int run_pfilter_path(Args& a, int path, cudaStream_t s);
 int run_stream_any(Args& a, cudaStream_t s);   // stream path, any model
 int run_mop(Args& a, const MopWork& w, cudaStream_t s);
+int run_if2(Args& a, cudaStream_t s);
 int reset_accumulators(Args& a, cudaStream_t s);
 size_t resident_smem_bytes(const Args& a);
 

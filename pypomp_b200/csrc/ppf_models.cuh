@@ -31,7 +31,7 @@ struct LG {
   static constexpr int NZ = DX;        // process normals per particle-step
   static constexpr int NZ0 = DX;       // initial-state normals per particle
   static constexpr int MAXDY = 4;
-  static constexpr int MAXP = 16 + 16 + 10 + 10 + 4;
+  static constexpr int MAXP = DX * DX + 4 * DX + DX * (DX + 1) / 2 + 10 + DX;  // dy <= 4
   struct Consts {
     int dx, dy;
     float A[16], C[16], LQ[16], L[16], Linv[4], X0[4];

@@ -102,127 +102,6 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
   }
 }
 
-// Fixed-point sums of the weights of one tile, then the decoupled-lookback
-// prefix over the tiles of the filter (Merrill & Garland 2016).
-template <class M, int TPB, int IT>
-__global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
-  constexpr int TILE = TPB * IT;
-  constexpr int DX = M::MAXDX;
-  __shared__ int s_v;
-  __shared__ uint64_t s_red[TPB / 32];
-  __shared__ double sd[TPB / 32];
-  if (threadIdx.x == 0) s_v = atomicAdd(a.counter + (t & 1), 1);
-  __syncthreads();
-  const int v = s_v;
-  if (v >= a.ntiles * a.F) {  // defensive: a stale counter must not index past the batch
-    if (threadIdx.x == 0) atomicOr(a.err, 4u);
-    return;
-  }
-  const int f = v / a.ntiles, b = v % a.ntiles;
-  const int u = filter_unit(a, f);
-  if (t >= filter_len(a, u)) return;
-  const int p = t & 1;
-  const Acc acc = a.acc[p][f];
-  if (b == 0 && threadIdx.x == 0) {
-    Acc* nx = a.acc[p ^ 1] + f;
-    nx->maxkey = 0u; nx->minkey = 0xffffffffu; nx->nan = 0u;
-    nx->s2 = 0.0;
-    for (int d = 0; d < 4; ++d) { nx->fx[d] = 0.0; nx->px[d] = 0.0; }
-  }
-  const bool nanf = acc.nan != 0;
-  const float Mx = keyf(acc.maxkey);
-  const bool collapsed = nanf || Mx == -INFINITY;
-  const int J = a.J;
-  const float* W = a.W[p] + (size_t)f * J;
-  const int jb = b * TILE + threadIdx.x * IT;
-  uint64_t qs = 0;
-  float wv[IT];
-  // float4 loads only when every filter's row starts 16-byte aligned (J % 4 == 0)
-  if (jb + IT <= J && (IT % 4) == 0 && (J & 3) == 0) {
-#pragma unroll
-    for (int i = 0; i < IT; i += 4) {
-      const float4 v4 = *reinterpret_cast<const float4*>(W + jb + i);
-      wv[i] = v4.x; wv[i + 1] = v4.y; wv[i + 2] = v4.z; wv[i + 3] = v4.w;
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < IT; ++i) wv[i] = (jb + i < J) ? W[jb + i] : -INFINITY;
-  }
-#pragma unroll
-  for (int i = 0; i < IT; ++i) qs += (jb + i < J) ? qweight(wv[i], Mx, collapsed) : 0ull;
-  // block total
-  {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t wsum = warp_sum_u64(qs);
-    if (lane == 0) s_red[warp] = wsum;
-    __syncthreads();
-  }
-  uint64_t* desc = a.desc[p] + (size_t)f * a.ntiles;
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    uint64_t btot = lane < TPB / 32 ? s_red[lane] : 0ull;
-    btot = warp_sum_u64(btot);
-    uint64_t excl = 0;
-    if (b == 0) {
-      if (lane == 0) st_release_u64(desc, kStatusIncl | btot);
-    } else {
-      if (lane == 0) st_release_u64(desc + b, kStatusAgg | btot);
-      int pos = b - 1;
-      long long spins = 0;
-      bool timed_out = false;
-      while (true) {
-        const int idx = pos - lane;
-        uint64_t d = idx >= 0 ? ld_acquire_u64(desc + idx) : kStatusIncl;
-        while (__any_sync(0xffffffffu, (d >> 62) == 0ull)) {
-          if (++spins > kSpinCap) { timed_out = true; break; }
-          if ((d >> 62) == 0ull) { __nanosleep(32); d = ld_acquire_u64(desc + idx); }
-        }
-        if (timed_out) break;
-        const unsigned int inc = __ballot_sync(0xffffffffu, (d >> 62) == 2ull);
-        if (inc) {
-          const int first = __ffs(inc) - 1;
-          excl += warp_sum_u64(lane <= first ? (d & kValueMask) : 0ull);
-          break;
-        }
-        excl += warp_sum_u64(d & kValueMask);
-        pos -= 32;
-      }
-      if (timed_out && lane == 0) atomicOr(a.err, 1u);
-      if (lane == 0) st_release_u64(desc + b, kStatusIncl | (excl + btot));
-    }
-    if (lane == 0) {
-      a.excl[(size_t)f * a.ntiles + b] = excl;
-      if (b == a.ntiles - 1) a.tot[f] = excl + btot;
-    }
-  }
-  if (a.flags & PPF_F_ESS) {
-    double s2 = 0.0;
-#pragma unroll
-    for (int i = 0; i < IT; ++i)
-      if (jb + i < J) {
-        const double e = collapsed ? 1.0 : (double)pp_expf(wv[i] - Mx);
-        s2 += e * e;
-      }
-    const double s = block_sum_f64<TPB>(s2, sd);
-    if (threadIdx.x == 0) atomicAdd(&a.acc[p][f].s2, s);
-  }
-  if (a.flags & PPF_F_FMEAN) {
-    const float* X = a.X[p] + (size_t)f * DX * J;
-#pragma unroll
-    for (int d = 0; d < DX; ++d) {
-      double s = 0.0;
-#pragma unroll
-      for (int i = 0; i < IT; ++i)
-        if (jb + i < J) {
-          const double e = collapsed ? 1.0 : (double)pp_expf(wv[i] - Mx);
-          s += (double)X[d * J + jb + i] * e;
-        }
-      s = block_sum_f64<TPB>(s, sd);
-      if (threadIdx.x == 0) atomicAdd(&a.acc[p][f].fx[d], s);
-    }
-  }
-}
-
 // Resample the parents of one tile and propagate their children to the next
 // observation (rproc + dmeas fused), writing the next step's X, W.
 //   1. fixed-point weights of the tile's parents, block scan, plus the tile's

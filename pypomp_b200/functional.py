@@ -296,3 +296,164 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
         th = th + eta_arr[m] * direction
         traces[:, m + 1] = th
     return nll, traces
+
+
+# ---------------------------------------------------------------------------
+# IF2
+# ---------------------------------------------------------------------------
+
+
+def run_perfilter(struct: PompStruct, swarm, seeds_f: np.ndarray, J: int, rw_sig, rw_sig0, cool, cool0,
+                  *, thresh: float = 0.0, unit_f=None, inject=None, CLL: bool = False,
+                  save_ancestors: bool = False):
+    """One batched call of ``ppf_perfilter``: one IF2 iteration over F swarms.
+
+    ``swarm`` is either a CUDA tensor (F, P, J) on the estimation scale (kept
+    on the device; the result swarm comes back the same way) or a host array
+    (F, J, P).  ``cool`` (T,) or (U, T) and ``cool0`` (scalar or (U,)) are the
+    cooling factors of the step and t0 perturbations.  ``inject`` optionally
+    holds host arrays ``zp0`` (F,J,P), ``zp`` (F,T,J,P), ``z0``, ``z``, ``u``
+    replacing the Philox draws.  Returns a dict with ``loglik`` (F,),
+    ``swarm`` and optionally ``cll`` / ``anc``.
+    """
+    torch = _ffi.require_cuda()
+    if J < 1:
+        raise ValueError("J should be greater than 0.")
+    if J > _ffi.PPF_MAX_J:
+        raise ValueError(f"J must be at most {_ffi.PPF_MAX_J}.")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    spec = struct.spec
+    P = spec.n_params
+    device_swarm = hasattr(swarm, "is_cuda")
+    if device_swarm:
+        sw_d = swarm.to(dev, torch.float32).contiguous()
+        F = sw_d.shape[0]
+    else:
+        sw = np.asarray(swarm, dtype=np.float32)
+        F = sw.shape[0]
+        sw_d = torch.from_numpy(np.ascontiguousarray(sw.transpose(0, 2, 1))).to(dev)
+    if tuple(sw_d.shape) != (F, P, J):
+        raise ValueError(f"swarm must hold {P} parameters of {J} particles per filter")
+    ys_d, ycon_d, Tu_d, U, T = _device_inputs(torch, struct, dev)
+    cool_h = np.ascontiguousarray(np.broadcast_to(np.asarray(cool, np.float32), (U, T)))
+    cool0_h = np.ascontiguousarray(np.broadcast_to(np.asarray(cool0, np.float32), (U,)))
+    f32d = dict(dtype=torch.float32, device=dev)
+    keep = {
+        "rw_sig": torch.tensor(np.asarray(rw_sig, np.float32), **f32d),
+        "rw_sig0": torch.tensor(np.asarray(rw_sig0, np.float32), **f32d),
+        "cool": torch.from_numpy(cool_h).to(dev),
+        "cool0": torch.from_numpy(cool0_h).to(dev),
+        "seeds": torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).copy()).to(dev),
+    }
+    unit_d = None
+    if unit_f is not None:
+        unit_d = torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
+    out = {"loglik": torch.zeros(F, dtype=torch.float64, device=dev),
+           "swarm": torch.empty(F, P, J, **f32d)}
+    flags = 0
+    if CLL:
+        flags |= _ffi.F_CLL
+        out["cll"] = torch.zeros(F, T, dtype=torch.float64, device=dev)
+    if save_ancestors:
+        flags |= _ffi.F_SAVE_ANC
+        out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=dev)
+    inj = {}
+    if inject is not None:
+        flags |= _ffi.F_INJECT
+        for k in ("zp0", "zp", "z0", "z", "u"):
+            if inject.get(k) is not None:
+                inj[k] = torch.from_numpy(np.ascontiguousarray(inject[k], dtype=np.float32)).to(dev)
+    d = _ffi.PerfilterDesc()
+    d.model = spec.ffi_model()
+    d.J, d.F, d.T, d.U = J, F, T, U
+    d.flags = flags
+    d.thresh = float(max(0.0, thresh))
+    d.swarm_in, d.swarm_out = _ffi.ptr(sw_d), _ffi.ptr(out["swarm"])
+    d.rw_sig, d.rw_sig0 = _ffi.ptr(keep["rw_sig"]), _ffi.ptr(keep["rw_sig0"])
+    d.cool, d.cool0 = _ffi.ptr(keep["cool"]), _ffi.ptr(keep["cool0"])
+    d.ys, d.ycon, d.unit, d.T_u = _ffi.ptr(ys_d), _ffi.ptr(ycon_d), _ffi.ptr(unit_d), _ffi.ptr(Tu_d)
+    d.seeds = _ffi.ptr(keep["seeds"])
+    for k in ("zp0", "zp", "z0", "z", "u"):
+        setattr(d, "inj_" + k, _ffi.ptr(inj.get(k)))
+    d.loglik, d.cll, d.anc = _ffi.ptr(out["loglik"]), _ffi.ptr(out.get("cll")), _ffi.ptr(out.get("anc"))
+    nbytes = _ffi.LIB.ppf_perfilter_workspace_bytes(d)
+    ws = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
+    d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    _ffi.check(_ffi.LIB.ppf_perfilter(d, stream), "ppf_perfilter")
+    _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_perfilter")
+    if device_swarm:
+        return out
+    res = {k: v.cpu().numpy() for k, v in out.items() if k != "swarm"}
+    res["swarm"] = out["swarm"].cpu().numpy().transpose(0, 2, 1).copy()
+    return res
+
+
+def mif(struct: PompStruct, thetas_array, rw_sd, M: int, J: int, keys, thresh: float = 0.0,
+        n_monitors: int = 0, *, inject=None):
+    """Iterated filtering 2 (``pypomp/functional/mif.py:15-122``,
+    ``_mif_internal`` / ``_mif_scan_body`` at ``pypomp/core/algorithms/mif.py:16-85``).
+
+    ``thetas_array`` (n_reps, J, P) starting swarms on the natural scale,
+    ``rw_sd`` an :class:`~pypomp_b200.optim.RWSigma`, ``keys`` (n_reps,).
+    Each iteration m runs one perturbed filter per replicate (all replicates
+    in one ``ppf_perfilter`` call, swarms resident on the GPU) with cooling
+    factors ``rw_sd.cooling_factor(t, m, T)``; with ``n_monitors`` >= 1 the
+    recorded log-likelihood is the mean over ``n_monitors`` unperturbed
+    filters at the swarm mean before the iteration (mean of the negative
+    log-likelihoods, as the reference averages them), else the perturbed
+    filter's.  Key tree per replicate: ``split(key, M+1)[1:]`` iteration keys;
+    the monitors use ``split(iteration key, n_monitors)``.  ``inject``
+    optionally replays external draws: one dict per iteration with
+    ``"perfilter"`` (arrays ``zp0``, ``zp``, ``z0``, ``z``, ``u`` with a
+    leading replicate axis) and ``"monitors"`` (a list of ``z0``/``z``/``u``
+    dicts, leading replicate axis).  Returns ``(logliks (n_reps, M), traces
+    (n_reps, M+1, P), final swarm (n_reps, J, P))``, natural scale.
+    """
+    from . import random as pprandom
+
+    torch = _ffi.require_cuda()
+    spec = struct.spec
+    names = list(spec.param_names)
+    th = np.asarray(thetas_array, dtype=np.float32)
+    if th.ndim != 3 or th.shape[1] != J or th.shape[2] != len(names):
+        raise ValueError(f"thetas_array must have shape (n_reps, {J}, {len(names)})")
+    if M < 0:
+        raise ValueError("M must be non-negative")
+    n = th.shape[0]
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    if keys.shape[0] != n:
+        raise ValueError("keys must have one key per replicate")
+    rw_sig, rw_sig0 = rw_sd.arrays(names)
+    T = np.asarray(struct.ys).shape[-2]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    est = spec.to_est(th.reshape(-1, len(names))).reshape(th.shape).astype(np.float32)
+    swarm = torch.from_numpy(np.ascontiguousarray(est.transpose(0, 2, 1))).to(dev)   # (n, P, J)
+    m_keys = np.stack([pprandom.split(k, M + 1)[1:] for k in keys]) if M > 0 else np.zeros((n, 0), np.uint64)
+    means = [swarm.mean(dim=2)]
+    logliks = np.zeros((n, M))
+    for it in range(M):
+        cool = np.array([rw_sd.cooling_factor(i, it, T) for i in range(T)], dtype=np.float32)
+        inj = inject[it] if inject is not None else None
+        res = run_perfilter(struct, swarm, m_keys[:, it], J, rw_sig, rw_sig0, cool, cool[0], thresh=thresh,
+                            inject=None if inj is None else inj["perfilter"])
+        if n_monitors >= 1:
+            mean = means[-1].cpu().numpy()
+            mon = np.stack([pprandom.split(k, n_monitors) for k in m_keys[:, it]])
+            minj = None
+            if inj is not None:
+                minj = {k: np.stack([np.stack([inj["monitors"][i][k][r] for i in range(n_monitors)])
+                                     for r in range(n)]).reshape((n * n_monitors,) + inj["monitors"][0][k].shape[1:])
+                        for k in ("z0", "z", "u")}
+            pf = run_pfilter(struct, np.repeat(mean, n_monitors, axis=0), mon.reshape(-1), J,
+                             thresh=thresh, est=True, inject=minj)
+            logliks[:, it] = -(-pf["loglik"].reshape(n, n_monitors)).mean(axis=1)
+        else:
+            logliks[:, it] = res["loglik"].cpu().numpy()
+        swarm = res["swarm"]
+        means.append(swarm.mean(dim=2))
+    traces = torch.stack(means, dim=1).cpu().numpy()                       # (n, M+1, P) est
+    traces = spec.from_est(traces.reshape(-1, len(names))).reshape(traces.shape)
+    final = swarm.cpu().numpy().transpose(0, 2, 1)
+    final = spec.from_est(final.reshape(-1, len(names))).reshape(final.shape)
+    return logliks, traces, final

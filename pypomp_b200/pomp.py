@@ -215,6 +215,74 @@ class Pomp:
             config={"J": J, "reps": reps, "thresh": thresh},
             execution_time=(time.time() - start) if track_time else None, key=old_key))
 
+    def mif(self, J: int, M: int, rw_sd, key=None, theta=None, thresh: float = 0.0,
+            n_monitors: int = 0, track_time: bool = True) -> None:
+        """Iterated filtering 2 (``pypomp/core/estimation_mixin.py:274-445``).
+
+        Starts every particle of replicate i at ``theta[i]``, runs
+        ``functional.mif`` with one key per replicate (``split(new_key,
+        n_reps)``), sets ``self.theta`` to the final swarm means with the
+        last iteration's log-likelihoods, and records the traces
+        (``logLik`` is NaN at iteration 0)."""
+        from . import functional as F
+
+        start = time.time()
+        thresh = float(max(0.0, thresh))
+        if set(rw_sd.param_names) != set(self.canonical_param_names):
+            raise ValueError(
+                "rw_sd.sigmas keys must match canonical_param_names up to reordering. "
+                f"Got {sorted(rw_sd.param_names)}, expected {sorted(self.canonical_param_names)}.")
+        theta_in = deepcopy(self._prepare_theta_input(theta))
+        theta_for_results = deepcopy(theta_in)
+        new_key, old_key = self._update_fresh_key(key)
+        n = theta_in.num_replicates()
+        if J < 1:
+            raise ValueError("J should be greater than 0.")
+        keys = pprandom.split(new_key, n)
+        thetas = theta_in.to_array(self.canonical_param_names)
+        swarms = np.repeat(thetas[:, None, :], J, axis=1)
+        logliks, traces, _ = F.mif(self.to_struct(), swarms, rw_sd, M, J, keys, thresh, n_monitors)
+        lls = np.concatenate([np.full((n, 1), np.nan), logliks], axis=1)
+        self.theta = PompParameters.from_array(traces[:, M, :], self.canonical_param_names)
+        self.theta.logLik = logliks[:, -1] if M > 0 else None
+        self.results_history.add(Result(
+            method="mif", theta=theta_for_results,
+            payload={"logLiks": lls, "traces": traces, "param_names": self.canonical_param_names},
+            config={"J": J, "M": M, "rw_sd": rw_sd, "thresh": thresh, "n_monitors": n_monitors},
+            execution_time=(time.time() - start) if track_time else None, key=old_key))
+
+    def train(self, J: int, M: int, eta, key=None, theta=None, optimizer=None, alpha: float = 0.97,
+              thresh: float = 0.0, alpha_cooling: float = 1.0, n_monitors: int = 1,
+              track_time: bool = True) -> None:
+        """MOP-alpha gradient training (``pypomp/core/estimation_mixin.py:446-620``)."""
+        from . import functional as F
+        from .optim import Adam, LearningRate
+
+        start = time.time()
+        optimizer = optimizer or Adam()
+        thresh = float(max(0.0, thresh))
+        theta_in = deepcopy(self._prepare_theta_input(theta))
+        theta_for_results = deepcopy(theta_in)
+        n = theta_in.num_replicates()
+        if J < 1:
+            raise ValueError("J should be greater than 0")
+        if not isinstance(eta, LearningRate):
+            raise TypeError("eta must be a LearningRate object")
+        new_key, old_key = self._update_fresh_key(key)
+        keys = pprandom.split(new_key, n)
+        th_est = self.spec.to_est(theta_in.to_array(self.canonical_param_names))
+        nll, traces = F.train(self.to_struct(), th_est, J, optimizer, M, eta, alpha, keys,
+                              alpha_cooling, thresh, n_monitors)
+        nat = self.spec.from_est(traces.reshape(-1, traces.shape[-1])).reshape(traces.shape)
+        self.theta = PompParameters.from_array(nat[:, -1, :], self.canonical_param_names)
+        self.theta.logLik = -nll[:, -1]
+        self.results_history.add(Result(
+            method="train", theta=theta_for_results,
+            payload={"logLiks": -nll, "traces": nat, "param_names": self.canonical_param_names},
+            config={"J": J, "M": M, "eta": eta, "alpha": alpha, "thresh": thresh,
+                    "alpha_cooling": alpha_cooling, "optimizer": optimizer},
+            execution_time=(time.time() - start) if track_time else None, key=old_key))
+
     # -- analysis ------------------------------------------------------------
     def results(self, index: int = -1, ignore_nan: bool = False) -> pd.DataFrame:
         return self.results_history.results(index=index, ignore_nan=ignore_nan)

@@ -13,7 +13,9 @@ Writes
                    key=jax.random.key(0))``, tests/test_regression/conftest.py:23)
                    regenerated through oracle/jaxrng.py, plus the exact
                    normals and uniforms the reference draws for each locked
-                   filter run (replayed key trees), for noise-injection runs
+                   filter run (replayed key trees), for noise-injection runs;
+                   ``mif_*`` / ``mift_*`` hold the draws of the locked mif runs
+                   (perturbation normals too) and their monitors
 """
 
 from __future__ import annotations
@@ -93,7 +95,29 @@ def main(ref_root: Path):
     rp.mop("LG", THETA_LG1D, ys, J, 0.5, rec)
     z0, z, u = rec.arrays()
     arrays.update(mop_z0=z0, mop_z=z, mop_u=u)
+    # mif regression (test_mif_regression.py): uniform rw sd 0.02, geometric
+    # cooling 0.5, thresh 0; 1 replicate M=3 without monitors, and 2 replicates
+    # (theta0, 1.05 theta0) M=4 with one monitor
+    sig = np.full(5, 0.02, f32)
+    sig0 = np.zeros(5, f32)
+    k = jr.split(jr.key(20260811), 1)[0]
+    _, _, _, draws = rp.mif("LG", THETA_LG1D, ys, J, 3, sig, sig0, mif_cooling, k, 0)
+    for key in ("zp0", "zp", "z0", "z", "u"):
+        arrays[f"mif_{key}"] = np.stack([d["perfilter"][key] for d in draws])          # (M, ...)
+    ks = jr.split(jr.key(20260812), 2)
+    reps = [rp.mif("LG", thetas[r], ys, J, 4, sig, sig0, mif_cooling, ks[r], 1)[3] for r in range(2)]
+    for key in ("zp0", "zp", "z0", "z", "u"):
+        arrays[f"mift_{key}"] = np.stack([np.stack([d["perfilter"][key] for d in reps[r]]) for r in range(2)])
+        if key in ("z0", "z", "u"):
+            arrays[f"mift_mon_{key}"] = np.stack([np.stack([d["monitors"][0][key] for d in reps[r]])
+                                                  for r in range(2)])                # (2, M, ...)
     np.savez(OUT / "ref_lg1d.npz", **arrays)
+
+
+def mif_cooling(nt, m, ntimes):
+    """Geometric cooling with a = 0.5 in float32 (``rw_sigma.py:193-224``)."""
+    frac = f32(f32(nt) / f32(ntimes) + f32(m))
+    return f32(f32(0.5 ** (1.0 / 50.0)) ** frac)
 
 
 

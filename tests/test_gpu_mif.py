@@ -1,0 +1,158 @@
+"""IF2 (perturbed filter + mif loop) on the GPU against the oracle.
+
+* ``ppf_perfilter`` is bit-identical to the C oracle's restatement
+  (``oracle/ppf_oracle.c`` ``ppfo_perfilter``) for LG 2-D, SV and Ricker:
+  ancestors, conditional log-likelihoods, log-likelihood and final swarm,
+  with one and several tiles per swarm, thresh 0 and 20;
+* with zero random-walk sds the perturbed filter is the bootstrap filter
+  (same ancestors and log-likelihoods bit for bit);
+* ``functional.mif`` replaying the reference's own draws reproduces the
+  locked ``test_mif_regression.csv`` and ``test_mif_full_trace_regression.csv``
+  (tolerance of the reference's regression tests);
+* ``Pomp.mif`` runs end to end on Philox draws and fills the result tables.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import cora
+
+pytestmark = pytest.mark.gpu
+f32 = np.float32
+
+
+def _F():
+    from pypomp_b200 import functional as F
+
+    return F
+
+
+def _case(model):
+    import pypomp_b200 as pp
+
+    from tests.conftest import LG2_Q, LG2_R
+
+    if model == "LG":
+        m = pp.LG(T=12, Q=LG2_Q, R=LG2_R, key=3)
+    elif model == "SV":
+        m = pp.SV(T=25, key=1)
+    else:
+        m = pp.Ricker(T=15, key=2)
+    st = m.to_struct()
+    th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(f32)
+    return m, st, th
+
+
+def _swarm(th, F, J, seed):
+    rng = np.random.default_rng(seed)
+    P = th.shape[1]
+    return (np.repeat(th[:, :, None], J, axis=2).repeat(F, axis=0)
+            + f32(0.01) * rng.standard_normal((F, P, J)).astype(f32)).astype(f32)
+
+
+@pytest.mark.parametrize("thresh", [0.0, 20.0])
+@pytest.mark.parametrize("J", [1000, 5000])
+@pytest.mark.parametrize("model", ["LG", "SV", "Ricker"])
+def test_perfilter_bit_exact_vs_oracle(model, J, thresh):
+    F = _F()
+    m, st, th = _case(model)
+    spec = m.spec
+    nF, P, T = 3, th.shape[1], st.ys.shape[0]
+    swarm = _swarm(th, nF, J, 5)
+    sig = np.full(P, 0.02, f32)
+    sig0 = np.zeros(P, f32)
+    sig0[-1] = 0.05
+    cool = (0.98 ** np.arange(T)).astype(f32)
+    seeds = np.array([11, 12, 13], np.uint64)
+    want = cora.perfilter(spec.kind, spec.dx, spec.dy, swarm, st.ys, J, sig, sig0, cool, f32(0.99),
+                          seeds=seeds, ycon=spec.ycon(st.ys), dt=spec.dt, thresh=thresh, CLL=True, anc=True)
+    got = F.run_perfilter(st, swarm.transpose(0, 2, 1), seeds, J, sig, sig0, cool, f32(0.99), thresh=thresh,
+                          CLL=True, save_ancestors=True)
+    assert np.array_equal(got["anc"], want["anc"])
+    assert np.array_equal(got["swarm"], want["swarm"].transpose(0, 2, 1))
+    np.testing.assert_allclose(got["cll"], want["cll"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(got["loglik"], want["loglik"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("thresh", [0.0, 20.0])
+def test_perfilter_without_perturbation_is_pfilter(lg2d, thresh):
+    F = _F()
+    st = lg2d.to_struct()
+    th = lg2d.spec.to_est(lg2d.theta.to_array(lg2d.canonical_param_names)).astype(f32)
+    P, J, T = th.shape[1], 4096, st.ys.shape[0]
+    th2 = np.repeat(th, 2, axis=0)
+    th2[1, 0] += f32(0.01)
+    seeds = np.array([7, 8], np.uint64)
+    zero = np.zeros(P, f32)
+    swarm = np.repeat(th2[:, None, :], J, axis=1)
+    got = F.run_perfilter(st, swarm, seeds, J, zero, zero, np.ones(T, f32), 1.0, thresh=thresh,
+                          CLL=True, save_ancestors=True)
+    want = F.run_pfilter(st, th2, seeds, J, thresh=thresh, est=True, CLL=True, save_ancestors=True,
+                         path="stream")
+    assert np.array_equal(got["anc"], want["anc"])
+    assert np.array_equal(got["cll"], want["cll"])
+    assert np.array_equal(got["loglik"], want["loglik"])
+
+
+def _rw():
+    from pypomp_b200.optim import RWSigma
+
+    return RWSigma({n: 0.02 for n in ("A11", "C11", "Q11", "R11", "X0_1")}).geometric_cooling(0.5)
+
+
+def _struct(ref_lg1d):
+    from pypomp_b200.functional import PompStruct
+    from pypomp_b200.models import lg_spec
+
+    return PompStruct(spec=lg_spec(1, 1), ys=ref_lg1d["ys"], times=np.arange(1, 5.0), t0=0.0)
+
+
+def test_mif_reference_fixture_through_injection(ref_values, ref_lg1d):
+    F = _F()
+    tol = ref_values["tolerance"]
+    st = _struct(ref_lg1d)
+    theta = ref_lg1d["theta"]
+    inj = [{"perfilter": {k: ref_lg1d[f"mif_{k}"][it][None] for k in ("zp0", "zp", "z0", "z", "u")},
+            "monitors": []} for it in range(3)]
+    swarm = np.repeat(theta[None, None, :], 12, axis=1)
+    ll, tr, final = F.mif(st, swarm, _rw(), 3, 12, np.zeros(1, np.uint64), 0.0, 0, inject=inj)
+    np.testing.assert_allclose(ll[0, -1], ref_values["mif"]["final_loglik"][0], **tol)
+    np.testing.assert_allclose(tr[0, -1], ref_values["mif"]["final_theta"], **tol)
+    assert final.shape == (1, 12, 5)
+
+
+def test_mif_full_trace_fixture_through_injection(ref_values, ref_lg1d):
+    F = _F()
+    tol = ref_values["tolerance"]
+    gold = ref_values["mif_full_trace"]
+    st = _struct(ref_lg1d)
+    theta = ref_lg1d["theta"]
+    thetas = np.stack([theta, (theta * f32(1.05)).astype(f32)])
+    inj = [{"perfilter": {k: ref_lg1d[f"mift_{k}"][:, it] for k in ("zp0", "zp", "z0", "z", "u")},
+            "monitors": [{k: ref_lg1d[f"mift_mon_{k}"][:, it] for k in ("z0", "z", "u")}]}
+           for it in range(4)]
+    swarm = np.repeat(thetas[:, None, :], 12, axis=1)
+    ll, tr, _ = F.mif(st, swarm, _rw(), 4, 12, np.zeros(2, np.uint64), 0.0, 1, inject=inj)
+    names = ["A11", "C11", "Q11", "R11", "X0_1"]
+    for r in range(2):
+        np.testing.assert_allclose(ll[r], [gold[f"loglik_rep{r}_m{m}"][0] for m in range(4)], **tol)
+        want = [[gold[f"{n}_rep{r}_m{m}"][0] for n in names] for m in range(5)]
+        np.testing.assert_allclose(tr[r], want, **tol)
+
+
+def test_pomp_mif_end_to_end(lg2d):
+    import copy
+
+    from pypomp_b200.optim import RWSigma
+
+    m = copy.deepcopy(lg2d)
+    names = m.canonical_param_names
+    rw = RWSigma({n: 0.02 for n in names}, init_names=[names[-1]]).geometric_cooling(0.5)
+    th = m.theta.params()[0]
+    m.mif(J=2000, M=3, rw_sd=rw, key=5, theta=[th, th], n_monitors=1)
+    res = m.results()
+    assert list(res.columns[:3]) == ["theta_idx", "logLik", "se"]
+    assert len(res) == 2 and np.all(np.isfinite(res["logLik"]))
+    tr = m.traces()
+    assert len(tr) == 2 * 4 and np.isnan(tr[tr["iteration"] == 0]["logLik"]).all()
+    assert m.theta.num_replicates() == 2
