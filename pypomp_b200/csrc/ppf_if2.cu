@@ -33,23 +33,45 @@ __device__ __forceinline__ float if2_measure(float m, float log1e18) {
   return m;
 }
 
-// Normals of particle k for IF2 perturbations (P per particle, tag PERTURB).
+// Perturb the parameter row th[0..P) of particle k in place:
+// th[p] += (cool * sig[p]) * z_p, z_p the P normals of counter s (tag PERTURB),
+// drawn one at a time from the particle's Philox blocks (the same values
+// pp_normals gives), or read from the injected arrays.  The row lives in
+// shared memory: per-thread arrays passed by pointer and indexed at run time
+// are kept out of these kernels.
 template <bool INJ>
-__device__ __forceinline__ void perturb_noise(const Args& a, int f, int k, int s, int P, float* z) {
+__device__ __forceinline__ void perturb_row(const Args& a, int f, int k, int s, int P, float cool,
+                                            const float* sig, float* th) {
   if (INJ) {
     const float* src = (s == 0) ? a.inj_zp0 + ((size_t)f * a.J + k) * P
                                 : a.inj_zp + (((size_t)f * a.T + (s - 1)) * a.J + k) * P;
-    for (int i = 0; i < P; ++i) z[i] = src[i];
-  } else {
-    pp_normals(a.seeds[f], (uint32_t)k, (uint32_t)s, PPF_TAG_PERTURB, P, z);
+    for (int p = 0; p < P; ++p) th[p] = th[p] + (cool * sig[p]) * src[p];
+    return;
+  }
+  const uint64_t seed = a.seeds[f];
+  uint32_t cached = 0xffffffffu;
+  float z4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  for (int p = 0; p < P; ++p) {
+    const uint32_t i = (uint32_t)k * (uint32_t)P + (uint32_t)p;
+    if ((i >> 2) != cached) {
+      cached = i >> 2;
+      pp_normal4(seed, cached, (uint32_t)s, PPF_TAG_PERTURB, z4);
+    }
+    const uint32_t e = i & 3u;
+    const float z = e == 0u ? z4[0] : e == 1u ? z4[1] : e == 2u ? z4[2] : z4[3];
+    th[p] = th[p] + (cool * sig[p]) * z;
   }
 }
 
+// Parameter rows of the block's threads in dynamic shared memory: thread r
+// owns row r, stride P | 1 (odd, so a warp's rows fall in distinct banks).
+__device__ __forceinline__ int if2_row_stride(int P) { return P | 1; }
+
 template <class M, int TPB, bool INJ>
 __global__ void __launch_bounds__(TPB) k_if2_init(Args a) {
+  extern __shared__ __align__(16) float s_rows[];   // [TPB][P | 1]
   __shared__ unsigned int smk[2 * (TPB / 32)];
   constexpr int DX = M::MAXDX;
-  constexpr int MP = M::MAXP;
   const int f = blockIdx.y;
   const int u = filter_unit(a, f);
   const int J = a.J, P = a.model.n_params;
@@ -61,27 +83,19 @@ __global__ void __launch_bounds__(TPB) k_if2_init(Args a) {
   float* W = a.W[0] + (size_t)f * J;
   float* TH = a.TH[0] + (size_t)f * P * J;
   const float* S = a.swarm_in + (size_t)f * P * J;
+  float* th = s_rows + threadIdx.x * if2_row_stride(P);
   unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
   const int k = blockIdx.x * TPB + threadIdx.x;
   if (k < J) {
-    float th[MP];
-    float zp[MP];
-#pragma unroll
-    for (int p = 0; p < MP; ++p) th[p] = (p < P) ? S[(size_t)p * J + k] : 0.0f;
-    perturb_noise<INJ>(a, f, k, 0, P, zp);
-#pragma unroll
-    for (int p = 0; p < MP; ++p)
-      if (p < P) th[p] = th[p] + (c0 * a.rw_sig0[p]) * zp[p];
+    for (int p = 0; p < P; ++p) th[p] = S[(size_t)p * J + k];
+    perturb_row<INJ>(a, f, k, 0, P, c0, a.rw_sig0, th);
     typename M::Consts c;
     M::prepare(c, th, a.model, true);
     float x[DX];
     float z0[M::NZ0 > 0 ? M::NZ0 : 1];
     step_noise<M>(a, f, k, 0, M::NZ0, z0);
     M::rinit(c, z0, x);
-    perturb_noise<INJ>(a, f, k, 1, P, zp);
-#pragma unroll
-    for (int p = 0; p < MP; ++p)
-      if (p < P) th[p] = th[p] + (c1 * a.rw_sig[p]) * zp[p];
+    perturb_row<INJ>(a, f, k, 1, P, c1, a.rw_sig, th);
     M::prepare(c, th, a.model, true);
     float z[M::NZ];
     step_noise<M>(a, f, k, 1, M::NZ, z);
@@ -90,9 +104,7 @@ __global__ void __launch_bounds__(TPB) k_if2_init(Args a) {
 #pragma unroll
     for (int d = 0; d < DX; ++d) X[d * J + k] = x[d];
     W[k] = w;
-#pragma unroll
-    for (int p = 0; p < MP; ++p)
-      if (p < P) TH[(size_t)p * J + k] = th[p];
+    for (int p = 0; p < P; ++p) TH[(size_t)p * J + k] = th[p];
     accum_maxmin(w, mx, mn, nn);
   }
   block_maxmin_u32<TPB>(mx, mn, smk);
@@ -115,12 +127,12 @@ template <class M, int TPB, int IT, bool INJ>
 __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
-  constexpr int MP = M::MAXP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int P = a.model.n_params;
   float* xs = reinterpret_cast<float*>(smem_raw);                 // [DX][TILE]
   int* st = reinterpret_cast<int*>(xs + DX * TILE);               // [TILE + 1]
   float* wcar = reinterpret_cast<float*>(st + TILE + 4);          // [TILE]
+  float* th = wcar + TILE + threadIdx.x * if2_row_stride(P);      // [TPB][P | 1]
   __shared__ uint64_t s_scan[TPB / 32 + 1];
   __shared__ unsigned int smk[2 * (TPB / 32)];
 
@@ -208,20 +220,12 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
   for (int k = klo + threadIdx.x; k < khi; k += TPB) {
     const int l = find_parent(st, ntile, k);
     if (anc) anc[k] = jt + l;
-    float th[MP];
-#pragma unroll
-    for (int p = 0; p < MP; ++p) th[p] = (p < P) ? THc[(size_t)p * J + jt + l] : 0.0f;
+    for (int p = 0; p < P; ++p) th[p] = THc[(size_t)p * J + jt + l];
     if (last) {
-#pragma unroll
-      for (int p = 0; p < MP; ++p)
-        if (p < P) Sout[(size_t)p * J + k] = th[p];
+      for (int p = 0; p < P; ++p) Sout[(size_t)p * J + k] = th[p];
       continue;
     }
-    float zp[MP];
-    perturb_noise<INJ>(a, f, k, t + 2, P, zp);
-#pragma unroll
-    for (int p = 0; p < MP; ++p)
-      if (p < P) th[p] = th[p] + (cl * a.rw_sig[p]) * zp[p];
+    perturb_row<INJ>(a, f, k, t + 2, P, cl, a.rw_sig, th);
     typename M::Consts c;
     M::prepare(c, th, a.model, true);
     float x[DX];
@@ -234,9 +238,7 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
 #pragma unroll
     for (int d = 0; d < DX; ++d) Xn[d * J + k] = x[d];
     Wn[k] = w;
-#pragma unroll
-    for (int p = 0; p < MP; ++p)
-      if (p < P) THn[(size_t)p * J + k] = th[p];
+    for (int p = 0; p < P; ++p) THn[(size_t)p * J + k] = th[p];
     accum_maxmin(w, mx, mn, nn);
   }
   if (last) return;
@@ -250,18 +252,25 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
   }
 }
 
+static int if2_row_stride_host(int P) { return P | 1; }
+
 template <class M, bool INJ>
 int run_if2_t(Args& a, cudaStream_t s) {
   constexpr int TPB = 256, IT = 8, TILE = TPB * IT;
   if (a.tile != TILE) return PPF_EINVAL;   // the workspace was carved for this tile
-  const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4) + sizeof(float) * TILE;
+  const size_t rows = sizeof(float) * TPB * if2_row_stride_host(a.model.n_params);
+  const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4) + sizeof(float) * TILE + rows;
+  if (smem > kResidentSmemMax) return PPF_EUNSUPPORTED;
   if (cudaFuncSetAttribute(k_if2_resprop<M, TPB, IT, INJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
+    return PPF_ECUDA;
+  if (cudaFuncSetAttribute(k_if2_init<M, TPB, INJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)rows) != cudaSuccess)
     return PPF_ECUDA;
   dim3 grid_init((a.J + TPB - 1) / TPB, a.F);
   dim3 grid(a.ntiles, a.F);
   PROF_BEGIN(KIND_IF2);
-  k_if2_init<M, TPB, INJ><<<grid_init, TPB, 0, s>>>(a);
+  k_if2_init<M, TPB, INJ><<<grid_init, TPB, rows, s>>>(a);
   for (int t = 0; t < a.T; ++t) {
     k_sum<M, TPB, IT><<<a.ntiles * a.F, TPB, 0, s>>>(a, t);
     k_if2_resprop<M, TPB, IT, INJ><<<grid, TPB, smem, s>>>(a, t);

@@ -335,8 +335,8 @@ def run_perfilter(struct: PompStruct, swarm, seeds_f: np.ndarray, J: int, rw_sig
     if tuple(sw_d.shape) != (F, P, J):
         raise ValueError(f"swarm must hold {P} parameters of {J} particles per filter")
     ys_d, ycon_d, Tu_d, U, T = _device_inputs(torch, struct, dev)
-    cool_h = np.ascontiguousarray(np.broadcast_to(np.asarray(cool, np.float32), (U, T)))
-    cool0_h = np.ascontiguousarray(np.broadcast_to(np.asarray(cool0, np.float32), (U,)))
+    cool_h = np.array(np.broadcast_to(np.asarray(cool, np.float32), (U, T)), dtype=np.float32)
+    cool0_h = np.array(np.broadcast_to(np.asarray(cool0, np.float32), (U,)), dtype=np.float32)
     f32d = dict(dtype=torch.float32, device=dev)
     keep = {
         "rw_sig": torch.tensor(np.asarray(rw_sig, np.float32), **f32d),
