@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -323,6 +324,144 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# The other configurations (one JSON line each; not the headline line)
+# ---------------------------------------------------------------------------
+
+def _timed(fn, steps, warmup, stream):
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, clk.summary()
+
+
+def _line(args, workload, value, ms, extra):
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": {"workload": workload}}
+    line.update(extra)
+    print(json.dumps(line))
+
+
+def run_c1(args):
+    """LG 2-D, T=50, J=1000, one filter (resident path); the spread over 256 seeds
+    is reported (the Kalman comparison lives in the tests)."""
+    import torch
+
+    import pypomp_b200 as pp
+    from pypomp_b200 import functional as F
+
+    m = pp.LG(T=50, Q=LG_Q, R=LG_R, key=0)
+    st = m.to_struct()
+    th = m.theta.to_array(m.canonical_param_names).astype(np.float32)
+    stream = torch.cuda.current_stream()
+    out = {}
+
+    def fn():
+        out["r"] = F.run_pfilter(st, th, np.array([1], np.uint64), 1000, path="resident", return_torch=True)
+
+    ms, clk = _timed(fn, args.steps, args.warmup, stream)
+    reps = F.run_pfilter(st, np.repeat(th, 256, 0), np.arange(256, dtype=np.uint64), 1000, path="resident")
+    ll = reps["loglik"]
+    _line(args, "LG 2-D pfilter, T=50, J=1000, one filter, resident path (configs[0])",
+          1000 * 50 / (ms / 1e3), ms,
+          {"e2e": {"value": 1000 * 50 / (ms / 1e3), "unit": UNIT, "api": "functional.run_pfilter",
+                   "h2d_bytes_per_step": int(st.ys.nbytes + th.nbytes + 8), "d2h_bytes_per_step": 0},
+           "pf_loglik_mean_256_seeds": float(np.mean(ll)),
+           "pf_loglik_sd": float(np.std(ll)), "clocks": clk, "roofline": None,
+           "note": "one CTA; latency bound, no HBM traffic to speak of"})
+
+
+def run_c3(args):
+    """SV MOP-alpha value + gradient: T=2000, J=65536, alpha=0.97, one parameter set."""
+    import torch
+
+    import pypomp_b200 as pp
+    from pypomp_b200 import _ffi
+    from pypomp_b200.functional import MopCall
+
+    Jm, Tm = 65536, 2000
+    m = pp.SV(T=Tm, key=0)
+    st = m.to_struct()
+    th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(np.float32)
+    call = MopCall(st, th, np.array([1], np.uint64), Jm, 0.97)
+    stream = torch.cuda.current_stream()
+    ms, clk = _timed(lambda: call.forward(grad=True), args.steps, args.warmup, stream)
+    torch.cuda.synchronize()
+    _ffi.profile_begin()
+    call.forward(grad=True)
+    prof = _ffi.profile_end()
+    value = Jm * Tm / (ms / 1e3)
+    # algorithmic bytes per particle-step of each MOP kernel (SV, dx = 2):
+    # forward resample+propagate 24 + ancestor 4 + first-child offset 4; sums 4;
+    # recompute 8 + 4 + 8; adjoint 8 (x) + 4 (anc) + 4 (offset) + 12 (adjoint in)
+    # + 12 (adjoint out)
+    bytes_kind = {"resample_propagate": 32, "sum_lookback": 4, "mop_recompute": 20, "mop_adjoint": 40}
+    peak, peak_kind = peaks()
+    kern = {}
+    for k, (tms, n) in prof.items():
+        if k in bytes_kind and n:
+            avg = tms / n
+            per_launch_units = Jm
+            kern[k] = {"launches": n, "total_ms": tms, "avg_ms": avg,
+                       "GBps": bytes_kind[k] * per_launch_units / (avg / 1e3) / 1e9}
+    dom = max(kern, key=lambda k: kern[k]["total_ms"])
+    res = call.out
+    _line(args, "SV MOP-alpha value+grad, T=2000, J=65536, alpha=0.97 (configs[2])", value, ms,
+          {"e2e": None, "clocks": clk, "kernels": kern,
+           "roofline": {"bound": "hbm", "achieved": kern[dom]["GBps"], "peak": peak, "unit": "GB/s",
+                        "frac": kern[dom]["GBps"] / peak, "traffic": None, "kernel": dom,
+                        "peak_source": peak_kind},
+           "value_out": float(res["value"][0]), "grad_out": res["grad"][0].tolist()})
+
+
+def run_c4(args):
+    """Ricker profile grid: 32 x 32 (log r, sigma) x J=16384, T=500, one launch."""
+    import torch
+
+    import pypomp_b200 as pp
+    from pypomp_b200 import _ffi
+    from pypomp_b200 import functional as F
+
+    Jr, Tr = 16384, 500
+    m = pp.Ricker(T=Tr, key=0)
+    st = m.to_struct()
+    lr = np.linspace(3.0, 4.6, 32)
+    sg = np.linspace(0.05, 0.8, 32)
+    grid = np.array([[math.exp(a), b, 10.0, 7.0] for a in lr for b in sg], np.float32)
+    Fg = grid.shape[0]
+    stream = torch.cuda.current_stream()
+    seeds = np.arange(Fg, dtype=np.uint64)
+    res = {}
+    for path in ("resident", "stream"):
+        ms, clk = _timed(lambda: F.run_pfilter(st, grid, seeds, Jr, path=path, return_torch=True),
+                         args.steps, args.warmup, stream)
+        res[path] = (ms, clk)
+    best = min(res, key=lambda k: res[k][0])
+    ms, clk = res[best]
+    value = Fg * Jr * Tr / (ms / 1e3)
+    _line(args, "Ricker 32x32 (log r, sigma) grid x J=16384, T=500 (configs[3])", value, ms,
+          {"e2e": {"value": value, "unit": UNIT, "api": "functional.run_pfilter (host inputs)",
+                   "h2d_bytes_per_step": int(grid.nbytes + st.ys.nbytes + seeds.nbytes),
+                   "d2h_bytes_per_step": 0},
+           "clocks": clk, "path": best,
+           "paths_ms": {k: v[0] for k, v in res.items()},
+           "roofline": {"bound": "issue", "achieved": None, "peak": None, "unit": None, "frac": None,
+                        "traffic": None,
+                        "note": "resident path keeps each swarm in shared memory for all T: "
+                                "no HBM claim; HBM-equivalent 24 B/particle-step = "
+                                f"{24 * value / 1e9:.0f} GB/s"}})
+
+
 def run_profile_case(args):
     """A small case of the same kernels for ncu captures: the headline model
     and J, 24 seeds (state 2 x 24 x 262144 x 12 B = 151 MB, larger than L2),
@@ -352,7 +491,12 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="run one small call of the same kernels (for ncu) and exit")
     ap.add_argument("--path", default="stream")
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"],
+                    help="c2 (default) is the headline line; c1/c3/c4 print their own lines")
     args = ap.parse_args()
+    if args.config != "c2" and args.impl == "ours" and not args.profile_case:
+        {"c1": run_c1, "c3": run_c3, "c4": run_c4}[args.config](args)
+        return
     if args.profile_case:
         run_profile_case(args)
     elif args.impl == "reference":

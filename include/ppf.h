@@ -147,6 +147,16 @@ typedef struct ppf_mop_desc {
 size_t ppf_mop_workspace_bytes(const ppf_mop_desc* d);
 int ppf_mop(const ppf_mop_desc* d, void* stream);
 
+/* The adjoint sweep alone, for a caller that separates the forward from the
+ * backward pass (a torch.autograd.Function; the reference gets both at once
+ * from jax.value_and_grad at pypomp/core/algorithms/ad_helpers.py:6-54).
+ * Call it after ppf_mop with the SAME descriptor and workspace, untouched in
+ * between: the forward leaves the ancestors, first-child offsets, state
+ * checkpoints and per-step maxima there.  Writes
+ * grad[f][p] = dvalue[f] * d value[f] / d theta[f][p] (dvalue: device [F],
+ * NULL for all ones); d->grad must be set. */
+int ppf_mop_backward(const ppf_mop_desc* d, const double* dvalue, void* stream);
+
 /* One IF2 iteration: the perturbed particle filter over F independent
  * parameter swarms.  Replaces _perfilter_internal / _perfilter_scan_body
  * (pypomp/core/algorithms/mif.py:88-258) with _resampler_thetas

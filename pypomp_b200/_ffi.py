@@ -39,6 +39,7 @@ EXPORTED = (
     "ppf_pfilter",
     "ppf_mop_workspace_bytes",
     "ppf_mop",
+    "ppf_mop_backward",
     "ppf_perfilter_workspace_bytes",
     "ppf_perfilter",
     "ppf_workspace_status",
@@ -179,6 +180,8 @@ def _load():
     lib.ppf_mop_workspace_bytes.restype = ctypes.c_size_t
     lib.ppf_mop.argtypes = [ctypes.POINTER(MopDesc), _vp]
     lib.ppf_mop.restype = ctypes.c_int
+    lib.ppf_mop_backward.argtypes = [ctypes.POINTER(MopDesc), _vp, _vp]
+    lib.ppf_mop_backward.restype = ctypes.c_int
     lib.ppf_perfilter_workspace_bytes.argtypes = [ctypes.POINTER(PerfilterDesc)]
     lib.ppf_perfilter_workspace_bytes.restype = ctypes.c_size_t
     lib.ppf_perfilter.argtypes = [ctypes.POINTER(PerfilterDesc), _vp]

@@ -330,6 +330,38 @@ int ppf_perfilter(const ppf_perfilter_desc* d, void* stream) {
   return run_if2(a, s);
 }
 
+// grad[f][p] *= dvalue[f]
+__global__ void k_scale_rows(double* g, const double* dv, int F, int P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < F * P) g[i] *= dv[i / P];
+}
+
+int ppf_mop_backward(const ppf_mop_desc* d, const double* dvalue, void* stream) {
+  int rc = validate_mop(d);
+  if (rc) return rc;
+  if (!d->grad) return PPF_EINVAL;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  ppf_pfilter_desc p;
+  mop_to_pfilter(d, &p);
+  Args a;
+  fill_args(&p, a, MODE_MOP);
+  a.flags |= PPF_F_SAVE_ANC;
+  MopWork w;
+  memset(&w, 0, sizeof(w));
+  const size_t need = carve_mop(a, w, d, nullptr);
+  if (!d->workspace || d->ws_bytes < need) return PPF_EINVAL;
+  carve_mop(a, w, d, reinterpret_cast<unsigned char*>(d->workspace));
+  w.grad = d->grad;
+  w.alpha = d->alpha;
+  rc = run_mop_backward(a, w, s);
+  if (rc) return rc;
+  if (dvalue) {
+    const int n = d->F * d->model.n_params;
+    k_scale_rows<<<(n + 255) / 256, 256, 0, s>>>(d->grad, dvalue, d->F, d->model.n_params);
+  }
+  return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
 int ppf_workspace_status(const void* workspace, void* stream) {
   if (!workspace) return PPF_EINVAL;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

@@ -108,6 +108,7 @@ struct MopWork {
 int run_pfilter_path(Args& a, int path, cudaStream_t s);
 int run_stream_any(Args& a, cudaStream_t s);   // stream path, any model
 int run_mop(Args& a, const MopWork& w, cudaStream_t s);
+int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s);
 int run_if2(Args& a, cudaStream_t s);
 int reset_accumulators(Args& a, cudaStream_t s);
 size_t resident_smem_bytes(const Args& a);

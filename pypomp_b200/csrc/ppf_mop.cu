@@ -313,4 +313,25 @@ int run_mop(Args& a, const MopWork& w, cudaStream_t s) {
   }
 }
 
+template <class M>
+int run_mop_backward_model(Args& a, const MopWork& w, cudaStream_t s) {
+  return (a.flags & PPF_F_INJECT) ? mop_backward<M, true>(a, w, s) : mop_backward<M, false>(a, w, s);
+}
+
+int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s) {
+  switch (a.model.kind) {
+    case PPF_MODEL_LG:
+      switch (a.model.dx) {
+        case 1: return run_mop_backward_model<LG<1>>(a, w, s);
+        case 2: return run_mop_backward_model<LG<2>>(a, w, s);
+        case 3: return run_mop_backward_model<LG<3>>(a, w, s);
+        case 4: return run_mop_backward_model<LG<4>>(a, w, s);
+        default: return PPF_EUNSUPPORTED;
+      }
+    case PPF_MODEL_SV: return run_mop_backward_model<SV>(a, w, s);
+    case PPF_MODEL_RICKER: return run_mop_backward_model<Ricker>(a, w, s);
+    default: return PPF_EINVAL;
+  }
+}
+
 }  // namespace ppf

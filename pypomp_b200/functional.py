@@ -155,56 +155,105 @@ def pfilter(struct: PompStruct, thetas_array, J: int, keys, thresh: float = 0.0,
     return out
 
 
+class MopCall:
+    """One batched MOP-alpha evaluation on the device: inputs, outputs and the
+    workspace that keeps the forward's saves (ancestors, first-child offsets,
+    state checkpoints) for a later adjoint sweep.
+
+    ``theta_est`` is a (F, P) host array or CUDA tensor on the estimation
+    scale.  ``forward(grad)`` runs ``ppf_mop`` (the adjoint too when
+    ``grad``); ``backward(dvalue)`` runs ``ppf_mop_backward`` on the same
+    workspace and returns ``dvalue[f] * d value[f] / d theta[f]``.
+    """
+
+    def __init__(self, struct: PompStruct, theta_est, seeds_f, J: int, alpha: float, *, unit_f=None,
+                 inject=None, ckpt_every: int = 0, save_ancestors: bool = False):
+        torch = _ffi.require_cuda()
+        if J < 1:
+            raise ValueError("J should be greater than 0.")
+        if J > _ffi.PPF_MAX_J:
+            raise ValueError(f"J must be at most {_ffi.PPF_MAX_J}.")
+        if not 0.0 <= float(alpha) <= 1.0:
+            raise ValueError("alpha must be in [0, 1]")
+        self.torch = torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.dev = dev
+        spec = struct.spec
+        if hasattr(theta_est, "is_cuda"):
+            th_d = theta_est.detach().to(dev, torch.float32).reshape(-1, spec.n_params).contiguous()
+        else:
+            th = np.ascontiguousarray(np.atleast_2d(theta_est), dtype=np.float32)
+            th_d = torch.from_numpy(th).to(dev)
+        F = th_d.shape[0]
+        ys_d, ycon_d, Tu_d, U, T = _device_inputs(torch, struct, dev)
+        seeds_d = torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).copy()).to(dev)
+        unit_d = None
+        if unit_f is not None:
+            unit_d = torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
+        self.out = {"value": torch.zeros(F, dtype=torch.float64, device=dev),
+                    "grad": torch.zeros(F, spec.n_params, dtype=torch.float64, device=dev)}
+        if save_ancestors:
+            self.out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=dev)
+        inj = {}
+        flags = 0
+        if inject is not None:
+            flags |= _ffi.F_INJECT
+            for k in ("z0", "z", "u"):
+                if inject.get(k) is not None:
+                    inj[k] = torch.from_numpy(np.ascontiguousarray(inject[k], dtype=np.float32)).to(dev)
+        d = _ffi.MopDesc()
+        d.model = spec.ffi_model()
+        d.J, d.F, d.T, d.U = J, F, T, U
+        d.flags = flags
+        d.alpha = float(alpha)
+        d.ckpt_every = int(ckpt_every)
+        d.theta, d.ys, d.ycon = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(ycon_d)
+        d.unit, d.T_u, d.seeds = _ffi.ptr(unit_d), _ffi.ptr(Tu_d), _ffi.ptr(seeds_d)
+        d.inj_z0, d.inj_z, d.inj_u = _ffi.ptr(inj.get("z0")), _ffi.ptr(inj.get("z")), _ffi.ptr(inj.get("u"))
+        d.value, d.anc = _ffi.ptr(self.out["value"]), _ffi.ptr(self.out.get("anc"))
+        nbytes = _ffi.LIB.ppf_mop_workspace_bytes(d)
+        self.ws = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
+        d.workspace, d.ws_bytes = _ffi.ptr(self.ws), self.ws.numel()
+        self.d = d
+        self.keep = (th_d, ys_d, ycon_d, Tu_d, seeds_d, unit_d, inj)
+        self.forward_done = False
+
+    def _stream(self):
+        return self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def forward(self, grad: bool = False) -> dict:
+        d = self.d
+        d.grad = _ffi.ptr(self.out["grad"]) if grad else 0
+        stream = self._stream()
+        _ffi.check(_ffi.LIB.ppf_mop(d, stream), "ppf_mop")
+        _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_mop")
+        self.forward_done = True
+        return self.out
+
+    def backward(self, dvalue=None):
+        if not self.forward_done:
+            raise RuntimeError("MopCall.backward needs a forward pass on the same workspace first")
+        d = self.d
+        d.grad = _ffi.ptr(self.out["grad"])
+        dv = None
+        if dvalue is not None:
+            dv = self.torch.as_tensor(dvalue, dtype=self.torch.float64, device=self.dev).reshape(-1).contiguous()
+        stream = self._stream()
+        _ffi.check(_ffi.LIB.ppf_mop_backward(d, _ffi.ptr(dv), stream), "ppf_mop_backward")
+        _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_mop_backward")
+        return self.out["grad"]
+
+
 def run_mop(struct: PompStruct, theta_est_f: np.ndarray, seeds_f: np.ndarray, J: int, alpha: float,
             *, grad: bool = True, unit_f=None, inject=None, ckpt_every: int = 0,
             save_ancestors: bool = False, return_torch: bool = False):
     """One batched call of ``ppf_mop``: MOP-alpha value (negative log-likelihood,
     summed over time) and, when ``grad``, its gradient on the estimation scale."""
-    torch = _ffi.require_cuda()
-    if J < 1:
-        raise ValueError("J should be greater than 0.")
-    if J > _ffi.PPF_MAX_J:
-        raise ValueError(f"J must be at most {_ffi.PPF_MAX_J}.")
-    if not 0.0 <= float(alpha) <= 1.0:
-        raise ValueError("alpha must be in [0, 1]")
-    dev = torch.device("cuda", torch.cuda.current_device())
-    spec = struct.spec
-    theta_est_f = np.ascontiguousarray(np.atleast_2d(theta_est_f), dtype=np.float32)
-    F = theta_est_f.shape[0]
-    ys_d, ycon_d, Tu_d, U, T = _device_inputs(torch, struct, dev)
-    th_d = torch.from_numpy(theta_est_f).to(dev)
-    seeds_d = torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).copy()).to(dev)
-    unit_d = None
-    if unit_f is not None:
-        unit_d = torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
-    out = {"value": torch.zeros(F, dtype=torch.float64, device=dev)}
-    if grad:
-        out["grad"] = torch.zeros(F, spec.n_params, dtype=torch.float64, device=dev)
-    if save_ancestors:
-        out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=dev)
-    inj = {}
-    flags = 0
-    if inject is not None:
-        flags |= _ffi.F_INJECT
-        for k in ("z0", "z", "u"):
-            if inject.get(k) is not None:
-                inj[k] = torch.from_numpy(np.ascontiguousarray(inject[k], dtype=np.float32)).to(dev)
-    d = _ffi.MopDesc()
-    d.model = spec.ffi_model()
-    d.J, d.F, d.T, d.U = J, F, T, U
-    d.flags = flags
-    d.alpha = float(alpha)
-    d.ckpt_every = int(ckpt_every)
-    d.theta, d.ys, d.ycon = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(ycon_d)
-    d.unit, d.T_u, d.seeds = _ffi.ptr(unit_d), _ffi.ptr(Tu_d), _ffi.ptr(seeds_d)
-    d.inj_z0, d.inj_z, d.inj_u = _ffi.ptr(inj.get("z0")), _ffi.ptr(inj.get("z")), _ffi.ptr(inj.get("u"))
-    d.value, d.grad, d.anc = _ffi.ptr(out["value"]), _ffi.ptr(out.get("grad")), _ffi.ptr(out.get("anc"))
-    nbytes = _ffi.LIB.ppf_mop_workspace_bytes(d)
-    ws = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
-    d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    _ffi.check(_ffi.LIB.ppf_mop(d, stream), "ppf_mop")
-    _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_mop")
+    call = MopCall(struct, theta_est_f, seeds_f, J, alpha, unit_f=unit_f, inject=inject,
+                   ckpt_every=ckpt_every, save_ancestors=save_ancestors)
+    out = dict(call.forward(grad=grad))
+    if not grad:
+        out.pop("grad")
     if return_torch:
         return out
     return {k: v.cpu().numpy() for k, v in out.items()}
