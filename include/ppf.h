@@ -70,6 +70,10 @@ typedef struct ppf_model {
 #define PPF_F_SAVE_ANC (1u << 5) /* write resampling ancestors */
 #define PPF_F_SAVE_W (1u << 6)   /* write unnormalised log-weights */
 #define PPF_F_EST (1u << 7)      /* theta on the estimation scale */
+/* ppf_mop / ppf_perfilter: parameters on the natural scale (an identity
+ * parameter transform, pypomp's ParTrans(); the default for these two entry
+ * points is the estimation scale) */
+#define PPF_F_NATURAL (1u << 8)
 
 /* Execution paths; all produce bit-identical results. */
 enum {
@@ -125,7 +129,7 @@ typedef struct ppf_pfilter_desc {
 typedef struct ppf_mop_desc {
   ppf_model model;
   int32_t J, F, T, U;
-  uint32_t flags;         /* PPF_F_INJECT only */
+  uint32_t flags;         /* PPF_F_INJECT, PPF_F_NATURAL */
   float alpha;            /* MOP discount in [0, 1] */
   int32_t ckpt_every;     /* 0 = ceil(sqrt(T)) */
   const float* theta;     /* [F][P] estimation scale */
@@ -173,7 +177,7 @@ int ppf_mop_backward(const ppf_mop_desc* d, const double* dvalue, void* stream);
 typedef struct ppf_perfilter_desc {
   ppf_model model;
   int32_t J, F, T, U;
-  uint32_t flags;          /* PPF_F_INJECT, PPF_F_CLL, PPF_F_SAVE_ANC */
+  uint32_t flags;          /* PPF_F_INJECT, PPF_F_CLL, PPF_F_SAVE_ANC, PPF_F_NATURAL */
   float thresh;            /* resample when max(nw) - min(nw) > log(thresh) */
   const float* swarm_in;   /* [F][P][J] estimation scale */
   float* swarm_out;        /* out [F][P][J]; may not alias swarm_in */

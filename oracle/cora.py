@@ -140,7 +140,7 @@ def pfilter(kind, dx, dy, theta_f, ys, J, *, seeds=None, ycon=None, unit=None, T
 
 
 def mop_surrogate(kind, dx, dy, theta_est, ys, J, alpha, anc, m0=None, *, seeds=None,
-                  ycon=None, dt=0.0, inject=None):
+                  ycon=None, dt=0.0, inject=None, natural=False):
     """MOP-alpha surrogate value (frozen ancestry, frozen stop_gradient(m)).
 
     ``anc`` (F,T,J) ancestors; ``m0`` (F,T,J) or None to record it.  Returns
@@ -155,7 +155,7 @@ def mop_surrogate(kind, dx, dy, theta_est, ys, J, alpha, anc, m0=None, *, seeds=
     d = _Desc()
     d.model = _Model(kind, dx, dy, P, dt, 0)
     d.J, d.F, d.T, d.U = J, F, T, U
-    flags = 128
+    flags = 0 if natural else 128
     d.theta, d.ys = _p(theta_est), _p(ys)
     if ycon is not None:
         ycon = np.ascontiguousarray(ycon, dtype=np.float32)
@@ -186,7 +186,7 @@ def mop_surrogate(kind, dx, dy, theta_est, ys, J, alpha, anc, m0=None, *, seeds=
 
 def perfilter(kind, dx, dy, swarm, ys, J, rw_sig, rw_sig0, cool, cool0, *, seeds=None,
               ycon=None, unit=None, T_u=None, dt=0.0, thresh=0.0, inject=None, CLL=False,
-              anc=False, nthreads=1):
+              anc=False, nthreads=1, natural=False):
     """One IF2 iteration over F swarms (``swarm`` (F, P, J), estimation scale).
 
     ``cool`` (U, T) and ``cool0`` (U,) are the cooling factors; ``inject`` may
@@ -208,7 +208,7 @@ def perfilter(kind, dx, dy, swarm, ys, J, rw_sig, rw_sig0, cool, cool0, *, seeds
     d.model = _Model(kind, dx, dy, P, dt, 0)
     d.J, d.F, d.T, d.U = J, F, T, U
     d.thresh = thresh
-    flags = (1 if CLL else 0) | (32 if anc else 0)
+    flags = (1 if CLL else 0) | (32 if anc else 0) | (256 if natural else 0)
     d.swarm_in, d.ys = _p(swarm), _p(ys)
     d.rw_sig, d.rw_sig0, d.cool, d.cool0 = _p(rw_sig), _p(rw_sig0), _p(cool), _p(cool0)
     for name, a, dt_ in (("ycon", ycon, np.float32), ("unit", unit, np.int32), ("T_u", T_u, np.int32),

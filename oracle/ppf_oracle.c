@@ -475,7 +475,7 @@ static float if2_step(const ppf_perfilter_desc* d, int f, int u, int j, int t, i
   if2_perturb_noise(d, f, j, s, P, zp);
   for (int p = 0; p < P; ++p) th[p] = th[p] + (cool * d->rw_sig[p]) * zp[p];
   consts_t c;
-  prepare(&c, th, &d->model, 1);
+  prepare(&c, th, &d->model, !(d->flags & PPF_F_NATURAL));
   float z[4];
   if2_noise(d, f, j, s, n_step(&c), z);
   rproc(&c, x, z);
@@ -507,7 +507,7 @@ static void run_perfilter(const ppf_perfilter_desc* d, int f) {
     if2_perturb_noise(d, f, j, 0, P, zp);
     for (int p = 0; p < P; ++p) tj[p] = tj[p] + (d->cool0[u] * d->rw_sig0[p]) * zp[p];
     consts_t c;
-    prepare(&c, tj, &d->model, 1);
+    prepare(&c, tj, &d->model, !(d->flags & PPF_F_NATURAL));
     if2_noise(d, f, j, 0, n_init(&c), z);
     rinit(&c, z, xj);
     const float m = if2_step(d, f, u, j, 0, 1, cool[0], tj, xj);

@@ -404,18 +404,19 @@ class RecordingPerfilterNoise:
                 "u": np.asarray(r["u"], f32)}
 
 
-def _per_particle(m, th_est, fn):
+def _per_particle(m, th_est, fn, natural=False):
     """Apply ``fn(par, j)`` for each particle's natural-scale parameters."""
-    nat = m.from_est(th_est)
+    nat = th_est if natural else m.from_est(th_est)
     return [fn(m.unpack(nat[j]), j) for j in range(th_est.shape[0])]
 
 
-def perfilter(model, swarm_est, ys, J, rw_sig, rw_sig0, cool, cool0, noise, thresh=0.0):
+def perfilter(model, swarm_est, ys, J, rw_sig, rw_sig0, cool, cool0, noise, thresh=0.0, natural=False):
     """``_perfilter_internal`` + ``_perfilter_scan_body`` (mif.py:88-258).
 
-    ``swarm_est`` (J, P) on the estimation scale; ``cool`` (T,) and ``cool0``
-    are the cooling factors.  Returns ``(swarm (J, P) after the last
-    resampling, loglik float32)``.
+    ``swarm_est`` (J, P) on the estimation scale (the natural scale with
+    ``natural``: an identity ``ParTrans``); ``cool`` (T,) and ``cool0`` are the
+    cooling factors.  Returns ``(swarm (J, P) after the last resampling,
+    loglik float32)``.
     """
     m = MODELS[model]
     ys = np.asarray(ys, f32)
@@ -425,7 +426,7 @@ def perfilter(model, swarm_est, ys, J, rw_sig, rw_sig0, cool, cool0, noise, thre
     th = np.asarray(swarm_est, f32)
     th = (th + (f32(cool0) * rw_sig0)[None, :] * noise.perturb0()).astype(f32)
     z0 = noise.init_normals()
-    X = np.concatenate(_per_particle(m, th, lambda p, j: m.rinit(p, z0[j:j + 1])), axis=0).astype(f32)
+    X = np.concatenate(_per_particle(m, th, lambda p, j: m.rinit(p, z0[j:j + 1]), natural), axis=0).astype(f32)
     nw = np.full(J, -np.log(f32(J)), f32)
     loglik = f32(0.0)
     logthresh = np.log(f32(thresh)) if thresh > 0 else f32(-np.inf)
@@ -433,9 +434,10 @@ def perfilter(model, swarm_est, ys, J, rw_sig, rw_sig0, cool, cool0, noise, thre
     for t in range(T):
         thp = (th + (f32(cool[t]) * rw_sig)[None, :] * noise.perturb(t)).astype(f32)
         z = noise.step_normals(t)
-        X = np.concatenate(_per_particle(m, thp, lambda p, j: m.rproc(p, X[j:j + 1], z[j:j + 1], t)),
+        X = np.concatenate(_per_particle(m, thp, lambda p, j: m.rproc(p, X[j:j + 1], z[j:j + 1], t), natural),
                            axis=0).astype(f32)
-        meas = np.concatenate(_per_particle(m, thp, lambda p, j: m.dmeas(p, ys[t], X[j:j + 1]))).astype(f32)
+        meas = np.concatenate(_per_particle(m, thp, lambda p, j: m.dmeas(p, ys[t], X[j:j + 1]),
+                                            natural)).astype(f32)
         meas = np.nan_to_num(meas, nan=log1e18).astype(f32)
         w = (nw + meas).astype(f32)
         nwn, lt = normalize(w)
@@ -494,3 +496,80 @@ def mif(model, theta, ys, J, M, rw_sig, rw_sig0, cooling, key: jr.Key, n_monitor
         means.append(swarm.mean(axis=0, dtype=f32))
     traces = m.from_est(np.stack(means))
     return np.asarray(logliks, f32), traces, m.from_est(swarm), draws
+
+
+def panel_pfilter(model, thetas, ys_units, J, keys, thresh=0.0):
+    """``_chunked_panel_pfilter_internal`` (pfilter.py:248-304): one bootstrap
+    filter per unit, natural-scale ``thetas`` (U, P), ``keys`` (U,) jaxrng
+    keys.  Returns (logLiks (U,), recorded draws per unit)."""
+    lls, draws = [], []
+    for u, ys in enumerate(ys_units):
+        rec = RecordingNoise(JaxKeyNoise(keys[u], J, 1, 1))
+        lls.append(pfilter(model, thetas[u], ys, J, rec, thresh)["logLik"])
+        z0, z, uu = rec.arrays()
+        draws.append({"z0": z0, "z": z, "u": uu})
+    return np.asarray(lls, f32), draws
+
+
+def panel_mif(model, shared0, unit0, ys_units, J, M, rw_sig, rw_sig0, cooling, key: jr.Key,
+              host_identity=False, thresh=0.0):
+    """``_panel_mif_internal`` (panel_mif.py:17-247) for one replicate with
+    ``block=True``, no monitors, and units whose canonical order is
+    [shared | unit-specific] (the identity permutation).
+
+    ``shared0`` (ns,) and ``unit0`` (U, nu) natural scale.  ``host_identity``
+    restates a unit whose ``par_trans`` was replaced by ``ParTrans()`` after
+    construction: the host-side transforms are the identity while the model
+    mechanics keep the model's own transform (``pomp.py:271-313`` binds it to
+    the components at construction).  Returns ``(shared_traces (M+1, ns+1),
+    unit_traces (M+1, U, nu+1), draws[m][u])``.
+    """
+    m_ = MODELS[model]
+    ns, U = len(shared0), len(ys_units)
+    natural = False
+    to_e = (lambda v: np.asarray(v, f32)) if host_identity else m_.to_est
+    from_e = (lambda v: np.asarray(v, f32)) if host_identity else m_.from_est
+    est = [to_e(np.concatenate([shared0, unit0[u]]).astype(f32)) for u in range(U)]
+    S = np.repeat(est[0][None, :ns], J, axis=0).astype(f32)
+    Us = np.stack([np.repeat(est[u][None, ns:], J, axis=0) for u in range(U)], axis=1).astype(f32)
+    P = ns + Us.shape[2]
+    par0 = m_.unpack(m_.from_est(est[0]))
+    n_init, n_step = m_.n_init(par0), m_.n_step(par0)
+    m_keys = jr.split(key, M + 1)[1:]
+
+    def trace_row(ll_units):
+        s_row = np.concatenate([[np.sum(ll_units)], S.mean(axis=0, dtype=f32)]) if ll_units is not None \
+            else np.concatenate([[np.nan], S.mean(axis=0, dtype=f32)])
+        u_rows = [np.concatenate([[np.nan if ll_units is None else ll_units[u]], Us[:, u].mean(axis=0, dtype=f32)])
+                  for u in range(U)]
+        return s_row, np.stack(u_rows)
+
+    s_tr, u_tr = [], []
+    a, b = trace_row(None)
+    s_tr.append(a)
+    u_tr.append(b)
+    draws = []
+    for it in range(M):
+        unit_keys = jr.split(m_keys[it], U)
+        lls = np.zeros(U, f32)
+        dm = []
+        for u in range(U):
+            ys = np.asarray(ys_units[u], f32)
+            T = ys.shape[0]
+            cool = np.array([cooling(i, it, T) for i in range(T)], f32)
+            th = np.concatenate([S, Us[:, u]], axis=1).astype(f32)
+            rec = RecordingPerfilterNoise(JaxPerfilterNoise(unit_keys[u], J, P, n_init, n_step, T))
+            new, ll = perfilter(model, th, ys, J, rw_sig, rw_sig0, cool, cool[0], rec, thresh, natural)
+            S = new[:, :ns].astype(f32)
+            Us[:, u] = new[:, ns:]
+            lls[u] = ll
+            dm.append({"perfilter": rec.arrays(), "monitors": []})
+        draws.append(dm)
+        a, b = trace_row(lls)
+        s_tr.append(a)
+        u_tr.append(b)
+    s_tr, u_tr = np.stack(s_tr), np.stack(u_tr)
+    if not host_identity:
+        raise NotImplementedError("trace back-transform is only restated for identity host transforms")
+    del from_e
+    return s_tr, u_tr, draws

@@ -10,8 +10,9 @@ from . import _ffi  # noqa: F401  (loads libppf.so; fails loudly if it is missin
 from . import functional, maths, random  # noqa: F401
 from .maths import logmeanexp, logmeanexp_se  # noqa: F401
 from .models import LG, SV, Ricker  # noqa: F401
-from .pomp import Pomp, PompParameters  # noqa: F401
+from .pomp import ParTrans, Pomp, PompParameters  # noqa: F401
 from .autograd import mop_objective  # noqa: F401
+from .panel import PanelParameters, PanelPomp  # noqa: F401
 from .optim import SGD, Adam, LearningRate, RWSigma  # noqa: F401
 
 __all__ = ["LG", "SV", "Ricker", "Pomp", "PompParameters", "functional", "random",

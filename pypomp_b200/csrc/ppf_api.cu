@@ -181,7 +181,7 @@ static void mop_to_pfilter(const ppf_mop_desc* d, ppf_pfilter_desc* p) {
   p->model = d->model;
   p->J = d->J; p->F = d->F; p->T = d->T; p->U = d->U;
   p->path = PPF_PATH_STREAM;
-  p->flags = (d->flags & PPF_F_INJECT) | PPF_F_EST;
+  p->flags = (d->flags & PPF_F_INJECT) | ((d->flags & PPF_F_NATURAL) ? 0u : PPF_F_EST);
   p->thresh = 0.0f;
   p->theta = d->theta; p->ys = d->ys; p->ycon = d->ycon; p->unit = d->unit; p->T_u = d->T_u;
   p->seeds = d->seeds; p->inj_z0 = d->inj_z0; p->inj_z = d->inj_z; p->inj_u = d->inj_u;
@@ -220,7 +220,8 @@ static void fill_if2(const ppf_perfilter_desc* d, Args& a) {
   memset(&p, 0, sizeof(p));
   p.model = d->model;
   p.J = d->J; p.F = d->F; p.T = d->T; p.U = d->U;
-  p.flags = (d->flags & (PPF_F_INJECT | PPF_F_CLL | PPF_F_SAVE_ANC)) | PPF_F_EST;
+  p.flags = (d->flags & (PPF_F_INJECT | PPF_F_CLL | PPF_F_SAVE_ANC)) |
+            ((d->flags & PPF_F_NATURAL) ? 0u : PPF_F_EST);
   p.thresh = d->thresh;
   p.ys = d->ys; p.ycon = d->ycon; p.unit = d->unit; p.T_u = d->T_u;
   p.seeds = d->seeds; p.inj_z0 = d->inj_z0; p.inj_z = d->inj_z; p.inj_u = d->inj_u;

@@ -90,13 +90,13 @@ __global__ void __launch_bounds__(TPB) k_if2_init(Args a) {
     for (int p = 0; p < P; ++p) th[p] = S[(size_t)p * J + k];
     perturb_row<INJ>(a, f, k, 0, P, c0, a.rw_sig0, th);
     typename M::Consts c;
-    M::prepare(c, th, a.model, true);
+    M::prepare(c, th, a.model, (a.flags & PPF_F_EST) != 0);
     float x[DX];
     float z0[M::NZ0 > 0 ? M::NZ0 : 1];
     step_noise<M>(a, f, k, 0, M::NZ0, z0);
     M::rinit(c, z0, x);
     perturb_row<INJ>(a, f, k, 1, P, c1, a.rw_sig, th);
-    M::prepare(c, th, a.model, true);
+    M::prepare(c, th, a.model, (a.flags & PPF_F_EST) != 0);
     float z[M::NZ];
     step_noise<M>(a, f, k, 1, M::NZ, z);
     const float m = if2_measure(step1<M>(c, ob, x, z), log1e18);
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
     }
     perturb_row<INJ>(a, f, k, t + 2, P, cl, a.rw_sig, th);
     typename M::Consts c;
-    M::prepare(c, th, a.model, true);
+    M::prepare(c, th, a.model, (a.flags & PPF_F_EST) != 0);
     float x[DX];
 #pragma unroll
     for (int d = 0; d < DX; ++d) x[d] = xs[d * TILE + l];

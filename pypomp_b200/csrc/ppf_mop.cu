@@ -182,13 +182,14 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_init(Args a, MopBwd mb) {
   reduce_grad<TPB, M::NG>(g, mb.gnat + (size_t)f * kMaxNG, sd);
 }
 
-// Canonical-order, estimation-scale gradient from the natural-scale sums.
+// Canonical-order gradient from the natural-scale sums, chained to the
+// estimation scale unless the parameters are given on the natural scale.
 template <class M>
 struct Chain;
 
 template <int DX>
 struct Chain<LG<DX>> {
-  __device__ static double map(const ppf_model& m, const float* th, const double* gn, int p) {
+  __device__ static double map(const ppf_model& m, const float* th, const double* gn, int p, bool est) {
     const int dy = m.dy;
     const int nA = DX * DX, nC = dy * DX, nQ = DX * (DX + 1) / 2, nR = dy * (dy + 1) / 2;
     if (p < nA) return gn[LG<DX>::GA + p];
@@ -198,14 +199,14 @@ struct Chain<LG<DX>> {
     if (p < nQ) {
       double v = gn[LG<DX>::GQ + p];
       for (int i = 0; i < DX; ++i)
-        if (p == i * (i + 1) / 2 + i) v *= (double)pp_expf(th[nA + nC + p]);
+        if (est && p == i * (i + 1) / 2 + i) v *= (double)pp_expf(th[nA + nC + p]);
       return v;
     }
     p -= nQ;
     if (p < nR) {
       double v = gn[LG<DX>::GR + p];
       for (int i = 0; i < dy; ++i)
-        if (p == i * (i + 1) / 2 + i) v *= (double)pp_expf(th[nA + nC + nQ + p]);
+        if (est && p == i * (i + 1) / 2 + i) v *= (double)pp_expf(th[nA + nC + nQ + p]);
       return v;
     }
     p -= nR;
@@ -214,7 +215,8 @@ struct Chain<LG<DX>> {
 };
 template <>
 struct Chain<SV> {
-  __device__ static double map(const ppf_model&, const float* th, const double* gn, int p) {
+  __device__ static double map(const ppf_model&, const float* th, const double* gn, int p, bool est) {
+    if (!est) return gn[p];
     if (p < 3) return gn[p] * (double)pp_expf(th[p]);
     if (p == 3) {
       const double r = (double)pp_tanhf_det(th[3]);
@@ -225,8 +227,8 @@ struct Chain<SV> {
 };
 template <>
 struct Chain<Ricker> {
-  __device__ static double map(const ppf_model&, const float* th, const double* gn, int p) {
-    return gn[p] * (double)pp_expf(th[p]);
+  __device__ static double map(const ppf_model&, const float* th, const double* gn, int p, bool est) {
+    return est ? gn[p] * (double)pp_expf(th[p]) : gn[p];
   }
 };
 
@@ -235,8 +237,8 @@ __global__ void k_mop_chain(Args a, const double* gnat, double* grad) {
   const int f = blockIdx.x;
   const int P = a.model.n_params;
   for (int p = threadIdx.x; p < P; p += blockDim.x)
-    grad[(size_t)f * P + p] =
-        Chain<M>::map(a.model, a.theta + (size_t)f * P, gnat + (size_t)f * kMaxNG, p);
+    grad[(size_t)f * P + p] = Chain<M>::map(a.model, a.theta + (size_t)f * P, gnat + (size_t)f * kMaxNG, p,
+                                            (a.flags & PPF_F_EST) != 0);
 }
 
 // ---------------------------------------------------------------------------

@@ -161,13 +161,13 @@ class MopCall:
     state checkpoints) for a later adjoint sweep.
 
     ``theta_est`` is a (F, P) host array or CUDA tensor on the estimation
-    scale.  ``forward(grad)`` runs ``ppf_mop`` (the adjoint too when
+    scale (natural scale with ``natural``, ``PPF_F_NATURAL``).  ``forward(grad)`` runs ``ppf_mop`` (the adjoint too when
     ``grad``); ``backward(dvalue)`` runs ``ppf_mop_backward`` on the same
     workspace and returns ``dvalue[f] * d value[f] / d theta[f]``.
     """
 
     def __init__(self, struct: PompStruct, theta_est, seeds_f, J: int, alpha: float, *, unit_f=None,
-                 inject=None, ckpt_every: int = 0, save_ancestors: bool = False):
+                 inject=None, ckpt_every: int = 0, save_ancestors: bool = False, natural: bool = False):
         torch = _ffi.require_cuda()
         if J < 1:
             raise ValueError("J should be greater than 0.")
@@ -195,7 +195,7 @@ class MopCall:
         if save_ancestors:
             self.out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=dev)
         inj = {}
-        flags = 0
+        flags = _ffi.F_NATURAL if natural else 0
         if inject is not None:
             flags |= _ffi.F_INJECT
             for k in ("z0", "z", "u"):
@@ -354,7 +354,7 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
 
 def run_perfilter(struct: PompStruct, swarm, seeds_f: np.ndarray, J: int, rw_sig, rw_sig0, cool, cool0,
                   *, thresh: float = 0.0, unit_f=None, inject=None, CLL: bool = False,
-                  save_ancestors: bool = False):
+                  save_ancestors: bool = False, natural: bool = False):
     """One batched call of ``ppf_perfilter``: one IF2 iteration over F swarms.
 
     ``swarm`` is either a CUDA tensor (F, P, J) on the estimation scale (kept
@@ -362,8 +362,10 @@ def run_perfilter(struct: PompStruct, swarm, seeds_f: np.ndarray, J: int, rw_sig
     (F, J, P).  ``cool`` (T,) or (U, T) and ``cool0`` (scalar or (U,)) are the
     cooling factors of the step and t0 perturbations.  ``inject`` optionally
     holds host arrays ``zp0`` (F,J,P), ``zp`` (F,T,J,P), ``z0``, ``z``, ``u``
-    replacing the Philox draws.  Returns a dict with ``loglik`` (F,),
-    ``swarm`` and optionally ``cll`` / ``anc``.
+    replacing the Philox draws.  ``natural`` hands the kernels natural-scale
+    parameters (``PPF_F_NATURAL``: no transform inside the mechanics).
+    Returns a dict with ``loglik`` (F,), ``swarm`` and optionally ``cll`` /
+    ``anc``.
     """
     torch = _ffi.require_cuda()
     if J < 1:
@@ -399,7 +401,7 @@ def run_perfilter(struct: PompStruct, swarm, seeds_f: np.ndarray, J: int, rw_sig
         unit_d = torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
     out = {"loglik": torch.zeros(F, dtype=torch.float64, device=dev),
            "swarm": torch.empty(F, P, J, **f32d)}
-    flags = 0
+    flags = _ffi.F_NATURAL if natural else 0
     if CLL:
         flags |= _ffi.F_CLL
         out["cll"] = torch.zeros(F, T, dtype=torch.float64, device=dev)
@@ -506,3 +508,348 @@ def mif(struct: PompStruct, thetas_array, rw_sd, M: int, J: int, keys, thresh: f
     final = swarm.cpu().numpy().transpose(0, 2, 1)
     final = spec.from_est(final.reshape(-1, len(names))).reshape(final.shape)
     return logliks, traces, final
+
+
+# ---------------------------------------------------------------------------
+# Panels
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class PanelPompStruct:
+    """What the kernels need from a panel (``pypomp/functional/structs.py:156``).
+
+    Units share one built-in model; their series may have different lengths:
+    ``ys`` is (U, Tmax, dy) padded after ``T_u[u]`` observations (the
+    reference stacks equal-length units only).  ``permutations[u][i]`` is the
+    panel-order index ([shared | unit-specific] names) of the unit model's
+    canonical parameter i.
+    """
+
+    spec: ModelSpec
+    ys: np.ndarray
+    T_u: np.ndarray
+    times: list
+    t0: float
+    unit_names: list
+    shared_param_names: list
+    unit_param_names: list
+    permutations: np.ndarray
+
+    @property
+    def param_names(self):
+        return list(self.shared_param_names) + list(self.unit_param_names)
+
+    @property
+    def U(self):
+        return len(self.unit_names)
+
+    def all_units(self) -> PompStruct:
+        return PompStruct(spec=self.spec, ys=self.ys, times=np.arange(self.ys.shape[1]), t0=self.t0,
+                          T_u=np.asarray(self.T_u, np.int32))
+
+    def unit(self, u: int) -> PompStruct:
+        T = int(self.T_u[u])
+        return PompStruct(spec=self.spec, ys=np.ascontiguousarray(self.ys[u, :T]),
+                          times=np.asarray(self.times[u]), t0=self.t0)
+
+
+def _mask_ragged(arr, T_u, unit_of_row):
+    """NaN after each row's own series length (diagnostics of ragged panels)."""
+    arr = np.array(arr, dtype=np.float64 if arr.dtype == np.float64 else np.float32, copy=True)
+    for i, u in enumerate(unit_of_row):
+        arr[i, int(T_u[u]):] = np.nan
+    return arr
+
+
+def panel_pfilter(struct: PanelPompStruct, thetas_array, J: int, keys, thresh: float = 0.0,
+                  chunk_size: int = 1, CLL: bool = False, ESS: bool = False, filter_mean: bool = False,
+                  prediction_mean: bool = False, *, inject=None) -> dict:
+    """Panel particle filter (``pypomp/functional/pfilter.py:93-140``).
+
+    ``thetas_array`` (n_reps, U, P) in each unit's canonical order, natural
+    scale; ``keys`` (n_reps, U).  All n_reps x U filters run in one call
+    (``chunk_size`` is accepted for signature compatibility; there is nothing
+    to chunk).  Returns ``logLik`` (n_reps, U) and the requested diagnostics
+    with a (n_reps, U, Tmax[, dx]) layout, NaN after a unit's last observation.
+    ``inject`` optionally replays external draws (``run_pfilter``'s arrays
+    with a leading n_reps * U filter axis).
+    """
+    del chunk_size
+    th = np.asarray(thetas_array, dtype=np.float32)
+    n, U, P = th.shape
+    keys = np.asarray(keys, dtype=np.uint64).reshape(n, U)
+    unit_f = np.tile(np.arange(U, dtype=np.int32), n)
+    res = run_pfilter(struct.all_units(), th.reshape(n * U, P), keys.reshape(-1), J, thresh=thresh,
+                      CLL=CLL, ESS=ESS, filter_mean=filter_mean, prediction_mean=prediction_mean,
+                      unit_f=unit_f, inject=inject)
+    out = {"logLik": res["loglik"].reshape(n, U)}
+    for name, key in (("CLL", "cll"), ("ESS", "ess"), ("filter_mean", "fmean"), ("prediction_mean", "pmean")):
+        if key in res:
+            a = _mask_ragged(res[key], struct.T_u, unit_f)
+            out[name] = a.reshape((n, U) + a.shape[1:])
+    return out
+
+
+def _panel_thetas(shared, unit, perms):
+    """Unit-order parameters from [shared | unit] panel blocks.
+
+    ``shared`` (..., ns), ``unit`` (..., U, nu) -> (..., U, P) with
+    theta_u[i] = panel_u[perms[u][i]]."""
+    U = unit.shape[-2]
+    sh = np.broadcast_to(shared[..., None, :], shared.shape[:-1] + (U, shared.shape[-1]))
+    panel = np.concatenate([sh, unit], axis=-1)
+    out = np.empty(panel.shape[:-1] + (perms.shape[1],), dtype=panel.dtype)
+    for u in range(U):
+        out[..., u, :] = panel[..., u, perms[u]]
+    return out
+
+
+def panel_mop(struct: PanelPompStruct, thetas_array, J: int, alpha: float, keys, grad: bool = False):
+    """MOP-alpha values of every (replicate, unit) filter in one call
+    (``_panel_mop_internal_vmap``, ``pypomp/core/algorithms/mop.py:161-179``).
+
+    ``thetas_array`` (n, U, P) on the estimation scale, unit order; ``keys``
+    (n, U).  Returns value (n, U) and, with ``grad``, d value / d theta
+    (n, U, P)."""
+    th = np.asarray(thetas_array, dtype=np.float32)
+    n, U, P = th.shape
+    keys = np.asarray(keys, dtype=np.uint64).reshape(n, U)
+    unit_f = np.tile(np.arange(U, dtype=np.int32), n)
+    res = run_mop(struct.all_units(), th.reshape(n * U, P), keys.reshape(-1), J, alpha, grad=grad,
+                  unit_f=unit_f)
+    out = {"value": res["value"].reshape(n, U)}
+    if grad:
+        out["grad"] = res["grad"].reshape(n, U, P)
+    return out
+
+
+def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, J: int, keys,
+              thresh: float = 0.0, n_monitors: int = 0, block: bool = True, *, inject=None):
+    """Panel iterated filtering (``pypomp/functional/mif.py:125-259``;
+    ``_panel_mif_internal`` / ``_panel_mif_unit_scan_fn`` at
+    ``pypomp/core/algorithms/panel_mif.py:17-247``).
+
+    ``shared_array`` (n_reps, J, n_shared) and ``unit_array``
+    (n_reps, J, U, n_spec), natural scale.  Every iteration visits the units
+    in order; for unit u the swarms [shared | unit u] are permuted to the
+    unit's canonical order, run through one perturbed filter (all replicates
+    in one ``ppf_perfilter`` call, swarms resident on the GPU), and written
+    back; the shared swarm carries from unit to unit.  With ``block=False``
+    the other units' swarms are reordered by unit u's resampling ancestry.
+    Keys: per replicate ``split(key, M+1)[1:]`` iteration keys, then
+    ``split(iteration key, U)`` unit keys (monitors ``split(unit key,
+    n_monitors)``).  The cooling factor of a unit uses that unit's own
+    series length.  ``inject``, for replaying external draws, is indexed
+    ``inject[m][u]`` like ``mif``'s.  Returns (shared_traces (n, M+1, ns+1),
+    unit_traces (n, M+1, U, nu+1), final shared swarm (n, J, ns), final unit
+    swarm (n, J, U, nu)); column 0 of the traces is the log-likelihood
+    (summed over units for the shared trace), the rest are swarm means.
+    """
+    from . import random as pprandom
+
+    torch = _ffi.require_cuda()
+    spec = struct.spec
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sh = np.asarray(shared_array, dtype=np.float64)
+    un = np.asarray(unit_array, dtype=np.float64)
+    n = sh.shape[0]
+    ns, nu, U = sh.shape[2], un.shape[3], struct.U
+    if sh.shape[1] != J or un.shape[1] != J or un.shape[2] != U:
+        raise ValueError("shared_array must be (n_reps, J, n_shared) and unit_array (n_reps, J, U, n_spec)")
+    if M < 1:
+        raise ValueError("M must be greater than 0.")
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    perms = np.asarray(struct.permutations, dtype=np.int64)
+    inv_perms = np.argsort(perms, axis=1)
+    names = struct.param_names
+    sig_p, sig0_p = rw_sd.arrays(names)                      # panel order
+    # estimation-scale swarms on the device: shared (n, ns, J), unit (n, U, nu, J)
+    panel0 = np.concatenate([sh[:, :, None, :].repeat(U, axis=2), un], axis=3)   # (n, J, U, Pp)
+    est_unit = np.empty_like(panel0)
+    for u in range(U):
+        th_u = spec.to_est(panel0[:, :, u, perms[u]])        # unit order
+        est_unit[:, :, u, :] = th_u[:, :, inv_perms[u]]      # back to panel order
+    S = torch.tensor(est_unit[:, :, 0, :ns].transpose(0, 2, 1).copy(), dtype=torch.float32, device=dev)
+    Us = torch.tensor(est_unit[:, :, :, ns:].transpose(0, 2, 3, 1).copy(), dtype=torch.float32, device=dev)
+    m_keys = np.stack([pprandom.split(k, M + 1)[1:] for k in keys])        # (n, M)
+
+    def means():
+        return S.mean(dim=2).cpu().numpy(), Us.mean(dim=3).cpu().numpy()  # (n, ns), (n, U, nu)
+
+    def nat_means(s_mean, u_mean):
+        s_out = np.empty((n, ns))
+        u_out = np.empty((n, U, nu))
+        for u in range(U):
+            panel = np.concatenate([s_mean, u_mean[:, u]], axis=1)
+            nat = spec.from_est(panel[:, perms[u]])[:, inv_perms[u]]
+            u_out[:, u] = nat[:, ns:]
+            if u == 0:
+                s_out = nat[:, :ns]
+        return s_out, u_out
+
+    s0, u0 = nat_means(*means())
+    shared_tr = np.full((n, M + 1, ns + 1), np.nan)
+    unit_tr = np.full((n, M + 1, U, nu + 1), np.nan)
+    shared_tr[:, 0, 1:], unit_tr[:, 0, :, 1:] = s0, u0
+    perm_t = [torch.tensor(perms[u], device=dev) for u in range(U)]
+    inv_t = [torch.tensor(inv_perms[u], device=dev) for u in range(U)]
+    for it in range(M):
+        unit_keys = np.stack([pprandom.split(k, U) for k in m_keys[:, it]])    # (n, U)
+        ll_units = np.zeros((n, U))
+        for u in range(U):
+            st_u = struct.unit(u)
+            T = st_u.ys.shape[0]
+            panel = torch.cat([S, Us[:, u]], dim=1)                             # (n, Pp, J)
+            swarm = panel.index_select(1, perm_t[u]).contiguous()               # unit order
+            cool = np.array([rw_sd.cooling_factor(i, it, T) for i in range(T)], dtype=np.float32)
+            inj = inject[it][u] if inject is not None else None
+            res = run_perfilter(st_u, swarm, unit_keys[:, u], J, sig_p[perms[u]], sig0_p[perms[u]], cool,
+                                cool[0], thresh=thresh, save_ancestors=not block,
+                                inject=None if inj is None else inj["perfilter"])
+            if n_monitors >= 1:
+                mean = swarm.mean(dim=2).cpu().numpy()
+                mon = np.stack([pprandom.split(k, n_monitors) for k in unit_keys[:, u]])
+                minj = None
+                if inj is not None:
+                    minj = {k: np.stack([np.stack([inj["monitors"][i][k][r] for i in range(n_monitors)])
+                                         for r in range(n)]).reshape(
+                                             (n * n_monitors,) + inj["monitors"][0][k].shape[1:])
+                            for k in ("z0", "z", "u")}
+                pf = run_pfilter(st_u, np.repeat(mean, n_monitors, axis=0), mon.reshape(-1), J, thresh=thresh,
+                                 est=True, inject=minj)
+                ll_units[:, u] = -(-pf["loglik"].reshape(n, n_monitors)).mean(axis=1)
+            else:
+                ll_units[:, u] = res["loglik"].cpu().numpy()
+            new_panel = res["swarm"].index_select(1, inv_t[u])                  # panel order
+            if ns > 0:
+                S = new_panel[:, :ns].contiguous()
+            if nu > 0:
+                if not block:
+                    anc = res["anc"]                                           # (n, T, J)
+                    origin = torch.arange(J, device=dev).expand(n, J).contiguous()
+                    for t in range(T):
+                        origin = torch.gather(origin, 1, anc[:, t].long())
+                    idx = origin[:, None, None, :].expand(n, U, nu, J)
+                    Us = torch.gather(Us, 3, idx)
+                Us = Us.clone()
+                Us[:, u] = new_panel[:, ns:]
+        s_mean, u_mean = nat_means(*means())
+        shared_tr[:, it + 1, 0] = ll_units.sum(axis=1)
+        shared_tr[:, it + 1, 1:] = s_mean
+        unit_tr[:, it + 1, :, 0] = ll_units
+        unit_tr[:, it + 1, :, 1:] = u_mean
+    # final swarms on the natural scale
+    s_fin = S.cpu().numpy().transpose(0, 2, 1)                 # (n, J, ns)
+    u_fin = Us.cpu().numpy().transpose(0, 3, 1, 2)             # (n, J, U, nu)
+    fs = np.empty((n, J, ns))
+    fu = np.empty((n, J, U, nu))
+    for u in range(U):
+        panel = np.concatenate([s_fin, u_fin[:, :, u]], axis=2)
+        nat = spec.from_est(panel[:, :, perms[u]])[:, :, inv_perms[u]]
+        fu[:, :, u] = nat[:, :, ns:]
+        if u == 0:
+            fs = nat[:, :, :ns]
+    return shared_tr, unit_tr, fs, fu
+
+
+def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optimizer, M: int, eta,
+                alpha: float, keys, alpha_cooling: float = 1.0, chunk_size: int = 1, *, inject=None):
+    """Panel MOP-alpha gradient training (``pypomp/functional/train.py:112-190``;
+    ``_panel_train_internal`` / ``_chunk_scan_step`` at
+    ``pypomp/core/algorithms/train.py:191-413``).
+
+    ``shared_array`` (n_reps, n_shared), ``unit_array`` (n_reps, U, n_spec),
+    natural scale; ``keys`` (n_reps, M, U) (or (n_reps,), split into M x U).
+    Each iteration walks the units in chunks of ``chunk_size``; a chunk's
+    MOP values and gradients for every replicate come from one ``ppf_mop``
+    call.  Chunk loss = sum of its units' MOP values / (chunk_size * Tmax);
+    the shared parameters take one optimiser step per chunk with rate
+    eta / n_chunks (global step count), the unit parameters one step with the
+    gradient scaled by chunk_size (iteration count).  Returns
+    (neg_logliks (n, M+1), shared (n, M+1, ns), unit (n, M+1, U, nu)),
+    natural scale, NaN first log-likelihood.  ``inject[m][c]`` optionally
+    replays external draws for chunk c of iteration m.
+    """
+    from . import random as pprandom
+    from .optim import LearningRate, cosine_alpha
+
+    if optimizer.ls:
+        raise NotImplementedError("line search is not supported by the CUDA train loop")
+    spec = struct.spec
+    U, Tn = struct.U, struct.ys.shape[1]
+    cs = max(1, int(chunk_size))
+    if U % cs:
+        raise ValueError("chunk_size must divide the number of units")
+    nch = U // cs
+    sh = np.asarray(shared_array, dtype=np.float64)
+    un = np.asarray(unit_array, dtype=np.float64)
+    n, ns = sh.shape
+    nu = un.shape[2]
+    keys = np.asarray(keys, dtype=np.uint64)
+    if keys.ndim == 1:
+        keys = np.stack([pprandom.split(k, M * U) for k in keys]).reshape(n, M, U)
+    keys = keys.reshape(n, M, U)
+    perms = np.asarray(struct.permutations, dtype=np.int64)
+    inv_perms = np.argsort(perms, axis=1)
+    eta_s = eta.to_array(struct.shared_param_names, M) if (ns and isinstance(eta, LearningRate)) else \
+        np.broadcast_to(np.asarray(eta, np.float64), (max(M, 1), ns)) if ns else np.zeros((max(M, 1), 0))
+    eta_u = eta.to_array(struct.unit_param_names, M) if (nu and isinstance(eta, LearningRate)) else \
+        np.broadcast_to(np.asarray(eta, np.float64), (max(M, 1), nu)) if nu else np.zeros((max(M, 1), 0))
+
+    def to_est_blocks(s_nat, u_nat):
+        th = _panel_thetas(s_nat, u_nat, perms)                       # (n, U, P) unit order
+        est = spec.to_est(th)
+        panel = np.stack([est[:, u, inv_perms[u]] for u in range(U)], axis=1)   # (n, U, Pp)
+        return panel[:, 0, :ns].copy(), panel[:, :, ns:].copy()
+
+    def from_est_blocks(s_est, u_est):
+        th = _panel_thetas(s_est, u_est, perms)
+        nat = spec.from_est(th)
+        panel = np.stack([nat[:, u, inv_perms[u]] for u in range(U)], axis=1)
+        return panel[:, 0, :ns].copy(), panel[:, :, ns:].copy()
+
+    s_est, u_est = to_est_blocks(sh, un)
+    st_s = optimizer.init_state(s_est)
+    st_u = optimizer.init_state(u_est)
+    gstep = 0
+    nll = np.full((n, M + 1), np.nan)
+    hist_s = np.zeros((n, M + 1, ns))
+    hist_u = np.zeros((n, M + 1, U, nu))
+    hist_s[:, 0], hist_u[:, 0] = sh, un
+    all_units = struct.all_units()
+    for m in range(M):
+        alpha_m = 1.0 - (1.0 - alpha) * cosine_alpha(m, M, alpha_cooling)
+        chunk_nll = np.zeros((n, nch))
+        for c in range(nch):
+            units = np.arange(c * cs, (c + 1) * cs)
+            th = _panel_thetas(s_est, u_est[:, units], perms[units])    # (n, cs, P)
+            inj = inject[m][c] if inject is not None else None
+            res = run_mop(all_units, th.reshape(n * cs, -1).astype(np.float32), keys[:, m, units].reshape(-1),
+                          J, alpha_m, grad=True, unit_f=np.tile(units.astype(np.int32), n), inject=inj)
+            val = res["value"].reshape(n, cs)
+            g = res["grad"].reshape(n, cs, -1)
+            gp = np.zeros((n, cs, ns + nu))
+            for j, u in enumerate(units):
+                gp[:, j, perms[u]] = g[:, j]
+            scale = 1.0 / (cs * Tn)
+            grad_s = gp[:, :, :ns].sum(axis=1) * scale
+            grad_u = gp[:, :, ns:] * scale * cs
+            chunk_nll[:, c] = val.sum(axis=1) * scale * (Tn * U)
+            if optimizer.clip_norm is not None:
+                grad_s = np.clip(grad_s, -optimizer.clip_norm, optimizer.clip_norm)
+                grad_u = np.clip(grad_u, -optimizer.clip_norm, optimizer.clip_norm)
+            d_s, st_s = optimizer.step(grad_s, st_s, gstep)
+            st_uc = tuple(x[:, units] for x in st_u)
+            d_u, st_uc = optimizer.step(grad_u, st_uc, m)
+            for x, y in zip(st_u, st_uc):
+                x[:, units] = y
+            if optimizer.scale:
+                d_s = d_s / np.maximum(np.linalg.norm(d_s, axis=-1, keepdims=True), 1e-8)
+                d_u = d_u / np.maximum(np.linalg.norm(d_u, axis=-1, keepdims=True), 1e-8)
+            s_est = s_est + (eta_s[m] / nch) * d_s
+            u_est[:, units] = u_est[:, units] + eta_u[m] * d_u
+            gstep += 1
+        nll[:, m + 1] = chunk_nll.mean(axis=1)
+        hist_s[:, m + 1], hist_u[:, m + 1] = from_est_blocks(s_est, u_est)
+    return nll, hist_s, hist_u

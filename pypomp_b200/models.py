@@ -40,6 +40,7 @@ class ModelSpec:
     est_log: tuple = ()     # indices transformed by log / exp
     est_atanh: tuple = ()   # indices transformed by atanh / tanh
     name: str = ""
+    natural: bool = False   # host-side identity transform (ParTrans() assigned after construction)
 
     @property
     def n_params(self) -> int:
@@ -50,6 +51,8 @@ class ModelSpec:
 
     def to_est(self, theta: np.ndarray) -> np.ndarray:
         t = np.array(theta, dtype=np.float64, copy=True)
+        if self.natural:
+            return t
         if self.est_log:
             t[..., list(self.est_log)] = np.log(t[..., list(self.est_log)])
         if self.est_atanh:
@@ -58,6 +61,8 @@ class ModelSpec:
 
     def from_est(self, theta: np.ndarray) -> np.ndarray:
         t = np.array(theta, dtype=np.float64, copy=True)
+        if self.natural:
+            return t
         if self.est_log:
             t[..., list(self.est_log)] = np.exp(t[..., list(self.est_log)])
         if self.est_atanh:

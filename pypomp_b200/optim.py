@@ -90,11 +90,12 @@ class LearningRate:
             self._rates[str(k)] = arr
 
     def to_array(self, param_names: Sequence[str], M: int) -> np.ndarray:
-        """(M, P) schedule in ``param_names`` order (``learning_rate.py:137-167``)."""
+        """(M, P) schedule in ``param_names`` order (``learning_rate.py:113-167``);
+        every requested name must have a rate, extra rates are ignored."""
         names = list(param_names)
-        if set(names) != set(self._rates):
-            raise ValueError(
-                f"LearningRate names must match the model's parameters: {sorted(self._rates)} vs {sorted(names)}")
+        for n in names:
+            if n not in self._rates:
+                raise ValueError(f"Parameter '{n}' not found in learning rates")
         M_eff = max(int(M), 1)
         cols = []
         for n in names:

@@ -132,8 +132,51 @@ class ResultsHistory:
         return [r.execution_time for r in self._results]
 
 
+class ParTrans:
+    """Parameter transform between the natural and the estimation scale
+    (``pypomp/core/par_trans.py:70``).
+
+    ``ParTrans()`` is the identity, as in the reference.  The built-in models
+    carry their own default transform (logs / atanh, in their ``ModelSpec``).
+    Assigning ``ParTrans()`` to ``Pomp.par_trans`` after construction behaves
+    as it does in the reference: the host-side conversions (``to_est`` /
+    ``from_est`` of the swarms, traces and results) become the identity, while
+    the model mechanics keep the transform the model was built with (the
+    reference binds it to the rinit/rproc/dmeas components when the ``Pomp``
+    is constructed, ``pypomp/core/pomp.py:271-313``).  User-written transform
+    functions cannot reach the device code, so they are refused.
+    """
+
+    def __init__(self, to_est=None, from_est=None):
+        if to_est is not None or from_est is not None:
+            raise NotImplementedError(
+                "custom parameter transforms are not supported by the CUDA path; "
+                "use the model's default transform or ParTrans() (identity)")
+        self.identity = True
+
+    def __repr__(self):
+        return "ParTrans()"
+
+
 class Pomp:
     """A partially observed Markov process on one of the built-in CUDA models."""
+
+    @property
+    def par_trans(self):
+        """``ParTrans()`` when the host-side identity transform is active, else
+        the model's default transform (represented by its ``ModelSpec``)."""
+        return ParTrans() if self.spec.natural else self.spec
+
+    @par_trans.setter
+    def par_trans(self, value):
+        from dataclasses import replace
+
+        if isinstance(value, ParTrans):
+            self.spec = replace(self.spec, natural=True)
+        elif value is None or value is self.spec or getattr(value, "kind", None) == self.spec.kind:
+            self.spec = replace(self.spec, natural=False)
+        else:
+            raise TypeError("par_trans must be a ParTrans instance")
 
     def __init__(self, spec, ys: pd.DataFrame, theta, t0: float = 0.0, fresh_key=None):
         self.spec = spec

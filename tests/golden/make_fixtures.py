@@ -15,7 +15,8 @@ Writes
                    normals and uniforms the reference draws for each locked
                    filter run (replayed key trees), for noise-injection runs;
                    ``mif_*`` / ``mift_*`` hold the draws of the locked mif runs
-                   (perturbation normals too) and their monitors
+                   (perturbation normals too) and their monitors; ``ppf_*``,
+                   ``pmif_*``, ``ptrain_*`` those of the locked panel runs
 """
 
 from __future__ import annotations
@@ -63,6 +64,9 @@ def main(ref_root: Path):
         "mif": _read_csv(reg / "test_mif_regression" / "test_mif_regression.csv"),
         "mif_full_trace": _read_csv(reg / "test_mif_regression" / "test_mif_full_trace_regression.csv"),
         "train": _read_csv(reg / "test_train_regression" / "test_train_regression.csv"),
+        "panel_pfilter": _read_csv(reg / "test_panel_pfilter_regression" / "test_panel_pfilter_regression.csv"),
+        "panel_mif": _read_csv(reg / "test_panel_mif_regression" / "test_panel_mif_regression.csv"),
+        "panel_train": _read_csv(reg / "test_panel_train_regression" / "test_panel_train_regression.csv"),
         "tolerance": {"atol": 1e-6, "rtol": 1e-4},
         "source": "pypomp 0.4.10.2 tests/test_regression (tolerance: tests/test_regression/conftest.py:118-125)",
     }
@@ -111,6 +115,30 @@ def main(ref_root: Path):
         if key in ("z0", "z", "u"):
             arrays[f"mift_mon_{key}"] = np.stack([np.stack([d["monitors"][0][key] for d in reps[r]])
                                                   for r in range(2)])                # (2, M, ...)
+    # panel of two LG units (tests/test_regression/conftest.py:61-110): unit 2's
+    # data from key(1); identity host transform; shared A11, C11; unit Q11, R11, X0_1
+    _, Y2 = rp.pomp_simulate_data("LG", THETA_LG1D, 4, jr.key(1))
+    ys2 = Y2.astype(f32)
+    arrays["panel_ys2"] = ys2
+    pkey = jr.key(20260811)
+    _, pdraws = rp.panel_pfilter("LG", np.stack([THETA_LG1D, THETA_LG1D]), [ys, ys2], J, jr.split(pkey, 2))
+    for key in ("z0", "z", "u"):
+        arrays[f"ppf_{key}"] = np.stack([d[key] for d in pdraws])                       # (U, ...)
+    _, _, mdraws = rp.panel_mif("LG", THETA_LG1D[:2], np.stack([THETA_LG1D[2:]] * 2), [ys, ys2], J, 3, sig,
+                                sig0, mif_cooling, jr.split(pkey, 1)[0], host_identity=True)
+    for key in ("zp0", "zp", "z0", "z", "u"):
+        arrays[f"pmif_{key}"] = np.stack([np.stack([d["perfilter"][key] for d in dm]) for dm in mdraws])  # (M, U, ...)
+    # panel train: keys split(key, n_reps * M * U) -> (M, U); each a MOP key tree
+    tkeys = jr.split(pkey, 3 * 2)
+    tz0, tz, tu = [], [], []
+    for i in range(6):
+        rec = rp.RecordingNoise(rp.JaxKeyNoise(tkeys[i], J, 1, 1))
+        rp.mop("LG", THETA_LG1D, ys, J, 0.97, rec)
+        a, b, c = rec.arrays()
+        tz0.append(a); tz.append(b); tu.append(c)
+    arrays["ptrain_z0"] = np.stack(tz0).reshape((3, 2) + tz0[0].shape)
+    arrays["ptrain_z"] = np.stack(tz).reshape((3, 2) + tz[0].shape)
+    arrays["ptrain_u"] = np.stack(tu).reshape((3, 2) + tu[0].shape)
     np.savez(OUT / "ref_lg1d.npz", **arrays)
 
 
