@@ -462,6 +462,75 @@ def run_c4(args):
                                 f"{24 * value / 1e9:.0f} GB/s"}})
 
 
+def run_c5(args):
+    """Panel IF2 then MOP training on 128 Ricker units of uneven length.
+
+    T_u ~ U{50..800}, log r_u ~ N(3.8, 0.2^2), shared sigma = 0.3, phi = 10,
+    J = 8192, rw sd 0.02 with geometric cooling 0.5.  The job is M = 100 IF2
+    iterations then 50 gradient steps; the bench times ``--steps`` of each
+    (after ``--warmup`` untimed ones) and reports particle-steps/s, where one
+    IF2 iteration or one training step processes sum(T_u) x J particle-steps.
+    """
+    import torch
+
+    import pypomp_b200 as pp
+    from pypomp_b200 import functional as F
+    from pypomp_b200.optim import Adam, LearningRate, RWSigma
+
+    rng = np.random.default_rng(0)
+    U, Jp = 128, 8192
+    T_u = rng.integers(50, 801, size=U)
+    logr = rng.normal(3.8, 0.2, size=U)
+    units = {f"unit{u}": pp.Ricker(T=int(T_u[u]), r=math.exp(logr[u]), key=1000 + u) for u in range(U)}
+    names = list(units)
+    import pandas as pd
+
+    shared = pd.DataFrame({"shared": [0.3, 10.0]}, index=["sigma", "phi"])
+    spec = pd.DataFrame([np.exp(logr), np.full(U, 7.0)], index=["r", "N_0"], columns=names)
+    pan = pp.PanelPomp(units, pp.PanelParameters({"shared": shared, "unit_specific": spec}))
+    st = pan.to_struct()
+    rw = RWSigma({n: 0.02 for n in pan.canonical_param_names}).geometric_cooling(0.5)
+    sh = np.repeat(pan.theta.shared_array()[:, None, :], Jp, axis=1)
+    un = np.repeat(pan.theta.unit_array(names)[:, None], Jp, axis=1)
+    steps_units = int(T_u.sum()) * Jp
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, n):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        fn(n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), time.perf_counter() - t0
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        F.panel_mif(st, sh, un, rw, max(args.warmup, 1), Jp, np.array([1], np.uint64))
+        mif_ms, mif_wall = timed(lambda n: F.panel_mif(st, sh, un, rw, n, Jp, np.array([2], np.uint64)),
+                                 args.steps)
+        eta = LearningRate({n: 0.01 for n in pan.canonical_param_names})
+        s0, u0 = pan.theta.shared_array(), pan.theta.unit_array(names)
+        F.panel_train(st, s0, u0, Jp, Adam(), max(args.warmup, 1), eta, 0.97, np.array([3], np.uint64),
+                      chunk_size=U)
+        tr_ms, tr_wall = timed(lambda n: F.panel_train(st, s0, u0, Jp, Adam(), n, eta, 0.97,
+                                                        np.array([4], np.uint64), chunk_size=U), args.steps)
+    mif_rate = steps_units * args.steps / (mif_ms / 1e3)
+    tr_rate = steps_units * args.steps / (tr_ms / 1e3)
+    job_s = 100 * mif_ms / args.steps / 1e3 + 50 * tr_ms / args.steps / 1e3
+    _line(args, "Ricker panel: 128 units, T_u in [50, 800], J=8192; IF2 then MOP train (configs[4])",
+          mif_rate, mif_ms / args.steps,
+          {"e2e": {"value": mif_rate, "unit": UNIT, "api": "functional.panel_mif (host inputs)",
+                   "h2d_bytes_per_step": int(sh.nbytes + un.nbytes + st.ys.nbytes), "d2h_bytes_per_step": 0},
+           "train": {"value": tr_rate, "unit": UNIT, "ms_per_step": tr_ms / args.steps,
+                     "api": "functional.panel_train, chunk_size=U (one MOP call per step)"},
+           "sum_T_u": int(T_u.sum()), "full_job_seconds_estimate": job_s,
+           "wall_s": {"mif": mif_wall, "train": tr_wall}, "clocks": clk.summary(),
+           "roofline": None,
+           "note": "IF2 visits the units one after another (the shared swarm carries from unit to unit), "
+                   "so each perturbed filter runs J=8192 particles = 4 tiles: launch- and latency-bound"})
+
+
 def run_profile_case(args):
     """A small case of the same kernels for ncu captures: the headline model
     and J, 24 seeds (state 2 x 24 x 262144 x 12 B = 151 MB, larger than L2),
@@ -491,11 +560,11 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="run one small call of the same kernels (for ncu) and exit")
     ap.add_argument("--path", default="stream")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default) is the headline line; c1/c3/c4 print their own lines")
     args = ap.parse_args()
     if args.config != "c2" and args.impl == "ours" and not args.profile_case:
-        {"c1": run_c1, "c3": run_c3, "c4": run_c4}[args.config](args)
+        {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args)
         return
     if args.profile_case:
         run_profile_case(args)

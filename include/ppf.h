@@ -97,7 +97,9 @@ typedef struct ppf_pfilter_desc {
   int32_t path;         /* PPF_PATH_* */
   uint32_t flags;       /* PPF_F_* */
   float thresh;         /* resampling threshold as in pfilter.py:159 */
-  int32_t tile;         /* particles per CTA tile (0 = autotuned) */
+  int32_t tile;         /* particles per CTA on the stream path: 2048, 512 or 256;
+                           0 = the ppf_autotune choice for this shape, else the
+                           largest tile that still launches 2 CTAs per SM */
   const float* theta;   /* [F][P] parameters (natural scale unless PPF_F_EST) */
   const float* ys;      /* [U][T][dy] observations */
   const float* ycon;    /* [U][T] per-observation constant (Ricker: lgamma(y+1)) or NULL */
@@ -210,6 +212,16 @@ size_t ppf_pfilter_workspace_bytes(const ppf_pfilter_desc* d);
 
 /* Run the batched particle filter.  `stream` is a cudaStream_t. */
 int ppf_pfilter(const ppf_pfilter_desc* d, void* stream);
+
+/* Measure the stream path's tile configurations (2048, 512, 256 particles
+ * per CTA) on this descriptor -- a prefix of at most 16 observations, each
+ * configuration run twice, timed with CUDA events on `stream` -- and remember
+ * the fastest for descriptors of the same shape (model, J, F, U, injection)
+ * that leave `tile` at 0.  Writes it to *best_tile (0 when the call would take
+ * the resident path).  Runs the filter, so it overwrites the outputs and uses
+ * the workspace; host-side cache, not thread-safe.  No counterpart in the
+ * reference: XLA picks its own tiling. */
+int ppf_autotune(const ppf_pfilter_desc* d, void* stream, int* best_tile);
 
 /* Synchronise `stream` and report the device-side status of the last call
  * that used `workspace`: PPF_ETIMEOUT if a bounded wait gave up,

@@ -43,6 +43,7 @@ EXPORTED = (
     "ppf_mop_backward",
     "ppf_perfilter_workspace_bytes",
     "ppf_perfilter",
+    "ppf_autotune",
     "ppf_workspace_status",
     "ppf_pfilter_noalloc",
     "ppf_profile_begin",
@@ -189,6 +190,8 @@ def _load():
     lib.ppf_perfilter.restype = ctypes.c_int
     lib.ppf_pfilter_noalloc.argtypes = [ctypes.POINTER(PfilterDesc), _vp]
     lib.ppf_pfilter_noalloc.restype = ctypes.c_int
+    lib.ppf_autotune.argtypes = [ctypes.POINTER(PfilterDesc), _vp, ctypes.POINTER(ctypes.c_int)]
+    lib.ppf_autotune.restype = ctypes.c_int
     lib.ppf_workspace_status.argtypes = [_vp, _vp]
     lib.ppf_workspace_status.restype = ctypes.c_int
     lib.ppf_profile_begin.argtypes = []

@@ -25,12 +25,14 @@ static size_t carve(Args& a, int path, unsigned char* base) {
   a.err = reinterpret_cast<uint32_t*>(take(64));
   a.counter = reinterpret_cast<unsigned int*>(base ? base + 16 : nullptr);
   if (path == PPF_PATH_STREAM) {
-    const int TILE = 2048;
-    a.tile = TILE;
-    a.ntiles = (a.J + TILE - 1) / TILE;
+    // a.tile is chosen before carving; the per-tile arrays are sized for the
+    // smallest tile so that one workspace serves every tile configuration
+    if (a.tile != kTileLarge && a.tile != kTileMid && a.tile != kTileSmall) a.tile = kTileLarge;
+    a.ntiles = (a.J + a.tile - 1) / a.tile;
+    const size_t nt_alloc = (size_t)(a.J + kTileSmall - 1) / kTileSmall;
     for (int i = 0; i < 2; ++i) a.acc[i] = reinterpret_cast<Acc*>(take(sizeof(Acc) * a.F));
-    for (int i = 0; i < 2; ++i) a.desc[i] = reinterpret_cast<uint64_t*>(take(8ull * a.F * a.ntiles));
-    a.excl = reinterpret_cast<uint64_t*>(take(8ull * a.F * a.ntiles));
+    for (int i = 0; i < 2; ++i) a.desc[i] = reinterpret_cast<uint64_t*>(take(8ull * a.F * nt_alloc));
+    a.excl = reinterpret_cast<uint64_t*>(take(8ull * a.F * nt_alloc));
     a.tot = reinterpret_cast<uint64_t*>(take(8ull * a.F));
     a.ctrl_bytes = off;
     a.consts = take(512ull * a.F);
@@ -90,6 +92,50 @@ static int choose_path(const ppf_pfilter_desc* d) {
   return PPF_PATH_STREAM;
 }
 
+// ---------------------------------------------------------------------------
+// Tile choice: an explicit desc->tile, else a measured choice from
+// ppf_autotune for the same shape, else the smallest tile that still gives
+// two CTAs per SM (more, smaller CTAs when there are few particles).
+// ---------------------------------------------------------------------------
+struct TuneEntry {
+  int kind, dx, dy, J, F, U, inj, tile;
+};
+constexpr int kTuneCap = 64;
+static TuneEntry g_tune[kTuneCap];
+static int g_tune_n = 0;
+
+static int tune_lookup(const ppf_model& m, int J, int F, int U, int inj) {
+  for (int i = 0; i < g_tune_n; ++i) {
+    const TuneEntry& e = g_tune[i];
+    if (e.kind == m.kind && e.dx == m.dx && e.dy == m.dy && e.J == J && e.F == F && e.U == U && e.inj == inj)
+      return e.tile;
+  }
+  return 0;
+}
+
+static void tune_store(const ppf_model& m, int J, int F, int U, int inj, int tile) {
+  for (int i = 0; i < g_tune_n; ++i) {
+    TuneEntry& e = g_tune[i];
+    if (e.kind == m.kind && e.dx == m.dx && e.dy == m.dy && e.J == J && e.F == F && e.U == U && e.inj == inj) {
+      e.tile = tile;
+      return;
+    }
+  }
+  TuneEntry e{m.kind, m.dx, m.dy, J, F, U, inj, tile};
+  g_tune[g_tune_n < kTuneCap ? g_tune_n++ : (kTuneCap - 1)] = e;
+}
+
+static int choose_tile(const ppf_model& m, int J, int F, int U, int inj, int requested) {
+  if (requested == kTileLarge || requested == kTileMid || requested == kTileSmall) return requested;
+  const int tuned = tune_lookup(m, J, F, U, inj);
+  if (tuned) return tuned;
+  const long long want = 2LL * kNumSMs;
+  const int cand[2] = {kTileLarge, kTileMid};
+  for (int c : cand)
+    if ((long long)F * ((J + c - 1) / c) >= want) return c;
+  return kTileSmall;
+}
+
 static int fill_args(const ppf_pfilter_desc* d, Args& a, int mode) {
   memset(&a, 0, sizeof(a));
   a.model = d->model;
@@ -109,6 +155,7 @@ static int fill_args(const ppf_pfilter_desc* d, Args& a, int mode) {
   a.pmean = (d->flags & PPF_F_PMEAN) ? d->pmean : nullptr;
   a.anc = (d->flags & PPF_F_SAVE_ANC) ? d->anc : nullptr;
   a.logw = (d->flags & PPF_F_SAVE_W) ? d->logw : nullptr;
+  a.tile = choose_tile(d->model, d->J, d->F, d->U, (d->flags & PPF_F_INJECT) ? 1 : 0, d->tile);
   return PPF_OK;
 }
 
@@ -129,6 +176,7 @@ static int validate(const ppf_pfilter_desc* d) {
   if ((d->flags & PPF_F_SAVE_ANC) && !d->anc) return PPF_EINVAL;
   if ((d->flags & PPF_F_SAVE_W) && !d->logw) return PPF_EINVAL;
   if (d->path < PPF_PATH_AUTO || d->path > PPF_PATH_RESIDENT) return PPF_EINVAL;
+  if (d->tile != 0 && d->tile != kTileLarge && d->tile != kTileMid && d->tile != kTileSmall) return PPF_EINVAL;
   return PPF_OK;
 }
 
@@ -361,6 +409,47 @@ int ppf_mop_backward(const ppf_mop_desc* d, const double* dvalue, void* stream) 
     k_scale_rows<<<(n + 255) / 256, 256, 0, s>>>(d->grad, dvalue, d->F, d->model.n_params);
   }
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
+int ppf_autotune(const ppf_pfilter_desc* d, void* stream, int* best_tile) {
+  int rc = validate(d);
+  if (rc) return rc;
+  if (!best_tile) return PPF_EINVAL;
+  if (choose_path(d) != PPF_PATH_STREAM) {
+    *best_tile = 0;
+    return PPF_OK;
+  }
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  ppf_pfilter_desc t;
+  memcpy(&t, d, sizeof(t));
+  t.path = PPF_PATH_STREAM;
+  if (t.T > 16) t.T = 16;   // a prefix of the time loop; the per-step cost does not depend on t
+  t.T_u = nullptr;
+  const int tiles[3] = {kTileLarge, kTileMid, kTileSmall};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return PPF_ECUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return PPF_ECUDA; }
+  float best_ms = 0.0f;
+  int best = 0;
+  for (int tile : tiles) {
+    t.tile = tile;
+    float ms = 0.0f;
+    for (int rep = 0; rep < 2 && rc == PPF_OK; ++rep) {   // first run warms up, second is timed
+      if (cudaEventRecord(e0, s) != cudaSuccess) rc = PPF_ECUDA;
+      if (!rc) rc = ppf_pfilter(&t, stream);
+      if (!rc && cudaEventRecord(e1, s) != cudaSuccess) rc = PPF_ECUDA;
+      if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = PPF_ECUDA;
+      if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (rc) break;
+    if (!best || ms < best_ms) { best = tile; best_ms = ms; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  tune_store(d->model, d->J, d->F, d->U, (d->flags & PPF_F_INJECT) ? 1 : 0, best);
+  *best_tile = best;
+  return PPF_OK;
 }
 
 int ppf_workspace_status(const void* workspace, void* stream) {

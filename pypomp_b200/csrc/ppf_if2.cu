@@ -254,10 +254,10 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
 
 static int if2_row_stride_host(int P) { return P | 1; }
 
-template <class M, bool INJ>
+template <class M, int TPB, int IT, bool INJ>
 int run_if2_t(Args& a, cudaStream_t s) {
-  constexpr int TPB = 256, IT = 8, TILE = TPB * IT;
-  if (a.tile != TILE) return PPF_EINVAL;   // the workspace was carved for this tile
+  constexpr int TILE = TPB * IT;
+  if (a.tile != TILE || a.ntiles != (a.J + TILE - 1) / TILE) return PPF_EINTERNAL;
   const size_t rows = sizeof(float) * TPB * if2_row_stride_host(a.model.n_params);
   const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4) + sizeof(float) * TILE + rows;
   if (smem > kResidentSmemMax) return PPF_EUNSUPPORTED;
@@ -279,9 +279,19 @@ int run_if2_t(Args& a, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
 
+template <class M, bool INJ>
+int run_if2_tiled(Args& a, cudaStream_t s) {
+  switch (a.tile) {
+    case kTileLarge: return run_if2_t<M, 256, 8, INJ>(a, s);
+    case kTileMid: return run_if2_t<M, 128, 4, INJ>(a, s);
+    case kTileSmall: return run_if2_t<M, 64, 4, INJ>(a, s);
+    default: return PPF_EINVAL;
+  }
+}
+
 template <class M>
 int run_if2_m(Args& a, cudaStream_t s) {
-  return (a.flags & PPF_F_INJECT) ? run_if2_t<M, true>(a, s) : run_if2_t<M, false>(a, s);
+  return (a.flags & PPF_F_INJECT) ? run_if2_tiled<M, true>(a, s) : run_if2_tiled<M, false>(a, s);
 }
 
 int run_if2(Args& a, cudaStream_t s) {

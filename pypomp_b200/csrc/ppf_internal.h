@@ -107,6 +107,13 @@ struct MopWork {
 
 int run_pfilter_path(Args& a, int path, cudaStream_t s);
 int run_stream_any(Args& a, cudaStream_t s);   // stream path, any model
+// Stream-path tile configurations (particles per CTA = threads x items per
+// thread): the tile sets how many CTAs one step launches, F x ceil(J / tile).
+constexpr int kTileLarge = 2048;   // 256 threads x 8
+constexpr int kTileMid = 512;      // 128 threads x 4
+constexpr int kTileSmall = 256;    // 64 threads x 4
+constexpr int kNumSMs = 148;
+
 int run_mop(Args& a, const MopWork& w, cudaStream_t s);
 int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s);
 int run_if2(Args& a, cudaStream_t s);

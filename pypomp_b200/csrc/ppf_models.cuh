@@ -379,14 +379,27 @@ struct Ricker {
                              float lm, float* lx, float* g) {
     const float Np = k.xP[0];
     const float N = xin[0];
-    // dmeas: y log(phi N') - phi N' - log y!
-    const float dgN = k.y / Np - c.phi;
-    g[2] += lm * (k.y / c.phi - Np);
-    const float lN = lx[0] + lm * dgN;
-    // rproc: N' = r N exp(-N + sigma z)
-    g[0] += lN * Np / c.r;
+    // dmeas: y log(phi N') - phi N' - log y!, d/dN' = y / N' - phi.  The
+    // weight adjoint lm carries the particle's weight, which scales like
+    // N'^y, so lm * y / N' is formed as (lm / N') * y: for a denormal N', y / N'
+    // alone overflows.  lm == 0 (an underflowed weight) contributes nothing.
+    float lN = lx[0];
+    if (lm != 0.0f) {
+      g[2] += lm * (k.y / c.phi - Np);
+      float dN = -lm * c.phi;
+      if (k.y != 0.0f) dN = dN + (lm / Np) * k.y;
+      lN = lN + dN;
+    }
+    if (lN == 0.0f) {
+      lx[0] = 0.0f;
+      return;
+    }
+    // rproc: N' = r N e, e = exp(-N + sigma z); dN'/dN = r e (1 - N), formed
+    // without dividing by N
+    const float re = c.r * pp_expf(pp_fma(c.sigma, z[0], -N));
+    g[0] += lN * (N * re) / c.r;
     g[1] += lN * Np * z[0];
-    lx[0] = lN * Np * (1.0f / N - 1.0f);
+    lx[0] = lN * re * (1.0f - N);
   }
   __device__ static void bwd_init(const Consts&, const float*, const float* lx0, float* g) {
     g[3] += lx0[0];

@@ -114,10 +114,11 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
 //      parent, then a linear walk; per group of 4 children one set of Philox
 //      calls (every word used), rproc + dmeas, float4 stores.
 template <class M, int TPB, int IT, bool INJ>
-__global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4)) k_resprop(Args a, int t) {
+__global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4) * (256 / TPB)) k_resprop(Args a, int t) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
-  constexpr int RUN = 8;
+  constexpr int RUN = IT;            // children per thread run: TPB runs cover a full tile
+  static_assert(RUN % 4 == 0, "children are drawn in groups of 4");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* xs = reinterpret_cast<float*>(smem_raw);                              // [DX][TILE]
   int* st = reinterpret_cast<int*>(smem_raw + sizeof(float) * DX * TILE);      // [TILE + 1]
@@ -703,11 +704,10 @@ void Profiler::mark(int kind, cudaStream_t s, bool start) {
 }
 
 
-template <class M, bool INJ>
+template <class M, int TPB, int IT, bool INJ>
 int run_stream_t(Args& a, cudaStream_t s) {
-  constexpr int TPB = 256, IT = 8, TILE = TPB * IT;
-  a.tile = TILE;
-  a.ntiles = (a.J + TILE - 1) / TILE;
+  constexpr int TILE = TPB * IT;
+  if (a.tile != TILE || a.ntiles != (a.J + TILE - 1) / TILE) return PPF_EINTERNAL;
   const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4) + sizeof(float) * TILE;
   if (cudaFuncSetAttribute(k_resprop<M, TPB, IT, INJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
@@ -728,9 +728,19 @@ int run_stream_t(Args& a, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
 
+template <class M, bool INJ>
+int run_stream_tiled(Args& a, cudaStream_t s) {
+  switch (a.tile) {
+    case kTileLarge: return run_stream_t<M, 256, 8, INJ>(a, s);
+    case kTileMid: return run_stream_t<M, 128, 4, INJ>(a, s);
+    case kTileSmall: return run_stream_t<M, 64, 4, INJ>(a, s);
+    default: return PPF_EINVAL;
+  }
+}
+
 template <class M>
 int run_stream(Args& a, cudaStream_t s) {
-  return (a.flags & PPF_F_INJECT) ? run_stream_t<M, true>(a, s) : run_stream_t<M, false>(a, s);
+  return (a.flags & PPF_F_INJECT) ? run_stream_tiled<M, true>(a, s) : run_stream_tiled<M, false>(a, s);
 }
 
 template <class M>

@@ -56,7 +56,9 @@ def run_pfilter(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J:
 
     ``theta_f`` (F, P) parameters, ``seeds_f`` (F,) keys.  ``inject`` is an
     optional dict of host arrays ``z0`` (F,J,n0), ``z`` (F,T,J,nz), ``u``
-    (F,T) that replaces the Philox draws.  Returns a dict of NumPy arrays.
+    (F,T) that replaces the Philox draws.  ``path`` is "plain", "stream",
+    "resident", "stream@<tile>" (tile 2048, 512 or 256 particles per CTA) or
+    None (automatic).  Returns a dict of NumPy arrays.
     """
     torch = _ffi.require_cuda()
     if J < 1:
@@ -100,7 +102,12 @@ def run_pfilter(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J:
     d = _ffi.PfilterDesc()
     d.model = spec.ffi_model()
     d.J, d.F, d.T, d.U = J, F, T, U
+    tile = 0
+    if isinstance(path, str) and "@" in path:     # "stream@512": stream path with a fixed tile
+        path, tile = path.split("@")
+        tile = int(tile)
     d.path = _ffi.env_path() if path is None else _ffi.PATHS[path] if isinstance(path, str) else int(path)
+    d.tile = tile
     d.flags = flags
     d.thresh = float(max(0.0, thresh))
     d.theta, d.ys, d.ycon = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(ycon_d)
@@ -119,6 +126,38 @@ def run_pfilter(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J:
     if return_torch:
         return out
     return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+def autotune(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J: int, *, unit_f=None,
+             thresh: float = 0.0) -> int:
+    """Time the stream path's tile sizes for this shape (``ppf_autotune``) and
+    keep the fastest for later calls of the same shape; returns the tile (0 if
+    the shape runs on the resident path)."""
+    import ctypes
+
+    torch = _ffi.require_cuda()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    theta_f = np.ascontiguousarray(theta_f, dtype=np.float32)
+    F = theta_f.shape[0]
+    ys_d, ycon_d, Tu_d, U, T = _device_inputs(torch, struct, dev)
+    th_d = torch.from_numpy(theta_f).to(dev)
+    seeds_d = torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).copy()).to(dev)
+    unit_d = None if unit_f is None else torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
+    ll = torch.zeros(F, dtype=torch.float64, device=dev)
+    d = _ffi.PfilterDesc()
+    d.model = struct.spec.ffi_model()
+    d.J, d.F, d.T, d.U = J, F, T, U
+    d.path = _ffi.env_path()
+    d.thresh = float(max(0.0, thresh))
+    d.theta, d.ys, d.ycon = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(ycon_d)
+    d.unit, d.T_u, d.seeds, d.loglik = _ffi.ptr(unit_d), _ffi.ptr(Tu_d), _ffi.ptr(seeds_d), _ffi.ptr(ll)
+    ws = torch.empty(max(int(_ffi.LIB.ppf_pfilter_workspace_bytes(d)), 256), dtype=torch.uint8, device=dev)
+    d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
+    best = ctypes.c_int(0)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    _ffi.check(_ffi.LIB.ppf_autotune(d, stream, ctypes.byref(best)), "ppf_autotune")
+    _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_autotune")
+    return int(best.value)
 
 
 def pfilter(struct: PompStruct, thetas_array, J: int, keys, thresh: float = 0.0,

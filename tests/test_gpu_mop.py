@@ -121,3 +121,24 @@ def test_mop_gradient_independent_of_checkpoint_spacing():
         # accumulation of the gradient sums may change the last bits
         np.testing.assert_allclose(got["grad"], ref["grad"], rtol=1e-12, atol=1e-12, err_msg=str(ck))
         assert np.array_equal(got["value"], ref["value"])
+
+
+def test_mop_gradient_finite_for_chaotic_ricker_with_zero_counts():
+    """Chaotic Ricker series have runs of zero counts and particles whose
+    predicted count all but vanishes; their weights underflow, and the adjoint
+    must form y / N' products without overflowing (no 0 * inf or inf - inf).
+    The series are kept to 120 steps: along a chaotic lineage the pathwise
+    state derivative grows by the map's Lyapunov factor every step and leaves
+    float32 range after a few hundred steps, whatever the arithmetic order."""
+    import math
+
+    import pypomp_b200 as pp
+
+    F = _F()
+    for i, logr in enumerate((3.75, 3.87, 4.12)):
+        m = pp.Ricker(T=120, r=math.exp(logr), key=1000 + i)
+        st = m.to_struct()
+        assert np.any(st.ys == 0)
+        th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(f32)
+        got = F.run_mop(st, th, np.array([i], np.uint64), 8192, 0.97, grad=True)
+        assert np.all(np.isfinite(got["value"])) and np.all(np.isfinite(got["grad"])), (logr, got["grad"])

@@ -6,7 +6,7 @@ and Philox modes; log-likelihoods agree to float64 rounding of log().  The
 reference's own locked fixtures are reproduced by feeding the reference's
 draws through the injection mode.  Edge cases: J=1, T=1, partial tiles,
 thresh > 1 (steps without resampling), ragged panels, collapsed weights,
-non-finite parameters.
+non-finite parameters; the stream path with each of its tile sizes.
 """
 
 import numpy as np
@@ -16,7 +16,7 @@ from oracle import cora, kalman
 
 pytestmark = pytest.mark.gpu
 
-PATHS = ["plain", "stream", "resident"]
+PATHS = ["plain", "stream", "stream@2048", "stream@512", "stream@256", "resident"]
 f32 = np.float32
 
 
@@ -209,3 +209,18 @@ def test_j_validation():
         F.run_pfilter(m.to_struct(), th, np.array([1], np.uint64), 0)
     with pytest.raises(ValueError):
         F.run_pfilter(m.to_struct(), th, np.array([1], np.uint64), (1 << 21) + 1)
+
+
+def test_autotune_picks_a_tile_and_keeps_results():
+    F = _F()
+    m = _models()["SV"]
+    st = m.to_struct()
+    th = _thetas(m, 2)
+    seeds = np.array([5, 6], np.uint64)
+    J = 40000
+    best = F.autotune(st, th, seeds, J)
+    assert best in (2048, 512, 256)
+    auto = F.run_pfilter(st, th, seeds, J, path="stream", save_ancestors=True)
+    fixed = F.run_pfilter(st, th, seeds, J, path=f"stream@{best}", save_ancestors=True)
+    assert np.array_equal(auto["anc"], fixed["anc"])
+    assert np.array_equal(auto["loglik"], fixed["loglik"])
