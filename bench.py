@@ -188,6 +188,7 @@ def run_ours(args):
     d.model = m.spec.ffi_model()
     d.J, d.F, d.T, d.U = J, NSEED, T, 1
     d.path = _ffi.PATH_STREAM
+    d.tile = args.tile
     d.theta, d.ys, d.seeds, d.loglik = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(seeds_d), _ffi.ptr(ll_d)
     ws = torch.empty(_ffi.LIB.ppf_pfilter_workspace_bytes(d), dtype=torch.uint8, device=dev)
     d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
@@ -560,6 +561,7 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="run one small call of the same kernels (for ncu) and exit")
     ap.add_argument("--path", default="stream")
+    ap.add_argument("--tile", type=int, default=0, help="stream-path tile (0 = automatic)")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default) is the headline line; c1/c3/c4 print their own lines")
     args = ap.parse_args()

@@ -55,6 +55,37 @@ __device__ __forceinline__ void group_noise(const Args& a, int f, int s, int k0,
   }
 }
 
+// Children per Philox group: a run of consecutive particles whose normals fill
+// whole Philox blocks (G * NZ a multiple of 4), so every word is used.  Four
+// children (two or more independent Philox chains for NZ >= 2) measured faster
+// than the smallest group for the 2-D LG batch, the chains overlapping, and
+// pairs of 4-D LG children spilled more than groups of four.
+template <int NZ>
+struct ChildGroup {
+  static constexpr int G = 4;
+  static_assert((G * NZ) % 4 == 0 || NZ == 0, "a group must fill whole Philox blocks");
+};
+
+// Normals of the G consecutive particles k0..k0+G-1 (k0 % G == 0) at step s,
+// N per particle: z[e*N + r].  Philox calls (k0 N)/4 ... cover them exactly.
+template <int G, int N, bool INJ>
+__device__ __forceinline__ void group_noise_g(const Args& a, int f, int s, int k0, float* z) {
+  if (N == 0) return;
+  if (INJ) {
+    const float* src = (s == 0) ? a.inj_z0 + (size_t)f * a.J * N
+                                : a.inj_z + (((size_t)f * a.T + (s - 1)) * a.J) * N;
+#pragma unroll
+    for (int e = 0; e < G; ++e)
+#pragma unroll
+      for (int r = 0; r < N; ++r) z[e * N + r] = (k0 + e < a.J) ? src[(size_t)(k0 + e) * N + r] : 0.0f;
+  } else {
+    const uint64_t seed = a.seeds[f];
+    const uint32_t c0 = (uint32_t)k0 * N / 4;
+#pragma unroll
+    for (int c = 0; c < G * N / 4; ++c) pp_normal4(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
+  }
+}
+
 __device__ __forceinline__ uint32_t resample_u32(const Args& a, int f, int t) {
   if (a.flags & PPF_F_INJECT) return pp_u32_from_float(a.inj_u[(size_t)f * a.T + t]);
   return pp_resample_u32(a.seeds[f], (uint32_t)(t + 1));
@@ -294,6 +325,35 @@ __device__ __forceinline__ void store_group(float* Xn, float* Wn, float* logw, i
   }
 }
 
+
+// Store the G children k0..k0+G-1 (valid in [lo, hi)): one vector store per
+// row when the whole group is valid and the rows are aligned to G floats.
+template <int G, int DX>
+__device__ __forceinline__ void store_group_g(float* Xn, float* Wn, float* logw, int J, int k0,
+                                              const float (&xo)[G][DX], const float (&wo)[G], int lo, int hi) {
+  if (G == 4) {
+    store_group<DX>(Xn, Wn, logw, J, k0, reinterpret_cast<const float(&)[4][DX]>(xo),
+                    reinterpret_cast<const float(&)[4]>(wo), lo, hi);
+    return;
+  }
+  const bool full = (lo == 0) & (hi == G) & ((J & (G - 1)) == 0);
+  if (G == 2 && full) {
+#pragma unroll
+    for (int d = 0; d < DX; ++d)
+      *reinterpret_cast<float2*>(Xn + d * J + k0) = make_float2(xo[0][d], xo[G > 1 ? 1 : 0][d]);
+    *reinterpret_cast<float2*>(Wn + k0) = make_float2(wo[0], wo[G > 1 ? 1 : 0]);
+    if (logw) *reinterpret_cast<float2*>(logw + k0) = make_float2(wo[0], wo[G > 1 ? 1 : 0]);
+    return;
+  }
+#pragma unroll
+  for (int e = 0; e < G; ++e) {
+    if (e < lo || e >= hi) continue;
+#pragma unroll
+    for (int d = 0; d < DX; ++d) Xn[d * J + k0 + e] = xo[e][d];
+    Wn[k0 + e] = wo[e];
+    if (logw) logw[k0 + e] = wo[e];
+  }
+}
 
 // Fixed-point sums of the weights of one tile, then the decoupled-lookback
 // prefix over the tiles of the filter (Merrill & Garland 2016).

@@ -109,12 +109,21 @@ __global__ void __launch_bounds__(TPB) k_init(Args a) {
 //   2. closed-form first-child offset st[l] = nchild(C_{l-1}) per parent into
 //      shared memory (st[l] = l on steps without resampling), parent states
 //      staged in shared memory;
-//   3. merge-path partition of the tile's children [st[0], st[n]) into equal
-//      runs of RUN children per thread: one binary search for the run's first
-//      parent, then a linear walk; per group of 4 children one set of Philox
-//      calls (every word used), rproc + dmeas, float4 stores.
+//   3. merge-path partition of the tile's children [st[0], st[n]) into TPB
+//      near-equal chunks of whole groups: one binary search for a chunk's
+//      first parent, then a linear walk; per group of 4 children one set of
+//      Philox calls (every word used), rproc + dmeas, float4 stores.
+// CTAs per SM the register budget is sized for (256-thread CTAs): 4 (64
+// registers) for one-variable states and for 2-D states with two normals per
+// child (measured on the 2-D LG batch: 4 CTAs per SM beat 3 by 7 %), else 3
+// (80 registers; the SV kernel spills at 64).
+template <class M>
+struct RespropOccupancy {
+  static constexpr int B = (M::MAXDX == 1 || (M::MAXDX == 2 && M::NZ == 2)) ? 4 : 3;
+};
+
 template <class M, int TPB, int IT, bool INJ>
-__global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4) * (256 / TPB)) k_resprop(Args a, int t) {
+__global__ void __launch_bounds__(TPB, RespropOccupancy<M>::B * (256 / TPB)) k_resprop(Args a, int t) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
   constexpr int RUN = IT;            // children per thread run: TPB runs cover a full tile
@@ -265,23 +274,30 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4) * (256 / TPB)) k_
   if (a.mop_ckpt && (t + 1) % a.ckpt_every == 0 && (t + 1) / a.ckpt_every < a.nseg)
     ckpt = a.mop_ckpt + ((size_t)f * a.nseg + (t + 1) / a.ckpt_every) * DX * J;
 
-  // 3. children, in runs of RUN per thread
+  // 3. children, drawn in Philox groups of G: the tile's groups are split into
+  //    TPB contiguous, near-equal chunks (a tile's child count fluctuates around
+  //    TILE; fixed-size runs left a second run to a few threads whenever it
+  //    exceeded TILE, and the whole CTA waited for them)
+  constexpr int G = ChildGroup<M::NZ>::G;
+  static_assert((RUN % G) == 0 && (4 % G) == 0, "groups align with the 4-aligned start");
   const int kA = klo & ~3;
-  const int nrun = (khi - kA + RUN - 1) / RUN;
-  for (int r = threadIdx.x; r < nrun; r += TPB) {
-    const int ka = kA + r * RUN;
+  const int ngr = (khi - kA + G - 1) / G;
+  const int g0 = (int)(((long long)threadIdx.x * ngr) / TPB);
+  const int g1 = (int)(((long long)(threadIdx.x + 1) * ngr) / TPB);
+  if (g0 < g1) {
+    const int ka = kA + G * g0;
     int l = find_parent(st, ntile, max(ka, klo));
-#pragma unroll
-    for (int g = 0; g < RUN / 4; ++g) {
-      const int k0 = ka + 4 * g;
+#pragma unroll 1
+    for (int g = 0; g < g1 - g0; ++g) {
+      const int k0 = ka + G * g;
       if (k0 >= khi) break;
-      const int lo = max(0, klo - k0), hi = min(4, khi - k0);   // valid e in [lo, hi)
-      float z[4 * M::NZ];
-      if (!last) group_noise<M::NZ, INJ>(a, f, t + 2, k0, z);
-      float xo[4][DX];
-      float wo[4];
+      const int lo = max(0, klo - k0), hi = min(G, khi - k0);   // valid e in [lo, hi)
+      float z[G * M::NZ];
+      if (!last) group_noise_g<G, M::NZ, INJ>(a, f, t + 2, k0, z);
+      float xo[G][DX];
+      float wo[G];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
+      for (int e = 0; e < G; ++e) {
         const int k = k0 + e;
         const bool valid = (e >= lo) & (e < hi);
         if (valid) {
@@ -309,7 +325,7 @@ __global__ void __launch_bounds__(TPB, (M::MAXDX >= 2 ? 3 : 4) * (256 / TPB)) k_
             for (int d = 0; d < DX; ++d) px[d] += (double)x[d];
         }
       }
-      if (!last) store_group<DX>(Xn, Wn, logw, J, k0, xo, wo, lo, hi);
+      if (!last) store_group_g<G, DX>(Xn, Wn, logw, J, k0, xo, wo, lo, hi);
     }
   }
   if (last) return;
