@@ -298,10 +298,10 @@ int run_if2(Args& a, cudaStream_t s) {
   switch (a.model.kind) {
     case PPF_MODEL_LG:
       switch (a.model.dx) {
-        case 1: return run_if2_m<LG<1>>(a, s);
-        case 2: return run_if2_m<LG<2>>(a, s);
-        case 3: return run_if2_m<LG<3>>(a, s);
-        case 4: return run_if2_m<LG<4>>(a, s);
+        case 1: return a.model.dy == 1 ? run_if2_m<LG<1, 1>>(a, s) : run_if2_m<LG<1>>(a, s);
+        case 2: return a.model.dy == 2 ? run_if2_m<LG<2, 2>>(a, s) : run_if2_m<LG<2>>(a, s);
+        case 3: return a.model.dy == 3 ? run_if2_m<LG<3, 3>>(a, s) : run_if2_m<LG<3>>(a, s);
+        case 4: return a.model.dy == 4 ? run_if2_m<LG<4, 4>>(a, s) : run_if2_m<LG<4>>(a, s);
         default: return PPF_EUNSUPPORTED;
       }
     case PPF_MODEL_SV: return run_if2_m<SV>(a, s);

@@ -24,21 +24,26 @@ namespace ppf {
 // A (row-major dx*dx), C (row-major dy*dx), lower triangle of chol(Q)
 // row-major, lower triangle of chol(R) row-major, X0 (dx).
 // ---------------------------------------------------------------------------
-template <int DX>
+// DYS > 0 fixes the observation dimension at compile time (the dispatch uses
+// it for dy == dx): the measurement loops become static and the model
+// constants stay in registers.  DYS == 0 reads dy (<= 4) at run time.
+template <int DX, int DYS = 0>
 struct LG {
   static constexpr int kind = PPF_MODEL_LG;
   static constexpr int MAXDX = DX;     // state dimension, fixed per instantiation
   static constexpr int NZ = DX;        // process normals per particle-step
   static constexpr int NZ0 = DX;       // initial-state normals per particle
-  static constexpr int MAXDY = 4;
-  static constexpr int MAXP = DX * DX + 4 * DX + DX * (DX + 1) / 2 + 10 + DX;  // dy <= 4
+  static constexpr int MAXDY = DYS > 0 ? DYS : 4;
+  static constexpr int MAXP = DYS > 0 ? DX * DX + DYS * DX + DX * (DX + 1) / 2 + DYS * (DYS + 1) / 2 + DX
+                                      : DX * DX + 4 * DX + DX * (DX + 1) / 2 + 10 + DX;  // dy <= 4
   struct Consts {
     int dx, dy;
     float A[16], C[16], LQ[16], L[16], Linv[4], X0[4];
     float c0;
   };
+  __device__ static __forceinline__ int ndy(const Consts& c) { return DYS > 0 ? DYS : c.dy; }
   __device__ static void prepare(Consts& c, const float* th, const ppf_model& m, bool est) {
-    const int dx = DX, dy = m.dy;
+    const int dx = DX, dy = DYS > 0 ? DYS : m.dy;   // DYS, when set, equals m.dy (the dispatch checks)
     c.dx = dx; c.dy = dy;
     int p = 0;
     for (int i = 0; i < dx; ++i)
@@ -113,7 +118,7 @@ struct LG {
     float q = 0.0f;
 #pragma unroll
     for (int i = 0; i < MAXDY; ++i) {
-      if (i < c.dy) {
+      if (i < ndy(c)) {
         float a = 0.0f;
 #pragma unroll
         for (int k = 0; k < DX; ++k) a = pp_fma(c.C[i * 4 + k], x[k], a);
@@ -146,7 +151,7 @@ struct LG {
 #pragma unroll
     for (int i = 0; i < MAXDY; ++i) {
       k.s[i] = 0.0f;
-      if (i < c.dy) {
+      if (i < ndy(c)) {
         float a = 0.0f;
 #pragma unroll
         for (int kk = 0; kk < DX; ++kk) a = pp_fma(c.C[i * 4 + kk], k.xP[kk], a);
@@ -167,11 +172,11 @@ struct LG {
 #pragma unroll
     for (int i = MAXDY - 1; i >= 0; --i) {
       v[i] = 0.0f;
-      if (i < c.dy) {
+      if (i < ndy(c)) {
         float r = k.s[i];
 #pragma unroll
         for (int l = i + 1; l < MAXDY; ++l)
-          if (l < c.dy) r = r - c.L[l * 4 + i] * v[l];
+          if (l < ndy(c)) r = r - c.L[l * 4 + i] * v[l];
         v[i] = r * c.Linv[i];
       }
     }
@@ -181,12 +186,12 @@ struct LG {
       float a = lx[kk];
 #pragma unroll
       for (int i = 0; i < MAXDY; ++i)
-        if (i < c.dy) a = a + lm * c.C[i * 4 + kk] * v[i];
+        if (i < ndy(c)) a = a + lm * c.C[i * 4 + kk] * v[i];
       lxP[kk] = a;
     }
 #pragma unroll
     for (int i = 0; i < MAXDY; ++i)
-      if (i < c.dy) {
+      if (i < ndy(c)) {
 #pragma unroll
         for (int kk = 0; kk < DX; ++kk) g[GC + i * DX + kk] += lm * v[i] * k.xP[kk];
 #pragma unroll

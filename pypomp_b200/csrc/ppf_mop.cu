@@ -187,30 +187,30 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_init(Args a, MopBwd mb) {
 template <class M>
 struct Chain;
 
-template <int DX>
-struct Chain<LG<DX>> {
+template <int DX, int DYS>
+struct Chain<LG<DX, DYS>> {
   __device__ static double map(const ppf_model& m, const float* th, const double* gn, int p, bool est) {
     const int dy = m.dy;
     const int nA = DX * DX, nC = dy * DX, nQ = DX * (DX + 1) / 2, nR = dy * (dy + 1) / 2;
-    if (p < nA) return gn[LG<DX>::GA + p];
+    if (p < nA) return gn[LG<DX, DYS>::GA + p];
     p -= nA;
-    if (p < nC) return gn[LG<DX>::GC + p];
+    if (p < nC) return gn[LG<DX, DYS>::GC + p];
     p -= nC;
     if (p < nQ) {
-      double v = gn[LG<DX>::GQ + p];
+      double v = gn[LG<DX, DYS>::GQ + p];
       for (int i = 0; i < DX; ++i)
         if (est && p == i * (i + 1) / 2 + i) v *= (double)pp_expf(th[nA + nC + p]);
       return v;
     }
     p -= nQ;
     if (p < nR) {
-      double v = gn[LG<DX>::GR + p];
+      double v = gn[LG<DX, DYS>::GR + p];
       for (int i = 0; i < dy; ++i)
         if (est && p == i * (i + 1) / 2 + i) v *= (double)pp_expf(th[nA + nC + nQ + p]);
       return v;
     }
     p -= nR;
-    return gn[LG<DX>::GX0 + p];
+    return gn[LG<DX, DYS>::GX0 + p];
   }
 };
 template <>
@@ -303,10 +303,10 @@ int run_mop(Args& a, const MopWork& w, cudaStream_t s) {
   switch (a.model.kind) {
     case PPF_MODEL_LG:
       switch (a.model.dx) {
-        case 1: return run_mop_model<LG<1>>(a, w, s);
-        case 2: return run_mop_model<LG<2>>(a, w, s);
-        case 3: return run_mop_model<LG<3>>(a, w, s);
-        case 4: return run_mop_model<LG<4>>(a, w, s);
+        case 1: return a.model.dy == 1 ? run_mop_model<LG<1, 1>>(a, w, s) : run_mop_model<LG<1>>(a, w, s);
+        case 2: return a.model.dy == 2 ? run_mop_model<LG<2, 2>>(a, w, s) : run_mop_model<LG<2>>(a, w, s);
+        case 3: return a.model.dy == 3 ? run_mop_model<LG<3, 3>>(a, w, s) : run_mop_model<LG<3>>(a, w, s);
+        case 4: return a.model.dy == 4 ? run_mop_model<LG<4, 4>>(a, w, s) : run_mop_model<LG<4>>(a, w, s);
         default: return PPF_EUNSUPPORTED;
       }
     case PPF_MODEL_SV: return run_mop_model<SV>(a, w, s);
@@ -324,10 +324,10 @@ int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s) {
   switch (a.model.kind) {
     case PPF_MODEL_LG:
       switch (a.model.dx) {
-        case 1: return run_mop_backward_model<LG<1>>(a, w, s);
-        case 2: return run_mop_backward_model<LG<2>>(a, w, s);
-        case 3: return run_mop_backward_model<LG<3>>(a, w, s);
-        case 4: return run_mop_backward_model<LG<4>>(a, w, s);
+        case 1: return a.model.dy == 1 ? run_mop_backward_model<LG<1, 1>>(a, w, s) : run_mop_backward_model<LG<1>>(a, w, s);
+        case 2: return a.model.dy == 2 ? run_mop_backward_model<LG<2, 2>>(a, w, s) : run_mop_backward_model<LG<2>>(a, w, s);
+        case 3: return a.model.dy == 3 ? run_mop_backward_model<LG<3, 3>>(a, w, s) : run_mop_backward_model<LG<3>>(a, w, s);
+        case 4: return a.model.dy == 4 ? run_mop_backward_model<LG<4, 4>>(a, w, s) : run_mop_backward_model<LG<4>>(a, w, s);
         default: return PPF_EUNSUPPORTED;
       }
     case PPF_MODEL_SV: return run_mop_backward_model<SV>(a, w, s);

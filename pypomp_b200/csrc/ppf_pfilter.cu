@@ -834,10 +834,10 @@ int run_pfilter_path(Args& a, int path, cudaStream_t s) {
   switch (a.model.kind) {
     case PPF_MODEL_LG:
       switch (a.model.dx) {
-        case 1: return dispatch_model<LG<1>>(a, path, s);
-        case 2: return dispatch_model<LG<2>>(a, path, s);
-        case 3: return dispatch_model<LG<3>>(a, path, s);
-        case 4: return dispatch_model<LG<4>>(a, path, s);
+        case 1: return a.model.dy == 1 ? dispatch_model<LG<1, 1>>(a, path, s) : dispatch_model<LG<1>>(a, path, s);
+        case 2: return a.model.dy == 2 ? dispatch_model<LG<2, 2>>(a, path, s) : dispatch_model<LG<2>>(a, path, s);
+        case 3: return a.model.dy == 3 ? dispatch_model<LG<3, 3>>(a, path, s) : dispatch_model<LG<3>>(a, path, s);
+        case 4: return a.model.dy == 4 ? dispatch_model<LG<4, 4>>(a, path, s) : dispatch_model<LG<4>>(a, path, s);
         default: return PPF_EUNSUPPORTED;
       }
     case PPF_MODEL_SV: return dispatch_model<SV>(a, path, s);
