@@ -92,6 +92,28 @@ PPF_HD float pp_expf(float x) {
   return (x != x) ? x : y;
 }
 
+/* pp_expf restricted to the weight quantiser's range: for x in [-32, 0] it
+ * returns exactly pp_expf(x) (there k = rint(x / ln2) lies in [-47, 0], so the
+ * two half-scalings of pp_expf are one exact scaling by 2^k), and 0 below
+ * -32, where pp_expf(x) < 2^-46 and rint(e 2^40) is 0 either way.  NaN and
+ * +inf inputs are the caller's to handle. */
+PPF_HD float pp_expq(float x) {
+  const float k = pp_rint(x * 1.44269502162933349609375f);
+  float r = pp_fma(-k, 0.693145751953125f, x);
+  r = pp_fma(-k, 1.428606765330187045e-06f, r);
+  float p = 1.98412698412698413e-04f;
+  p = pp_fma(p, r, 1.38888888888888889e-03f);
+  p = pp_fma(p, r, 8.33333333333333333e-03f);
+  p = pp_fma(p, r, 4.16666666666666667e-02f);
+  p = pp_fma(p, r, 1.66666666666666667e-01f);
+  p = pp_fma(p, r, 0.5f);
+  p = pp_fma(p, r, 1.0f);
+  p = pp_fma(p, r, 1.0f);
+  const int ki = (int)k;
+  const float y = p * pp_pow2i(ki < -126 ? -126 : ki);
+  return (x < -32.0f) ? 0.0f : y;
+}
+
 /* log(1+f) for f in [sqrt(1/2)-1, sqrt(2)-1] as f - f^2/2 + f^3 R(f), R a
  * degree-8 polynomial fitted by least squares on Chebyshev nodes of the
  * interval (float64 fit, coefficients rounded to float32); < 0.75 ulp. */

@@ -621,6 +621,7 @@ int ppfo_perfilter(const ppf_perfilter_desc* d, int nthreads) {
 
 /* Elementary functions and Philox, exported for the tests that pin them. */
 float ppfo_expf(float x) { return pp_expf(x); }
+float ppfo_expq(float x) { return pp_expq(x); }
 float ppfo_logf(float x) { return pp_logf(x); }
 void ppfo_sincos2pif(float u, float* s, float* c) { pp_sincos2pif(u, s, c); }
 void ppfo_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {

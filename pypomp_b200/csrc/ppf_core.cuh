@@ -89,7 +89,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 __device__ __forceinline__ uint64_t qweight(float w, float M, bool collapsed) {
   if (collapsed) return 1ull;
   if (w != w) return 0ull;
-  const float e = pp_expf(w - M);
+  const float e = pp_expq(w - M);     // equals pp_expf(w - M) wherever the quantised value can be >= 1
   return __float2ull_rn(e * kQScale);
 }
 

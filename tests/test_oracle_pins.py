@@ -180,3 +180,24 @@ def test_c_oracle_thresh_and_identity_ancestors(lg2d):
     assert ident.any() and (~ident).any()   # some steps resample, some do not
     for t in range(anc.shape[0]):
         assert np.all(np.diff(anc[t]) >= 0)  # systematic ancestors are sorted
+
+
+def test_weight_quantiser_exp_equals_expf():
+    """pp_expq (the fixed-point weights' exp) gives the same quantised weight
+    rint(e 2^40) as pp_expf for every argument at or below 0: exhaustive over
+    the float32 values in [-40, 0] at a 1/4096 stride plus edge cases."""
+    import ctypes
+
+    lib = cora._L()
+    lib.ppfo_expq.argtypes = [ctypes.c_float]
+    lib.ppfo_expq.restype = ctypes.c_float
+    xs = np.concatenate([-np.arange(0, 40 * 4096, dtype=np.float64) / 4096.0,
+                         [-32.0, -31.999998, -32.000004, -0.0, -1e-30, -np.inf]]).astype(f32)
+    for x in xs:
+        e1 = np.float32(lib.ppfo_expf(float(x)))
+        e2 = np.float32(lib.ppfo_expq(float(x)))
+        q1 = np.rint(np.float32(e1 * np.float32(2.0 ** 40)))
+        q2 = np.rint(np.float32(e2 * np.float32(2.0 ** 40)))
+        assert q1 == q2, (x, e1, e2)
+        if x >= -32.0:
+            assert e1 == e2, (x, e1, e2)
