@@ -50,6 +50,10 @@ LG_R = np.array([[1.0, 0.1], [0.1, 1.0]]) / 10
 # read parent log-weight 4 + parent state 8, write child state 8 + log-weight 4
 RESPROP_BYTES = 24
 SUM_BYTES = 4
+# DRAM traffic of one k_resprop launch per particle, from an ncu capture of a
+# 24-seed case (dram__bytes_read.sum + dram__bytes_write.sum = 114.8 MB for
+# 6.29 M particles); traffic is proportional to the particles processed
+RESPROP_TRAFFIC_PER_PARTICLE = 18.25
 
 
 def workload():
@@ -308,7 +312,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "api": "pypomp_b200.functional.pfilter"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": RESPROP_TRAFFIC_PER_PARTICLE * J * NSEED,
                          "kernel": "k_resprop (resample + propagate)",
                          "algorithmic_bytes_per_particle": RESPROP_BYTES,
                          "avg_launch_ms": rp_avg, "peak_source": peak_kind,
