@@ -56,6 +56,27 @@ SUM_BYTES = 4
 RESPROP_TRAFFIC_PER_PARTICLE = 18.25
 
 
+def rank_seeds(rank: int) -> np.ndarray:
+    """Each rank filters its own 64 seeds (weak scaling, disjoint streams)."""
+    return np.arange(NSEED, dtype=np.uint64) + np.uint64(1000 * rank)
+
+
+def max_over_ranks(x: float, dev) -> float:
+    """The slowest rank's value (device time is reported as the max over ranks)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank_step: float, world: int, steps: int, ms_max: float) -> float:
+    """Units all ranks processed per second of the slowest rank's device time."""
+    return units_per_rank_step * world * steps / (ms_max / 1e3)
+
+
 def workload():
     import pypomp_b200 as pp
 
@@ -181,7 +202,7 @@ def run_ours(args):
     m = workload()
     st = m.to_struct()
     th = np.repeat(m.theta.to_array(m.canonical_param_names), NSEED, axis=0).astype(np.float32)
-    seeds = (np.arange(NSEED, dtype=np.uint64) + np.uint64(1000 * rank))
+    seeds = rank_seeds(rank)
 
     # ---- device-resident inputs, one descriptor, C-ABI calls -------------
     ys_d = torch.from_numpy(np.ascontiguousarray(st.ys)).to(dev)
@@ -221,12 +242,9 @@ def run_ours(args):
         torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, dev)
     units_per_step = NSEED * J * T * world
-    value = units_per_step * args.steps / (ms_max / 1e3)
+    value = whole_job_rate(NSEED * J * T, world, args.steps, ms_max)
     loglik = ll_d.cpu().numpy()
     launches_per_step = 1 + 2 * T
 
@@ -255,10 +273,7 @@ def run_ours(args):
         out = F.pfilter(struct, thetas_host, J, keys_host)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = units_per_step * e2e_steps / float(e2e_t.item())
+    e2e_value = units_per_step * e2e_steps / max_over_ranks(e2e_s, dev)
     assert np.allclose(out["logLik"].ravel(), loglik, rtol=1e-12, equal_nan=True)
     h2d = struct.ys.nbytes + thetas_host.nbytes + keys_host.nbytes
     d2h = NSEED * 8
