@@ -214,6 +214,7 @@ def run_ours(args):
     d.J, d.F, d.T, d.U = J, NSEED, T, 1
     d.path = _ffi.PATH_STREAM
     d.tile = args.tile
+    d.flags = _ffi.F_GRAPH if args.graph else 0
     d.theta, d.ys, d.seeds, d.loglik = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(seeds_d), _ffi.ptr(ll_d)
     ws = torch.empty(_ffi.LIB.ppf_pfilter_workspace_bytes(d), dtype=torch.uint8, device=dev)
     d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
@@ -323,6 +324,7 @@ def run_ours(args):
             "config": {"workload": "LG 2-D pfilter, T=1000, J=262144, 64 seeds per GPU (configs[1])",
                        "model": "LG", "global_batch": NSEED * world, "seq_len": T, "particles": J,
                        "parallelism": f"replicas{world}", "path": "stream",
+                       "cuda_graph": bool(args.graph),
                        "l2": "inputs larger than L2 (state 2x64x262144x12 B = 403 MB per step)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "api": "pypomp_b200.functional.pfilter"},
@@ -414,6 +416,8 @@ def run_c3(args):
     st = m.to_struct()
     th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(np.float32)
     call = MopCall(st, th, np.array([1], np.uint64), Jm, 0.97)
+    if args.graph:
+        call.d.flags |= _ffi.F_GRAPH
     stream = torch.cuda.current_stream()
     ms, clk = _timed(lambda: call.forward(grad=True), args.steps, args.warmup, stream)
     torch.cuda.synchronize()
@@ -581,6 +585,8 @@ def main():
                     help="run one small call of the same kernels (for ncu) and exit")
     ap.add_argument("--path", default="stream")
     ap.add_argument("--tile", type=int, default=0, help="stream-path tile (0 = automatic)")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="launch the step loop directly instead of replaying it as a CUDA graph")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default) is the headline line; c1/c3/c4 print their own lines")
     args = ap.parse_args()

@@ -74,6 +74,14 @@ typedef struct ppf_model {
  * parameter transform, pypomp's ParTrans(); the default for these two entry
  * points is the estimation scale) */
 #define PPF_F_NATURAL (1u << 8)
+/* ppf_pfilter (stream and resident paths), ppf_mop, ppf_perfilter: capture
+ * the call's launch sequence into a CUDA graph on first use and replay the
+ * graph on later calls whose descriptor is byte-identical (same buffers, same
+ * shapes, same flags).  The caller keeps those buffers alive and unchanged in
+ * layout while it reuses the descriptor; a call made while the stream is
+ * already being captured launches directly into that capture.  Host-side
+ * cache of 16 graphs per process, not thread-safe. */
+#define PPF_F_GRAPH (1u << 9)
 
 /* Execution paths; all produce bit-identical results. */
 enum {

@@ -30,6 +30,7 @@ F_SAVE_ANC = 1 << 5
 F_SAVE_W = 1 << 6
 F_EST = 1 << 7
 F_NATURAL = 1 << 8
+F_GRAPH = 1 << 9
 
 PATH_AUTO, PATH_PLAIN, PATH_STREAM, PATH_RESIDENT = 0, 1, 2, 3
 PATHS = {"auto": PATH_AUTO, "plain": PATH_PLAIN, "stream": PATH_STREAM, "resident": PATH_RESIDENT}

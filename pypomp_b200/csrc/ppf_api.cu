@@ -280,6 +280,70 @@ static void fill_if2(const ppf_perfilter_desc* d, Args& a) {
   a.inj_zp0 = d->inj_zp0; a.inj_zp = d->inj_zp;
 }
 
+// ---------------------------------------------------------------------------
+// CUDA graphs (PPF_F_GRAPH): the launch sequence of a call is captured once
+// and replayed for byte-identical descriptors.
+// ---------------------------------------------------------------------------
+constexpr int kGraphCap = 16;
+constexpr size_t kGraphKeyMax = 512;
+struct GraphEntry {
+  unsigned char key[kGraphKeyMax];
+  size_t klen;
+  int dev;
+  cudaGraphExec_t exec;
+};
+static GraphEntry g_graphs[kGraphCap];
+static int g_graph_n = 0, g_graph_next = 0;
+
+template <class Fn>
+static int run_graphed(const void* key, size_t klen, cudaStream_t s, Fn&& launch) {
+  if (klen > kGraphKeyMax || g_prof.enabled) return launch(s);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return PPF_ECUDA;
+  if (cs != cudaStreamCaptureStatusNone) return launch(s);   // the caller is capturing
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PPF_ECUDA;
+  for (int i = 0; i < g_graph_n; ++i) {
+    GraphEntry& e = g_graphs[i];
+    if (e.dev == dev && e.klen == klen && memcmp(e.key, key, klen) == 0)
+      return cudaGraphLaunch(e.exec, s) == cudaSuccess ? PPF_OK : PPF_ECUDA;
+  }
+  // capture on a private stream (the caller's may be the legacy default
+  // stream, which cannot be captured); the graph is then launched on theirs
+  static cudaStream_t cap_stream[64] = {nullptr};
+  if (dev < 0 || dev >= 64) return launch(s);
+  if (!cap_stream[dev] && cudaStreamCreateWithFlags(&cap_stream[dev], cudaStreamNonBlocking) != cudaSuccess)
+    return PPF_ECUDA;
+  cudaStream_t cst = cap_stream[dev];
+  if (cudaStreamBeginCapture(cst, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return PPF_ECUDA;
+  const int rc = launch(cst);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(cst, &g);
+  if (rc != PPF_OK || ec != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return rc != PPF_OK ? rc : PPF_ECUDA;
+  }
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return PPF_ECUDA;
+  int idx;
+  if (g_graph_n < kGraphCap) {
+    idx = g_graph_n++;
+  } else {                                   // full: replace the oldest entry
+    idx = g_graph_next;
+    g_graph_next = (g_graph_next + 1) % kGraphCap;
+    cudaGraphExecDestroy(g_graphs[idx].exec);
+  }
+  GraphEntry& slot = g_graphs[idx];
+  memcpy(slot.key, key, klen);
+  slot.klen = klen;
+  slot.dev = dev;
+  slot.exec = ex;
+  return cudaGraphLaunch(ex, s) == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
 }  // namespace ppf
 
 using namespace ppf;
@@ -303,14 +367,17 @@ int ppf_pfilter(const ppf_pfilter_desc* d, void* stream) {
   const size_t need = carve(a, path, nullptr);
   if (!d->workspace || d->ws_bytes < need) return PPF_EINVAL;
   carve(a, path, reinterpret_cast<unsigned char*>(d->workspace));
-  if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, s) != cudaSuccess) return PPF_ECUDA;
-  if (path == PPF_PATH_STREAM) {
-    // accumulators start at (max=-, min=+, nan=0)
-    rc = reset_accumulators(a, s);
-    if (rc) return rc;
-  }
-  rc = run_pfilter_path(a, path, s);
-  return rc;
+  auto launch = [&](cudaStream_t st) -> int {
+    if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, st) != cudaSuccess) return PPF_ECUDA;
+    if (path == PPF_PATH_STREAM) {
+      // accumulators start at (max=-, min=+, nan=0)
+      const int r = reset_accumulators(a, st);
+      if (r) return r;
+    }
+    return run_pfilter_path(a, path, st);
+  };
+  if ((d->flags & PPF_F_GRAPH) && path != PPF_PATH_PLAIN) return run_graphed(d, sizeof(*d), s, launch);
+  return launch(s);
 }
 
 size_t ppf_mop_workspace_bytes(const ppf_mop_desc* d) {
@@ -347,13 +414,17 @@ int ppf_mop(const ppf_mop_desc* d, void* stream) {
   carve_mop(a, w, d, reinterpret_cast<unsigned char*>(d->workspace));
   w.grad = d->grad;
   w.alpha = d->alpha;
-  if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, s) != cudaSuccess) return PPF_ECUDA;
-  rc = reset_accumulators(a, s);
-  if (rc) return rc;
-  rc = run_mop(a, w, s);
-  if (rc) return rc;
-  k_negate<<<(d->F + 127) / 128, 128, 0, s>>>(d->value, d->F);
-  return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+  auto launch = [&](cudaStream_t st) -> int {
+    if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, st) != cudaSuccess) return PPF_ECUDA;
+    int r = reset_accumulators(a, st);
+    if (r) return r;
+    r = run_mop(a, w, st);
+    if (r) return r;
+    k_negate<<<(d->F + 127) / 128, 128, 0, st>>>(d->value, d->F);
+    return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+  };
+  if (d->flags & PPF_F_GRAPH) return run_graphed(d, sizeof(*d), s, launch);
+  return launch(s);
 }
 
 size_t ppf_perfilter_workspace_bytes(const ppf_perfilter_desc* d) {
@@ -373,10 +444,14 @@ int ppf_perfilter(const ppf_perfilter_desc* d, void* stream) {
   const size_t need = carve_if2(a, nullptr);
   if (!d->workspace || d->ws_bytes < need) return PPF_EINVAL;
   carve_if2(a, reinterpret_cast<unsigned char*>(d->workspace));
-  if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, s) != cudaSuccess) return PPF_ECUDA;
-  rc = reset_accumulators(a, s);
-  if (rc) return rc;
-  return run_if2(a, s);
+  auto launch = [&](cudaStream_t st) -> int {
+    if (cudaMemsetAsync(d->workspace, 0, a.ctrl_bytes, st) != cudaSuccess) return PPF_ECUDA;
+    const int r = reset_accumulators(a, st);
+    if (r) return r;
+    return run_if2(a, st);
+  };
+  if (d->flags & PPF_F_GRAPH) return run_graphed(d, sizeof(*d), s, launch);
+  return launch(s);
 }
 
 // grad[f][p] *= dvalue[f]

@@ -224,3 +224,41 @@ def test_autotune_picks_a_tile_and_keeps_results():
     fixed = F.run_pfilter(st, th, seeds, J, path=f"stream@{best}", save_ancestors=True)
     assert np.array_equal(auto["anc"], fixed["anc"])
     assert np.array_equal(auto["loglik"], fixed["loglik"])
+
+
+@pytest.mark.parametrize("path", ["stream", "resident"])
+def test_graph_replay_matches_direct_launches(path):
+    """PPF_F_GRAPH: the first call captures, later calls with the same
+    descriptor replay the graph; results equal direct launches bit for bit."""
+    import torch
+
+    from pypomp_b200 import _ffi
+
+    m = _models()["SV"]
+    st = m.to_struct()
+    th = _thetas(m, 2)
+    seeds = np.array([21, 22], np.uint64)
+    J = 3000 if path == "stream" else 1500
+    want = _F().run_pfilter(st, th, seeds, J, path=path, save_ancestors=True)
+    dev = torch.device("cuda", 0)
+    ys = torch.from_numpy(np.ascontiguousarray(st.ys[None], dtype=f32)).to(dev)
+    thd = torch.from_numpy(th).to(dev)
+    sd = torch.from_numpy(seeds.view(np.int64).copy()).to(dev)
+    ll = torch.zeros(2, dtype=torch.float64, device=dev)
+    anc = torch.zeros(2, st.ys.shape[0], J, dtype=torch.int32, device=dev)
+    d = _ffi.PfilterDesc()
+    d.model = m.spec.ffi_model()
+    d.J, d.F, d.T, d.U = J, 2, st.ys.shape[0], 1
+    d.path = _ffi.PATHS[path]
+    d.flags = _ffi.F_GRAPH | _ffi.F_SAVE_ANC
+    d.theta, d.ys, d.seeds, d.loglik, d.anc = _ffi.ptr(thd), _ffi.ptr(ys), _ffi.ptr(sd), _ffi.ptr(ll), _ffi.ptr(anc)
+    ws = torch.empty(_ffi.LIB.ppf_pfilter_workspace_bytes(d), dtype=torch.uint8, device=dev)
+    d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
+    stream = torch.cuda.current_stream().cuda_stream
+    for call in range(3):
+        ll.zero_()
+        anc.zero_()
+        _ffi.check(_ffi.LIB.ppf_pfilter(d, stream), "ppf_pfilter")
+        _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_pfilter")
+        assert np.array_equal(anc.cpu().numpy(), want["anc"]), call
+        assert np.array_equal(ll.cpu().numpy(), want["loglik"]), call
