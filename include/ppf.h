@@ -82,13 +82,18 @@ typedef struct ppf_model {
  * already being captured launches directly into that capture.  Host-side
  * cache of 16 graphs per process, not thread-safe. */
 #define PPF_F_GRAPH (1u << 9)
+/* ppf_perfilter: use the streaming kernels even where the cluster-resident
+ * path would be chosen (small swarms); for comparisons and tests */
+#define PPF_F_NO_CLUSTER (1u << 10)
 
 /* Execution paths; all produce bit-identical results. */
 enum {
   PPF_PATH_AUTO = 0,     /* autotuner / size heuristic */
   PPF_PATH_PLAIN = 1,    /* one filter at a time, textbook kernels (1x baseline) */
   PPF_PATH_STREAM = 2,   /* batched, HBM-streaming, 2 fused kernels per step */
-  PPF_PATH_RESIDENT = 3  /* batched, one CTA per filter, swarm in shared memory */
+  PPF_PATH_RESIDENT = 3, /* batched, one CTA per filter, swarm in shared memory */
+  PPF_PATH_CLUSTER = 4   /* one thread-block cluster (<= 16 CTAs) per filter, swarm in
+                            the cluster's distributed shared memory for all T steps */
 };
 
 /* Inputs and outputs of one batched bootstrap particle filter call over F

@@ -31,9 +31,11 @@ F_SAVE_W = 1 << 6
 F_EST = 1 << 7
 F_NATURAL = 1 << 8
 F_GRAPH = 1 << 9
+F_NO_CLUSTER = 1 << 10
 
-PATH_AUTO, PATH_PLAIN, PATH_STREAM, PATH_RESIDENT = 0, 1, 2, 3
-PATHS = {"auto": PATH_AUTO, "plain": PATH_PLAIN, "stream": PATH_STREAM, "resident": PATH_RESIDENT}
+PATH_AUTO, PATH_PLAIN, PATH_STREAM, PATH_RESIDENT, PATH_CLUSTER = 0, 1, 2, 3, 4
+PATHS = {"auto": PATH_AUTO, "plain": PATH_PLAIN, "stream": PATH_STREAM, "resident": PATH_RESIDENT,
+         "cluster": PATH_CLUSTER}
 
 # Every extern "C" symbol include/*.h declares; tests check the library exports them.
 EXPORTED = (

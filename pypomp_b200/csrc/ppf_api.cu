@@ -86,9 +86,15 @@ static int check_model(const ppf_model& m) {
 static int choose_path(const ppf_pfilter_desc* d) {
   if (d->path != PPF_PATH_AUTO) return d->path;
   Args a{};
-  a.J = d->J; a.model = d->model;
+  a.J = d->J; a.model = d->model; a.mode = MODE_PF;
   // swarm fits one CTA's shared memory: keep it on chip for the whole loop
-  if (resident_smem_bytes(a) <= kResidentSmemMax && d->J <= 16384) return PPF_PATH_RESIDENT;
+  const bool resident = resident_smem_bytes(a) <= kResidentSmemMax && d->J <= 16384;
+  if (resident && d->F >= kNumSMs) return PPF_PATH_RESIDENT;
+  // few filters of a few thousand particles or more: the streaming kernels
+  // would leave most SMs idle; a cluster per filter keeps the swarm on chip
+  const long long tiles = (long long)d->F * ((d->J + kTileLarge - 1) / kTileLarge);
+  if (d->J > 2048 && tiles < 2LL * kNumSMs && cluster_fits(a, false)) return PPF_PATH_CLUSTER;
+  if (resident) return PPF_PATH_RESIDENT;
   return PPF_PATH_STREAM;
 }
 
@@ -175,7 +181,7 @@ static int validate(const ppf_pfilter_desc* d) {
   if ((d->flags & PPF_F_PMEAN) && !d->pmean) return PPF_EINVAL;
   if ((d->flags & PPF_F_SAVE_ANC) && !d->anc) return PPF_EINVAL;
   if ((d->flags & PPF_F_SAVE_W) && !d->logw) return PPF_EINVAL;
-  if (d->path < PPF_PATH_AUTO || d->path > PPF_PATH_RESIDENT) return PPF_EINVAL;
+  if (d->path < PPF_PATH_AUTO || d->path > PPF_PATH_CLUSTER) return PPF_EINVAL;
   if (d->tile != 0 && d->tile != kTileLarge && d->tile != kTileMid && d->tile != kTileSmall) return PPF_EINVAL;
   return PPF_OK;
 }
@@ -268,7 +274,7 @@ static void fill_if2(const ppf_perfilter_desc* d, Args& a) {
   memset(&p, 0, sizeof(p));
   p.model = d->model;
   p.J = d->J; p.F = d->F; p.T = d->T; p.U = d->U;
-  p.flags = (d->flags & (PPF_F_INJECT | PPF_F_CLL | PPF_F_SAVE_ANC)) |
+  p.flags = (d->flags & (PPF_F_INJECT | PPF_F_CLL | PPF_F_SAVE_ANC | PPF_F_NO_CLUSTER)) |
             ((d->flags & PPF_F_NATURAL) ? 0u : PPF_F_EST);
   p.thresh = d->thresh;
   p.ys = d->ys; p.ycon = d->ycon; p.unit = d->unit; p.T_u = d->T_u;

@@ -1,0 +1,425 @@
+// ppf_cluster.cu -- cluster-resident filters for small swarms.
+//
+// A filter whose swarm is too small to fill the GPU through the streaming
+// kernels (few filters of a few thousand to ~10^5 particles: the IF2 unit
+// filters of a panel, a single large-ish filter) is latency-bound there: every
+// observation costs two dependent launches over a handful of CTAs.  Here one
+// thread-block cluster of NC CTAs (NC <= 16, one per SM) owns one filter for
+// the whole time loop.  CTA c keeps particles [c JC, (c+1) JC) -- state,
+// log-weight and, for IF2, the parameter vector -- in its shared memory.  Per
+// observation:
+//   1. each CTA reduces its slice's max / min / NaN key; cluster barrier; every
+//      CTA reads all slices' keys through distributed shared memory (DSMEM);
+//   2. each CTA forms the slice's fixed-point weights, block-scans them and
+//      publishes the slice total; cluster barrier; every CTA reads all totals
+//      (the exclusive prefix of its slice and the filter total);
+//   3. each CTA computes the exact systematic first-child offsets of its own
+//      parents (the same integer walk as the streaming path) and propagates
+//      their children, writing each child's state and weight straight into the
+//      shared memory of the CTA that owns the child's index; cluster barrier.
+// The arithmetic is the streaming path's (same Philox streams per particle,
+// same fixed-point CDF, same offsets), so results are bit-identical to it and
+// to the oracle.  Cluster barriers are hardware barriers (barrier.cluster):
+// no spin loop, and every CTA of a cluster runs the same number of them.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include "ppf.h"
+#include "ppf_core.cuh"
+#include "ppf_internal.h"
+#include "ppf_kernels.cuh"
+#include "ppf_models.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace ppf {
+
+constexpr int kClusterTPB = 512;
+
+// One per CTA; the other CTAs of the cluster read it through DSMEM.
+struct CStat {
+  unsigned int maxkey, minkey, nan, pad;
+  unsigned long long sum;   // fixed-point weight sum of the slice
+  double s2, fx[4], px[4];  // ESS and mean sums of the slice (when requested)
+};
+
+// Dynamic shared memory of one CTA, in 4-byte words: X[2][DX][JC], W[2][JC],
+// (IF2) TH[2][P][JC], st[JC + 4], (IF2) per-thread parameter rows [TPB][P|1].
+template <class M, bool IF2>
+size_t cluster_smem_words(int JC, int P, int TPB) {
+  size_t w = 2ull * M::MAXDX * JC + 2ull * JC + (size_t)JC + 4;
+  if (IF2) w += 2ull * P * JC + (size_t)TPB * (P | 1);
+  return w;
+}
+
+template <class M, int TPB, bool IF2, bool INJ>
+__global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
+  cg::cluster_group cl = cg::this_cluster();
+  constexpr int DX = M::MAXDX;
+  constexpr int G = ChildGroup<M::NZ>::G;
+  extern __shared__ __align__(16) float smf[];
+  __shared__ CStat stat;
+  __shared__ typename M::Consts csh;
+  __shared__ uint64_t s_scan[TPB / 32 + 1];
+  __shared__ unsigned int smk[2 * (TPB / 32)];
+  __shared__ double sd[TPB / 32];
+
+  const int NC = (int)cl.num_blocks();
+  const int c = (int)cl.block_rank();
+  const int f = blockIdx.y;
+  const int u = filter_unit(a, f);
+  const int Tf = filter_len(a, u);
+  const int J = a.J, P = a.model.n_params;
+  const int base = c * JC;
+  const int nc = max(0, min(JC, J - base));
+  const bool est = (a.flags & PPF_F_EST) != 0;
+  float* X[2];
+  float* W[2];
+  float* TH[2] = {nullptr, nullptr};
+  X[0] = smf;
+  X[1] = X[0] + DX * JC;
+  W[0] = X[1] + DX * JC;
+  W[1] = W[0] + JC;
+  float* rest = W[1] + JC;
+  if (IF2) {
+    TH[0] = rest;
+    TH[1] = TH[0] + P * JC;
+    rest = TH[1] + P * JC;
+  }
+  int* st = reinterpret_cast<int*>(rest);
+  float* th = IF2 ? reinterpret_cast<float*>(st + JC + 4) + threadIdx.x * if2_row_stride(P) : nullptr;
+  const float log1e18 = pp_logf(1e-18f);
+  const bool want_ess = (a.flags & PPF_F_ESS) != 0, want_fm = (a.flags & PPF_F_FMEAN) != 0;
+  const bool want_pm = (a.flags & PPF_F_PMEAN) != 0;
+  const bool want_sums = want_ess || want_fm || want_pm;
+
+  if (!IF2 && threadIdx.x == 0) M::prepare(csh, a.theta + (size_t)f * P, a.model, est);
+  __syncthreads();
+
+  // ---- initial states, propagated into observation 0 -----------------------
+  {
+    Obs<M> ob;
+    ob.load(a, u, 0);
+    float* logw0 = a.logw ? a.logw + (size_t)f * a.T * J : nullptr;
+    for (int l = threadIdx.x; l < nc; l += TPB) {
+      const int k = base + l;
+      float x[DX];
+      float m;
+      if (IF2) {
+        for (int p = 0; p < P; ++p) th[p] = a.swarm_in[((size_t)f * P + p) * J + k];
+        perturb_row<INJ>(a, f, k, 0, P, a.cool0[u], a.rw_sig0, th);
+        typename M::Consts ci;
+        M::prepare(ci, th, a.model, est);
+        float z0[M::NZ0 > 0 ? M::NZ0 : 1];
+        step_noise<M>(a, f, k, 0, M::NZ0, z0);
+        M::rinit(ci, z0, x);
+        perturb_row<INJ>(a, f, k, 1, P, a.cool[(size_t)u * a.T], a.rw_sig, th);
+        M::prepare(ci, th, a.model, est);
+        float z[M::NZ];
+        step_noise<M>(a, f, k, 1, M::NZ, z);
+        m = if2_measure(step1<M>(ci, ob, x, z), log1e18);
+        for (int p = 0; p < P; ++p) TH[0][p * JC + l] = th[p];
+      } else {
+        const typename M::Consts cr = csh;
+        float z0[M::NZ0 > 0 ? M::NZ0 : 1];
+        step_noise<M>(a, f, k, 0, M::NZ0, z0);
+        M::rinit(cr, z0, x);
+        float z[M::NZ];
+        step_noise<M>(a, f, k, 1, M::NZ, z);
+        m = step1<M>(cr, ob, x, z);
+      }
+      const float w = a.base_init + m;
+#pragma unroll
+      for (int d = 0; d < DX; ++d) X[0][d * JC + l] = x[d];
+      W[0][l] = w;
+      if (logw0) logw0[k] = w;
+    }
+    if (c == 0 && threadIdx.x == 0) a.loglik[f] = 0.0;
+  }
+  cl.sync();
+
+  const int ITC = (JC + TPB - 1) / TPB;        // parents per thread (contiguous)
+  const int l0 = threadIdx.x * ITC;
+  const int l1 = min(l0 + ITC, nc);
+  for (int t = 0; t < Tf; ++t) {
+    const int pc = t & 1, pn = pc ^ 1;
+    const bool last = (t == Tf - 1);
+    const float* Wc = W[pc];
+
+    // 1. max / min / NaN of the swarm
+    unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
+    for (int l = threadIdx.x; l < nc; l += TPB) accum_maxmin(Wc[l], mx, mn, nn);
+    block_maxmin_u32<TPB>(mx, mn, smk);
+    nn = __syncthreads_or(nn);
+    if (threadIdx.x == 0) {
+      stat.maxkey = mx;
+      stat.minkey = mn;
+      stat.nan = nn;
+    }
+    cl.sync();
+    Acc acc;
+    acc.maxkey = 0u;
+    acc.minkey = 0xffffffffu;
+    acc.nan = 0u;
+    acc.pad = 0u;
+    acc.s2 = 0.0;
+    acc.pad2 = 0.0;
+    for (int d = 0; d < 4; ++d) { acc.fx[d] = 0.0; acc.px[d] = 0.0; }
+    for (int r = 0; r < NC; ++r) {
+      const CStat* o = cl.map_shared_rank(&stat, r);
+      acc.maxkey = max(acc.maxkey, o->maxkey);
+      acc.minkey = min(acc.minkey, o->minkey);
+      acc.nan |= o->nan;
+    }
+    const bool nanf = acc.nan != 0;
+    const float Mx = keyf(acc.maxkey);
+    const bool collapsed = !nanf && Mx == -INFINITY;
+    const bool qc = nanf || Mx == -INFINITY;
+
+    // 2. fixed-point weights of the slice: totals and this thread's prefix
+    uint64_t qs = 0;
+    double s2 = 0.0, fx[DX], px[DX];
+#pragma unroll
+    for (int d = 0; d < DX; ++d) { fx[d] = 0.0; px[d] = 0.0; }
+    for (int l = l0; l < l1; ++l) {
+      qs += qweight(Wc[l], Mx, qc);
+      if (want_sums) {
+        const double e = qc ? 1.0 : (double)pp_expf(Wc[l] - Mx);
+        s2 += e * e;
+#pragma unroll
+        for (int d = 0; d < DX; ++d) {
+          const double xv = (double)X[pc][d * JC + l];
+          fx[d] += xv * e;
+          px[d] += xv;
+        }
+      }
+    }
+    uint64_t btot;
+    const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
+    if (want_sums) {
+      const double b2 = block_sum_f64<TPB>(s2, sd);
+      if (threadIdx.x == 0) stat.s2 = b2;
+#pragma unroll
+      for (int d = 0; d < DX; ++d) {
+        const double bf = block_sum_f64<TPB>(fx[d], sd);
+        const double bp = block_sum_f64<TPB>(px[d], sd);
+        if (threadIdx.x == 0) { stat.fx[d] = bf; stat.px[d] = bp; }
+      }
+    }
+    if (threadIdx.x == 0) stat.sum = btot;
+    cl.sync();
+    uint64_t E = 0, tot = 0;
+    for (int r = 0; r < NC; ++r) {
+      const CStat* o = cl.map_shared_rank(&stat, r);
+      if (r < c) E += o->sum;
+      tot += o->sum;
+      if (c == 0 && threadIdx.x == 0 && want_sums) {
+        acc.s2 += o->s2;
+        for (int d = 0; d < DX; ++d) { acc.fx[d] += o->fx[d]; acc.px[d] += o->px[d]; }
+      }
+    }
+    if (c == 0 && threadIdx.x == 0) finalize_step(a, f, t, acc, tot, a.loglik + f);
+    const bool rs = decide_resample(a, acc);
+
+    // 3. first-child offsets of this CTA's parents (global child indices)
+    float lt32 = 0.0f;
+    if (rs) {
+      const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
+      if (l0 < nc) {
+        OffWalk wk = offwalk_init(o, E + tex);
+        st[l0] = wk.k;
+        for (int l = l0; l < l1; ++l) {
+          const int kn = offwalk_add(o, wk, qweight(Wc[l], Mx, qc));
+          if (l + 1 < l1 || l + 1 == nc) st[l + 1] = kn;
+        }
+      }
+    } else {
+      if (nanf) lt32 = __int_as_float(0x7fc00000);
+      else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
+      for (int l = l0; l < l1; ++l) st[l] = base + l;
+      if (l0 < nc && l1 == nc) st[nc] = base + nc;
+    }
+    __syncthreads();
+
+    // 4. children of this CTA's parents, into the owners' shared memory
+    if (nc > 0) {
+      const int klo = st[0], khi = st[nc];
+      Obs<M> ob;
+      if (!last) ob.load(a, u, t + 1);
+      const float coolt = (IF2 && !last) ? a.cool[(size_t)u * a.T + t + 1] : 0.0f;
+      const float nwc = -pp_logf((float)J);
+      int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
+      float* logw = (a.logw && !last) ? a.logw + ((size_t)f * a.T + t + 1) * J : nullptr;
+      const typename M::Consts cr = csh;
+      const int kA = klo & ~3;
+      const int ngr = (khi - kA + G - 1) / G;
+      const int g0 = (int)(((long long)threadIdx.x * ngr) / TPB);
+      const int g1 = (int)(((long long)(threadIdx.x + 1) * ngr) / TPB);
+      if (g0 < g1) {
+        int l = find_parent(st, nc, max(kA + G * g0, klo));
+#pragma unroll 1
+        for (int g = g0; g < g1; ++g) {
+          const int k0 = kA + G * g;
+          if (k0 >= khi) break;
+          float z[G * M::NZ];
+          if (!last) group_noise_g<G, M::NZ, INJ>(a, f, t + 2, k0, z);
+#pragma unroll
+          for (int e = 0; e < G; ++e) {
+            const int k = k0 + e;
+            if (k < klo || k >= khi) continue;
+            int adv = 0;
+            while (l + 1 < nc && st[l + 1] <= k) {
+              ++l;
+              if (++adv > 8) { l = find_parent(st, nc, k); break; }
+            }
+            if (anc) anc[k] = base + l;
+            if (last) {
+              if (IF2)
+                for (int p = 0; p < P; ++p) a.swarm_out[((size_t)f * P + p) * J + k] = TH[pc][p * JC + l];
+              continue;
+            }
+            float x[DX];
+#pragma unroll
+            for (int d = 0; d < DX; ++d) x[d] = X[pc][d * JC + l];
+            float m;
+            if (IF2) {
+              for (int p = 0; p < P; ++p) th[p] = TH[pc][p * JC + l];
+              perturb_row<INJ>(a, f, k, t + 2, P, coolt, a.rw_sig, th);
+              typename M::Consts cc;
+              M::prepare(cc, th, a.model, est);
+              m = if2_measure(step1<M>(cc, ob, x, z + e * M::NZ), log1e18);
+            } else {
+              m = step1<M>(cr, ob, x, z + e * M::NZ);
+            }
+            const float wb = rs ? a.base_rs : (collapsed ? nwc : Wc[l] - lt32);
+            const float w = wb + m;
+            const int r = k / JC, lk = k - r * JC;
+            float* xr = cl.map_shared_rank(X[pn], r);
+#pragma unroll
+            for (int d = 0; d < DX; ++d) xr[d * JC + lk] = x[d];
+            cl.map_shared_rank(W[pn], r)[lk] = w;
+            if (IF2) {
+              float* tr = cl.map_shared_rank(TH[pn], r);
+              for (int p = 0; p < P; ++p) tr[p * JC + lk] = th[p];
+            }
+            if (logw) logw[k] = w;
+          }
+        }
+      }
+    }
+    cl.sync();   // children visible to their owners; nobody leaves while others read its memory
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+// Cluster size and slice: the largest cluster (<= 16 CTAs) that keeps at least
+// 256 particles per CTA (2 CTAs at the least), with a slice that fits one CTA's
+// shared memory.
+template <class M, bool IF2>
+static bool cluster_plan_t(const Args& a, int& NC, int& JC) {
+  for (int n = 16; n >= 2; n >>= 1) {
+    const int jc = ((a.J + n - 1) / n + 3) & ~3;
+    if (jc < 256 && n != 2) continue;
+    if (cluster_smem_words<M, IF2>(jc, a.model.n_params, kClusterTPB) * 4 > (size_t)kResidentSmemMax) continue;
+    NC = n;
+    JC = jc;
+    return true;
+  }
+  return false;
+}
+
+template <class M, bool IF2, bool INJ>
+static int run_cluster_t(Args& a, cudaStream_t s) {
+  int NC = 0, JC = 0;
+  if (!cluster_plan_t<M, IF2>(a, NC, JC)) return PPF_EUNSUPPORTED;
+  constexpr int TPB = kClusterTPB;
+  const size_t smem = cluster_smem_words<M, IF2>(JC, a.model.n_params, TPB) * 4;
+  auto kern = k_cluster<M, TPB, IF2, INJ>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return PPF_ECUDA;
+  if (NC > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return PPF_ECUDA;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(NC, a.F, 1);
+  cfg.blockDim = dim3(TPB, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = NC;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int nclusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) != cudaSuccess || nclusters < 1) {
+    cudaGetLastError();
+    return PPF_EUNSUPPORTED;
+  }
+  PROF_BEGIN(KIND_CLUSTER);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, JC);
+  PROF_END(KIND_CLUSTER);
+  return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
+template <class M, bool IF2>
+static int run_cluster_m(Args& a, cudaStream_t s) {
+  return (a.flags & PPF_F_INJECT) ? run_cluster_t<M, IF2, true>(a, s) : run_cluster_t<M, IF2, false>(a, s);
+}
+
+template <class M, bool IF2>
+static bool fits_m(const Args& a) {
+  int NC = 0, JC = 0;
+  return cluster_plan_t<M, IF2>(a, NC, JC);
+}
+
+template <bool IF2>
+static bool fits_any(const Args& a) {
+  switch (a.model.kind) {
+    case PPF_MODEL_LG:
+      switch (a.model.dx) {
+        case 1: return a.model.dy == 1 ? fits_m<LG<1, 1>, IF2>(a) : fits_m<LG<1>, IF2>(a);
+        case 2: return a.model.dy == 2 ? fits_m<LG<2, 2>, IF2>(a) : fits_m<LG<2>, IF2>(a);
+        case 3: return a.model.dy == 3 ? fits_m<LG<3, 3>, IF2>(a) : fits_m<LG<3>, IF2>(a);
+        case 4: return a.model.dy == 4 ? fits_m<LG<4, 4>, IF2>(a) : fits_m<LG<4>, IF2>(a);
+        default: return false;
+      }
+    case PPF_MODEL_SV: return fits_m<SV, IF2>(a);
+    case PPF_MODEL_RICKER: return fits_m<Ricker, IF2>(a);
+    default: return false;
+  }
+}
+
+template <bool IF2>
+static int run_any(Args& a, cudaStream_t s) {
+  switch (a.model.kind) {
+    case PPF_MODEL_LG:
+      switch (a.model.dx) {
+        case 1: return a.model.dy == 1 ? run_cluster_m<LG<1, 1>, IF2>(a, s) : run_cluster_m<LG<1>, IF2>(a, s);
+        case 2: return a.model.dy == 2 ? run_cluster_m<LG<2, 2>, IF2>(a, s) : run_cluster_m<LG<2>, IF2>(a, s);
+        case 3: return a.model.dy == 3 ? run_cluster_m<LG<3, 3>, IF2>(a, s) : run_cluster_m<LG<3>, IF2>(a, s);
+        case 4: return a.model.dy == 4 ? run_cluster_m<LG<4, 4>, IF2>(a, s) : run_cluster_m<LG<4>, IF2>(a, s);
+        default: return PPF_EUNSUPPORTED;
+      }
+    case PPF_MODEL_SV: return run_cluster_m<SV, IF2>(a, s);
+    case PPF_MODEL_RICKER: return run_cluster_m<Ricker, IF2>(a, s);
+    default: return PPF_EINVAL;
+  }
+}
+
+bool cluster_fits(const Args& a, bool if2) {
+  if (a.mode == MODE_MOP) return false;
+  return if2 ? fits_any<true>(a) : fits_any<false>(a);
+}
+
+int run_cluster(Args& a, bool if2, cudaStream_t s) {
+  if (a.mode == MODE_MOP) return PPF_EUNSUPPORTED;
+  return if2 ? run_any<true>(a, s) : run_any<false>(a, s);
+}
+
+}  // namespace ppf

@@ -82,7 +82,7 @@ struct Args {
 };
 
 enum { KIND_INIT = 0, KIND_SUM = 1, KIND_RESPROP = 2, KIND_RESIDENT = 3, KIND_PLAIN = 4,
-       KIND_MOP_FWD = 5, KIND_MOP_RECOMP = 6, KIND_MOP_BWD = 7, KIND_IF2 = 8, KIND_COUNT = 16 };
+       KIND_MOP_FWD = 5, KIND_MOP_RECOMP = 6, KIND_MOP_BWD = 7, KIND_IF2 = 8, KIND_CLUSTER = 9, KIND_COUNT = 16 };
 
 struct Profiler {
   struct Ev { cudaEvent_t a, b; int kind; };
@@ -117,6 +117,10 @@ constexpr int kNumSMs = 148;
 int run_mop(Args& a, const MopWork& w, cudaStream_t s);
 int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s);
 int run_if2(Args& a, cudaStream_t s);
+// cluster-resident filters (ppf_cluster.cu): whether a cluster plan exists for
+// this shape, and the launch
+bool cluster_fits(const Args& a, bool if2);
+int run_cluster(Args& a, bool if2, cudaStream_t s);
 int reset_accumulators(Args& a, cudaStream_t s);
 size_t resident_smem_bytes(const Args& a);
 

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <float.h>
 #include <stdint.h>
 
 #include "ppf.h"
@@ -354,6 +355,53 @@ __device__ __forceinline__ void store_group_g(float* Xn, float* Wn, float* logw,
     if (logw) logw[k0 + e] = wo[e];
   }
 }
+
+// ------------------------------ IF2 helpers --------------------------------
+// (shared by the streaming IF2 kernels, ppf_if2.cu, and the cluster kernels,
+// ppf_cluster.cu)
+
+// jnp.nan_to_num(m, nan=log(1e-18)): NaN -> log(1e-18), +inf -> FLT_MAX,
+// -inf -> -FLT_MAX.
+__device__ __forceinline__ float if2_measure(float m, float log1e18) {
+  if (m != m) return log1e18;
+  if (m == INFINITY) return FLT_MAX;
+  if (m == -INFINITY) return -FLT_MAX;
+  return m;
+}
+
+// Perturb the parameter row th[0..P) of particle k in place:
+// th[p] += (cool * sig[p]) * z_p, z_p the P normals of counter s (tag PERTURB),
+// drawn one at a time from the particle's Philox blocks (the same values
+// pp_normals gives), or read from the injected arrays.  The row lives in
+// shared memory: per-thread arrays passed by pointer and indexed at run time
+// are kept out of these kernels.
+template <bool INJ>
+__device__ __forceinline__ void perturb_row(const Args& a, int f, int k, int s, int P, float cool,
+                                            const float* sig, float* th) {
+  if (INJ) {
+    const float* src = (s == 0) ? a.inj_zp0 + ((size_t)f * a.J + k) * P
+                                : a.inj_zp + (((size_t)f * a.T + (s - 1)) * a.J + k) * P;
+    for (int p = 0; p < P; ++p) th[p] = th[p] + (cool * sig[p]) * src[p];
+    return;
+  }
+  const uint64_t seed = a.seeds[f];
+  uint32_t cached = 0xffffffffu;
+  float z4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  for (int p = 0; p < P; ++p) {
+    const uint32_t i = (uint32_t)k * (uint32_t)P + (uint32_t)p;
+    if ((i >> 2) != cached) {
+      cached = i >> 2;
+      pp_normal4(seed, cached, (uint32_t)s, PPF_TAG_PERTURB, z4);
+    }
+    const uint32_t e = i & 3u;
+    const float z = e == 0u ? z4[0] : e == 1u ? z4[1] : e == 2u ? z4[2] : z4[3];
+    th[p] = th[p] + (cool * sig[p]) * z;
+  }
+}
+
+// Parameter rows of the block's threads in dynamic shared memory: thread r
+// owns row r, stride P | 1 (odd, so a warp's rows fall in distinct banks).
+__device__ __forceinline__ int if2_row_stride(int P) { return P | 1; }
 
 // Fixed-point sums of the weights of one tile, then the decoupled-lookback
 // prefix over the tiles of the filter (Merrill & Garland 2016).

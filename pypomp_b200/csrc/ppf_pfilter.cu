@@ -831,6 +831,7 @@ int dispatch_model(Args& a, int path, cudaStream_t s) {
 }
 
 int run_pfilter_path(Args& a, int path, cudaStream_t s) {
+  if (path == PPF_PATH_CLUSTER) return run_cluster(a, false, s);
   switch (a.model.kind) {
     case PPF_MODEL_LG:
       switch (a.model.dx) {

@@ -57,8 +57,8 @@ def run_pfilter(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J:
     ``theta_f`` (F, P) parameters, ``seeds_f`` (F,) keys.  ``inject`` is an
     optional dict of host arrays ``z0`` (F,J,n0), ``z`` (F,T,J,nz), ``u``
     (F,T) that replaces the Philox draws.  ``path`` is "plain", "stream",
-    "resident", "stream@<tile>" (tile 2048, 512 or 256 particles per CTA) or
-    None (automatic).  Returns a dict of NumPy arrays.
+    "resident", "cluster", "stream@<tile>" (tile 2048, 512 or 256 particles
+    per CTA) or None (automatic).  Returns a dict of NumPy arrays.
     """
     torch = _ffi.require_cuda()
     if J < 1:
@@ -132,7 +132,7 @@ def autotune(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J: in
              thresh: float = 0.0) -> int:
     """Time the stream path's tile sizes for this shape (``ppf_autotune``) and
     keep the fastest for later calls of the same shape; returns the tile (0 if
-    the shape runs on the resident path)."""
+    the shape runs on the resident or cluster path)."""
     import ctypes
 
     torch = _ffi.require_cuda()
@@ -151,7 +151,9 @@ def autotune(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J: in
     d.thresh = float(max(0.0, thresh))
     d.theta, d.ys, d.ycon = _ffi.ptr(th_d), _ffi.ptr(ys_d), _ffi.ptr(ycon_d)
     d.unit, d.T_u, d.seeds, d.loglik = _ffi.ptr(unit_d), _ffi.ptr(Tu_d), _ffi.ptr(seeds_d), _ffi.ptr(ll)
-    ws = torch.empty(max(int(_ffi.LIB.ppf_pfilter_workspace_bytes(d)), 256), dtype=torch.uint8, device=dev)
+    # zeroed: on a shape that runs on another path nothing is launched, and the
+    # status word read below must then read as success
+    ws = torch.zeros(max(int(_ffi.LIB.ppf_pfilter_workspace_bytes(d)), 256), dtype=torch.uint8, device=dev)
     d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
     best = ctypes.c_int(0)
     stream = torch.cuda.current_stream(dev).cuda_stream
@@ -393,7 +395,7 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
 
 def run_perfilter(struct: PompStruct, swarm, seeds_f: np.ndarray, J: int, rw_sig, rw_sig0, cool, cool0,
                   *, thresh: float = 0.0, unit_f=None, inject=None, CLL: bool = False,
-                  save_ancestors: bool = False, natural: bool = False):
+                  save_ancestors: bool = False, natural: bool = False, stream_only: bool = False):
     """One batched call of ``ppf_perfilter``: one IF2 iteration over F swarms.
 
     ``swarm`` is either a CUDA tensor (F, P, J) on the estimation scale (kept
@@ -402,7 +404,9 @@ def run_perfilter(struct: PompStruct, swarm, seeds_f: np.ndarray, J: int, rw_sig
     cooling factors of the step and t0 perturbations.  ``inject`` optionally
     holds host arrays ``zp0`` (F,J,P), ``zp`` (F,T,J,P), ``z0``, ``z``, ``u``
     replacing the Philox draws.  ``natural`` hands the kernels natural-scale
-    parameters (``PPF_F_NATURAL``: no transform inside the mechanics).
+    parameters (``PPF_F_NATURAL``: no transform inside the mechanics);
+    ``stream_only`` keeps the streaming kernels where few small swarms would
+    otherwise run cluster-resident (``PPF_F_NO_CLUSTER``).
     Returns a dict with ``loglik`` (F,), ``swarm`` and optionally ``cll`` /
     ``anc``.
     """
@@ -440,7 +444,7 @@ def run_perfilter(struct: PompStruct, swarm, seeds_f: np.ndarray, J: int, rw_sig
         unit_d = torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
     out = {"loglik": torch.zeros(F, dtype=torch.float64, device=dev),
            "swarm": torch.empty(F, P, J, **f32d)}
-    flags = _ffi.F_NATURAL if natural else 0
+    flags = (_ffi.F_NATURAL if natural else 0) | (_ffi.F_NO_CLUSTER if stream_only else 0)
     if CLL:
         flags |= _ffi.F_CLL
         out["cll"] = torch.zeros(F, T, dtype=torch.float64, device=dev)

@@ -3,7 +3,9 @@
 * ``ppf_perfilter`` is bit-identical to the C oracle's restatement
   (``oracle/ppf_oracle.c`` ``ppfo_perfilter``) for LG 2-D, SV and Ricker:
   ancestors, conditional log-likelihoods, log-likelihood and final swarm,
-  with one and several tiles per swarm, thresh 0 and 20;
+  with one and several tiles per swarm, thresh 0 and 20, on the
+  cluster-resident path (chosen for these few small swarms) and on the
+  streaming kernels;
 * with zero random-walk sds the perturbed filter is the bootstrap filter
   (same ancestors and log-likelihoods bit for bit);
 * ``functional.mif`` replaying the reference's own draws reproduces the
@@ -50,10 +52,11 @@ def _swarm(th, F, J, seed):
             + f32(0.01) * rng.standard_normal((F, P, J)).astype(f32)).astype(f32)
 
 
+@pytest.mark.parametrize("stream_only", [False, True])
 @pytest.mark.parametrize("thresh", [0.0, 20.0])
 @pytest.mark.parametrize("J", [1000, 5000])
 @pytest.mark.parametrize("model", ["LG", "SV", "Ricker"])
-def test_perfilter_bit_exact_vs_oracle(model, J, thresh):
+def test_perfilter_bit_exact_vs_oracle(model, J, thresh, stream_only):
     F = _F()
     m, st, th = _case(model)
     spec = m.spec
@@ -67,7 +70,7 @@ def test_perfilter_bit_exact_vs_oracle(model, J, thresh):
     want = cora.perfilter(spec.kind, spec.dx, spec.dy, swarm, st.ys, J, sig, sig0, cool, f32(0.99),
                           seeds=seeds, ycon=spec.ycon(st.ys), dt=spec.dt, thresh=thresh, CLL=True, anc=True)
     got = F.run_perfilter(st, swarm.transpose(0, 2, 1), seeds, J, sig, sig0, cool, f32(0.99), thresh=thresh,
-                          CLL=True, save_ancestors=True)
+                          CLL=True, save_ancestors=True, stream_only=stream_only)
     assert np.array_equal(got["anc"], want["anc"])
     assert np.array_equal(got["swarm"], want["swarm"].transpose(0, 2, 1))
     np.testing.assert_allclose(got["cll"], want["cll"], rtol=1e-12, atol=1e-12)

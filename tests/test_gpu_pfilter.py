@@ -6,7 +6,9 @@ and Philox modes; log-likelihoods agree to float64 rounding of log().  The
 reference's own locked fixtures are reproduced by feeding the reference's
 draws through the injection mode.  Edge cases: J=1, T=1, partial tiles,
 thresh > 1 (steps without resampling), ragged panels, collapsed weights,
-non-finite parameters; the stream path with each of its tile sizes.
+non-finite parameters; the stream path with each of its tile sizes; the
+cluster-resident path (swarm split over a thread-block cluster's shared
+memory).
 """
 
 import numpy as np
@@ -16,7 +18,7 @@ from oracle import cora, kalman
 
 pytestmark = pytest.mark.gpu
 
-PATHS = ["plain", "stream", "stream@2048", "stream@512", "stream@256", "resident"]
+PATHS = ["plain", "stream", "stream@2048", "stream@512", "stream@256", "resident", "cluster"]
 f32 = np.float32
 
 
@@ -215,8 +217,9 @@ def test_autotune_picks_a_tile_and_keeps_results():
     F = _F()
     m = _models()["SV"]
     st = m.to_struct()
-    th = _thetas(m, 2)
-    seeds = np.array([5, 6], np.uint64)
+    # 16 filters x 20 large tiles: enough CTAs that the automatic choice is the stream path
+    th = np.repeat(_thetas(m, 2), 8, axis=0)
+    seeds = np.arange(5, 21, dtype=np.uint64)
     J = 40000
     best = F.autotune(st, th, seeds, J)
     assert best in (2048, 512, 256)
@@ -224,6 +227,8 @@ def test_autotune_picks_a_tile_and_keeps_results():
     fixed = F.run_pfilter(st, th, seeds, J, path=f"stream@{best}", save_ancestors=True)
     assert np.array_equal(auto["anc"], fixed["anc"])
     assert np.array_equal(auto["loglik"], fixed["loglik"])
+    # two filters of the same size run cluster-resident: nothing to tune
+    assert F.autotune(st, th[:2], seeds[:2], J) == 0
 
 
 @pytest.mark.parametrize("path", ["stream", "resident"])
@@ -262,3 +267,21 @@ def test_graph_replay_matches_direct_launches(path):
         _ffi.check(_ffi.LIB.ppf_workspace_status(d.workspace, stream), "ppf_pfilter")
         assert np.array_equal(anc.cpu().numpy(), want["anc"]), call
         assert np.array_equal(ll.cpu().numpy(), want["loglik"]), call
+
+
+def test_largest_swarm_bit_exact():
+    """J = 2^21 (PPF_MAX_J, the largest swarm the 128-bit offset arithmetic
+    admits): stream path against the oracle, ancestors bit for bit."""
+    from pypomp_b200 import _ffi
+
+    F = _F()
+    m = _models()["Ricker"]
+    st = m.to_struct()
+    st.ys = np.ascontiguousarray(st.ys[:3])
+    th = _thetas(m, 1)
+    seeds = np.array([99], np.uint64)
+    J = _ffi.PPF_MAX_J
+    want = cora.pfilter(m.spec.kind, 1, 1, th, st.ys, J, seeds=seeds, ycon=m.spec.ycon(st.ys), anc=True)
+    got = F.run_pfilter(st, th, seeds, J, path="stream", save_ancestors=True)
+    assert np.array_equal(got["anc"], want["anc"])
+    np.testing.assert_allclose(got["loglik"], want["loglik"], rtol=1e-12)
