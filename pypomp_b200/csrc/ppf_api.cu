@@ -86,12 +86,13 @@ static int check_model(const ppf_model& m) {
 static int choose_path(const ppf_pfilter_desc* d) {
   if (d->path != PPF_PATH_AUTO) return d->path;
   Args a{};
-  a.J = d->J; a.model = d->model; a.mode = MODE_PF;
+  a.J = d->J; a.F = d->F; a.flags = d->flags; a.model = d->model; a.mode = MODE_PF;
   // swarm fits one CTA's shared memory: keep it on chip for the whole loop
   const bool resident = resident_smem_bytes(a) <= kResidentSmemMax && d->J <= 16384;
   if (resident && d->F >= kNumSMs) return PPF_PATH_RESIDENT;
   // few filters of a few thousand particles or more: the streaming kernels
   // would leave most SMs idle; a cluster per filter keeps the swarm on chip
+  // (when all filters' clusters are resident at once)
   const long long tiles = (long long)d->F * ((d->J + kTileLarge - 1) / kTileLarge);
   if (d->J > 2048 && tiles < 2LL * kNumSMs && cluster_fits(a, false)) return PPF_PATH_CLUSTER;
   if (resident) return PPF_PATH_RESIDENT;

@@ -6,25 +6,34 @@
 // observation costs two dependent launches over a handful of CTAs.  Here one
 // thread-block cluster of NC CTAs (NC <= 16, one per SM) owns one filter for
 // the whole time loop.  CTA c keeps particles [c JC, (c+1) JC) -- state,
-// log-weight and, for IF2, the parameter vector -- in its shared memory.  Per
-// observation:
-//   1. each CTA reduces its slice's max / min / NaN key; cluster barrier; every
-//      CTA reads all slices' keys through distributed shared memory (DSMEM);
-//   2. each CTA forms the slice's fixed-point weights, block-scans them and
-//      publishes the slice total; cluster barrier; every CTA reads all totals
-//      (the exclusive prefix of its slice and the filter total);
-//   3. each CTA computes the exact systematic first-child offsets of its own
-//      parents (the same integer walk as the streaming path) and propagates
-//      their children, writing each child's state and weight straight into the
-//      shared memory of the CTA that owns the child's index; cluster barrier.
-// The arithmetic is the streaming path's (same Philox streams per particle,
-// same fixed-point CDF, same offsets), so results are bit-identical to it and
-// to the oracle.  Cluster barriers are hardware barriers (barrier.cluster):
-// no spin loop, and every CTA of a cluster runs the same number of them.
+// log-weight and, for IF2, the parameter vector -- in its shared memory.
+//
+// CTAs exchange per-step numbers by PUSHING them: CTA c writes its numbers
+// into slot c of every CTA's slot array (distributed shared memory stores,
+// which need no round trip), and after the next cluster barrier each CTA
+// reads all slots from its own shared memory.  Per observation:
+//   A. every CTA finds the swarm's max / min / NaN key in its slots (pushed
+//      by the producers of the weights at the end of the previous step), forms
+//      its slice's fixed-point weights, block-scans them and pushes the slice
+//      total; cluster barrier;
+//   B. every CTA sums the slots (the exclusive prefix of its slice and the
+//      filter total), computes the exact systematic first-child offsets of its
+//      own parents (the same integer walk as the streaming path) and
+//      propagates their children, writing each child's state and weight
+//      straight into the shared memory of the CTA that owns the child's index;
+//      it reduces the max / min / NaN of the weights it produced and pushes
+//      them; cluster barrier.
+// Two cluster barriers per observation.  The arithmetic is the streaming
+// path's (same Philox streams per particle, same fixed-point CDF, same
+// offsets), so results are bit-identical to it and to the oracle.  Cluster
+// barriers are hardware barriers (barrier.cluster): no spin loop, and every
+// CTA of a cluster runs the same number of them.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <stdint.h>
+
+#include <mutex>
 
 #include "ppf.h"
 #include "ppf_core.cuh"
@@ -37,12 +46,13 @@ namespace cg = cooperative_groups;
 namespace ppf {
 
 constexpr int kClusterTPB = 512;
+constexpr int kMaxCluster = 16;
 
-// One per CTA; the other CTAs of the cluster read it through DSMEM.
-struct CStat {
-  unsigned int maxkey, minkey, nan, pad;
-  unsigned long long sum;   // fixed-point weight sum of the slice
-  double s2, fx[4], px[4];  // ESS and mean sums of the slice (when requested)
+// What CTA c publishes to the CTAs of its cluster: slot c of each CTA's array.
+struct Slot {
+  unsigned int maxkey, minkey, nan, pad;  // keys of the weights c produced for the next observation
+  unsigned long long sum;                 // fixed-point weight sum of c's slice
+  double s2, fx[4], px[4];                // ESS / mean sums of c's slice (pushed to CTA 0 only)
 };
 
 // Dynamic shared memory of one CTA, in 4-byte words: X[2][DX][JC], W[2][JC],
@@ -54,13 +64,29 @@ size_t cluster_smem_words(int JC, int P, int TPB) {
   return w;
 }
 
+// Block max / min / NaN of the weights a CTA produced, pushed into slot c of
+// every CTA of the cluster (lanes 0..NC-1 of warp 0 hold the block result).
+template <int TPB>
+__device__ __forceinline__ void push_maxmin(cg::cluster_group& cl, Slot* slots, int c, int NC,
+                                            unsigned int mx, unsigned int mn, unsigned int nn,
+                                            unsigned int* smk) {
+  block_maxmin_u32<TPB>(mx, mn, smk);
+  nn = __syncthreads_or(nn);
+  if ((int)threadIdx.x < NC) {
+    Slot* o = cl.map_shared_rank(slots, (int)threadIdx.x) + c;
+    o->maxkey = mx;
+    o->minkey = mn;
+    o->nan = nn;
+  }
+}
+
 template <class M, int TPB, bool IF2, bool INJ>
 __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
   cg::cluster_group cl = cg::this_cluster();
   constexpr int DX = M::MAXDX;
   constexpr int G = ChildGroup<M::NZ>::G;
   extern __shared__ __align__(16) float smf[];
-  __shared__ CStat stat;
+  __shared__ Slot slots[kMaxCluster];
   __shared__ typename M::Consts csh;
   __shared__ uint64_t s_scan[TPB / 32 + 1];
   __shared__ unsigned int smk[2 * (TPB / 32)];
@@ -103,6 +129,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     Obs<M> ob;
     ob.load(a, u, 0);
     float* logw0 = a.logw ? a.logw + (size_t)f * a.T * J : nullptr;
+    unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
     for (int l = threadIdx.x; l < nc; l += TPB) {
       const int k = base + l;
       float x[DX];
@@ -134,9 +161,11 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
 #pragma unroll
       for (int d = 0; d < DX; ++d) X[0][d * JC + l] = x[d];
       W[0][l] = w;
+      accum_maxmin(w, mx, mn, nn);
       if (logw0) logw0[k] = w;
     }
     if (c == 0 && threadIdx.x == 0) a.loglik[f] = 0.0;
+    push_maxmin<TPB>(cl, slots, c, NC, mx, mn, nn, smk);
   }
   cl.sync();
 
@@ -147,18 +176,12 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     const int pc = t & 1, pn = pc ^ 1;
     const bool last = (t == Tf - 1);
     const float* Wc = W[pc];
+    // the next observation, fetched now so its latency hides behind phase A
+    Obs<M> ob;
+    if (!last) ob.load(a, u, t + 1);
+    const float coolt = (IF2 && !last) ? a.cool[(size_t)u * a.T + t + 1] : 0.0f;
 
-    // 1. max / min / NaN of the swarm
-    unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
-    for (int l = threadIdx.x; l < nc; l += TPB) accum_maxmin(Wc[l], mx, mn, nn);
-    block_maxmin_u32<TPB>(mx, mn, smk);
-    nn = __syncthreads_or(nn);
-    if (threadIdx.x == 0) {
-      stat.maxkey = mx;
-      stat.minkey = mn;
-      stat.nan = nn;
-    }
-    cl.sync();
+    // A. max / min / NaN of the swarm from every producer's slot
     Acc acc;
     acc.maxkey = 0u;
     acc.minkey = 0xffffffffu;
@@ -168,17 +191,16 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     acc.pad2 = 0.0;
     for (int d = 0; d < 4; ++d) { acc.fx[d] = 0.0; acc.px[d] = 0.0; }
     for (int r = 0; r < NC; ++r) {
-      const CStat* o = cl.map_shared_rank(&stat, r);
-      acc.maxkey = max(acc.maxkey, o->maxkey);
-      acc.minkey = min(acc.minkey, o->minkey);
-      acc.nan |= o->nan;
+      acc.maxkey = max(acc.maxkey, slots[r].maxkey);
+      acc.minkey = min(acc.minkey, slots[r].minkey);
+      acc.nan |= slots[r].nan;
     }
     const bool nanf = acc.nan != 0;
     const float Mx = keyf(acc.maxkey);
     const bool collapsed = !nanf && Mx == -INFINITY;
     const bool qc = nanf || Mx == -INFINITY;
 
-    // 2. fixed-point weights of the slice: totals and this thread's prefix
+    // fixed-point weights of the slice: totals and this thread's prefix
     uint64_t qs = 0;
     double s2 = 0.0, fx[DX], px[DX];
 #pragma unroll
@@ -199,31 +221,37 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     uint64_t btot;
     const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
     if (want_sums) {
+      Slot* o0 = cl.map_shared_rank(slots, 0) + c;
       const double b2 = block_sum_f64<TPB>(s2, sd);
-      if (threadIdx.x == 0) stat.s2 = b2;
+      if (threadIdx.x == 0) o0->s2 = b2;
 #pragma unroll
       for (int d = 0; d < DX; ++d) {
         const double bf = block_sum_f64<TPB>(fx[d], sd);
         const double bp = block_sum_f64<TPB>(px[d], sd);
-        if (threadIdx.x == 0) { stat.fx[d] = bf; stat.px[d] = bp; }
+        if (threadIdx.x == 0) { o0->fx[d] = bf; o0->px[d] = bp; }
       }
     }
-    if (threadIdx.x == 0) stat.sum = btot;
+    if ((int)threadIdx.x < NC) (cl.map_shared_rank(slots, (int)threadIdx.x) + c)->sum = btot;
     cl.sync();
+
+    // B. filter total, this slice's prefix, the step's log-likelihood
     uint64_t E = 0, tot = 0;
     for (int r = 0; r < NC; ++r) {
-      const CStat* o = cl.map_shared_rank(&stat, r);
-      if (r < c) E += o->sum;
-      tot += o->sum;
-      if (c == 0 && threadIdx.x == 0 && want_sums) {
-        acc.s2 += o->s2;
-        for (int d = 0; d < DX; ++d) { acc.fx[d] += o->fx[d]; acc.px[d] += o->px[d]; }
-      }
+      const uint64_t v = slots[r].sum;
+      E += (r < c) ? v : 0ull;
+      tot += v;
     }
-    if (c == 0 && threadIdx.x == 0) finalize_step(a, f, t, acc, tot, a.loglik + f);
+    if (c == 0 && threadIdx.x == 0) {
+      if (want_sums)
+        for (int r = 0; r < NC; ++r) {
+          acc.s2 += slots[r].s2;
+          for (int d = 0; d < DX; ++d) { acc.fx[d] += slots[r].fx[d]; acc.px[d] += slots[r].px[d]; }
+        }
+      finalize_step(a, f, t, acc, tot, a.loglik + f);
+    }
     const bool rs = decide_resample(a, acc);
 
-    // 3. first-child offsets of this CTA's parents (global child indices)
+    // first-child offsets of this CTA's parents (global child indices)
     float lt32 = 0.0f;
     if (rs) {
       const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
@@ -243,12 +271,10 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     }
     __syncthreads();
 
-    // 4. children of this CTA's parents, into the owners' shared memory
+    // children of this CTA's parents, into the owners' shared memory
+    unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
     if (nc > 0) {
       const int klo = st[0], khi = st[nc];
-      Obs<M> ob;
-      if (!last) ob.load(a, u, t + 1);
-      const float coolt = (IF2 && !last) ? a.cool[(size_t)u * a.T + t + 1] : 0.0f;
       const float nwc = -pp_logf((float)J);
       int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
       float* logw = (a.logw && !last) ? a.logw + ((size_t)f * a.T + t + 1) * J : nullptr;
@@ -295,6 +321,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
             }
             const float wb = rs ? a.base_rs : (collapsed ? nwc : Wc[l] - lt32);
             const float w = wb + m;
+            accum_maxmin(w, mx, mn, nn);
             const int r = k / JC, lk = k - r * JC;
             float* xr = cl.map_shared_rank(X[pn], r);
 #pragma unroll
@@ -309,7 +336,8 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
         }
       }
     }
-    cl.sync();   // children visible to their owners; nobody leaves while others read its memory
+    if (!last) push_maxmin<TPB>(cl, slots, c, NC, mx, mn, nn, smk);
+    cl.sync();   // children and slots visible to their owners; nobody leaves while others write to it
   }
 }
 
@@ -317,15 +345,81 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
 // host side
 // ---------------------------------------------------------------------------
 
+// Launch attributes: the largest dynamic shared memory any plan asks for and,
+// for 16-CTA clusters, the non-portable cluster size.
+template <class M, bool IF2, bool INJ>
+static bool cluster_attrs() {
+  auto kern = k_cluster<M, kClusterTPB, IF2, INJ>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kResidentSmemMax) != cudaSuccess ||
+      cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return true;
+}
+
+static cudaLaunchConfig_t cluster_config(int NC, int F, size_t smem, cudaStream_t s, cudaLaunchAttribute* at) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(NC, F, 1);
+  cfg.blockDim = dim3(kClusterTPB, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = NC;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+// How many clusters of NC CTAs with `smem` bytes each can be resident at once
+// (cudaOccupancyMaxActiveClusters), cached per kernel, cluster size and size
+// class of the shared memory; 0 when the query fails.
+struct OccEntry {
+  const void* fn;
+  int nc, smem_kb, n;
+};
+static OccEntry g_occ[64];
+static int g_occ_n = 0;
+static std::mutex g_occ_mu;
+
+template <class M, bool IF2, bool INJ>
+static int max_active_clusters(int NC, size_t smem) {
+  auto kern = k_cluster<M, kClusterTPB, IF2, INJ>;
+  const void* fn = reinterpret_cast<const void*>(kern);
+  const int kb = (int)((smem + 4095) / 4096) * 4;
+  {
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    for (int i = 0; i < g_occ_n; ++i)
+      if (g_occ[i].fn == fn && g_occ[i].nc == NC && g_occ[i].smem_kb == kb) return g_occ[i].n;
+  }
+  int n = 0;
+  if (cluster_attrs<M, IF2, INJ>()) {
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = cluster_config(NC, 1, (size_t)kb * 1024, nullptr, at);
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      n = 0;
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_occ_mu);
+  if (g_occ_n < 64) g_occ[g_occ_n++] = OccEntry{fn, NC, kb, n};
+  return n;
+}
+
 // Cluster size and slice: the largest cluster (<= 16 CTAs) that keeps at least
-// 256 particles per CTA (2 CTAs at the least), with a slice that fits one CTA's
-// shared memory.
-template <class M, bool IF2>
-static bool cluster_plan_t(const Args& a, int& NC, int& JC) {
-  for (int n = 16; n >= 2; n >>= 1) {
+// 256 particles per CTA (2 CTAs at the least) and fits the slice in one CTA's
+// shared memory.  With one_wave, also all F filters' clusters resident at once
+// (the automatic choice: a second wave would double the time).
+template <class M, bool IF2, bool INJ>
+static bool cluster_plan_t(const Args& a, bool one_wave, int& NC, int& JC) {
+  for (int n = kMaxCluster; n >= 2; n >>= 1) {
     const int jc = ((a.J + n - 1) / n + 3) & ~3;
     if (jc < 256 && n != 2) continue;
-    if (cluster_smem_words<M, IF2>(jc, a.model.n_params, kClusterTPB) * 4 > (size_t)kResidentSmemMax) continue;
+    const size_t smem = cluster_smem_words<M, IF2>(jc, a.model.n_params, kClusterTPB) * 4;
+    if (smem > (size_t)kResidentSmemMax) continue;
+    if (one_wave && max_active_clusters<M, IF2, INJ>(n, smem) < a.F) continue;
     NC = n;
     JC = jc;
     return true;
@@ -336,33 +430,16 @@ static bool cluster_plan_t(const Args& a, int& NC, int& JC) {
 template <class M, bool IF2, bool INJ>
 static int run_cluster_t(Args& a, cudaStream_t s) {
   int NC = 0, JC = 0;
-  if (!cluster_plan_t<M, IF2>(a, NC, JC)) return PPF_EUNSUPPORTED;
-  constexpr int TPB = kClusterTPB;
-  const size_t smem = cluster_smem_words<M, IF2>(JC, a.model.n_params, TPB) * 4;
-  auto kern = k_cluster<M, TPB, IF2, INJ>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return PPF_ECUDA;
-  if (NC > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
-    return PPF_ECUDA;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(NC, a.F, 1);
-  cfg.blockDim = dim3(TPB, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = NC;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  int nclusters = 0;
-  if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) != cudaSuccess || nclusters < 1) {
-    cudaGetLastError();
+  if (!cluster_plan_t<M, IF2, INJ>(a, true, NC, JC) && !cluster_plan_t<M, IF2, INJ>(a, false, NC, JC))
     return PPF_EUNSUPPORTED;
-  }
+  if (max_active_clusters<M, IF2, INJ>(NC, cluster_smem_words<M, IF2>(JC, a.model.n_params, kClusterTPB) * 4) < 1)
+    return PPF_EUNSUPPORTED;
+  const size_t smem = cluster_smem_words<M, IF2>(JC, a.model.n_params, kClusterTPB) * 4;
+  if (!cluster_attrs<M, IF2, INJ>()) return PPF_ECUDA;
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = cluster_config(NC, a.F, smem, s, at);
   PROF_BEGIN(KIND_CLUSTER);
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, JC);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_cluster<M, kClusterTPB, IF2, INJ>, a, JC);
   PROF_END(KIND_CLUSTER);
   return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
@@ -375,7 +452,8 @@ static int run_cluster_m(Args& a, cudaStream_t s) {
 template <class M, bool IF2>
 static bool fits_m(const Args& a) {
   int NC = 0, JC = 0;
-  return cluster_plan_t<M, IF2>(a, NC, JC);
+  return (a.flags & PPF_F_INJECT) ? cluster_plan_t<M, IF2, true>(a, true, NC, JC)
+                                  : cluster_plan_t<M, IF2, false>(a, true, NC, JC);
 }
 
 template <bool IF2>
@@ -412,6 +490,8 @@ static int run_any(Args& a, cudaStream_t s) {
   }
 }
 
+// True when the automatic choice may use the cluster path: a plan exists with
+// all filters resident in one wave.
 bool cluster_fits(const Args& a, bool if2) {
   if (a.mode == MODE_MOP) return false;
   return if2 ? fits_any<true>(a) : fits_any<false>(a);

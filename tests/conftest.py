@@ -41,8 +41,10 @@ LG2_Q = np.array([[1.0, 1e-4], [1e-4, 1.0]]) / 100
 LG2_R = np.array([[1.0, 0.1], [0.1, 1.0]]) / 10
 
 
-@pytest.fixture(scope="session")
+@pytest.fixture
 def lg2d():
+    """A fresh model per test: methods record results on the object, so a
+    shared one would carry one test's history into the next."""
     import pypomp_b200 as pp
 
     return pp.LG(T=50, Q=LG2_Q, R=LG2_R, key=0)
