@@ -555,6 +555,74 @@ def run_c5(args):
                    "so each perturbed filter runs J=8192 particles = 4 tiles: launch- and latency-bound"})
 
 
+def run_sim(args):
+    """Simulation (ppf_simulate): LG 2-D, 4 parameter sets x 65536 replicates x
+    T = 1000 (X 2.1 GB + Y 2.1 GB written per step, larger than L2), plus the
+    Ricker model (Poisson draws) on the same shape as a second figure."""
+    import torch
+
+    import pypomp_b200 as pp
+    from pypomp_b200 import _ffi
+    from pypomp_b200 import functional as F
+
+    Fs, nsim, Ts = 4, 65536, 1000
+    m = pp.LG(T=Ts, Q=LG_Q, R=LG_R, key=0)
+    st = m.to_struct()
+    th = np.repeat(m.theta.to_array(m.canonical_param_names).astype(np.float32), Fs, 0)
+    keys = np.arange(1, Fs + 1, dtype=np.uint64)
+    stream = torch.cuda.current_stream()
+    out = {}
+
+    def fn():
+        out["xy"] = F.simulate(st, th, nsim, keys, return_torch=True)
+
+    ms, clk = _timed(fn, args.steps, args.warmup, stream)
+    torch.cuda.synchronize()
+    _ffi.profile_begin()
+    fn()
+    prof = _ffi.profile_end()
+    k_ms, k_n = prof["simulate"]
+    steps = Fs * nsim * Ts
+    value = steps / (ms / 1e3)
+    bytes_per_step = (2 + 2) * 4              # X (dx = 2) and Y (dy = 2) written, float32
+    achieved = bytes_per_step * steps / (k_ms / k_n / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    # end to end: host parameters in, both arrays back to host memory
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        X, Y = F.simulate(st, th, nsim, keys)
+    e2e_s = (time.perf_counter() - t0) / max(1, args.steps // 2)
+    rk = pp.Ricker(T=Ts, key=0)
+    rth = np.repeat(rk.theta.to_array(rk.canonical_param_names).astype(np.float32), Fs, 0)
+    rms, _ = _timed(lambda: F.simulate(rk.to_struct(), rth, nsim, keys, return_torch=True),
+                    args.steps, args.warmup, stream)
+    cpu = {}
+    if not args.skip_cpu:
+        from oracle import cora
+
+        t0 = time.perf_counter()
+        cora.simulate(1, 2, 2, th[:1], 256, Ts, keys[:1])
+        cs = time.perf_counter() - t0
+        cpu = {"value": 256 * Ts / cs, "unit": "trajectory-steps/s", "cores": 1, "kind": "port",
+               "sample": "1 parameter set x 256 replicates x T=1000, oracle/ppf_oracle.c single thread"}
+    print(json.dumps({
+        "metric": "trajectory-steps/s (simulate)", "value": value, "unit": "trajectory-steps/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "LG 2-D simulate, 4 parameter sets x 65536 replicates x T=1000",
+                   "l2": "outputs (4.2 GB per step) larger than L2"},
+        "e2e": {"value": steps / e2e_s, "unit": "trajectory-steps/s", "api": "functional.simulate",
+                "h2d_bytes_per_step": int(th.nbytes + keys.nbytes),
+                "d2h_bytes_per_step": int(4 * Fs * nsim * ((Ts + 1) * 2 + Ts * 2))},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "k_simulate",
+                     "peak_source": peak_kind},
+        "ricker": {"value": steps / (rms / 1e3), "ms_per_step": rms, "unit": "trajectory-steps/s"},
+        "cpu_baseline": cpu or None, "clocks": clk, "gpu_launches": k_n * args.steps}))
+
+
 def run_profile_case(args):
     """A small case of the same kernels for ncu captures: the headline model
     and J, 24 seeds (state 2 x 24 x 262144 x 12 B = 151 MB, larger than L2),
@@ -587,11 +655,11 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="stream-path tile (0 = automatic)")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch the step loop directly instead of replaying it as a CUDA graph")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "sim"],
                     help="c2 (default) is the headline line; c1/c3/c4 print their own lines")
     args = ap.parse_args()
     if args.config != "c2" and args.impl == "ours" and not args.profile_case:
-        {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args)
+        {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "sim": run_sim}[args.config](args)
         return
     if args.profile_case:
         run_profile_case(args)

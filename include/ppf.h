@@ -247,7 +247,7 @@ int ppf_workspace_status(const void* workspace, void* stream);
  * the summed milliseconds ms[k] and launch count count[k].  Kinds: 0 init,
  * 1 weight-sum + lookback, 2 resample + propagate, 3 resident filter,
  * 4 plain-path step (four kernels), 5..8 MOP forward / recompute / adjoint /
- * IF2.  Not reentrant. */
+ * IF2, 9 cluster filter, 10 simulation.  Not reentrant. */
 int ppf_profile_begin(void);
 int ppf_profile_end(double* ms, int* count, int n);
 
@@ -265,6 +265,33 @@ int ppf_profile_end(double* ms, int* count, int n);
  * before any stream capture; the call synchronises the stream. */
 #define PPF_NOALLOC_SCRATCH_BYTES (16u << 20)
 int ppf_pfilter_noalloc(const ppf_pfilter_desc* d, void* stream);
+
+/* Simulated trajectories of the model: for each parameter set f and replicate
+ * k, the initial state (rinit), then for each of the T observation times one
+ * process step (rproc) and a draw of the observation (rmeas).  Replaces
+ * _simulate_internal / _simulate_helper (pypomp/core/algorithms/simulate.py:15-142),
+ * vmapped over parameter sets by functional.simulate
+ * (pypomp/functional/simulate.py:8-72) and called by Pomp.simulate
+ * (pypomp/core/estimation_mixin.py:1101-1222).  Output layouts are the
+ * reference's: X[f][k][t][:] for t = 0..T (t = 0 the initial state) and
+ * Y[f][k][t][:] for t = 0..T-1.  Replicate k of parameter set f draws from
+ * the key seeds[f]: process normals as the filters' particle k does, the
+ * observation's normals / counts from the measurement streams of
+ * include/ppf_sample.h.  Ricker counts are Poisson draws (inversion below a
+ * mean of 10, Hoermann's PTRS above). */
+typedef struct ppf_simulate_desc {
+  ppf_model model;
+  int32_t F;               /* parameter sets, 1..65535 */
+  int32_t nsim;            /* replicates per parameter set, >= 1 */
+  int32_t T;               /* observation times, >= 0 */
+  uint32_t flags;          /* PPF_F_EST: theta on the estimation scale */
+  const float* theta;      /* [F][P] natural scale (estimation scale with PPF_F_EST) */
+  const uint64_t* seeds;   /* [F] one key per parameter set */
+  float* X;                /* out [F][nsim][T+1][dx] */
+  float* Y;                /* out [F][nsim][T][dy] (may be NULL when T == 0) */
+} ppf_simulate_desc;
+
+int ppf_simulate(const ppf_simulate_desc* d, void* stream);
 
 /* Human-readable message for a return code (static storage). */
 const char* ppf_error_string(int code);

@@ -38,6 +38,12 @@ class _IF2Desc(ctypes.Structure):
                            "inj_u", "loglik", "cll", "anc", "workspace")] + [("ws_bytes", ctypes.c_size_t)]
 
 
+class _SimDesc(ctypes.Structure):
+    _fields_ = [("model", _Model), ("F", ctypes.c_int32), ("nsim", ctypes.c_int32),
+                ("T", ctypes.c_int32), ("flags", ctypes.c_uint32)] + [
+        (n, _vp) for n in ("theta", "seeds", "X", "Y")]
+
+
 def lib():
     if not _SO.exists():
         raise ImportError(f"oracle library missing: {_SO} (run `make -C oracle`)")
@@ -56,6 +62,12 @@ def lib():
     L.ppfo_philox.argtypes = [_vp, _vp, _vp]
     L.ppfo_normals.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                ctypes.c_int, _vp]
+    L.ppfo_simulate.argtypes = [ctypes.POINTER(_SimDesc)]
+    L.ppfo_simulate.restype = ctypes.c_int
+    L.ppfo_poisson.argtypes = [ctypes.c_float, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
+    L.ppfo_poisson.restype = ctypes.c_float
+    L.ppfo_logfact.argtypes = [ctypes.c_float]
+    L.ppfo_logfact.restype = ctypes.c_float
     return L
 
 
@@ -265,3 +277,30 @@ def normals(seed, j, s, tag, n):
     z = np.zeros(n, np.float32)
     _L().ppfo_normals(int(seed), int(j), int(s), int(tag), int(n), _p(z))
     return z
+
+
+def simulate(kind, dx, dy, theta_f, nsim, T, seeds, *, dt=0.0, est=False):
+    """Trajectories of F parameter sets x nsim replicates (``ppfo_simulate``):
+    returns X (F, nsim, T+1, dx) and Y (F, nsim, T, dy) as float32."""
+    theta_f = np.ascontiguousarray(np.atleast_2d(theta_f), dtype=np.float32)
+    F, P = theta_f.shape
+    seeds = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).reshape(F))
+    X = np.zeros((F, nsim, T + 1, dx), np.float32)
+    Y = np.zeros((F, nsim, T, dy), np.float32)
+    d = _SimDesc()
+    d.model = _Model(kind, dx, dy, P, dt, 0)
+    d.F, d.nsim, d.T, d.flags = F, nsim, T, (1 << 7) if est else 0
+    d.theta, d.seeds, d.X, d.Y = _p(theta_f), _p(seeds), _p(X), _p(Y)
+    rc = _L().ppfo_simulate(ctypes.byref(d))
+    if rc != 0:
+        raise RuntimeError(f"ppfo_simulate returned {rc}")
+    return X, Y
+
+
+def poisson(lam, seed, k, s):
+    """One draw of the shared Poisson sampler (include/ppf_sample.h)."""
+    return float(_L().ppfo_poisson(float(lam), int(seed), int(k), int(s)))
+
+
+def logfact(k):
+    return float(_L().ppfo_logfact(float(k)))

@@ -12,6 +12,8 @@
  *   _perfilter_internal / scan body     pypomp/core/algorithms/mif.py:88-258
  *   _resampler_thetas                   pypomp/core/algorithms/helpers.py:103-141
  *   LG _rinit/_rproc/_dmeas             pypomp/models/linear_gaussian.py:139-177
+ *   LG _rmeas                           pypomp/models/linear_gaussian.py:180-191
+ *   _simulate_internal / _helper        pypomp/core/algorithms/simulate.py:15-142
  * -- but with the arithmetic definitions of include/ppf.h: float32 model math
  * in a fixed order, ppf_detmath.h elementary functions, the fixed-point CDF
  * summed sequentially in uint64, and ancestors found by a sequential
@@ -31,6 +33,7 @@
 #include "ppf.h"
 #include "ppf_detmath.h"
 #include "ppf_philox.h"
+#include "ppf_sample.h"
 
 #define LOG2PI_F 1.83787706640934548356f
 
@@ -42,7 +45,7 @@ typedef unsigned __int128 u128;
 
 typedef struct {
   int kind, dx, dy;
-  float A[16], C[16], LQ[16], L[16], Linv[4], X0[4], c0;          /* LG */
+  float A[16], C[16], LQ[16], L[16], Linv[4], X0[4], c0, LR[16];  /* LG */
   float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, svc0, kdt, xsq; /* SV */
   float r, sigma, phi, N0;                                         /* Ricker */
 } consts_t;
@@ -59,7 +62,7 @@ static void prepare(consts_t* c, const float* th, const ppf_model* m, int est) {
   if (m->kind == PPF_MODEL_LG) {
     const int dx = m->dx, dy = m->dy;
     int p = 0;
-    float LR[16] = {0};
+    float* LR = c->LR;
     for (int i = 0; i < dx; ++i)
       for (int k = 0; k < dx; ++k) c->A[i * 4 + k] = th[p++];
     for (int i = 0; i < dy; ++i)
@@ -618,6 +621,67 @@ int ppfo_perfilter(const ppf_perfilter_desc* d, int nthreads) {
   for (int i = 0; i < nthreads; ++i) pthread_join(th[i], NULL);
   return PPF_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Simulation                                                               */
+/* ------------------------------------------------------------------------ */
+
+/* Observation draw of replicate k at step s (linear_gaussian.py:180-191 for
+ * LG: y = C x + L_R w; SV: the conditional normal of the return given eps;
+ * Ricker: Poisson(phi N)). */
+static void rmeas(const consts_t* c, const float* x, uint64_t seed, uint32_t k, uint32_t s, float* y) {
+  if (c->kind == PPF_MODEL_LG) {
+    float w[4];
+    pp_normals(seed, k, s, PPF_TAG_MEASURE, c->dy, w);
+    for (int i = 0; i < c->dy; ++i) {
+      float a = 0.0f;
+      for (int q = 0; q < c->dx; ++q) a = fmaf(c->C[i * 4 + q], x[q], a);
+      for (int l = 0; l <= i; ++l) a = fmaf(c->LR[i * 4 + l], w[l], a);
+      y[i] = a;
+    }
+  } else if (c->kind == PPF_MODEL_SV) {
+    float w[1];
+    pp_normals(seed, k, s, PPF_TAG_MEASURE, 1, w);
+    const float sd = pp_expf(0.5f * x[0]) * c->sqdt;
+    const float mean = fmaf(c->rho * sd, x[1], c->mudt);
+    y[0] = fmaf(c->rhoc * sd, w[0], mean);
+  } else {
+    y[0] = pp_poisson(c->phi * x[0], seed, k, s);
+  }
+}
+
+/* Trajectories of F parameter sets x nsim replicates (all pointers HOST
+ * memory, layouts of ppf_simulate_desc): rinit from the process normals of
+ * step 0, then per observation t the process normals of step t + 1 (rproc)
+ * and the measurement draws of step t + 1 (rmeas). */
+int ppfo_simulate(const ppf_simulate_desc* d) {
+  if (!d || d->F < 1 || d->nsim < 1 || d->T < 0 || !d->X || (d->T > 0 && !d->Y)) return PPF_EINVAL;
+  const int dx = d->model.dx, dy = d->model.dy, P = d->model.n_params;
+  for (int f = 0; f < d->F; ++f) {
+    consts_t c;
+    prepare(&c, d->theta + (size_t)f * P, &d->model, (d->flags & PPF_F_EST) != 0);
+    const uint64_t seed = d->seeds[f];
+    for (int k = 0; k < d->nsim; ++k) {
+      float* X = d->X + ((size_t)f * d->nsim + k) * (size_t)(d->T + 1) * dx;
+      float* Y = d->Y ? d->Y + ((size_t)f * d->nsim + k) * (size_t)d->T * dy : NULL;
+      float x[4], z[4];
+      const int n0 = n_init(&c), n1 = n_step(&c);
+      if (n0 > 0) pp_normals(seed, (uint32_t)k, 0u, PPF_TAG_PROCESS, n0, z);
+      rinit(&c, z, x);
+      for (int i = 0; i < dx; ++i) X[i] = x[i];
+      for (int t = 0; t < d->T; ++t) {
+        pp_normals(seed, (uint32_t)k, (uint32_t)(t + 1), PPF_TAG_PROCESS, n1, z);
+        rproc(&c, x, z);
+        rmeas(&c, x, seed, (uint32_t)k, (uint32_t)(t + 1), Y + (size_t)t * dy);
+        for (int i = 0; i < dx; ++i) X[(size_t)(t + 1) * dx + i] = x[i];
+      }
+    }
+  }
+  return PPF_OK;
+}
+
+float ppfo_poisson(float lam, uint64_t seed, uint32_t k, uint32_t s) { return pp_poisson(lam, seed, k, s); }
+float ppfo_logfact(float k) { return pp_logfact(k); }
 
 /* Elementary functions and Philox, exported for the tests that pin them. */
 float ppfo_expf(float x) { return pp_expf(x); }

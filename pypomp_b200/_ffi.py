@@ -49,6 +49,7 @@ EXPORTED = (
     "ppf_autotune",
     "ppf_workspace_status",
     "ppf_pfilter_noalloc",
+    "ppf_simulate",
     "ppf_profile_begin",
     "ppf_profile_end",
     "ppf_error_string",
@@ -161,6 +162,20 @@ class PerfilterDesc(ctypes.Structure):
     ]
 
 
+class SimulateDesc(ctypes.Structure):
+    _fields_ = [
+        ("model", PpfModel),
+        ("F", ctypes.c_int32),
+        ("nsim", ctypes.c_int32),
+        ("T", ctypes.c_int32),
+        ("flags", ctypes.c_uint32),
+        ("theta", _vp),
+        ("seeds", _vp),
+        ("X", _vp),
+        ("Y", _vp),
+    ]
+
+
 class PpfError(RuntimeError):
     """A non-zero return code from libppf.so."""
 
@@ -195,6 +210,8 @@ def _load():
     lib.ppf_pfilter_noalloc.restype = ctypes.c_int
     lib.ppf_autotune.argtypes = [ctypes.POINTER(PfilterDesc), _vp, ctypes.POINTER(ctypes.c_int)]
     lib.ppf_autotune.restype = ctypes.c_int
+    lib.ppf_simulate.argtypes = [ctypes.POINTER(SimulateDesc), _vp]
+    lib.ppf_simulate.restype = ctypes.c_int
     lib.ppf_workspace_status.argtypes = [_vp, _vp]
     lib.ppf_workspace_status.restype = ctypes.c_int
     lib.ppf_profile_begin.argtypes = []
@@ -213,7 +230,7 @@ LIB_PATH = str(_LIB_PATH)
 
 
 KIND_NAMES = ("init", "sum_lookback", "resample_propagate", "resident", "plain_step",
-              "mop_forward", "mop_recompute", "mop_adjoint", "if2")
+              "mop_forward", "mop_recompute", "mop_adjoint", "if2", "cluster", "simulate")
 
 
 def profile_begin() -> None:

@@ -534,6 +534,15 @@ int ppf_autotune(const ppf_pfilter_desc* d, void* stream, int* best_tile) {
   return PPF_OK;
 }
 
+int ppf_simulate(const ppf_simulate_desc* d, void* stream) {
+  if (!d) return PPF_EINVAL;
+  if (d->F < 1 || d->F > 65535 || d->nsim < 1 || d->T < 0) return PPF_EINVAL;
+  const int rc = check_model(d->model);
+  if (rc) return rc;
+  if (!d->theta || !d->seeds || !d->X || (d->T > 0 && !d->Y)) return PPF_EINVAL;
+  return run_simulate(d, reinterpret_cast<cudaStream_t>(stream));
+}
+
 int ppf_workspace_status(const void* workspace, void* stream) {
   if (!workspace) return PPF_EINVAL;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

@@ -82,7 +82,8 @@ struct Args {
 };
 
 enum { KIND_INIT = 0, KIND_SUM = 1, KIND_RESPROP = 2, KIND_RESIDENT = 3, KIND_PLAIN = 4,
-       KIND_MOP_FWD = 5, KIND_MOP_RECOMP = 6, KIND_MOP_BWD = 7, KIND_IF2 = 8, KIND_CLUSTER = 9, KIND_COUNT = 16 };
+       KIND_MOP_FWD = 5, KIND_MOP_RECOMP = 6, KIND_MOP_BWD = 7, KIND_IF2 = 8, KIND_CLUSTER = 9, KIND_SIMULATE = 10,
+       KIND_COUNT = 16 };
 
 struct Profiler {
   struct Ev { cudaEvent_t a, b; int kind; };
@@ -121,6 +122,8 @@ int run_if2(Args& a, cudaStream_t s);
 // this shape, and the launch
 bool cluster_fits(const Args& a, bool if2);
 int run_cluster(Args& a, bool if2, cudaStream_t s);
+// Trajectories of the built-in models (ppf_simulate.cu); the descriptor is validated.
+int run_simulate(const ppf_simulate_desc* d, cudaStream_t s);
 int reset_accumulators(Args& a, cudaStream_t s);
 size_t resident_smem_bytes(const Args& a);
 

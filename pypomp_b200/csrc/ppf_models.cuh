@@ -6,6 +6,8 @@
 //   rinit  -- pypomp/models/linear_gaussian.py:139 (_rinit)
 //   rproc  -- linear_gaussian.py:151 (_rproc), one Euler step (nstep = 1)
 //   dmeas  -- linear_gaussian.py:166 (_dmeas)
+// plus rmeas (linear_gaussian.py:180-191, _rmeas) for simulation, drawing its
+// noise from the measurement streams of ppf_sample.h.
 // The operation order below is the arithmetic definition that the C oracle
 // (oracle/ppf_oracle.c) restates; float32 throughout, elementary functions
 // from ppf_detmath.h, compiled with -fmad=false so no contraction happens.
@@ -14,6 +16,7 @@
 #include <stdint.h>
 #include "ppf.h"
 #include "ppf_detmath.h"
+#include "ppf_sample.h"
 
 #define PPF_LOG2PI_F 1.83787706640934548356f
 
@@ -40,6 +43,7 @@ struct LG {
     int dx, dy;
     float A[16], C[16], LQ[16], L[16], Linv[4], X0[4];
     float c0;
+    float LR[16];   // the parameter factor of R, as rmeas draws with it
   };
   __device__ static __forceinline__ int ndy(const Consts& c) { return DYS > 0 ? DYS : c.dy; }
   __device__ static void prepare(Consts& c, const float* th, const ppf_model& m, bool est) {
@@ -50,7 +54,7 @@ struct LG {
       for (int k = 0; k < dx; ++k) c.A[i * 4 + k] = th[p++];
     for (int i = 0; i < dy; ++i)
       for (int k = 0; k < dx; ++k) c.C[i * 4 + k] = th[p++];
-    float LR[16];
+    float* LR = c.LR;
     for (int i = 0; i < 16; ++i) { c.LQ[i] = 0.0f; LR[i] = 0.0f; c.L[i] = 0.0f; }
     for (int i = 0; i < dx; ++i)
       for (int k = 0; k <= i; ++k) {
@@ -130,6 +134,24 @@ struct LG {
       }
     }
     return pp_fma(-0.5f, q, c.c0);
+  }
+
+  // y = C x + L_R w, w ~ N(0, I_dy)
+  __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
+                               float* y) {
+    float w[MAXDY];
+    pp_normals(seed, k, s, PPF_TAG_MEASURE, ndy(c), w);
+#pragma unroll
+    for (int i = 0; i < MAXDY; ++i) {
+      if (i < ndy(c)) {
+        float a = 0.0f;
+#pragma unroll
+        for (int q = 0; q < DX; ++q) a = pp_fma(c.C[i * 4 + q], x[q], a);
+#pragma unroll
+        for (int l = 0; l <= i; ++l) a = pp_fma(c.LR[i * 4 + l], w[l], a);
+        y[i] = a;
+      }
+    }
   }
 
   // ---- adjoint (MOP-alpha gradient).  Natural-scale gradient in a padded
@@ -284,6 +306,15 @@ struct SV {
     const float r = (y[0] - mean) / (c.rhoc * sd);
     return pp_fma(-0.5f * r, r, pp_fma(-0.5f, v, c.c0));
   }
+  // r = mu dt + rho sd eps + sqrt(1 - rho^2) sd w,  sd = e^{v/2} sqrt(dt)
+  __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
+                               float* y) {
+    float w[1];
+    pp_normals(seed, k, s, PPF_TAG_MEASURE, 1, w);
+    const float sd = pp_expf(0.5f * x[0]) * c.sqdt;
+    const float mean = pp_fma(c.rho * sd, x[1], c.mudt);
+    y[0] = pp_fma(c.rhoc * sd, w[0], mean);
+  }
 
   // ---- adjoint: natural-scale gradient in canonical order
   // (kappa, theta, xi, rho, mu, v0).
@@ -365,6 +396,11 @@ struct Ricker {
     const float lam = c.phi * x[0];
     if (y[0] == 0.0f) return -lam;
     return pp_fma(y[0], pp_logf(lam), -lam) - ycon;
+  }
+  // y ~ Poisson(phi N)
+  __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
+                               float* y) {
+    y[0] = pp_poisson(c.phi * x[0], seed, k, s);
   }
 
   // ---- adjoint: natural-scale gradient in canonical order (r, sigma, phi, N_0).

@@ -196,6 +196,51 @@ def pfilter(struct: PompStruct, thetas_array, J: int, keys, thresh: float = 0.0,
     return out
 
 
+def simulate(struct: PompStruct, thetas_array, nsim: int, keys, times=None, *, est: bool = False,
+             return_torch: bool = False):
+    """Simulated states and observations (``pypomp/functional/simulate.py:8-72``).
+
+    ``thetas_array`` (n_reps, P) on the natural scale (estimation scale with
+    ``est``), ``keys`` one key per row.  ``times`` only sets the number of
+    observation times, since the built-in models take one process step per
+    observation; it defaults to ``struct.times``.  Returns ``X_sims``
+    (n_reps, nsim, T+1, dx), the initial state first, and ``Y_sims``
+    (n_reps, nsim, T, dy): NumPy arrays, or CUDA tensors with
+    ``return_torch``.  One ``ppf_simulate`` launch per 65535 parameter sets.
+    """
+    torch = _ffi.require_cuda()
+    if int(nsim) < 1:
+        raise ValueError("nsim must be at least 1.")
+    nsim = int(nsim)
+    thetas = np.ascontiguousarray(np.atleast_2d(np.asarray(thetas_array, dtype=np.float32)))
+    n = thetas.shape[0]
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    if keys.shape[0] != n:
+        raise ValueError("keys must hold one key per parameter set")
+    spec = struct.spec
+    if thetas.shape[1] != spec.n_params:
+        raise ValueError(f"thetas_array must have {spec.n_params} columns")
+    T = len(struct.times if times is None else times)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    th_d = torch.from_numpy(thetas).to(dev)
+    seeds_d = torch.from_numpy(keys.view(np.int64).copy()).to(dev)
+    X = torch.empty(n, nsim, T + 1, spec.dx, dtype=torch.float32, device=dev)
+    Y = torch.empty(n, nsim, T, spec.dy, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for f0 in range(0, n, 65535):
+        f1 = min(n, f0 + 65535)
+        d = _ffi.SimulateDesc()
+        d.model = spec.ffi_model()
+        d.F, d.nsim, d.T = f1 - f0, nsim, T
+        d.flags = _ffi.F_EST if est else 0
+        d.theta, d.seeds = _ffi.ptr(th_d[f0:f1]), _ffi.ptr(seeds_d[f0:f1])
+        d.X, d.Y = _ffi.ptr(X[f0:f1]), (_ffi.ptr(Y[f0:f1]) if T > 0 else 0)
+        _ffi.check(_ffi.LIB.ppf_simulate(d, stream), "ppf_simulate")
+    if return_torch:
+        return X, Y
+    return X.cpu().numpy(), Y.cpu().numpy()
+
+
 class MopCall:
     """One batched MOP-alpha evaluation on the device: inputs, outputs and the
     workspace that keeps the forward's saves (ancestors, first-child offsets,

@@ -327,6 +327,53 @@ class Pomp:
             execution_time=(time.time() - start) if track_time else None, key=old_key))
 
     # -- analysis ------------------------------------------------------------
+    def simulate(self, key=None, theta=None, times=None, nsim: int = 1, as_pomp: bool = False):
+        """Simulated states and observations (``pypomp/core/estimation_mixin.py:1101-1222``).
+
+        Returns ``(states_df, obs_df)``, long-format DataFrames with columns
+        ``theta_idx``, ``sim``, ``time`` and one column per state (the initial
+        state at ``t0`` included) or observation variable; with ``as_pomp`` a
+        copy of the model whose ``ys`` is the first replicate of the first
+        parameter set (``nsim`` forced to 1).  One key per parameter set,
+        split from the model's key as the reference does."""
+        import warnings
+
+        from . import functional as F
+
+        if as_pomp:
+            if nsim > 1:
+                warnings.warn(
+                    "as_pomp is True, but nsim > 1. Only 1 simulation will be performed as_pomp overrides nsim.",
+                    UserWarning, stacklevel=2)
+            nsim = 1
+        theta_in = self._prepare_theta_input(theta)
+        thetas = theta_in.to_array(self.canonical_param_names)
+        new_key, _ = self._update_fresh_key(key)
+        keys = pprandom.split(new_key, thetas.shape[0])
+        times_array = self.ys.index.to_numpy(dtype=float) if times is None else np.asarray(times, dtype=float)
+        X, Y = F.simulate(self.to_struct(), thetas, nsim, keys, times=times_array)
+
+        def to_long(vals, times_vec, columns):
+            n_theta, n_sim, n_time, n_feat = vals.shape
+            df = pd.DataFrame(vals.reshape(n_theta * n_sim * n_time, n_feat), columns=pd.Index(columns))
+            df.insert(0, "time", np.tile(np.asarray(times_vec, dtype=float), n_theta * n_sim))
+            df.insert(0, "sim", np.tile(np.repeat(np.arange(n_sim), n_time), n_theta))
+            df.insert(0, "theta_idx", np.repeat(np.arange(n_theta), n_sim * n_time))
+            return df
+
+        times0 = np.concatenate([np.array([self.t0]), times_array])
+        states = to_long(X, times0, self.statenames)
+        obs = to_long(Y, times_array, list(self.ys.columns))
+        if as_pomp:
+            first = obs[(obs["theta_idx"] == 0) & (obs["sim"] == 0)]
+            ys = pd.DataFrame(first.drop(columns=["theta_idx", "sim", "time"]).to_numpy(),
+                              index=pd.Index(first["time"].to_numpy()), columns=self.ys.columns)
+            out = deepcopy(self)
+            out.ys = ys
+            out.theta = theta_in.subset([0])
+            return out
+        return states, obs
+
     def results(self, index: int = -1, ignore_nan: bool = False) -> pd.DataFrame:
         return self.results_history.results(index=index, ignore_nan=ignore_nan)
 

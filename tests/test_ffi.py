@@ -63,3 +63,19 @@ def test_validation_messages_without_gpu(lg2d):
     th = lg2d.theta.to_array(lg2d.canonical_param_names)
     with pytest.raises((ValueError, RuntimeError)):
         F.run_pfilter(st, th, np.array([1], np.uint64), 0)
+
+
+def test_simulate_validation_without_gpu():
+    """ppf_simulate rejects bad descriptors before touching the device."""
+    from pypomp_b200 import _ffi
+
+    d = _ffi.SimulateDesc()
+    d.model = _ffi.PpfModel(_ffi.MODEL_RICKER, 1, 1, 4, 0.0, 0)
+    d.F, d.nsim, d.T = 0, 10, 5
+    assert _ffi.LIB.ppf_simulate(d, None) == _ffi.PPF_EINVAL
+    d.F, d.nsim = 1, 0
+    assert _ffi.LIB.ppf_simulate(d, None) == _ffi.PPF_EINVAL
+    d.nsim = 10
+    assert _ffi.LIB.ppf_simulate(d, None) == _ffi.PPF_EINVAL      # null pointers
+    d.model = _ffi.PpfModel(_ffi.MODEL_RICKER, 1, 1, 3, 0.0, 0)   # wrong parameter count
+    assert _ffi.LIB.ppf_simulate(d, None) == _ffi.PPF_EINVAL
