@@ -97,6 +97,28 @@ PPF_HD void pp_normals(uint64_t seed, uint32_t k, uint32_t s, uint32_t tag, int 
   }
 }
 
+/* pp_normals evaluating only the Box-Muller pairs that particle k uses (a
+ * Philox block serves 4 normals; with n = 1 or 2 the other pair belongs to a
+ * neighbour).  Bit-identical to pp_normals: same words, same pair arithmetic. */
+PPF_HD void pp_normals_own(uint64_t seed, uint32_t k, uint32_t s, uint32_t tag, int n, float* z) {
+  uint32_t cblk = 0xffffffffu, cpair = 0xffffffffu;
+  pp_u32x4 w = {{0u, 0u, 0u, 0u}};
+  float p0 = 0.0f, p1 = 0.0f;
+  for (int r = 0; r < n; ++r) {
+    const uint32_t i = k * (uint32_t)n + (uint32_t)r;
+    if ((i >> 2) != cblk) {
+      cblk = i >> 2;
+      w = pp_philox4x32_10(cblk, s, tag, 0u, (uint32_t)seed, (uint32_t)(seed >> 32));
+    }
+    if ((i >> 1) != cpair) {
+      cpair = i >> 1;
+      const int hi = (int)(cpair & 1u);
+      pp_boxmuller(hi ? w.v[2] : w.v[0], hi ? w.v[3] : w.v[1], &p0, &p1);
+    }
+    z[r] = (i & 1u) ? p1 : p0;
+  }
+}
+
 /* Resampling uniform for step s as a 32-bit fraction (U = u32 * 2^-32). */
 PPF_HD uint32_t pp_resample_u32(uint64_t seed, uint32_t s) {
   const pp_u32x4 w = pp_philox4x32_10(0u, s, PPF_TAG_RESAMPLE, 0u, (uint32_t)seed,

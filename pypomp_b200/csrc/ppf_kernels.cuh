@@ -31,7 +31,7 @@ __device__ __forceinline__ void step_noise(const Args& a, int f, int j, int s, i
       for (int i = 0; i < n; ++i) z[i] = a.inj_z[base + i];
     }
   } else {
-    pp_normals(a.seeds[f], (uint32_t)j, (uint32_t)s, PPF_TAG_PROCESS, n, z);
+    pp_normals_own(a.seeds[f], (uint32_t)j, (uint32_t)s, PPF_TAG_PROCESS, n, z);
   }
 }
 

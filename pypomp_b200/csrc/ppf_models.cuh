@@ -140,7 +140,7 @@ struct LG {
   __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
                                float* y) {
     float w[MAXDY];
-    pp_normals(seed, k, s, PPF_TAG_MEASURE, ndy(c), w);
+    pp_normals_own(seed, k, s, PPF_TAG_MEASURE, ndy(c), w);
 #pragma unroll
     for (int i = 0; i < MAXDY; ++i) {
       if (i < ndy(c)) {
@@ -310,7 +310,7 @@ struct SV {
   __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
                                float* y) {
     float w[1];
-    pp_normals(seed, k, s, PPF_TAG_MEASURE, 1, w);
+    pp_normals_own(seed, k, s, PPF_TAG_MEASURE, 1, w);
     const float sd = pp_expf(0.5f * x[0]) * c.sqdt;
     const float mean = pp_fma(c.rho * sd, x[1], c.mudt);
     y[0] = pp_fma(c.rhoc * sd, w[0], mean);

@@ -34,6 +34,24 @@ struct SimArgs {
   float* Y;
 };
 
+// Copy nlive staged rows of L floats (shared row stride sstride) to global rows
+// of stride gstride.  A warp covers 32 / L rows per pass when L <= 32, so each
+// lane finds its row and offset once per flush rather than per element.
+__device__ __forceinline__ void flush_rows(float* g, size_t gstride, const float* sm, int sstride, int L,
+                                           int nlive) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = kSimTPB / 32;
+  if (L <= 32) {
+    const int rpi = 32 / L;
+    const int rr = lane / L, o = lane - rr * L;
+    if (rr < rpi)
+      for (int r = warp * rpi + rr; r < nlive; r += NW * rpi) g[(size_t)r * gstride + o] = sm[r * sstride + o];
+  } else {
+    for (int r = warp; r < nlive; r += NW)
+      for (int o = lane; o < L; o += 32) g[(size_t)r * gstride + o] = sm[r * sstride + o];
+  }
+}
+
 template <class M>
 __global__ void __launch_bounds__(kSimTPB) k_simulate(SimArgs s) {
   constexpr int DX = M::MAXDX, DYM = M::MAXDY;
@@ -61,17 +79,17 @@ __global__ void __launch_bounds__(kSimTPB) k_simulate(SimArgs s) {
     if (live) {
       if (tau == 0) {
         float z0[M::NZ0 > 0 ? M::NZ0 : 1];
-        if (M::NZ0 > 0) pp_normals(seed, (uint32_t)k, 0u, PPF_TAG_PROCESS, M::NZ0, z0);
+        if (M::NZ0 > 0) pp_normals_own(seed, (uint32_t)k, 0u, PPF_TAG_PROCESS, M::NZ0, z0);
         M::rinit(c, z0, x);
       } else {
         float z[M::NZ];
-        pp_normals(seed, (uint32_t)k, (uint32_t)tau, PPF_TAG_PROCESS, M::NZ, z);
+        pp_normals_own(seed, (uint32_t)k, (uint32_t)tau, PPF_TAG_PROCESS, M::NZ, z);
         M::rproc(c, x, z);
         float y[DYM];
         M::rmeas(c, x, seed, (uint32_t)k, (uint32_t)tau, y);
 #pragma unroll
         for (int i = 0; i < DYM; ++i)
-          if (i < dy) ys[threadIdx.x * YS + slot * DYM + i] = y[i];
+          if (i < dy) ys[threadIdx.x * YS + slot * dy + i] = y[i];
       }
 #pragma unroll
       for (int d = 0; d < DX; ++d) xs[threadIdx.x * XS + slot * DX + d] = x[d];
@@ -79,21 +97,12 @@ __global__ void __launch_bounds__(kSimTPB) k_simulate(SimArgs s) {
     if (slot == kSimChunk - 1 || tau == s.T) {
       __syncthreads();
       // states of time points tb..tau, one contiguous run per replicate
-      const int LX = (tau - tb + 1) * DX;
-      for (int e = threadIdx.x; e < nlive * LX; e += kSimTPB) {
-        const int r = e / LX, o = e - r * LX;
-        Xf[((size_t)r * (s.T + 1) + tb) * DX + o] = xs[r * XS + o];
-      }
+      flush_rows(Xf + (size_t)tb * DX, (size_t)(s.T + 1) * DX, xs, XS, (tau - tb + 1) * DX, nlive);
       // observations of time points max(tb, 1)..tau, i.e. y indices from max(tb, 1) - 1
       const int t0 = tb > 0 ? tb : 1;
-      if (tau >= t0) {
-        const int n = tau - t0 + 1, LY = n * dy, off = (t0 - tb) * DYM;
-        for (int e = threadIdx.x; e < nlive * LY; e += kSimTPB) {
-          const int r = e / LY, o = e - r * LY;
-          const int step = o / dy, i = o - step * dy;
-          Yf[((size_t)r * s.T + (t0 - 1)) * dy + o] = ys[r * YS + off + step * DYM + i];
-        }
-      }
+      if (tau >= t0)
+        flush_rows(Yf + (size_t)(t0 - 1) * dy, (size_t)s.T * dy, ys + (t0 - tb) * dy, YS, (tau - t0 + 1) * dy,
+                   nlive);
       __syncthreads();
       tb = tau + 1;
     }
