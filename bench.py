@@ -623,6 +623,41 @@ def run_sim(args):
         "cpu_baseline": cpu or None, "clocks": clk, "gpu_launches": k_n * args.steps}))
 
 
+def run_pmcmc(args):
+    """PMCMC: 8 chains of the Ricker model (T = 500, J = 4096), adaptive random
+    walk; every iteration filters all chains in one batched launch replayed
+    from a CUDA graph.  Reports particle-steps/s over whole iterations (host
+    proposal and accept step included) and iterations/s."""
+    import pypomp_b200 as pp
+    from pypomp_b200 import functional as F
+    from pypomp_b200.proposals import MVNRWAdaptive
+
+    n, Jc, Tc = 8, 4096, 500
+    m = pp.Ricker(T=Tc, key=0)
+    st = m.to_struct()
+    th = np.repeat(m.theta.to_array(m.canonical_param_names), n, 0)
+    prop = MVNRWAdaptive(rw_sd={"r": 0.02, "sigma": 0.02, "phi": 0.02}, scale_start=20, shape_start=20)
+    keys = np.arange(1, n + 1, dtype=np.uint64)
+    F.pmcmc(st, th, prop, max(args.warmup, 3), Jc, keys)          # warm-up: capture and first replays
+    Mi = max(20, 10 * args.steps)
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        ll, lp, tr, acc = F.pmcmc(st, th, prop, Mi, Jc, keys)
+        wall = time.perf_counter() - t0
+    value = n * Jc * Tc * (Mi + 1) / wall
+    print(json.dumps({
+        "metric": "particle-steps/s (pmcmc)", "value": value, "unit": "particle-steps/s", "n_gpus": 1,
+        "steps": Mi, "warmup": max(args.warmup, 3), "ms_per_step": wall / (Mi + 1) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "Ricker PMCMC, 8 chains x J=4096 x T=500, adaptive MVN random walk"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "api": "functional.pmcmc (host loop)",
+                "h2d_bytes_per_step": int(n * (4 * 4 + 8)), "d2h_bytes_per_step": int(8 * n)},
+        "iterations_per_s": (Mi + 1) / wall, "acceptance": (acc / Mi).tolist(),
+        "roofline": None, "clocks": clk.summary(),
+        "note": "wall clock of whole iterations; the filters run on the cluster path"}))
+
+
 def run_profile_case(args):
     """A small case of the same kernels for ncu captures: the headline model
     and J, 24 seeds (state 2 x 24 x 262144 x 12 B = 151 MB, larger than L2),
@@ -655,11 +690,11 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="stream-path tile (0 = automatic)")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch the step loop directly instead of replaying it as a CUDA graph")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "sim"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "sim", "pmcmc"],
                     help="c2 (default) is the headline line; c1/c3/c4 print their own lines")
     args = ap.parse_args()
     if args.config != "c2" and args.impl == "ours" and not args.profile_case:
-        {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "sim": run_sim}[args.config](args)
+        {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "sim": run_sim, "pmcmc": run_pmcmc}[args.config](args)
         return
     if args.profile_case:
         run_profile_case(args)

@@ -17,3 +17,5 @@ from .optim import SGD, Adam, LearningRate, RWSigma  # noqa: F401
 
 __all__ = ["LG", "SV", "Ricker", "Pomp", "PompParameters", "functional", "random",
            "logmeanexp", "logmeanexp_se"]
+from . import proposals  # noqa: F401
+from .proposals import MVNDiagRW, MVNRWAdaptive, MVNRWFull  # noqa: F401

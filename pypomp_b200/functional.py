@@ -241,6 +241,141 @@ def simulate(struct: PompStruct, thetas_array, nsim: int, keys, times=None, *, e
     return X.cpu().numpy(), Y.cpu().numpy()
 
 
+class PfilterCall:
+    """Repeated ``ppf_pfilter`` calls of one shape: device buffers, workspace
+    and descriptor made once, the launch sequence captured into a CUDA graph
+    on the first call (``PPF_F_GRAPH``) and replayed after copying the new
+    parameters and keys into the same buffers.  Used by :func:`pmcmc`, which
+    filters every chain once per iteration."""
+
+    def __init__(self, struct: PompStruct, F: int, J: int, *, thresh: float = 0.0, est: bool = False):
+        torch = _ffi.require_cuda()
+        if J < 1:
+            raise ValueError("J should be greater than 0.")
+        if J > _ffi.PPF_MAX_J:
+            raise ValueError(f"J must be at most {_ffi.PPF_MAX_J}.")
+        self.torch = torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        spec = struct.spec
+        self.P = spec.n_params
+        ys_d, ycon_d, Tu_d, U, T = _device_inputs(torch, struct, dev)
+        self.keep = [ys_d, ycon_d, Tu_d]
+        self.theta = torch.zeros(F, self.P, dtype=torch.float32, device=dev)
+        self.seeds = torch.zeros(F, dtype=torch.int64, device=dev)
+        self.ll = torch.zeros(F, dtype=torch.float64, device=dev)
+        d = _ffi.PfilterDesc()
+        d.model = spec.ffi_model()
+        d.J, d.F, d.T, d.U = J, F, T, U
+        d.path = _ffi.env_path()
+        d.flags = (_ffi.F_EST if est else 0) | _ffi.F_GRAPH
+        d.thresh = float(max(0.0, thresh))
+        d.theta, d.ys, d.ycon = _ffi.ptr(self.theta), _ffi.ptr(ys_d), _ffi.ptr(ycon_d)
+        d.T_u, d.seeds, d.loglik = _ffi.ptr(Tu_d), _ffi.ptr(self.seeds), _ffi.ptr(self.ll)
+        self.ws = torch.empty(max(int(_ffi.LIB.ppf_pfilter_workspace_bytes(d)), 256), dtype=torch.uint8,
+                              device=dev)
+        d.workspace, d.ws_bytes = _ffi.ptr(self.ws), self.ws.numel()
+        self.d = d
+        self.stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def __call__(self, theta_f: np.ndarray, seeds_f: np.ndarray) -> np.ndarray:
+        torch = self.torch
+        self.theta.copy_(torch.from_numpy(np.ascontiguousarray(theta_f, dtype=np.float32)))
+        self.seeds.copy_(torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).copy()))
+        _ffi.check(_ffi.LIB.ppf_pfilter(self.d, self.stream), "ppf_pfilter")
+        _ffi.check(_ffi.LIB.ppf_workspace_status(self.d.workspace, self.stream), "ppf_pfilter")
+        return self.ll.cpu().numpy().copy()
+
+
+def _split4(keys: np.ndarray):
+    from . import random as pprandom
+
+    out = np.stack([pprandom.split(k, 4) for k in keys])
+    return out[:, 0], out[:, 1], out[:, 2], out[:, 3]
+
+
+def pmcmc(struct: PompStruct, thetas_array, proposal, M: int, J: int, keys, thresh: float = 0.0,
+          dprior=None):
+    """Particle marginal Metropolis-Hastings (``pypomp/functional/pmcmc.py:18-113``,
+    ``pypomp/core/algorithms/pmcmc.py:30-163``; Andrieu, Doucet & Holenstein 2010).
+
+    One chain per row of ``thetas_array`` (natural scale), each with its own
+    key.  Chains move on the estimation scale; the acceptance ratio uses the
+    prior there (``dprior`` of the natural parameters plus the log-Jacobian of
+    the back-transform).  Per chain and iteration the key splits four ways
+    (carry, proposal, filter, acceptance), as the reference's scan does.  All
+    chains' particle filters of one iteration run as one batched
+    ``ppf_pfilter`` launch, replayed from a CUDA graph.
+
+    ``dprior`` is a callable on a dict of natural-scale parameters returning
+    a log density (``None``: flat).  Returns ``(loglik_traces (n, M+1),
+    log_prior_traces (n, M+1), theta_traces (n, M+1, d), accepts (n,))``,
+    traces on the natural scale, the log-prior recomputed there without the
+    Jacobian.
+    """
+    if int(M) < 1:
+        raise ValueError("M must be >= 1.")
+    thetas = np.atleast_2d(np.asarray(thetas_array, dtype=np.float64))
+    call = PfilterCall(struct, thetas.shape[0], J, thresh=thresh, est=True)
+    return _pmcmc_run(struct.spec, thetas, proposal, int(M), keys, call, dprior)
+
+
+def _pmcmc_run(spec, thetas, proposal, M: int, keys, loglik_fn, dprior=None):
+    """The chains of :func:`pmcmc` given ``loglik_fn(theta_est (n, d), keys (n,))``
+    -> log-likelihoods (n,): the batched GPU filter in the product, the C
+    oracle's filter in the CPU tests."""
+    from . import random as pprandom
+
+    names = list(spec.param_names)
+    thetas = np.atleast_2d(np.asarray(thetas, dtype=np.float64))
+    n, d = thetas.shape
+    if d != len(names):
+        raise ValueError(f"thetas_array must have {len(names)} columns")
+    keys = np.asarray(keys, dtype=np.uint64).reshape(n)
+    prop = proposal.canonicalize(names)
+
+    def prior_nat(th):
+        if dprior is None:
+            return 0.0
+        return float(dprior({nm: float(v) for nm, v in zip(names, th)}))
+
+    def prior_est(th_est):
+        return prior_nat(spec.from_est(th_est)) + float(spec.log_det_jac_from_est(th_est))
+
+    call = loglik_fn
+    th_cur = spec.to_est(thetas)
+    carry = np.empty(n, np.uint64)
+    pf0 = np.empty(n, np.uint64)
+    for c in range(n):
+        carry[c], pf0[c] = pprandom.split(keys[c], 2)
+    ll_cur = call(th_cur, pf0)
+    lp_cur = np.array([prior_est(t) for t in th_cur])
+    state = [prop.init_state(t) for t in th_cur]
+    accepts = np.zeros(n, np.int64)
+    ll_tr = np.empty((n, M + 1))
+    lp_tr = np.empty((n, M + 1))
+    th_tr = np.empty((n, M + 1, d))
+    ll_tr[:, 0], lp_tr[:, 0], th_tr[:, 0] = ll_cur, lp_cur, th_cur
+    for it in range(1, M + 1):
+        carry, k_prop, k_pf, k_acc = _split4(carry)
+        th_prop = np.empty_like(th_cur)
+        for c in range(n):
+            th_prop[c], state[c] = prop.step(state[c], th_cur[c], k_prop[c], it, int(accepts[c]))
+        lp_prop = np.array([prior_est(t) for t in th_prop])
+        ll_prop = call(th_prop, k_pf)
+        log_alpha = ll_prop + lp_prop - ll_cur - lp_cur
+        u = np.array([np.random.default_rng(int(k)).random() for k in k_acc])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            acc = np.isfinite(log_alpha) & np.isfinite(lp_prop) & (np.log(u) < log_alpha)
+        th_cur = np.where(acc[:, None], th_prop, th_cur)
+        ll_cur = np.where(acc, ll_prop, ll_cur)
+        lp_cur = np.where(acc, lp_prop, lp_cur)
+        accepts += acc
+        ll_tr[:, it], lp_tr[:, it], th_tr[:, it] = ll_cur, lp_cur, th_cur
+    th_nat = spec.from_est(th_tr)
+    lp_nat = np.array([[prior_nat(t) for t in chain] for chain in th_nat])
+    return ll_tr, lp_nat, th_nat, accepts.astype(np.int32)
+
+
 class MopCall:
     """One batched MOP-alpha evaluation on the device: inputs, outputs and the
     workspace that keeps the forward's saves (ancestors, first-child offsets,

@@ -69,6 +69,21 @@ class ModelSpec:
             t[..., list(self.est_atanh)] = np.tanh(t[..., list(self.est_atanh)])
         return t
 
+    def log_det_jac_from_est(self, theta_est: np.ndarray) -> np.ndarray:
+        """log |det d from_est / d theta_est| (the change of variables a prior on
+        the natural scale picks up on the estimation scale; the transforms are
+        element-wise, so the Jacobian is diagonal: d exp(x) = exp(x),
+        d tanh(x) = 1 - tanh(x)^2)."""
+        t = np.asarray(theta_est, dtype=np.float64)
+        out = np.zeros(t.shape[:-1])
+        if self.natural:
+            return out
+        if self.est_log:
+            out = out + t[..., list(self.est_log)].sum(axis=-1)
+        if self.est_atanh:
+            out = out + np.log1p(-np.tanh(t[..., list(self.est_atanh)]) ** 2).sum(axis=-1)
+        return out
+
     def ycon(self, ys: np.ndarray) -> np.ndarray | None:
         """Per-observation constant of dmeas (Ricker: log y!), else None."""
         if self.kind == _ffi.MODEL_RICKER:

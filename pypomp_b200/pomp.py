@@ -77,12 +77,42 @@ class Result:
             df = pd.DataFrame({"theta_idx": np.arange(len(self.theta)), "logLik": logLik,
                                "se": np.atleast_1d(se)})
             return pd.concat([df, pd.DataFrame(self.theta.params(as_list=True))], axis=1)
+        if self.method == "pmcmc":
+            # every iteration (pypomp/core/results/render.py:419-430)
+            df = self._pmcmc_frame()
+            return df.dropna() if ignore_nan else df
         # mif / train: final iteration of the trace
         tr = self.traces()
         last = tr[tr["iteration"] == tr["iteration"].max()].drop(columns=["iteration", "method"])
         return last.reset_index(drop=True)
 
+    def _pmcmc_frame(self) -> pd.DataFrame:
+        ll = np.asarray(self.payload["logLiks"])          # (n, M+1)
+        lp = np.asarray(self.payload["log_prior"])        # (n, M+1)
+        th = np.asarray(self.payload["traces"])           # (n, M+1, P)
+        n, M1 = ll.shape
+        df = pd.DataFrame({"theta_idx": np.repeat(np.arange(n), M1),
+                           "iteration": np.tile(np.arange(M1), n),
+                           "logLik": ll.reshape(-1), "log_prior": lp.reshape(-1)})
+        for p, nm in enumerate(self.payload["param_names"]):
+            df[nm] = th[:, :, p].reshape(-1)
+        return df
+
+    @property
+    def acceptance_rate(self) -> np.ndarray:
+        """Per-chain acceptance rate (pmcmc)."""
+        acc = self.payload.get("accepts")
+        if acc is None:
+            return np.zeros(0)
+        M = self.config.get("M")
+        return np.asarray(acc, float) / float(M) if M else np.zeros(len(acc))
+
     def traces(self) -> pd.DataFrame:
+        if self.method == "pmcmc":
+            df = self._pmcmc_frame()
+            df.insert(2, "method", "pmcmc")
+            df.insert(4, "se", np.nan)
+            return df
         if self.method == "pfilter":
             df = self.to_dataframe()
             df.insert(1, "iteration", 0)
@@ -327,6 +357,40 @@ class Pomp:
             execution_time=(time.time() - start) if track_time else None, key=old_key))
 
     # -- analysis ------------------------------------------------------------
+    def pmcmc(self, J: int, M: int, proposal, dprior=None, key=None, theta=None, thresh: float = 0.0,
+              track_time: bool = True) -> None:
+        """Particle marginal Metropolis-Hastings (``pypomp/core/estimation_mixin.py:823-935``).
+
+        One chain per parameter replicate of ``theta``, one key per chain
+        split from the model's key.  Sets ``self.theta`` to the chains' final
+        parameters with their last log-likelihoods and records a ``pmcmc``
+        result: traces of ``logLik``, ``log_prior`` (natural scale, no
+        Jacobian) and the parameters, plus accept counts."""
+        from . import functional as F
+
+        start = time.time()
+        if J < 1:
+            raise ValueError("J must be >= 1.")
+        if M < 1:
+            raise ValueError("M must be >= 1.")
+        theta_in = deepcopy(self._prepare_theta_input(theta))
+        theta_for_result = deepcopy(theta_in)
+        n = theta_in.num_replicates()
+        if n < 1:
+            raise ValueError("pmcmc requires at least one starting parameter set.")
+        new_key, old_key = self._update_fresh_key(key)
+        names = self.canonical_param_names
+        keys = pprandom.split(new_key, n)
+        ll, lp, th, acc = F.pmcmc(self.to_struct(), theta_in.to_array(names), proposal, M, J, keys,
+                                  thresh=thresh, dprior=dprior)
+        self.theta = PompParameters.from_array(th[:, -1], names)
+        self.theta.logLik = ll[:, -1]
+        self.results_history.add(Result(
+            method="pmcmc", theta=theta_for_result,
+            payload={"logLiks": ll, "log_prior": lp, "traces": th, "param_names": names, "accepts": acc},
+            config={"M": M, "J": J}, execution_time=(time.time() - start) if track_time else None,
+            key=old_key))
+
     def simulate(self, key=None, theta=None, times=None, nsim: int = 1, as_pomp: bool = False):
         """Simulated states and observations (``pypomp/core/estimation_mixin.py:1101-1222``).
 
