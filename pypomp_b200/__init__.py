@@ -13,7 +13,8 @@ from .models import LG, SV, Ricker  # noqa: F401
 from .pomp import ParTrans, Pomp, PompParameters  # noqa: F401
 from .autograd import mop_objective  # noqa: F401
 from .panel import PanelParameters, PanelPomp  # noqa: F401
-from .optim import SGD, Adam, LearningRate, RWSigma  # noqa: F401
+from .optim import (SGD, BFGS, Adam, FullMatrixAdam, LearningRate, Newton, RWSigma,  # noqa: F401
+                    WeightedNewton)
 
 __all__ = ["LG", "SV", "Ricker", "Pomp", "PompParameters", "functional", "random",
            "logmeanexp", "logmeanexp_se"]

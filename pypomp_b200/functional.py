@@ -518,12 +518,24 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
     the MOP value at the current parameters (n_monitors == 1) or the mean of
     ``n_monitors`` particle filters (n_monitors > 1; NaN for 0).  Returns
     ``(neg_logliks (n, M+1), thetas (n, M+1, P))`` with a NaN first entry.
+
+    ``optimizer.ls`` replaces the fixed step by the reference's Armijo
+    backtracking (``train.py:442-500``, :func:`_line_search`) on the particle
+    filter's negative log-likelihood under the iteration's MOP key.  Newton and
+    WeightedNewton get the Hessian of the mean MOP objective as central
+    differences of its gradient under the iteration's Hessian key (common
+    random numbers), all 2P perturbed gradients of all parameter sets in one
+    batched launch (:func:`mop_hessian_fd`).
     """
     from . import random as pprandom
     from .optim import LearningRate, cosine_alpha
 
-    if optimizer.ls:
-        raise NotImplementedError("line search is not supported by the CUDA train loop")
+    from .optim import BFGS, SGD, Adam, FullMatrixAdam, Newton, WeightedNewton
+
+    if n_monitors < 1 and optimizer.ls:
+        raise ValueError("Line search requires at least one monitor")
+    if not isinstance(optimizer, (SGD, Adam, FullMatrixAdam, Newton, WeightedNewton, BFGS)):
+        raise ValueError(f"Optimizer '{optimizer.__class__.__name__}' not supported")
     th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float64)).copy()
     n, P = th.shape
     keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
@@ -556,16 +568,76 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
             pf = run_pfilter(struct, np.repeat(th.astype(np.float32), n_monitors, axis=0),
                              mon.reshape(-1), J, thresh=thresh, est=True)
             nll[:, m + 1] = -pf["loglik"].reshape(n, n_monitors).mean(axis=1)
+        hkeys = np.zeros(n, np.uint64)
         for i in range(n):
-            chain[i] = int(pprandom.split(chain[i])[0])
+            chain[i], hkeys[i] = (int(v) for v in pprandom.split(chain[i]))
         if optimizer.clip_norm is not None:
             grad = np.clip(grad, -optimizer.clip_norm, optimizer.clip_norm)
-        direction, state = optimizer.step(grad, state, m)
+        hess_fn = (lambda: mop_hessian_fd(struct, th, hkeys, J, alpha_m)) if optimizer.needs_hessian else None
+        direction, state = optimizer.step(grad, state, m, compute_hessian_fn=hess_fn, eta_i=eta_arr[m])
         if optimizer.scale:
             direction = direction / np.linalg.norm(direction, axis=-1, keepdims=True)
-        th = th + eta_arr[m] * direction
+        if optimizer.ls:
+            step = _line_search(struct, th, subs, J, thresh, nll[:, m + 1], grad, direction,
+                                float(np.mean(eta_arr[m])), optimizer.max_ls_itn, optimizer.c, 0.5)
+            th = th + step[:, None] * direction
+        else:
+            th = th + eta_arr[m] * direction
         traces[:, m + 1] = th
     return nll, traces
+
+
+def mop_hessian_fd(struct: PompStruct, theta_est, keys, J: int, alpha: float, h: float = 1e-2):
+    """Hessian of the mean MOP-alpha objective at each row of ``theta_est``
+    (n, P) by central differences of its gradient, h_j = h max(1, |theta_j|),
+    every perturbed point under its row's key (common random numbers):
+    one ``ppf_mop`` launch of 2 n P filters.  Returns (n, P, P), symmetrised.
+    (The reference differentiates its estimator twice with jax.hessian,
+    ``ad_helpers.py``; there is no second-order adjoint kernel here.)  The
+    estimator's gradient jumps where a perturbation moves a resampling
+    boundary, so a small h amplifies those jumps; h = 1e-2 averages over them
+    (on LG 1-D with J = 1e5 the diagonal lands within 0.8-1.5x of the exact
+    Kalman Hessian; at h = 1e-3 it is dominated by the jumps)."""
+    th = np.atleast_2d(np.asarray(theta_est, dtype=np.float64))
+    n, P = th.shape
+    T = np.asarray(struct.ys).shape[-2]
+    step = h * np.maximum(1.0, np.abs(th))                       # (n, P)
+    pts = np.repeat(th[:, None, None, :], 2, axis=1).repeat(P, axis=2)   # (n, 2, P, P)
+    idx = np.arange(P)
+    pts[:, 0, idx, idx] += step
+    pts[:, 1, idx, idx] -= step
+    seeds = np.repeat(np.asarray(keys, dtype=np.uint64).reshape(n), 2 * P)
+    res = run_mop(struct, pts.reshape(-1, P).astype(np.float32), seeds, J, alpha, grad=True)
+    g = res["grad"].reshape(n, 2, P, P) / T
+    H = (g[:, 0] - g[:, 1]) / (2.0 * step[:, :, None])           # H[i, j, :] = d grad / d theta_j
+    return 0.5 * (H + np.swapaxes(H, 1, 2))
+
+
+def _line_search(struct, th, keys, J, thresh, curr_obj, grad, direction, eta0, tau, c, frac):
+    """Armijo backtracking of every row at once (``train.py:442-500``, stoch=False):
+    evaluate the particle filter's negative log-likelihood at
+    theta + eta direction under the row's key; while it exceeds
+    curr + eta c <grad, direction> (or is NaN) and fewer than tau reductions
+    were made, eta *= frac.  Rows still searching share one batched launch
+    per round."""
+    n = th.shape[0]
+    eta = np.full(n, eta0)
+    itn = np.zeros(n, np.int64)
+    active = np.ones(n, bool)
+    slope = np.sum(grad * direction, axis=-1)
+    keys = np.asarray(keys, dtype=np.uint64).reshape(n)
+    while active.any():
+        rows = np.nonzero(active)[0]
+        pts = th[rows] + eta[rows, None] * direction[rows]
+        res = run_pfilter(struct, pts.astype(np.float32), keys[rows], J, thresh=thresh, est=True)
+        nxt = -res["loglik"]
+        with np.errstate(invalid="ignore"):
+            cont = (nxt > curr_obj[rows] + eta[rows] * c * slope[rows]) | np.isnan(nxt)
+        more = cont & (itn[rows] < tau)
+        eta[rows] = np.where(more, eta[rows] * frac, eta[rows])
+        itn[rows] += 1
+        active[rows] = more
+    return eta
 
 
 # ---------------------------------------------------------------------------
@@ -995,10 +1067,11 @@ def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optim
     replays external draws for chunk c of iteration m.
     """
     from . import random as pprandom
-    from .optim import LearningRate, cosine_alpha
+    from .optim import SGD, Adam, FullMatrixAdam, LearningRate, cosine_alpha
 
-    if optimizer.ls:
-        raise NotImplementedError("line search is not supported by the CUDA train loop")
+    # as _panel_train_internal (train.py:191-200): these three only; `ls` is not used by panel train
+    if not isinstance(optimizer, (SGD, Adam, FullMatrixAdam)):
+        raise ValueError(f"Optimizer '{optimizer.__class__.__name__}' not supported for panel train")
     spec = struct.spec
     U, Tn = struct.U, struct.ys.shape[1]
     cs = max(1, int(chunk_size))

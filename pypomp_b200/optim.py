@@ -4,8 +4,12 @@ Mirrors the reference's optimiser, learning-rate and random-walk classes that
 sit around the hot path (the math here runs once per iteration on a
 parameter vector; the particle work is in the CUDA library):
 
-* ``SGD``, ``Adam``      -- ``pypomp/core/optimizer.py:95-160`` (update rule,
-                            bias correction, ``clip_norm`` / ``scale`` options)
+* ``SGD``, ``Adam``, ``FullMatrixAdam``, ``BFGS``, ``Newton``, ``WeightedNewton``
+                         -- ``pypomp/core/optimizer.py:95-320`` (update rules,
+                            bias correction, ``clip_norm`` / ``scale`` / ``ls``
+                            options).  Steps take a batch of parameter vectors
+                            (leading dimensions) and treat each row on its own,
+                            as the reference's vmapped train does.
 * ``LearningRate``       -- ``pypomp/core/learning_rate.py`` (per-parameter
                             rates, cosine / geometric / linear / hyperbolic decay)
 * ``RWSigma``            -- ``pypomp/core/rw_sigma.py`` (IF2 random-walk sds,
@@ -35,10 +39,12 @@ class Optimizer:
     c: float = 0.1
     max_ls_itn: int = 10
 
+    needs_hessian = False
+
     def init_state(self, theta: np.ndarray):
         raise NotImplementedError
 
-    def step(self, grad, state, step_num):
+    def step(self, grad, state, step_num, compute_hessian_fn=None, eta_i=None):
         raise NotImplementedError
 
 
@@ -47,7 +53,7 @@ class SGD(Optimizer):
     def init_state(self, theta):
         return ()
 
-    def step(self, grad, state, step_num):
+    def step(self, grad, state, step_num, compute_hessian_fn=None, eta_i=None):
         return -np.asarray(grad, dtype=np.float64), ()
 
 
@@ -61,7 +67,7 @@ class Adam(Optimizer):
         z = np.zeros_like(np.asarray(theta, dtype=np.float64))
         return (z, z.copy())
 
-    def step(self, grad, state, step_num):
+    def step(self, grad, state, step_num, compute_hessian_fn=None, eta_i=None):
         m, v = state
         g = np.asarray(grad, dtype=np.float64)
         m_new = self.beta1 * m + (1 - self.beta1) * g
@@ -69,6 +75,133 @@ class Adam(Optimizer):
         m_hat = m_new / (1 - self.beta1 ** (step_num + 1))
         v_hat = v_new / (1 - self.beta2 ** (step_num + 1))
         return -m_hat / (np.sqrt(v_hat) + self.epsilon), (m_new, v_new)
+
+
+def _rows(a):
+    a = np.asarray(a, dtype=np.float64)
+    return a.reshape(-1, a.shape[-1])
+
+
+def _pinv_sym(h):
+    """Pseudo-inverse of a symmetric matrix (``jnp.linalg.pinv(..., hermitian=True)``)."""
+    w, V = np.linalg.eigh(h)
+    cut = np.finfo(np.float64).eps * h.shape[-1] * (np.max(np.abs(w)) if w.size else 0.0)
+    inv = np.where(np.abs(w) > cut, 1.0 / np.where(np.abs(w) > cut, w, 1.0), 0.0)
+    return (V * inv) @ V.T
+
+
+@dataclass(frozen=True)
+class FullMatrixAdam(Optimizer):
+    """Adam with a full second-moment matrix (``optimizer.py:157-213``):
+    direction = -F_hat^{-1/2} m_hat, F_hat from the outer products of the
+    gradients, the inverse root through an eigendecomposition."""
+
+    beta1: float = 0.9
+    beta2: float = 0.999
+    epsilon: float = 1e-4
+
+    def init_state(self, theta):
+        t = np.asarray(theta, dtype=np.float64)
+        return np.zeros_like(t), np.zeros(t.shape + (t.shape[-1],))
+
+    def step(self, grad, state, step_num, compute_hessian_fn=None, eta_i=None):
+        m, v = state
+        g = np.asarray(grad, dtype=np.float64)
+        shape, P = g.shape, g.shape[-1]
+        m_new = self.beta1 * m + (1 - self.beta1) * g
+        m_hat = m_new / (1 - self.beta1 ** (step_num + 1))
+        v_new = self.beta2 * v + (1 - self.beta2) * (g[..., :, None] * g[..., None, :])
+        F_hat = v_new / (1 - self.beta2 ** (step_num + 1))
+        out = np.empty((int(np.prod(shape[:-1], dtype=int)), P))
+        for i, (Fh, mh) in enumerate(zip(F_hat.reshape(-1, P, P), _rows(m_hat))):
+            w, V = np.linalg.eigh(Fh)
+            out[i] = -(V @ np.diag(1.0 / np.sqrt(np.maximum(w, 0.0) + self.epsilon)) @ V.T) @ mh
+        return out.reshape(shape), (m_new, v_new)
+
+
+@dataclass(frozen=True)
+class BFGS(Optimizer):
+    """Quasi-Newton BFGS (``optimizer.py:216-267``), with the reference's
+    choices: from the third step on, s_k = mean(eta) * (-previous gradient),
+    y_k = grad - previous gradient, the inverse-Hessian update kept only when
+    1 / (y_k . s_k) is finite; earlier steps go along -grad."""
+
+    def init_state(self, theta):
+        t = np.asarray(theta, dtype=np.float64)
+        eye = np.broadcast_to(np.eye(t.shape[-1]), t.shape + (t.shape[-1],)).copy()
+        return eye, np.zeros_like(t)
+
+    def step(self, grad, state, step_num, compute_hessian_fn=None, eta_i=None):
+        if eta_i is None:
+            raise ValueError("BFGS optimizer requires eta_i")
+        hess, prev_grad = state
+        g = np.asarray(grad, dtype=np.float64)
+        shape, P = g.shape, g.shape[-1]
+        if step_num <= 1:
+            return -g, (hess, g)
+        eta_bar = float(np.mean(eta_i))
+        H = hess.reshape(-1, P, P).copy()
+        out = np.empty((H.shape[0], P))
+        for i, (gi, pg) in enumerate(zip(_rows(g), _rows(prev_grad))):
+            s_k = eta_bar * (-pg)
+            y_k = gi - pg
+            with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+                rho = 1.0 / np.dot(y_k, s_k)
+                Hy = H[i] @ y_k
+                new = (H[i] - rho * np.outer(s_k, Hy) - rho * np.outer(Hy, s_k)
+                       + rho * (rho * np.dot(y_k, Hy) + 1.0) * np.outer(s_k, s_k))
+            if np.isfinite(rho):
+                H[i] = new
+            out[i] = -H[i] @ gi
+        return out.reshape(shape), (H.reshape(hess.shape), g)
+
+
+@dataclass(frozen=True)
+class Newton(Optimizer):
+    """Newton-Raphson (``optimizer.py:270-289``): direction = -pinv(H) grad."""
+
+    needs_hessian = True
+
+    def init_state(self, theta):
+        return ()
+
+    def step(self, grad, state, step_num, compute_hessian_fn=None, eta_i=None):
+        if compute_hessian_fn is None:
+            raise ValueError("Newton optimizer requires compute_hessian_fn")
+        g = np.asarray(grad, dtype=np.float64)
+        P = g.shape[-1]
+        H = np.asarray(compute_hessian_fn(), dtype=np.float64).reshape(-1, P, P)
+        out = np.stack([-_pinv_sym(h) @ gi for h, gi in zip(H, _rows(g))])
+        return out.reshape(g.shape), ()
+
+
+@dataclass(frozen=True)
+class WeightedNewton(Optimizer):
+    """Newton on a decaying mixture of the previous and current Hessians
+    (``optimizer.py:292-320``): weight i^log(i) / (i+1)^log(i+1) on the
+    previous one from the second step on."""
+
+    needs_hessian = True
+
+    def init_state(self, theta):
+        t = np.asarray(theta, dtype=np.float64)
+        return (np.broadcast_to(np.eye(t.shape[-1]), t.shape + (t.shape[-1],)).copy(),)
+
+    def step(self, grad, state, step_num, compute_hessian_fn=None, eta_i=None):
+        if compute_hessian_fn is None:
+            raise ValueError("WeightedNewton optimizer requires compute_hessian_fn")
+        (prev,) = state
+        g = np.asarray(grad, dtype=np.float64)
+        P = g.shape[-1]
+        H = np.asarray(compute_hessian_fn(), dtype=np.float64).reshape(-1, P, P)
+        if step_num == 0:
+            use = H
+        else:
+            i = float(step_num)
+            wt = (i ** math.log(i)) / ((i + 1.0) ** math.log(i + 1.0))
+            use = wt * prev.reshape(-1, P, P) + (1.0 - wt) * H
+        out = np.stack([-_pinv_sym(h) @ gi for h, gi in zip(use, _rows(g))])
+        return out.reshape(g.shape), (H.reshape(prev.shape),)
 
 
 # ---------------------------------------------------------------------------
