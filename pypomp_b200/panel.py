@@ -249,6 +249,60 @@ class PanelPomp:
             t = PanelParameters(t)
         return deepcopy(t)
 
+    def get_unit_parameters(self, unit: str, theta=None) -> list:
+        """Each replicate's parameters of ``unit``: shared values updated with
+        the unit's own (``pypomp/panel/estimation_mixin.py:104-142``)."""
+        t = self._theta_in(theta)
+        out = []
+        for d in t.params(as_list=True):
+            p = {}
+            if d["shared"] is not None:
+                p.update({str(k): float(v) for k, v in d["shared"].iloc[:, 0].items()})
+            if d["unit_specific"] is not None:
+                p.update({str(k): float(v) for k, v in d["unit_specific"][unit].items()})
+            out.append(p)
+        return out
+
+    def simulate(self, key, theta=None, times=None, nsim: int = 1, as_pomp: bool = False):
+        """Simulated states and observations of every unit
+        (``pypomp/panel/estimation_mixin.py:229-311``): unit by unit with the
+        unit's parameters and a key split off the panel key, through
+        ``Pomp.simulate`` (one ``ppf_simulate`` launch per unit).  Returns
+        long-format frames with a leading ``unit`` column, or with
+        ``as_pomp`` a copy of the panel whose units hold the first replicate's
+        simulated data."""
+        import warnings
+
+        from .pomp import PompParameters
+
+        if as_pomp:
+            if nsim > 1:
+                warnings.warn(
+                    "as_pomp is True, but nsim > 1. Only 1 simulation will be performed as_pomp overrides nsim.",
+                    UserWarning, stacklevel=2)
+            nsim = 1
+        t = self._theta_in(theta)
+        key = pprandom.as_key(key)
+        xs, ys, units = [], [], {}
+        for unit, obj in self.unit_objects.items():
+            key, sub = pprandom.split(key)
+            res = obj.simulate(key=sub, theta=PompParameters(self.get_unit_parameters(unit, theta=t)),
+                               times=times, nsim=nsim, as_pomp=as_pomp)
+            if as_pomp:
+                units[unit] = res
+            else:
+                X, Y = res
+                X.insert(0, "unit", unit)
+                Y.insert(0, "unit", unit)
+                xs.append(X)
+                ys.append(Y)
+        if as_pomp:
+            out = deepcopy(self)
+            out.unit_objects = units
+            out.theta = PanelParameters(t.params(as_list=True)[:1])
+            return out
+        return pd.concat(xs), pd.concat(ys)
+
     # -- estimation ----------------------------------------------------------
     def pfilter(self, J: int, key=None, theta=None, thresh: float = 0.0, reps: int = 1, chunk_size: int = 1,
                 CLL: bool = False, ESS: bool = False, filter_mean: bool = False,

@@ -108,3 +108,33 @@ def test_simulate_rejects_bad_arguments():
         F.simulate(st, th, 0, [1])
     with pytest.raises(ValueError):
         F.simulate(st, th, 2, [1, 2])
+
+
+def test_panel_simulate_units_and_as_pomp():
+    import pandas as pd
+
+    import pypomp_b200 as pp
+    from pypomp_b200 import random as pprandom
+    from pypomp_b200.pomp import PompParameters
+
+    units = {f"u{i}": pp.Ricker(T=8 + 3 * i, key=i) for i in range(3)}
+    sh = pd.DataFrame({"shared": [0.3, 10.0]}, index=["sigma", "phi"])
+    sp = pd.DataFrame([[40.0, 45.0, 50.0], [7.0, 7.0, 7.0]], index=["r", "N_0"], columns=list(units))
+    pan = pp.PanelPomp(units, pp.PanelParameters({"shared": sh, "unit_specific": sp}))
+    X, Y = pan.simulate(key=9, nsim=2)
+    assert list(X.columns) == ["unit", "theta_idx", "sim", "time", "N"]
+    assert list(Y.columns) == ["unit", "theta_idx", "sim", "time", "y"]
+    for i, u in enumerate(units):
+        T = 8 + 3 * i
+        assert (X["unit"] == u).sum() == 2 * (T + 1) and (Y["unit"] == u).sum() == 2 * T
+    # unit u1 equals its own Pomp.simulate under the key the panel derives for it
+    k = pprandom.as_key(9)
+    k, _ = pprandom.split(k)
+    k, sub = pprandom.split(k)
+    one = pp.Ricker(T=11, key=1)
+    _, Y1 = one.simulate(key=sub, theta=PompParameters(pan.get_unit_parameters("u1")), nsim=2)
+    assert np.array_equal(Y[Y["unit"] == "u1"]["y"].to_numpy(), Y1["y"].to_numpy())
+    new = pan.simulate(key=9, as_pomp=True)
+    assert [len(new.unit_objects[u].ys) for u in units] == [8, 11, 14]
+    new.pfilter(J=300, key=2)
+    assert np.all(np.isfinite(new.results()["unit logLik"].to_numpy(dtype=float)))
