@@ -661,11 +661,32 @@ def run_pmcmc(args):
 def run_profile_case(args):
     """A small case of the same kernels for ncu captures: the headline model
     and J, 24 seeds (state 2 x 24 x 262144 x 12 B = 151 MB, larger than L2),
-    the first 12 observations, one call."""
+    the first 12 observations, one call.  ``--config sim`` and ``--config c5``
+    give small cases of the simulation and cluster-path kernels."""
     import torch
 
     from pypomp_b200 import functional as F
 
+    import pypomp_b200 as pp
+
+    if args.config == "sim":
+        # k_simulate: LG 2-D, one parameter set x 65536 replicates x T = 200
+        # (outputs 2 x 65536 x 201 x 8 B = 211 MB, larger than L2)
+        m = pp.LG(T=200, Q=LG_Q, R=LG_R, key=0)
+        th = m.theta.to_array(m.canonical_param_names).astype(np.float32)
+        X, Y = F.simulate(m.to_struct(), th, 65536, np.array([1], np.uint64), return_torch=True)
+        torch.cuda.synchronize()
+        print("profile case simulate", float(X[0, 0, -1, 0]))
+        return
+    if args.config == "c5":
+        # k_cluster: one Ricker unit filter as in the panel IF2 job (J = 8192,
+        # T = 500), 4 filters, cluster path
+        m = pp.Ricker(T=500, key=0)
+        th = np.repeat(m.theta.to_array(m.canonical_param_names), 4, axis=0).astype(np.float32)
+        out = F.run_pfilter(m.to_struct(), th, np.arange(4, dtype=np.uint64), 8192, path="cluster")
+        torch.cuda.synchronize()
+        print("profile case cluster logLik", out["loglik"][:2])
+        return
     m = workload()
     st = m.to_struct()
     st.ys = st.ys[:12]

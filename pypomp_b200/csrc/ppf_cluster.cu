@@ -279,59 +279,78 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
       int* anc = a.anc ? a.anc + ((size_t)f * a.T + t) * J : nullptr;
       float* logw = (a.logw && !last) ? a.logw + ((size_t)f * a.T + t + 1) * J : nullptr;
       const typename M::Consts cr = csh;
-      const int kA = klo & ~3;
-      const int ngr = (khi - kA + G - 1) / G;
-      const int g0 = (int)(((long long)threadIdx.x * ngr) / TPB);
-      const int g1 = (int)(((long long)(threadIdx.x + 1) * ngr) / TPB);
-      if (g0 < g1) {
-        int l = find_parent(st, nc, max(kA + G * g0, klo));
+      // one child k of parent l with its process normals z
+      auto child = [&](int k, int l, const float* z) {
+        if (anc) anc[k] = base + l;
+        if (last) {
+          if (IF2)
+            for (int p = 0; p < P; ++p) a.swarm_out[((size_t)f * P + p) * J + k] = TH[pc][p * JC + l];
+          return;
+        }
+        float x[DX];
+#pragma unroll
+        for (int d = 0; d < DX; ++d) x[d] = X[pc][d * JC + l];
+        float m;
+        if (IF2) {
+          for (int p = 0; p < P; ++p) th[p] = TH[pc][p * JC + l];
+          perturb_row<INJ>(a, f, k, t + 2, P, coolt, a.rw_sig, th);
+          typename M::Consts cc;
+          M::prepare(cc, th, a.model, est);
+          m = if2_measure(step1<M>(cc, ob, x, z), log1e18);
+        } else {
+          m = step1<M>(cr, ob, x, z);
+        }
+        const float wb = rs ? a.base_rs : (collapsed ? nwc : Wc[l] - lt32);
+        const float w = wb + m;
+        accum_maxmin(w, mx, mn, nn);
+        const int r = k / JC, lk = k - r * JC;
+        float* xr = cl.map_shared_rank(X[pn], r);
+#pragma unroll
+        for (int d = 0; d < DX; ++d) xr[d * JC + lk] = x[d];
+        cl.map_shared_rank(W[pn], r)[lk] = w;
+        if (IF2) {
+          float* tr = cl.map_shared_rank(TH[pn], r);
+          for (int p = 0; p < P; ++p) tr[p * JC + lk] = th[p];
+        }
+        if (logw) logw[k] = w;
+      };
+      if (khi - klo <= 2 * TPB) {
+        // the usual case, about one child per parent: one child per thread
+        // at a time, so every thread works and the step's critical path is
+        // one child long; each thread draws its own child's normals (the
+        // same numbers as the grouped draw below)
 #pragma unroll 1
-        for (int g = g0; g < g1; ++g) {
-          const int k0 = kA + G * g;
-          if (k0 >= khi) break;
-          float z[G * M::NZ];
-          if (!last) group_noise_g<G, M::NZ, INJ>(a, f, t + 2, k0, z);
+        for (int k = klo + (int)threadIdx.x; k < khi; k += TPB) {
+          float z[M::NZ];
+          if (!last) step_noise<M>(a, f, k, t + 2, M::NZ, z);
+          child(k, find_parent(st, nc, k), z);
+        }
+      } else {
+        // many children (a few heavy parents): groups of G consecutive
+        // children per thread share their Philox blocks
+        const int kA = klo & ~3;
+        const int ngr = (khi - kA + G - 1) / G;
+        const int g0 = (int)(((long long)threadIdx.x * ngr) / TPB);
+        const int g1 = (int)(((long long)(threadIdx.x + 1) * ngr) / TPB);
+        if (g0 < g1) {
+          int l = find_parent(st, nc, max(kA + G * g0, klo));
+#pragma unroll 1
+          for (int g = g0; g < g1; ++g) {
+            const int k0 = kA + G * g;
+            if (k0 >= khi) break;
+            float z[G * M::NZ];
+            if (!last) group_noise_g<G, M::NZ, INJ>(a, f, t + 2, k0, z);
 #pragma unroll
-          for (int e = 0; e < G; ++e) {
-            const int k = k0 + e;
-            if (k < klo || k >= khi) continue;
-            int adv = 0;
-            while (l + 1 < nc && st[l + 1] <= k) {
-              ++l;
-              if (++adv > 8) { l = find_parent(st, nc, k); break; }
+            for (int e = 0; e < G; ++e) {
+              const int k = k0 + e;
+              if (k < klo || k >= khi) continue;
+              int adv = 0;
+              while (l + 1 < nc && st[l + 1] <= k) {
+                ++l;
+                if (++adv > 8) { l = find_parent(st, nc, k); break; }
+              }
+              child(k, l, z + e * M::NZ);
             }
-            if (anc) anc[k] = base + l;
-            if (last) {
-              if (IF2)
-                for (int p = 0; p < P; ++p) a.swarm_out[((size_t)f * P + p) * J + k] = TH[pc][p * JC + l];
-              continue;
-            }
-            float x[DX];
-#pragma unroll
-            for (int d = 0; d < DX; ++d) x[d] = X[pc][d * JC + l];
-            float m;
-            if (IF2) {
-              for (int p = 0; p < P; ++p) th[p] = TH[pc][p * JC + l];
-              perturb_row<INJ>(a, f, k, t + 2, P, coolt, a.rw_sig, th);
-              typename M::Consts cc;
-              M::prepare(cc, th, a.model, est);
-              m = if2_measure(step1<M>(cc, ob, x, z + e * M::NZ), log1e18);
-            } else {
-              m = step1<M>(cr, ob, x, z + e * M::NZ);
-            }
-            const float wb = rs ? a.base_rs : (collapsed ? nwc : Wc[l] - lt32);
-            const float w = wb + m;
-            accum_maxmin(w, mx, mn, nn);
-            const int r = k / JC, lk = k - r * JC;
-            float* xr = cl.map_shared_rank(X[pn], r);
-#pragma unroll
-            for (int d = 0; d < DX; ++d) xr[d * JC + lk] = x[d];
-            cl.map_shared_rank(W[pn], r)[lk] = w;
-            if (IF2) {
-              float* tr = cl.map_shared_rank(TH[pn], r);
-              for (int p = 0; p < P; ++p) tr[p * JC + lk] = th[p];
-            }
-            if (logw) logw[k] = w;
           }
         }
       }
