@@ -85,12 +85,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// The fixed-point weight q = rint(exp(w - M) * 2^40) (collapsed filters: 1).
+// The fixed-point weight q = rint(exp(w - M) * 2^40) (collapsed filters: 1),
+// in two halves: the float e = qweight_e(w, M, collapsed) and
+// q = qweight_from_e(e).  On a resampling step the streaming path's k_sum
+// stores e over the parent log-weight, which nothing else reads afterwards,
+// and k_resprop forms q from it without repeating the exp.  e * 2^40 is exact
+// (e <= 1), so q is the same either way.
+__device__ __forceinline__ float qweight_e(float w, float M, bool collapsed) {
+  if (collapsed) return 9.094947017729282e-13f;   // 2^-40: q = 1
+  if (w != w) return 0.0f;
+  return pp_expq(w - M);     // equals pp_expf(w - M) wherever the quantised value can be >= 1
+}
+__device__ __forceinline__ uint64_t qweight_from_e(float e) { return __float2ull_rn(e * kQScale); }
 __device__ __forceinline__ uint64_t qweight(float w, float M, bool collapsed) {
-  if (collapsed) return 1ull;
-  if (w != w) return 0ull;
-  const float e = pp_expq(w - M);     // equals pp_expf(w - M) wherever the quantised value can be >= 1
-  return __float2ull_rn(e * kQScale);
+  return qweight_from_e(qweight_e(w, M, collapsed));
 }
 
 // Number of systematic points strictly below the CDF value C:

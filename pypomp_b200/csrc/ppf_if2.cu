@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
       uint64_t qs = 0;
 #pragma unroll
       for (int i = 0; i < IT; ++i) {
-        q[i] = (l0 + i < ntile) ? qweight(wv[i], Mx, qc) : 0ull;
+        q[i] = (l0 + i < ntile) ? qweight_from_e(wv[i]) : 0ull;   // k_sum left e = qweight_e(w)
         qs += q[i];
       }
       uint64_t btot;

@@ -434,12 +434,13 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
   const float Mx = keyf(acc.maxkey);
   const bool collapsed = nanf || Mx == -INFINITY;
   const int J = a.J;
-  const float* W = a.W[p] + (size_t)f * J;
+  float* W = a.W[p] + (size_t)f * J;
   const int jb = b * TILE + threadIdx.x * IT;
+  const bool vec = jb + IT <= J && (IT % 4) == 0 && (J & 3) == 0;
   uint64_t qs = 0;
-  float wv[IT];
+  float wv[IT], ev[IT];
   // float4 loads only when every filter's row starts 16-byte aligned (J % 4 == 0)
-  if (jb + IT <= J && (IT % 4) == 0 && (J & 3) == 0) {
+  if (vec) {
 #pragma unroll
     for (int i = 0; i < IT; i += 4) {
       const float4 v4 = *reinterpret_cast<const float4*>(W + jb + i);
@@ -450,7 +451,23 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
     for (int i = 0; i < IT; ++i) wv[i] = (jb + i < J) ? W[jb + i] : -INFINITY;
   }
 #pragma unroll
-  for (int i = 0; i < IT; ++i) qs += (jb + i < J) ? qweight(wv[i], Mx, collapsed) : 0ull;
+  for (int i = 0; i < IT; ++i) {
+    ev[i] = qweight_e(wv[i], Mx, collapsed);
+    qs += (jb + i < J) ? qweight_from_e(ev[i]) : 0ull;
+  }
+  // a resampling step reads its parents' weights only through q: keep e in
+  // their place for k_resprop (the step's carried weights need the originals)
+  if (decide_resample(a, acc)) {
+    if (vec) {
+#pragma unroll
+      for (int i = 0; i < IT; i += 4)
+        *reinterpret_cast<float4*>(W + jb + i) = make_float4(ev[i], ev[i + 1], ev[i + 2], ev[i + 3]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < IT; ++i)
+        if (jb + i < J) W[jb + i] = ev[i];
+    }
+  }
   // block total
   {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
