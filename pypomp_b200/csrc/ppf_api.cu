@@ -1,6 +1,8 @@
 // ppf_api.cu -- the extern "C" entry points of libppf.so (declared in
 // include/ppf.h): argument validation, workspace layout and path choice.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <math.h>
 #include <string.h>
 
@@ -36,6 +38,11 @@ static size_t carve(Args& a, int path, unsigned char* base) {
     a.tot = reinterpret_cast<uint64_t*>(take(8ull * a.F));
     a.ctrl_bytes = off;
     a.consts = take(512ull * a.F);
+    // per-thread run prefixes: ntiles x threads per tile, the largest over the tile configurations
+    const size_t J = (size_t)a.J;
+    const size_t nrun = std::max({(J + kTileLarge - 1) / kTileLarge * 256, (J + kTileMid - 1) / kTileMid * 128,
+                                  (J + kTileSmall - 1) / kTileSmall * 64});
+    a.runpre = reinterpret_cast<uint64_t*>(take(8ull * a.F * nrun));
     for (int i = 0; i < 2; ++i) a.X[i] = reinterpret_cast<float*>(take(4ull * a.F * dx * a.J));
     for (int i = 0; i < 2; ++i) a.W[i] = reinterpret_cast<float*>(take(4ull * a.F * a.J));
   } else if (path == PPF_PATH_PLAIN) {

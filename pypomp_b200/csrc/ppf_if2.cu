@@ -90,7 +90,6 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
   int* st = reinterpret_cast<int*>(xs + DX * TILE);               // [TILE + 1]
   float* wcar = reinterpret_cast<float*>(st + TILE + 4);          // [TILE]
   float* th = wcar + TILE + threadIdx.x * if2_row_stride(P);      // [TPB][P | 1]
-  __shared__ uint64_t s_scan[TPB / 32 + 1];
   __shared__ unsigned int smk[2 * (TPB / 32)];
 
   const int f = blockIdx.y, b = blockIdx.x;
@@ -135,14 +134,10 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
       const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
       const uint64_t E = a.excl[(size_t)f * a.ntiles + b];
       uint64_t q[IT];
-      uint64_t qs = 0;
 #pragma unroll
-      for (int i = 0; i < IT; ++i) {
-        q[i] = (l0 + i < ntile) ? qweight_from_e(wv[i]) : 0ull;   // k_sum left e = qweight_e(w)
-        qs += q[i];
-      }
-      uint64_t btot;
-      const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
+      for (int i = 0; i < IT; ++i) q[i] = (l0 + i < ntile) ? qweight_from_e(wv[i]) : 0ull;   // k_sum left e
+      // the exclusive prefix of this thread's run within the tile, from k_sum
+      const uint64_t tex = a.runpre[((size_t)f * a.ntiles + b) * TPB + threadIdx.x];
       if (l0 < ntile) {
         OffWalk wk = offwalk_init(o, E + tex);
         st[l0] = wk.k;

@@ -457,7 +457,8 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
   }
   // a resampling step reads its parents' weights only through q: keep e in
   // their place for k_resprop (the step's carried weights need the originals)
-  if (decide_resample(a, acc)) {
+  const bool rs = decide_resample(a, acc);
+  if (rs) {
     if (vec) {
 #pragma unroll
       for (int i = 0; i < IT; i += 4)
@@ -468,18 +469,28 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
         if (jb + i < J) W[jb + i] = ev[i];
     }
   }
-  // block total
+  // block scan: the tile total, and on a resampling step each thread's
+  // exclusive prefix for k_resprop (its threads own the same runs of parents)
+  // (one barrier: warp scans, then every thread adds the totals of the warps
+  // before its own; s_red is not reused, so no trailing barrier)
+  uint64_t btot = 0;
   {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t wsum = warp_sum_u64(qs);
-    if (lane == 0) s_red[warp] = wsum;
+    const uint64_t inc = warp_incl_scan_u64(qs);
+    if (lane == 31) s_red[warp] = inc;
     __syncthreads();
+    uint64_t before = 0;
+#pragma unroll
+    for (int w = 0; w < TPB / 32; ++w) {
+      const uint64_t v = s_red[w];
+      before += (w < warp) ? v : 0ull;
+      btot += v;
+    }
+    if (rs) a.runpre[((size_t)f * a.ntiles + b) * TPB + threadIdx.x] = before + inc - qs;
   }
   uint64_t* desc = a.desc[p] + (size_t)f * a.ntiles;
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
-    uint64_t btot = lane < TPB / 32 ? s_red[lane] : 0ull;
-    btot = warp_sum_u64(btot);
     uint64_t excl = 0;
     if (b == 0) {
       if (lane == 0) st_release_u64(desc, kStatusIncl | btot);

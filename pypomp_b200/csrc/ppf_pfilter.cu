@@ -135,7 +135,6 @@ __global__ void __launch_bounds__(TPB, RespropOccupancy<M>::B * (256 / TPB)) k_r
   float* wsm = wcar;                                                           // W row lands here first
   __shared__ __align__(8) uint64_t bar[2];                                     // [0]: W row, [1]: X rows
   __shared__ typename M::Consts c;
-  __shared__ uint64_t s_scan[TPB / 32 + 1];
   __shared__ unsigned int smk[2 * (TPB / 32)];
   __shared__ double sd[TPB / 32];
 
@@ -220,14 +219,10 @@ __global__ void __launch_bounds__(TPB, RespropOccupancy<M>::B * (256 / TPB)) k_r
       const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
       const uint64_t E = a.excl[(size_t)f * a.ntiles + b];
       uint64_t q[IT];
-      uint64_t qs = 0;
 #pragma unroll
-      for (int i = 0; i < IT; ++i) {
-        q[i] = (l0 + i < ntile) ? qweight_from_e(wv[i]) : 0ull;   // k_sum left e = qweight_e(w)
-        qs += q[i];
-      }
-      uint64_t btot;
-      const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
+      for (int i = 0; i < IT; ++i) q[i] = (l0 + i < ntile) ? qweight_from_e(wv[i]) : 0ull;   // k_sum left e
+      // the exclusive prefix of this thread's run within the tile, from k_sum
+      const uint64_t tex = a.runpre[((size_t)f * a.ntiles + b) * TPB + threadIdx.x];
       if (l0 < ntile) {
         OffWalk wk = offwalk_init(o, E + tex);
         st[l0] = wk.k;

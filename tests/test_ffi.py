@@ -49,9 +49,10 @@ def test_workspace_size_is_host_only():
     d.J, d.F, d.T, d.U = 262144, 64, 1000, 1
     d.path = _ffi.PATH_STREAM
     n = _ffi.LIB.ppf_pfilter_workspace_bytes(d)
-    # X and W double-buffered: 2 * 64 * 262144 * (2 + 1) * 4 bytes, plus control
-    assert n >= 2 * 64 * 262144 * 12
-    assert n < 2 * 64 * 262144 * 12 + (1 << 24)
+    # X and W double-buffered: 2 * 64 * 262144 * (2 + 1) * 4 bytes, the run
+    # prefixes (8 bytes per 4 particles), plus control
+    assert n >= 2 * 64 * 262144 * 12 + 64 * 262144 * 2
+    assert n < 2 * 64 * 262144 * 12 + 64 * 262144 * 2 + (1 << 24)
 
 
 def test_validation_messages_without_gpu(lg2d):
