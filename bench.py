@@ -51,9 +51,9 @@ LG_R = np.array([[1.0, 0.1], [0.1, 1.0]]) / 10
 RESPROP_BYTES = 24
 SUM_BYTES = 4
 # DRAM traffic of one k_resprop launch per particle, from an ncu capture of a
-# 24-seed case (dram__bytes_read.sum + dram__bytes_write.sum = 114.8 MB for
+# 24-seed case (dram__bytes_read.sum + dram__bytes_write.sum = 121.1 MB for
 # 6.29 M particles); traffic is proportional to the particles processed
-RESPROP_TRAFFIC_PER_PARTICLE = 18.25
+RESPROP_TRAFFIC_PER_PARTICLE = 19.25
 
 
 def rank_seeds(rank: int) -> np.ndarray:
