@@ -65,18 +65,36 @@ size_t cluster_smem_words(int JC, int P, int TPB) {
 }
 
 // Block max / min / NaN of the weights a CTA produced, pushed into slot c of
-// every CTA of the cluster (lanes 0..NC-1 of warp 0 hold the block result).
+// every CTA of the cluster.  One barrier: warp reductions land in smk, then
+// lanes 0..NC-1 of warp 0 each reduce all warps' values and push.  smk is
+// written again only after the cluster barrier that follows.
 template <int TPB>
 __device__ __forceinline__ void push_maxmin(cg::cluster_group& cl, Slot* slots, int c, int NC,
                                             unsigned int mx, unsigned int mn, unsigned int nn,
                                             unsigned int* smk) {
-  block_maxmin_u32<TPB>(mx, mn, smk);
-  nn = __syncthreads_or(nn);
+  constexpr int NW = TPB / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  mx = warp_max_u32(mx);
+  mn = warp_min_u32(mn);
+  nn = __any_sync(0xffffffffu, nn != 0u) ? 1u : 0u;
+  if (lane == 0) {
+    smk[warp] = mx;
+    smk[NW + warp] = mn;
+    smk[2 * NW + warp] = nn;
+  }
+  __syncthreads();
   if ((int)threadIdx.x < NC) {
-    Slot* o = cl.map_shared_rank(slots, (int)threadIdx.x) + c;
-    o->maxkey = mx;
-    o->minkey = mn;
-    o->nan = nn;
+    unsigned int a = 0u, b = 0xffffffffu, o = 0u;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      a = max(a, smk[w]);
+      b = min(b, smk[NW + w]);
+      o |= smk[2 * NW + w];
+    }
+    Slot* dst = cl.map_shared_rank(slots, (int)threadIdx.x) + c;
+    dst->maxkey = a;
+    dst->minkey = b;
+    dst->nan = o;
   }
 }
 
@@ -89,7 +107,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
   __shared__ Slot slots[kMaxCluster];
   __shared__ typename M::Consts csh;
   __shared__ uint64_t s_scan[TPB / 32 + 1];
-  __shared__ unsigned int smk[2 * (TPB / 32)];
+  __shared__ unsigned int smk[3 * (TPB / 32)];
   __shared__ double sd[TPB / 32];
 
   const int NC = (int)cl.num_blocks();
@@ -219,7 +237,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
       }
     }
     uint64_t btot;
-    const uint64_t tex = block_excl_scan_u64<TPB>(qs, s_scan, btot);
+    const uint64_t tex = block_excl_scan_u64_1b<TPB>(qs, s_scan, btot);
     if (want_sums) {
       Slot* o0 = cl.map_shared_rank(slots, 0) + c;
       const double b2 = block_sum_f64<TPB>(s2, sd);

@@ -182,6 +182,26 @@ __device__ __forceinline__ uint64_t block_excl_scan_u64(uint64_t v, uint64_t* sm
   return res;
 }
 
+// block_excl_scan_u64 with one barrier: warp scans, then every thread adds the
+// totals of the warps before its own.  The caller must not write `sm` again
+// before another barrier.
+template <int TPB>
+__device__ __forceinline__ uint64_t block_excl_scan_u64_1b(uint64_t v, uint64_t* sm, uint64_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t inc = warp_incl_scan_u64(v);
+  if (lane == 31) sm[warp] = inc;
+  __syncthreads();
+  uint64_t before = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < TPB / 32; ++w) {
+    const uint64_t x = sm[w];
+    before += (w < warp) ? x : 0ull;
+    tot += x;
+  }
+  total = tot;
+  return before + inc - v;
+}
+
 // Block exclusive max-scan of one int per thread (identity -1).
 template <int TPB>
 __device__ __forceinline__ int block_excl_max_i32(int v, int* sm, int& total) {

@@ -108,7 +108,6 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
   const bool nanf = acc.nan != 0;
   const float Mx = keyf(acc.maxkey);
   const bool collapsed = !nanf && Mx == -INFINITY;
-  const bool qc = nanf || Mx == -INFINITY;
   const bool rs = decide_resample(a, acc);
   const int J = a.J;
   const int jt = b * TILE;
@@ -248,9 +247,14 @@ int run_if2_m(Args& a, cudaStream_t s) {
 
 int run_if2(Args& a, cudaStream_t s) {
   // few small swarms (the unit filters of a panel): one cluster per filter
-  // keeps the swarm and its parameter rows on chip for the whole time loop
+  // keeps the swarm and its parameter rows on chip for the whole time loop.
+  // Measured on Ricker (T = 500): the cluster path wins up to F J = 65536
+  // particles in all (J = 8192, F = 8: 8.8 vs 15.0 ms) and loses at 262144
+  // (J = 32768, F = 8: 21.4 vs 17.7 ms), where a CTA holds several children
+  // per thread of heavy per-particle IF2 work.
   const long long tiles = (long long)a.F * ((a.J + kTileLarge - 1) / kTileLarge);
-  if (!(a.flags & PPF_F_NO_CLUSTER) && tiles < 2LL * kNumSMs && cluster_fits(a, true)) {
+  if (!(a.flags & PPF_F_NO_CLUSTER) && tiles < 2LL * kNumSMs && (long long)a.F * a.J <= 131072 &&
+      cluster_fits(a, true)) {
     const int rc = run_cluster(a, true, s);
     if (rc != PPF_EUNSUPPORTED) return rc;
   }
