@@ -136,11 +136,10 @@ struct LG {
     return pp_fma(-0.5f, q, c.c0);
   }
 
-  // y = C x + L_R w, w ~ N(0, I_dy)
-  __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
-                               float* y) {
-    float w[MAXDY];
-    pp_normals_own(seed, k, s, PPF_TAG_MEASURE, ndy(c), w);
+  // y = C x + L_R w, w ~ N(0, I_dy).  MEAS_NZ: measurement normals per draw
+  // when fixed at compile time (0: dy known only at run time).
+  static constexpr int MEAS_NZ = DYS;
+  __device__ static void rmeas_z(const Consts& c, const float* x, const float* w, float* y) {
 #pragma unroll
     for (int i = 0; i < MAXDY; ++i) {
       if (i < ndy(c)) {
@@ -152,6 +151,12 @@ struct LG {
         y[i] = a;
       }
     }
+  }
+  __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
+                               float* y) {
+    float w[MAXDY];
+    pp_normals_own(seed, k, s, PPF_TAG_MEASURE, ndy(c), w);
+    rmeas_z(c, x, w, y);
   }
 
   // ---- adjoint (MOP-alpha gradient).  Natural-scale gradient in a padded
@@ -307,13 +312,17 @@ struct SV {
     return pp_fma(-0.5f * r, r, pp_fma(-0.5f, v, c.c0));
   }
   // r = mu dt + rho sd eps + sqrt(1 - rho^2) sd w,  sd = e^{v/2} sqrt(dt)
+  static constexpr int MEAS_NZ = 1;
+  __device__ static void rmeas_z(const Consts& c, const float* x, const float* w, float* y) {
+    const float sd = pp_expf(0.5f * x[0]) * c.sqdt;
+    const float mean = pp_fma(c.rho * sd, x[1], c.mudt);
+    y[0] = pp_fma(c.rhoc * sd, w[0], mean);
+  }
   __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
                                float* y) {
     float w[1];
     pp_normals_own(seed, k, s, PPF_TAG_MEASURE, 1, w);
-    const float sd = pp_expf(0.5f * x[0]) * c.sqdt;
-    const float mean = pp_fma(c.rho * sd, x[1], c.mudt);
-    y[0] = pp_fma(c.rhoc * sd, w[0], mean);
+    rmeas_z(c, x, w, y);
   }
 
   // ---- adjoint: natural-scale gradient in canonical order
@@ -397,7 +406,9 @@ struct Ricker {
     if (y[0] == 0.0f) return -lam;
     return pp_fma(y[0], pp_logf(lam), -lam) - ycon;
   }
-  // y ~ Poisson(phi N)
+  // y ~ Poisson(phi N): counts, no measurement normals
+  static constexpr int MEAS_NZ = 0;
+  __device__ static void rmeas_z(const Consts&, const float*, const float*, float*) {}
   __device__ static void rmeas(const Consts& c, const float* x, uint64_t seed, uint32_t k, uint32_t s,
                                float* y) {
     y[0] = pp_poisson(c.phi * x[0], seed, k, s);

@@ -180,7 +180,6 @@ __global__ void __launch_bounds__(TPB, RespropOccupancy<M>::B * (256 / TPB)) k_r
   const bool nanf = acc.nan != 0;
   const float Mx = keyf(acc.maxkey);
   const bool collapsed = !nanf && Mx == -INFINITY;
-  const bool qc = nanf || Mx == -INFINITY;
   const bool rs = decide_resample(a, acc);
   float* Xn = a.X[p ^ 1] + (size_t)f * DX * J;
   float* Wn = a.W[p ^ 1] + (size_t)f * J;
