@@ -100,6 +100,47 @@ class PanelParameters:
     def params(self, as_list: bool = True):
         return deepcopy(self._list)
 
+    def pruned(self, n: int = 1, refill: bool = True) -> "PanelParameters":
+        """The top ``n`` replicates by panel log-likelihood, repeated to the previous
+        count with ``refill`` (``pypomp/core/parameters/base.py:138-181``; without
+        log-likelihoods every replicate ranks equal)."""
+        n_reps = self.num_replicates()
+        if n < 1:
+            raise ValueError("n must be at least 1.")
+        ll = self.logLik
+        if ll is None or np.all(np.isnan(ll)):
+            ll = np.zeros(n_reps)
+        top = np.asarray(ll).argsort()[-n:][::-1]
+        idx = np.tile(top, (n_reps + n - 1) // n)[:n_reps] if refill else top
+        return PanelParameters([self._list[i] for i in idx],
+                               logLik_unit=None if self.logLik_unit is None else self.logLik_unit[idx])
+
+    def mixed_and_matched(self, unit_names=None) -> "PanelParameters":
+        """Rank the shared parameters by panel log-likelihood and, unit by unit,
+        the unit-specific parameters by that unit's log-likelihood; replicate r
+        of the result pairs the r-th best of each
+        (``pypomp/core/parameters/panel.py:504-585``).  ``unit_names`` is the
+        order of the columns of ``logLik_unit`` (default: the unit-specific
+        frame's columns)."""
+        if self.logLik_unit is None:
+            raise ValueError("mix_and_match needs unit log-likelihoods (run pfilter first)")
+        units = list(self.get_unit_names() if unit_names is None else unit_names)
+        reps = self.num_replicates()
+        shared_ranks = self.logLik.argsort()[::-1]
+        unit_ranks = [self.logLik_unit[:, u].argsort()[::-1] for u in range(len(units))]
+        out, ll_unit = [], np.zeros_like(self.logLik_unit)
+        for r in range(reps):
+            sh = self._list[shared_ranks[r]]["shared"]
+            us = None
+            if self._list[0]["unit_specific"] is not None:
+                us = self._list[0]["unit_specific"].copy()
+                for u, name in enumerate(units):
+                    us[name] = self._list[unit_ranks[u][r]]["unit_specific"][name].to_numpy()
+            out.append({"shared": None if sh is None else sh.copy(), "unit_specific": us})
+            for u in range(len(units)):
+                ll_unit[r, u] = self.logLik_unit[unit_ranks[u][r], u]
+        return PanelParameters(out, logLik_unit=ll_unit)
+
     def __len__(self):
         return len(self._list)
 
@@ -401,6 +442,18 @@ class PanelPomp:
             time.time() - start, old_key))
 
     # -- analysis ------------------------------------------------------------
+    def time(self) -> pd.DataFrame:
+        return self.results_history.time()
+
+    def prune(self, n: int = 1, refill: bool = True) -> None:
+        """Keep the top ``n`` parameter sets (``pypomp/panel/analysis_mixin.py:38-49``)."""
+        self.theta = self.theta.pruned(n=n, refill=refill)
+
+    def mix_and_match(self) -> None:
+        """Cross-combine the best shared and unit-specific parameters
+        (``pypomp/panel/analysis_mixin.py:51-72``)."""
+        self.theta = self.theta.mixed_and_matched(self.get_unit_names())
+
     def results(self, index: int = -1, ignore_nan: bool = False) -> pd.DataFrame:
         return self.results_history[index].to_dataframe(ignore_nan=ignore_nan)
 

@@ -52,6 +52,23 @@ class PompParameters:
     def subset(self, idx):
         return PompParameters([self._list[i] for i in idx])
 
+    def pruned(self, n: int = 1, refill: bool = True) -> "PompParameters":
+        """The top ``n`` replicates by log-likelihood, repeated to the previous
+        count with ``refill`` (``pypomp/core/parameters/base.py:138-181``)."""
+        n_reps = self.num_replicates()
+        if n_reps == 0:
+            raise ValueError("No parameter sets available to prune.")
+        if n < 1:
+            raise ValueError("n must be at least 1.")
+        ll = self.logLik
+        if ll is None or np.all(np.isnan(ll)):
+            raise ValueError("No valid log-likelihoods available to prune (all nan).")
+        top = np.asarray(ll).argsort()[-n:][::-1]
+        idx = np.tile(top, (n_reps + n - 1) // n)[:n_reps] if refill else top
+        out = PompParameters([self._list[i] for i in idx])
+        out.logLik = np.asarray(ll)[idx]
+        return out
+
     def __len__(self):
         return len(self._list)
 
@@ -158,8 +175,13 @@ class ResultsHistory:
             frames.append(tr)
         return pd.concat(frames, ignore_index=True) if frames else pd.DataFrame()
 
-    def time(self):
-        return [r.execution_time for r in self._results]
+    def time(self) -> pd.DataFrame:
+        """Execution time of every run (``results/history.py:38-54``)."""
+        if not self._results:
+            return pd.DataFrame()
+        df = pd.DataFrame([{"method": r.method, "time": r.execution_time} for r in self._results])
+        df.index.name = "history_index"
+        return df
 
 
 class ParTrans:
@@ -444,8 +466,35 @@ class Pomp:
     def traces(self) -> pd.DataFrame:
         return self.results_history.traces()
 
-    def CLL(self, index: int = -1) -> np.ndarray:
-        return self.results_history[index].payload["CLL"]
+    def _per_step(self, key: str, index: int, average: bool) -> pd.DataFrame:
+        r = self.results_history[index]
+        if key not in r.payload:
+            return pd.DataFrame()
+        vals = np.asarray(r.payload[key])                  # (n_theta, reps, T)
+        times = self.ys.index.to_numpy(dtype=float)
+        n, reps, T = vals.shape
+        if average:
+            agg = logmeanexp(vals, axis=1) if key == "CLL" else vals.mean(axis=1)
+            return pd.DataFrame({"theta_idx": np.repeat(np.arange(n), T), "time": np.tile(times, n),
+                                 key: agg.reshape(-1)})
+        return pd.DataFrame({"theta_idx": np.repeat(np.arange(n), reps * T),
+                             "rep": np.tile(np.repeat(np.arange(reps), T), n),
+                             "time": np.tile(times, n * reps), key: vals.reshape(-1)})
 
-    def ESS(self, index: int = -1) -> np.ndarray:
-        return self.results_history[index].payload["ESS"]
+    def CLL(self, index: int = -1, average: bool = False) -> pd.DataFrame:
+        """Conditional log-likelihoods of a pfilter run with ``CLL=True`` as a tidy
+        frame (``theta_idx``, ``rep``, ``time``, ``CLL``); ``average`` takes the
+        log-mean-exp over replicates (``pypomp/core/results/render.py:77-95``)."""
+        return self._per_step("CLL", index, average)
+
+    def ESS(self, index: int = -1, average: bool = False) -> pd.DataFrame:
+        """Effective sample sizes of a pfilter run with ``ESS=True`` (columns as
+        :meth:`CLL`); ``average`` takes the mean over replicates."""
+        return self._per_step("ESS", index, average)
+
+    def time(self) -> pd.DataFrame:
+        return self.results_history.time()
+
+    def prune(self, n: int = 1, refill: bool = True) -> None:
+        """Keep the top ``n`` parameter sets by log-likelihood (``analysis_mixin.py:134-150``)."""
+        self.theta = self.theta.pruned(n=n, refill=refill)

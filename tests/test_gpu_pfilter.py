@@ -179,10 +179,25 @@ def test_lg_c1_against_kalman(lg2d):
     assert list(df.columns[:3]) == ["theta_idx", "logLik", "se"]
     lls = lg2d.results_history[-1].payload["logLiks"][0]
     assert abs(np.mean(lls) - exact) < 4 * np.std(lls) / np.sqrt(lls.size) + 0.05
-    cll = lg2d.CLL()
-    np.testing.assert_allclose(cll.sum(axis=-1), lg2d.results_history[-1].payload["logLiks"], rtol=1e-10)
+    cll = lg2d.CLL()          # tidy frame: theta_idx, rep, time, CLL
+    assert list(cll.columns) == ["theta_idx", "rep", "time", "CLL"] and len(cll) == 32 * 50
+    sums = cll.groupby(["theta_idx", "rep"])["CLL"].sum().to_numpy()
+    np.testing.assert_allclose(sums, lg2d.results_history[-1].payload["logLiks"][0], rtol=1e-10)
+    avg = lg2d.CLL(average=True)
+    assert list(avg.columns) == ["theta_idx", "time", "CLL"] and len(avg) == 50
     ess = lg2d.ESS()
-    assert np.all(ess >= 1) and np.all(ess <= 1000)
+    assert np.all(ess["ESS"] >= 1) and np.all(ess["ESS"] <= 1000)
+    assert list(lg2d.time().columns) == ["method", "time"]
+    # prune keeps the best parameter sets by log-likelihood
+    th2 = lg2d.theta.params()[0]
+    starts = [th2, {**th2, "A11": 0.2}, {**th2, "A11": 0.5}]
+    lg2d.pfilter(J=300, key=1, theta=starts)
+    lls = np.asarray(lg2d.theta.logLik)
+    best = int(np.argmax(lls))
+    lg2d.prune(n=1)
+    assert lg2d.theta.num_replicates() == 3
+    assert np.all(lg2d.theta.logLik == lls[best])
+    assert all(p["A11"] == starts[best]["A11"] for p in lg2d.theta.params())
 
 
 def test_lg_c2_full_width_properties(lg2d):
