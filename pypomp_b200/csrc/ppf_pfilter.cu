@@ -480,6 +480,44 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     }
     if (threadIdx.x == TPB - 1) st[J] = J;
     __syncthreads();
+    if (J <= 2 * TPB) {
+      // (d') few particles: one child per thread at a time, so every thread
+      // works (runs of 8 would leave most of them idle and put 8 children on
+      // each busy thread's critical path); each child draws its own normals,
+      // the same numbers as the grouped draw below
+      float cx[2][DX], cw[2];
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri) {
+        const int k = threadIdx.x + ri * TPB;
+        if (k < J) {
+          const int l = find_parent(st, J, k);
+          if (anc) anc[k] = l;
+          float x[DX];
+#pragma unroll
+          for (int d = 0; d < DX; ++d) x[d] = xs[d * J + l];
+          float z[M::NZ];
+          if (!last) step_noise<M>(a, f, k, t + 2, M::NZ, z);
+          const float wb = rs ? base : ws[l];
+          cw[ri] = last ? 0.0f : wb + step1<M>(cr, ob, x, z);
+#pragma unroll
+          for (int d = 0; d < DX; ++d) cx[ri][d] = x[d];
+        }
+      }
+      __syncthreads();
+      if (last) break;
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri) {
+        const int k = threadIdx.x + ri * TPB;
+        if (k < J) {
+#pragma unroll
+          for (int d = 0; d < DX; ++d) xs[d * J + k] = cx[ri][d];
+          ws[k] = cw[ri];
+          if (logw) logw[k] = cw[ri];
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     // (d) children: runs of 8, kept in registers until all parents are read
     float nx[MAXR][RUN][DX];
     float nw[MAXR][RUN];
