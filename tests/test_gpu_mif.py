@@ -159,3 +159,39 @@ def test_pomp_mif_end_to_end(lg2d):
     tr = m.traces()
     assert len(tr) == 2 * 4 and np.isnan(tr[tr["iteration"] == 0]["logLik"]).all()
     assert m.theta.num_replicates() == 2
+
+
+def test_mif_moves_toward_kalman_mle():
+    """IF2 from a perturbed start raises the exact (Kalman) log-likelihood of
+    its final mean parameters (the reference's accuracy check,
+    tests/test_accuracy/test_accuracy_pomp.py:73-97)."""
+    import pypomp_b200 as pp
+    from oracle.kalman import kalman_loglik, lg_matrices
+    from pypomp_b200.optim import RWSigma
+
+    m = pp.LG(T=100, A=[[0.8]], C=[[1.0]], Q=[[0.5]], R=[[0.5]], X0=[0.0], key=11)
+    names = m.canonical_param_names
+    truth = m.theta.params()[0]
+    start = {**truth, "A11": 0.4, "Q11": 1.2, "R11": 0.2}
+
+    def kal(p):
+        A, C, Q, R, X0 = lg_matrices(np.array([p[n] for n in names]), 1, 1)
+        return kalman_loglik(m.to_struct().ys, A, C, Q, R, X0)
+    rw = RWSigma({"A11": 0.02, "C11": 0.0, "Q11": 0.02, "R11": 0.02, "X0_1": 0.0}).geometric_cooling(0.5)
+    m.mif(J=2000, M=25, rw_sd=rw, key=3, theta=[start])
+    end = m.theta.params()[0]
+    assert kal(end) > kal(start) + 5.0, (kal(start), kal(end), end)
+
+
+def test_oo_and_functional_pfilter_agree_exactly(lg2d):
+    """Pomp.pfilter is functional.pfilter under the keys it derives
+    (the reference's tests/test_properties/test_layer_parity.py)."""
+    from pypomp_b200 import functional as F
+    from pypomp_b200 import random as pprandom
+
+    th = lg2d.theta.to_array(lg2d.canonical_param_names)
+    lg2d.pfilter(J=700, key=5, reps=3)
+    oo = lg2d.results_history[-1].payload["logLiks"]
+    keys = pprandom.split(pprandom.split(pprandom.as_key(5))[1], 3).reshape(1, 3)
+    fn = F.pfilter(lg2d.to_struct(), th, 700, keys)["logLik"]
+    assert np.array_equal(oo, fn)
