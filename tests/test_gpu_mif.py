@@ -195,3 +195,44 @@ def test_oo_and_functional_pfilter_agree_exactly(lg2d):
     keys = pprandom.split(pprandom.split(pprandom.as_key(5))[1], 3).reshape(1, 3)
     fn = F.pfilter(lg2d.to_struct(), th, 700, keys)["logLik"]
     assert np.array_equal(oo, fn)
+
+
+@pytest.mark.parametrize("J", [3000, 40000])
+def test_mif_graph_replay_equals_per_iteration_calls(J):
+    """functional.mif runs its iterations on persistent device buffers
+    (PerfilterCall); the result equals separate ppf_perfilter calls exactly,
+    on the cluster path (J = 3000) and the stream path (J = 40000), and so
+    does a graph-replayed PerfilterCall."""
+    import torch
+
+    import pypomp_b200 as pp
+    from pypomp_b200 import functional as F
+    from pypomp_b200 import random as pprandom
+    from pypomp_b200.optim import RWSigma
+
+    m = pp.Ricker(T=30, key=4)
+    st = m.to_struct()
+    names = m.canonical_param_names
+    th = m.theta.to_array(names)
+    starts = np.repeat(np.repeat(th[:, None, :], J, axis=1), 2, axis=0).astype(np.float32)
+    rw = RWSigma({n: 0.03 for n in names}).geometric_cooling(0.5)
+    keys = np.array([8, 9], np.uint64)
+    M = 3
+    ll, traces, final = F.mif(st, starts, rw, M, J, keys)
+    rw_sig, rw_sig0 = rw.arrays(names)
+    est = st.spec.to_est(starts.reshape(-1, 4)).reshape(starts.shape).astype(np.float32)
+    swarm = torch.from_numpy(np.ascontiguousarray(est.transpose(0, 2, 1))).cuda()
+    m_keys = np.stack([pprandom.split(k, M + 1)[1:] for k in keys])
+    for it in range(M):
+        cool = np.array([rw.cooling_factor(i, it, 30) for i in range(30)], dtype=np.float32)
+        res = F.run_perfilter(st, swarm, m_keys[:, it], J, rw_sig, rw_sig0, cool, cool[0])
+        assert np.array_equal(res["loglik"].cpu().numpy(), ll[:, it])
+        swarm = res["swarm"]
+    want = st.spec.from_est(swarm.cpu().numpy().transpose(0, 2, 1).reshape(-1, 4)).reshape(final.shape)
+    assert np.array_equal(want, final)
+    sw0 = torch.from_numpy(np.ascontiguousarray(est.transpose(0, 2, 1))).cuda()
+    call = F.PerfilterCall(st, sw0, J, rw_sig, rw_sig0, graph=True)
+    for it in range(M):
+        cool = np.array([rw.cooling_factor(i, it, 30) for i in range(30)], dtype=np.float32)
+        assert np.array_equal(call(m_keys[:, it], cool, cool[0]), ll[:, it])
+    assert np.array_equal(call.swarm.cpu().numpy(), swarm.cpu().numpy())
