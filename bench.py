@@ -170,7 +170,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": NSEED * J * T / value * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "LG 2-D pfilter, T=1000, J=262144, 64 seeds (configs[1])",
+        "config": {"workload": "LG 2-D pfilter, T=1000, J=262144, 64 seeds",
                    "model": "LG", "global_batch": NSEED, "seq_len": T, "particles": J},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
                          "sample": sample,
@@ -321,7 +321,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "LG 2-D pfilter, T=1000, J=262144, 64 seeds per GPU (configs[1])",
+            "config": {"workload": "LG 2-D pfilter, T=1000, J=262144, 64 seeds per GPU",
                        "model": "LG", "global_batch": NSEED * world, "seq_len": T, "particles": J,
                        "parallelism": f"replicas{world}", "path": "stream",
                        "cuda_graph": bool(args.graph),
@@ -394,7 +394,7 @@ def run_c1(args):
     ms, clk = _timed(fn, args.steps, args.warmup, stream)
     reps = F.run_pfilter(st, np.repeat(th, 256, 0), np.arange(256, dtype=np.uint64), 1000, path="resident")
     ll = reps["loglik"]
-    _line(args, "LG 2-D pfilter, T=50, J=1000, one filter, resident path (configs[0])",
+    _line(args, "LG 2-D pfilter, T=50, J=1000, one filter, resident path",
           1000 * 50 / (ms / 1e3), ms,
           {"e2e": {"value": 1000 * 50 / (ms / 1e3), "unit": UNIT, "api": "functional.run_pfilter",
                    "h2d_bytes_per_step": int(st.ys.nbytes + th.nbytes + 8), "d2h_bytes_per_step": 0},
@@ -440,7 +440,7 @@ def run_c3(args):
                        "GBps": bytes_kind[k] * per_launch_units / (avg / 1e3) / 1e9}
     dom = max(kern, key=lambda k: kern[k]["total_ms"])
     res = call.out
-    _line(args, "SV MOP-alpha value+grad, T=2000, J=65536, alpha=0.97 (configs[2])", value, ms,
+    _line(args, "SV MOP-alpha value+grad, T=2000, J=65536, alpha=0.97", value, ms,
           {"e2e": None, "clocks": clk, "kernels": kern,
            "roofline": {"bound": "hbm", "achieved": kern[dom]["GBps"], "peak": peak, "unit": "GB/s",
                         "frac": kern[dom]["GBps"] / peak, "traffic": None, "kernel": dom,
@@ -473,7 +473,7 @@ def run_c4(args):
     best = min(res, key=lambda k: res[k][0])
     ms, clk = res[best]
     value = Fg * Jr * Tr / (ms / 1e3)
-    _line(args, "Ricker 32x32 (log r, sigma) grid x J=16384, T=500 (configs[3])", value, ms,
+    _line(args, "Ricker 32x32 (log r, sigma) grid x J=16384, T=500", value, ms,
           {"e2e": {"value": value, "unit": UNIT, "api": "functional.run_pfilter (host inputs)",
                    "h2d_bytes_per_step": int(grid.nbytes + st.ys.nbytes + seeds.nbytes),
                    "d2h_bytes_per_step": 0},
@@ -542,7 +542,7 @@ def run_c5(args):
     mif_rate = steps_units * args.steps / (mif_ms / 1e3)
     tr_rate = steps_units * args.steps / (tr_ms / 1e3)
     job_s = 100 * mif_ms / args.steps / 1e3 + 50 * tr_ms / args.steps / 1e3
-    _line(args, "Ricker panel: 128 units, T_u in [50, 800], J=8192; IF2 then MOP train (configs[4])",
+    _line(args, "Ricker panel: 128 units, T_u in [50, 800], J=8192; IF2 then MOP train",
           mif_rate, mif_ms / args.steps,
           {"e2e": {"value": mif_rate, "unit": UNIT, "api": "functional.panel_mif (host inputs)",
                    "h2d_bytes_per_step": int(sh.nbytes + un.nbytes + st.ys.nbytes), "d2h_bytes_per_step": 0},
