@@ -679,13 +679,19 @@ def run_profile_case(args):
         print("profile case simulate", float(X[0, 0, -1, 0]))
         return
     if args.config == "c5":
-        # k_cluster: one Ricker unit filter as in the panel IF2 job (J = 8192,
-        # T = 500), 4 filters, cluster path
+        # k_cluster: first the pfilter variant on 4 Ricker filters (J = 8192,
+        # T = 500), then the IF2 variant on one unit filter as in the panel IF2
+        # job (same J and T, rw sd 0.02)
         m = pp.Ricker(T=500, key=0)
-        th = np.repeat(m.theta.to_array(m.canonical_param_names), 4, axis=0).astype(np.float32)
-        out = F.run_pfilter(m.to_struct(), th, np.arange(4, dtype=np.uint64), 8192, path="cluster")
+        st = m.to_struct()
+        th = m.theta.to_array(m.canonical_param_names).astype(np.float32)
+        out = F.run_pfilter(st, np.repeat(th, 4, axis=0), np.arange(4, dtype=np.uint64), 8192, path="cluster")
+        est = m.spec.to_est(th).astype(np.float32)
+        swarm = torch.from_numpy(np.ascontiguousarray(np.repeat(est[:, :, None], 8192, axis=2))).cuda()
+        sig = np.full(4, 0.02, np.float32)
+        res = F.run_perfilter(st, swarm, np.array([7], np.uint64), 8192, sig, sig, np.full(500, 0.5, np.float32), 0.5)
         torch.cuda.synchronize()
-        print("profile case cluster logLik", out["loglik"][:2])
+        print("profile case cluster logLik", out["loglik"][:2], float(res["loglik"][0]))
         return
     m = workload()
     st = m.to_struct()
