@@ -182,11 +182,13 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
       accum_maxmin(w, mx, mn, nn);
       if (logw0) logw0[k] = w;
     }
-    if (c == 0 && threadIdx.x == 0) a.loglik[f] = 0.0;
     push_maxmin<TPB>(cl, slots, c, NC, mx, mn, nn, smk);
   }
   cl.sync();
 
+  // the filter's log-likelihood, kept by thread 0 of CTA 0 and written once at
+  // the end rather than read and written in global memory every observation
+  double ll_acc = 0.0;
   const int ITC = (JC + TPB - 1) / TPB;        // parents per thread (contiguous)
   const int l0 = threadIdx.x * ITC;
   const int l1 = min(l0 + ITC, nc);
@@ -265,7 +267,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
           acc.s2 += slots[r].s2;
           for (int d = 0; d < DX; ++d) { acc.fx[d] += slots[r].fx[d]; acc.px[d] += slots[r].px[d]; }
         }
-      finalize_step(a, f, t, acc, tot, a.loglik + f);
+      finalize_step(a, f, t, acc, tot, &ll_acc);
     }
     const bool rs = decide_resample(a, acc);
 
@@ -376,6 +378,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     if (!last) push_maxmin<TPB>(cl, slots, c, NC, mx, mn, nn, smk);
     cl.sync();   // children and slots visible to their owners; nobody leaves while others write to it
   }
+  if (c == 0 && threadIdx.x == 0) a.loglik[f] = ll_acc;
 }
 
 // ---------------------------------------------------------------------------
