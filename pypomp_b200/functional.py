@@ -388,7 +388,8 @@ class MopCall:
     """
 
     def __init__(self, struct: PompStruct, theta_est, seeds_f, J: int, alpha: float, *, unit_f=None,
-                 inject=None, ckpt_every: int = 0, save_ancestors: bool = False, natural: bool = False):
+                 inject=None, ckpt_every: int = 0, save_ancestors: bool = False, natural: bool = False,
+                 graph: bool = False):
         torch = _ffi.require_cuda()
         if J < 1:
             raise ValueError("J should be greater than 0.")
@@ -416,7 +417,7 @@ class MopCall:
         if save_ancestors:
             self.out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=dev)
         inj = {}
-        flags = _ffi.F_NATURAL if natural else 0
+        flags = (_ffi.F_NATURAL if natural else 0) | (_ffi.F_GRAPH if graph else 0)
         if inject is not None:
             flags |= _ffi.F_INJECT
             for k in ("z0", "z", "u"):
@@ -441,6 +442,20 @@ class MopCall:
 
     def _stream(self):
         return self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def update(self, theta_est, seeds_f) -> None:
+        """New parameters and keys of the same shape, copied into this call's
+        device buffers: the descriptor stays byte-identical, so with ``graph``
+        the next forward replays the captured launch sequence on them.  (A call
+        built on a CUDA tensor reads that tensor, so this writes into it.)"""
+        torch = self.torch
+        th_d, seeds_d = self.keep[0], self.keep[4]
+        if hasattr(theta_est, "is_cuda"):
+            th_d.copy_(theta_est.detach().reshape(th_d.shape))
+        else:
+            th_d.copy_(torch.from_numpy(np.ascontiguousarray(theta_est, dtype=np.float32).reshape(th_d.shape)))
+        seeds_d.copy_(torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).reshape(-1).copy()))
+        self.forward_done = False
 
     def forward(self, grad: bool = False) -> dict:
         d = self.d
@@ -550,12 +565,21 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
     traces = np.zeros((n, M + 1, P))
     traces[:, 0] = th
     chain = [int(k) for k in keys]
+    alphas = [1.0 - (1.0 - alpha) * cosine_alpha(m, M, alpha_cooling) for m in range(M)]
+    # with one alpha for the whole run every step reuses one MOP call (its
+    # buffers, workspace and captured launch sequence)
+    reuse = len(set(alphas)) == 1
+    call = None
     for m in range(M):
-        alpha_m = 1.0 - (1.0 - alpha) * cosine_alpha(m, M, alpha_cooling)
+        alpha_m = alphas[m]
         subs = np.zeros(n, np.uint64)
         for i in range(n):
             chain[i], subs[i] = (int(v) for v in pprandom.split(chain[i]))
-        res = run_mop(struct, th.astype(np.float32), subs, J, alpha_m, grad=True)
+        if reuse and call is not None:
+            call.update(th.astype(np.float32), subs)
+        else:
+            call = MopCall(struct, th.astype(np.float32), subs, J, alpha_m, graph=reuse)
+        res = {k: v.cpu().numpy() for k, v in call.forward(grad=True).items()}
         grad = res["grad"] / T
         if n_monitors == 1:
             nll[:, m + 1] = res["value"]
@@ -1193,15 +1217,30 @@ def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optim
     hist_u = np.zeros((n, M + 1, U, nu))
     hist_s[:, 0], hist_u[:, 0] = sh, un
     all_units = struct.all_units()
+    alphas = [1.0 - (1.0 - alpha) * cosine_alpha(m, M, alpha_cooling) for m in range(M)]
+    # one alpha for the whole run and no injected draws: each chunk reuses one
+    # MOP call (buffers, workspace, captured launch sequence) across iterations
+    reuse = len(set(alphas)) == 1 and inject is None
+    calls = [None] * nch
     for m in range(M):
-        alpha_m = 1.0 - (1.0 - alpha) * cosine_alpha(m, M, alpha_cooling)
+        alpha_m = alphas[m]
         chunk_nll = np.zeros((n, nch))
         for c in range(nch):
             units = np.arange(c * cs, (c + 1) * cs)
             th = _panel_thetas(s_est, u_est[:, units], perms[units])    # (n, cs, P)
             inj = inject[m][c] if inject is not None else None
-            res = run_mop(all_units, th.reshape(n * cs, -1).astype(np.float32), keys[:, m, units].reshape(-1),
-                          J, alpha_m, grad=True, unit_f=np.tile(units.astype(np.int32), n), inject=inj)
+            th32 = th.reshape(n * cs, -1).astype(np.float32)
+            ks = keys[:, m, units].reshape(-1)
+            if reuse and calls[c] is not None:
+                calls[c].update(th32, ks)
+                res = {k: v.cpu().numpy() for k, v in calls[c].forward(grad=True).items()}
+            elif reuse:
+                calls[c] = MopCall(all_units, th32, ks, J, alpha_m, unit_f=np.tile(units.astype(np.int32), n),
+                                   graph=True)
+                res = {k: v.cpu().numpy() for k, v in calls[c].forward(grad=True).items()}
+            else:
+                res = run_mop(all_units, th32, ks, J, alpha_m, grad=True,
+                              unit_f=np.tile(units.astype(np.int32), n), inject=inj)
             val = res["value"].reshape(n, cs)
             g = res["grad"].reshape(n, cs, -1)
             gp = np.zeros((n, cs, ns + nu))

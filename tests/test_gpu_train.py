@@ -140,3 +140,35 @@ def test_hessian_fd_near_exact_kalman_hessian():
     H = F.mop_hessian_fd(st, est[None], np.array([7], np.uint64), 100000, 1.0)[0] * 50
     ratio = np.diag(H)[:4] / exact
     assert np.all((ratio > 0.5) & (ratio < 2.0)), (np.diag(H), exact)
+
+
+def test_train_reused_mop_call_equals_fresh_calls():
+    """With one alpha for the run, functional.train reuses one MOP call per step
+    (MopCall.update, graph replay); the trace equals fresh run_mop calls under
+    the same key tree (train.py:86-90: a MOP key, then a Hessian key per step)."""
+    import pypomp_b200 as pp
+    from pypomp_b200 import functional as F
+    from pypomp_b200 import random as pprandom
+    from pypomp_b200.optim import SGD, LearningRate
+
+    m = pp.SV(T=40, key=1)
+    st = m.to_struct()
+    names = m.canonical_param_names
+    est = np.repeat(st.spec.to_est(m.theta.to_array(names)), 2, axis=0)
+    est[1, 0] += 0.1
+    keys = np.array([31, 32], np.uint64)
+    J, M, rate = 3000, 4, 0.05
+    eta = LearningRate({n: rate for n in names})
+    nll, tr = F.train(st, est, J, SGD(), M, eta, 0.97, keys)
+    th = est.copy()
+    chain = [int(k) for k in keys]
+    for step in range(M):
+        subs = np.zeros(2, np.uint64)
+        for i in range(2):
+            chain[i], subs[i] = (int(v) for v in pprandom.split(chain[i]))
+        res = F.run_mop(st, th.astype(np.float32), subs, J, 0.97, grad=True)
+        assert np.array_equal(res["value"], nll[:, step + 1])
+        for i in range(2):
+            chain[i] = int(pprandom.split(chain[i])[0])
+        th = th + rate * (-res["grad"] / 40)
+        assert np.array_equal(th, tr[:, step + 1])
