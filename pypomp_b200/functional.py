@@ -1022,6 +1022,38 @@ def panel_mop(struct: PanelPompStruct, thetas_array, J: int, alpha: float, keys,
     return out
 
 
+def _perfilter_queued(st_u, unit_in, swarm, seeds_d, J, sig_d, sig0_d, cool_d, thresh, save_anc, ll_out,
+                      err_acc, stream):
+    """Queue one unit's ``ppf_perfilter`` on device-resident inputs without
+    waiting for it: the log-likelihoods land in ``ll_out`` (n,), the status
+    word is OR-ed into ``err_acc``.  ``cool_d`` is the unit's row of cooling
+    factors; its first entry is the t0 factor."""
+    torch = _ffi.require_cuda()
+    ys_d, ycon_d, Tu_d, U1, T = unit_in
+    spec = st_u.spec
+    F, P = swarm.shape[0], spec.n_params
+    out = {"swarm": torch.empty(F, P, J, dtype=torch.float32, device=swarm.device)}
+    d = _ffi.PerfilterDesc()
+    d.model = spec.ffi_model()
+    d.J, d.F, d.T, d.U = J, F, T, U1
+    d.flags = _ffi.F_SAVE_ANC if save_anc else 0
+    d.thresh = float(max(0.0, thresh))
+    if save_anc:
+        out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=swarm.device)
+    d.swarm_in, d.swarm_out = _ffi.ptr(swarm), _ffi.ptr(out["swarm"])
+    d.rw_sig, d.rw_sig0 = _ffi.ptr(sig_d), _ffi.ptr(sig0_d)
+    d.cool, d.cool0 = _ffi.ptr(cool_d), _ffi.ptr(cool_d)
+    d.ys, d.ycon, d.T_u = _ffi.ptr(ys_d), _ffi.ptr(ycon_d), _ffi.ptr(Tu_d)
+    d.seeds, d.loglik, d.anc = _ffi.ptr(seeds_d), _ffi.ptr(ll_out), _ffi.ptr(out.get("anc"))
+    ws = torch.empty(max(int(_ffi.LIB.ppf_perfilter_workspace_bytes(d)), 256), dtype=torch.uint8,
+                     device=swarm.device)
+    d.workspace, d.ws_bytes = _ffi.ptr(ws), ws.numel()
+    _ffi.check(_ffi.LIB.ppf_perfilter(d, stream), "ppf_perfilter")
+    err_acc.bitwise_or_(ws[:4].view(torch.int32))
+    out["loglik"] = ll_out
+    return out
+
+
 def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, J: int, keys,
               thresh: float = 0.0, n_monitors: int = 0, block: bool = True, *, inject=None):
     """Panel iterated filtering (``pypomp/functional/mif.py:125-259``;
@@ -1092,19 +1124,49 @@ def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, 
     shared_tr[:, 0, 1:], unit_tr[:, 0, :, 1:] = s0, u0
     perm_t = [torch.tensor(perms[u], device=dev) for u in range(U)]
     inv_t = [torch.tensor(inv_perms[u], device=dev) for u in range(U)]
+    # Without injected draws the unit filters are queued back to back: every
+    # unit's data and sds are uploaded once, each iteration's keys and cooling
+    # factors in one pinned copy, and the status words are folded into one
+    # device flag read once per iteration, so the host never waits for a unit
+    # filter before preparing the next.
+    fast = inject is None
+    if fast:
+        units_st = [struct.unit(u) for u in range(U)]
+        unit_in = [_device_inputs(torch, units_st[u], dev) for u in range(U)]
+        f32d = dict(dtype=torch.float32, device=dev)
+        sig_d = [torch.tensor(sig_p[perms[u]], **f32d) for u in range(U)]
+        sig0_d = [torch.tensor(sig0_p[perms[u]], **f32d) for u in range(U)]
+        Tmax = max(u_in[4] for u_in in unit_in)
+        err_acc = torch.zeros(1, dtype=torch.int32, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
     for it in range(M):
         unit_keys = np.stack([pprandom.split(k, U) for k in m_keys[:, it]])    # (n, U)
         ll_units = np.zeros((n, U))
+        if fast:
+            cool_h = np.zeros((U, Tmax), np.float32)
+            for u in range(U):
+                Tu = unit_in[u][4]
+                cool_h[u, :Tu] = [rw_sd.cooling_factor(i, it, Tu) for i in range(Tu)]
+            pinned = (torch.from_numpy(cool_h).pin_memory(),
+                      torch.from_numpy(np.ascontiguousarray(unit_keys.T).view(np.int64)).pin_memory())
+            cool_d = pinned[0].to(dev, non_blocking=True)                       # (U, Tmax)
+            keys_d = pinned[1].to(dev, non_blocking=True)                       # (U, n)
+            ll_d = torch.zeros(U, n, dtype=torch.float64, device=dev)
         for u in range(U):
             st_u = struct.unit(u)
             T = st_u.ys.shape[0]
             panel = torch.cat([S, Us[:, u]], dim=1)                             # (n, Pp, J)
             swarm = panel.index_select(1, perm_t[u]).contiguous()               # unit order
-            cool = np.array([rw_sd.cooling_factor(i, it, T) for i in range(T)], dtype=np.float32)
-            inj = inject[it][u] if inject is not None else None
-            res = run_perfilter(st_u, swarm, unit_keys[:, u], J, sig_p[perms[u]], sig0_p[perms[u]], cool,
-                                cool[0], thresh=thresh, save_ancestors=not block,
-                                inject=None if inj is None else inj["perfilter"])
+            if fast:
+                inj = None
+                res = _perfilter_queued(units_st[u], unit_in[u], swarm, keys_d[u], J, sig_d[u], sig0_d[u],
+                                        cool_d[u], thresh, not block, ll_d[u], err_acc, stream)
+            else:
+                cool = np.array([rw_sd.cooling_factor(i, it, T) for i in range(T)], dtype=np.float32)
+                inj = inject[it][u]
+                res = run_perfilter(st_u, swarm, unit_keys[:, u], J, sig_p[perms[u]], sig0_p[perms[u]], cool,
+                                    cool[0], thresh=thresh, save_ancestors=not block,
+                                    inject=None if inj is None else inj["perfilter"])
             if n_monitors >= 1:
                 mean = swarm.mean(dim=2).cpu().numpy()
                 mon = np.stack([pprandom.split(k, n_monitors) for k in unit_keys[:, u]])
@@ -1117,7 +1179,7 @@ def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, 
                 pf = run_pfilter(st_u, np.repeat(mean, n_monitors, axis=0), mon.reshape(-1), J, thresh=thresh,
                                  est=True, inject=minj)
                 ll_units[:, u] = -(-pf["loglik"].reshape(n, n_monitors)).mean(axis=1)
-            else:
+            elif not fast:
                 ll_units[:, u] = res["loglik"].cpu().numpy()
             new_panel = res["swarm"].index_select(1, inv_t[u])                  # panel order
             if ns > 0:
@@ -1132,6 +1194,13 @@ def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, 
                     Us = torch.gather(Us, 3, idx)
                 Us = Us.clone()
                 Us[:, u] = new_panel[:, ns:]
+        if fast:
+            err = int(err_acc.item())
+            if err:
+                _ffi.check(_ffi.PPF_ETIMEOUT if err & 1 else _ffi.PPF_EINTERNAL, "ppf_perfilter")
+            if n_monitors < 1:
+                ll_units = ll_d.T.cpu().numpy()
+            del pinned
         s_mean, u_mean = nat_means(*means())
         shared_tr[:, it + 1, 0] = ll_units.sum(axis=1)
         shared_tr[:, it + 1, 1:] = s_mean

@@ -156,3 +156,65 @@ def test_perfilter_natural_scale_bit_exact():
                           natural=True)
     assert np.array_equal(got["anc"], want["anc"])
     assert np.array_equal(got["swarm"], want["swarm"].transpose(0, 2, 1))
+
+
+@pytest.mark.parametrize("block", [True, False])
+def test_panel_mif_queued_units_equal_separate_calls(block):
+    """panel_mif queues its unit filters on device-resident inputs without
+    waiting between them; its swarms and unit log-likelihoods equal the
+    unit-by-unit run_perfilter calls they replace, bit for bit (ragged units)."""
+    import torch
+
+    from pypomp_b200 import functional as F
+    from pypomp_b200 import random as pprandom
+    from pypomp_b200.optim import RWSigma
+
+    pan = _ricker_panel()
+    st = pan.to_struct()
+    names = pan.get_unit_names()
+    J, M = 1500, 2
+    rw = RWSigma({n: 0.03 for n in pan.canonical_param_names}).geometric_cooling(0.5)
+    sh = np.repeat(pan.theta.shared_array()[:, None, :], J, axis=1)
+    un = np.repeat(pan.theta.unit_array(names)[:, None], J, axis=1)
+    keys = np.array([17], np.uint64)
+    s_tr, u_tr, s_fin, u_fin = F.panel_mif(st, sh, un, rw, M, J, keys, block=block)
+    # the same iterations unit by unit (the loop panel_mif runs with injected draws)
+    spec, U = st.spec, st.U
+    perms = np.asarray(st.permutations)
+    inv = np.argsort(perms, axis=1)
+    ns, nu = sh.shape[2], un.shape[3]
+    sig_p, sig0_p = rw.arrays(st.param_names)
+    panel0 = np.concatenate([sh[:, :, None, :].repeat(U, axis=2), un], axis=3)
+    est = np.empty_like(panel0)
+    for u in range(U):
+        est[:, :, u, :] = spec.to_est(panel0[:, :, u, perms[u]])[:, :, inv[u]]
+    S = torch.tensor(est[:, :, 0, :ns].transpose(0, 2, 1).copy(), dtype=torch.float32).cuda()
+    Us = torch.tensor(est[:, :, :, ns:].transpose(0, 2, 3, 1).copy(), dtype=torch.float32).cuda()
+    m_keys = np.stack([pprandom.split(k, M + 1)[1:] for k in keys])
+    for it in range(M):
+        unit_keys = np.stack([pprandom.split(k, U) for k in m_keys[:, it]])
+        for u in range(U):
+            st_u = st.unit(u)
+            T = st_u.ys.shape[0]
+            swarm = torch.cat([S, Us[:, u]], dim=1)[:, torch.tensor(perms[u]).cuda()].contiguous()
+            cool = np.array([rw.cooling_factor(i, it, T) for i in range(T)], dtype=np.float32)
+            res = F.run_perfilter(st_u, swarm, unit_keys[:, u], J, sig_p[perms[u]], sig0_p[perms[u]], cool,
+                                  cool[0], save_ancestors=not block)
+            assert res["loglik"].cpu().numpy()[0] == u_tr[0, it + 1, u, 0]
+            new = res["swarm"][:, torch.tensor(inv[u]).cuda()]
+            S = new[:, :ns].contiguous()
+            if not block:
+                origin = torch.arange(J).cuda().expand(1, J).contiguous()
+                for t in range(T):
+                    origin = torch.gather(origin, 1, res["anc"][:, t].long())
+                Us = torch.gather(Us, 3, origin[:, None, None, :].expand(1, U, nu, J))
+            Us = Us.clone()
+            Us[:, u] = new[:, ns:]
+    # final swarms on the natural scale, converted as panel_mif converts them
+    s_e = S.cpu().numpy().transpose(0, 2, 1)
+    u_e = Us.cpu().numpy().transpose(0, 3, 1, 2)
+    for u in range(U):
+        nat = spec.from_est(np.concatenate([s_e, u_e[:, :, u]], axis=2)[:, :, perms[u]])[:, :, inv[u]]
+        assert np.array_equal(nat[:, :, ns:], u_fin[:, :, u])
+        if u == 0:
+            assert np.array_equal(nat[:, :, :ns], s_fin)
