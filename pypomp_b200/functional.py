@@ -1139,14 +1139,19 @@ def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, 
         Tmax = max(u_in[4] for u_in in unit_in)
         err_acc = torch.zeros(1, dtype=torch.int32, device=dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
+
+        def unit_cooling(it):
+            c = np.zeros((U, Tmax), np.float32)
+            for u in range(U):
+                Tu = unit_in[u][4]
+                c[u, :Tu] = [rw_sd.cooling_factor(i, it, Tu) for i in range(Tu)]
+            return c
+        cool_next = unit_cooling(0)
     for it in range(M):
         unit_keys = np.stack([pprandom.split(k, U) for k in m_keys[:, it]])    # (n, U)
         ll_units = np.zeros((n, U))
         if fast:
-            cool_h = np.zeros((U, Tmax), np.float32)
-            for u in range(U):
-                Tu = unit_in[u][4]
-                cool_h[u, :Tu] = [rw_sd.cooling_factor(i, it, Tu) for i in range(Tu)]
+            cool_h = cool_next
             pinned = (torch.from_numpy(cool_h).pin_memory(),
                       torch.from_numpy(np.ascontiguousarray(unit_keys.T).view(np.int64)).pin_memory())
             cool_d = pinned[0].to(dev, non_blocking=True)                       # (U, Tmax)
@@ -1195,6 +1200,9 @@ def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, 
                 Us = Us.clone()
                 Us[:, u] = new_panel[:, ns:]
         if fast:
+            # the next iteration's cooling factors while this one's filters run
+            if it + 1 < M:
+                cool_next = unit_cooling(it + 1)
             err = int(err_acc.item())
             if err:
                 _ffi.check(_ffi.PPF_ETIMEOUT if err & 1 else _ffi.PPF_EINTERNAL, "ppf_perfilter")
