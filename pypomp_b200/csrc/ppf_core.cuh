@@ -47,6 +47,16 @@ __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
 __device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+// Strong relaxed accesses at GPU scope (coherent through L2, no ordering of
+// other memory): enough for a word that carries its own status and value.
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 
 // ---- TMA 1-D bulk copies (global -> this CTA's shared memory, no multicast)
 // tracked by an mbarrier transaction count.  Addresses and sizes must be

@@ -488,23 +488,27 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
     }
     if (rs) a.runpre[((size_t)f * a.ntiles + b) * TPB + threadIdx.x] = before + inc - qs;
   }
+  // Decoupled lookback.  Each descriptor word packs its status (2 bits) with the
+  // value, written by one 64-bit store, and nothing else is published through
+  // it (e, the run prefixes, excl and tot are read by the next kernel), so
+  // strong relaxed accesses suffice; release / acquire would only add fences.
   uint64_t* desc = a.desc[p] + (size_t)f * a.ntiles;
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     uint64_t excl = 0;
     if (b == 0) {
-      if (lane == 0) st_release_u64(desc, kStatusIncl | btot);
+      if (lane == 0) st_relaxed_u64(desc, kStatusIncl | btot);
     } else {
-      if (lane == 0) st_release_u64(desc + b, kStatusAgg | btot);
+      if (lane == 0) st_relaxed_u64(desc + b, kStatusAgg | btot);
       int pos = b - 1;
       long long spins = 0;
       bool timed_out = false;
       while (true) {
         const int idx = pos - lane;
-        uint64_t d = idx >= 0 ? ld_acquire_u64(desc + idx) : kStatusIncl;
+        uint64_t d = idx >= 0 ? ld_relaxed_u64(desc + idx) : kStatusIncl;
         while (__any_sync(0xffffffffu, (d >> 62) == 0ull)) {
           if (++spins > kSpinCap) { timed_out = true; break; }
-          if ((d >> 62) == 0ull) { __nanosleep(32); d = ld_acquire_u64(desc + idx); }
+          if ((d >> 62) == 0ull) { __nanosleep(32); d = ld_relaxed_u64(desc + idx); }
         }
         if (timed_out) break;
         const unsigned int inc = __ballot_sync(0xffffffffu, (d >> 62) == 2ull);
@@ -517,7 +521,7 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
         pos -= 32;
       }
       if (timed_out && lane == 0) atomicOr(a.err, 1u);
-      if (lane == 0) st_release_u64(desc + b, kStatusIncl | (excl + btot));
+      if (lane == 0) st_relaxed_u64(desc + b, kStatusIncl | (excl + btot));
     }
     if (lane == 0) {
       a.excl[(size_t)f * a.ntiles + b] = excl;
