@@ -34,6 +34,16 @@ class PompStruct:
         return list(self.spec.param_names)
 
 
+def align_params(params, names, axis: int = -1) -> np.ndarray:
+    """Stack named parameter values in the order ``names``
+    (``pypomp/functional/utils.py:7-48``), e.g. ``struct.param_names``."""
+    try:
+        return np.stack([np.asarray(params[name]) for name in names], axis=axis)
+    except KeyError as e:
+        raise KeyError(
+            f"Parameter '{e.args[0]}' is required by the model structure but missing from inputs.") from e
+
+
 def _device_inputs(torch, struct: PompStruct, dev):
     ys = np.asarray(struct.ys, dtype=np.float32)
     if ys.ndim == 2:

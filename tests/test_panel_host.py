@@ -46,3 +46,13 @@ def test_pruned_keeps_the_best_and_refills():
     assert [d["shared"].loc["sigma", "shared"] for d in q2.params()] == pytest.approx([0.2, 0.1])
     with pytest.raises(ValueError):
         p.pruned(n=0)
+
+
+def test_align_params_orders_and_reports_missing_names():
+    from pypomp_b200 import functional as F
+
+    assert F.align_params({"beta": 0.5, "gamma": 0.1}, ["gamma", "beta"]).tolist() == [0.1, 0.5]
+    out = F.align_params({"beta": np.array([0.5, 0.6]), "gamma": np.array([0.1, 0.2])}, ["gamma", "beta"])
+    assert out.shape == (2, 2) and out[:, 0].tolist() == [0.1, 0.2] and out[:, 1].tolist() == [0.5, 0.6]
+    with pytest.raises(KeyError, match="required by the model structure"):
+        F.align_params({"beta": 0.5}, ["gamma", "beta"])
