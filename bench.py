@@ -54,6 +54,11 @@ SUM_BYTES = 4
 # 24-seed case (dram__bytes_read.sum + dram__bytes_write.sum = 121.1 MB for
 # 6.29 M particles); traffic is proportional to the particles processed
 RESPROP_TRAFFIC_PER_PARTICLE = 19.25
+# DRAM traffic of one k_simulate launch per trajectory-step, from an ncu capture
+# of LG 2-D, 1 parameter set x 65536 replicates x T = 200 (188.0 MB written +
+# 37.0 MB read for 13.1 M trajectory-steps); the writes and the partial-sector
+# reads both grow with the trajectory-steps written
+SIM_TRAFFIC_PER_TRAJ_STEP = 225.0e6 / (65536 * 200)
 
 
 def rank_seeds(rank: int) -> np.ndarray:
@@ -617,7 +622,7 @@ def run_sim(args):
                 "h2d_bytes_per_step": int(th.nbytes + keys.nbytes),
                 "d2h_bytes_per_step": int(4 * Fs * nsim * ((Ts + 1) * 2 + Ts * 2))},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "kernel": "k_simulate",
+                     "frac": achieved / peak, "traffic": SIM_TRAFFIC_PER_TRAJ_STEP * steps, "kernel": "k_simulate",
                      "peak_source": peak_kind},
         "ricker": {"value": steps / (rms / 1e3), "ms_per_step": rms, "unit": "trajectory-steps/s"},
         "cpu_baseline": cpu or None, "clocks": clk, "gpu_launches": k_n * args.steps}))
