@@ -19,8 +19,17 @@ cores; ``plain`` times the one-filter-at-a-time baseline kernels.
 
 ``--impl reference`` times the reference's CPU path.  The reference (pypomp on
 JAX) cannot run on this image (no jax), so the arm times the oracle's C
-restatement of the same algorithm with every host thread, on a bounded sample
-of the workload, and reports the same metric.
+restatement of the path with every host thread, on a bounded sample of the
+workload (a prefix of the observations for a subset of the seeds), and reports
+the same metric and config.  The restatement uses this library's exact
+arithmetic (fixed-point resampling CDF, polynomial exp / log), not the
+reference's float32 running-sum CDF.  That arm builds its inputs from
+``oracle/workloads.py`` and never loads the CUDA library.
+
+Accuracy: the LG lines state the particle filter's log-likelihood error
+against the exact FP64 Kalman log-likelihood of the same data
+(``loglik_err_vs_kalman``: relative error of the mean over the filters, and
+its z-score against the Monte Carlo standard error).
 """
 
 from __future__ import annotations
@@ -46,6 +55,7 @@ UNIT = "particle-steps/s"
 J, T, NSEED = 262144, 1000, 64
 LG_Q = np.array([[1.0, 1e-4], [1e-4, 1.0]]) / 100
 LG_R = np.array([[1.0, 0.1], [0.1, 1.0]]) / 10
+LG_A = np.array([[math.cos(0.2), -math.sin(0.2)], [math.sin(0.2), math.cos(0.2)]])
 # algorithmic bytes per particle of the resample+propagate kernel (LG, dx=2):
 # read parent log-weight 4 + parent state 8, write child state 8 + log-weight 4
 RESPROP_BYTES = 24
@@ -87,6 +97,48 @@ def workload():
 
     m = pp.LG(T=T, Q=LG_Q, R=LG_R, key=0)
     return m
+
+
+def headline_config(world: int) -> dict:
+    """The workload's config, printed identically by both arms."""
+    return {"workload": "LG 2-D pfilter, T=1000, J=262144, 64 seeds per GPU",
+            "model": "LG", "global_batch": NSEED * world, "seq_len": T, "particles": J,
+            "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (state 2x64x262144x12 B = 403 MB per step)"}
+
+
+def kalman_loglik(ys, A, C, Q, R, X0) -> float:
+    """Exact FP64 log-likelihood of the LG model (x0 ~ N(X0, Q) at t0, one
+    transition before the first observation, so the filter starts from P = Q)."""
+    ys = np.asarray(ys, dtype=np.float64)
+    x = np.asarray(X0, dtype=np.float64).copy()
+    P = np.asarray(Q, dtype=np.float64).copy()
+    ll = 0.0
+    for y in ys:
+        xp, Pp = A @ x, A @ P @ A.T + Q
+        S = C @ Pp @ C.T + R
+        L = np.linalg.cholesky(S)
+        v = y - C @ xp
+        a = np.linalg.solve(L, v)
+        ll -= 0.5 * (len(v) * math.log(2 * math.pi) + a @ a) + float(np.sum(np.log(np.diag(L))))
+        K = np.linalg.solve(S, C @ Pp).T
+        x, P = xp + K @ v, Pp - K @ C @ Pp
+    return float(ll)
+
+
+def loglik_error(logliks, exact: float) -> dict:
+    """The filters' log-likelihood estimate against the exact value: the
+    log-mean-exp over the filters (pypomp's logLik over replicates) with its
+    jackknife standard error, its relative error and the z-score of the
+    difference; the plain mean and sd of the estimates are listed beside."""
+    from pypomp_b200.maths import logmeanexp, logmeanexp_se
+
+    ll = np.asarray(logliks, dtype=np.float64)
+    lme, se = float(logmeanexp(ll)), float(logmeanexp_se(ll))
+    return {"kalman": exact, "pf_logmeanexp": lme, "se": se, "n_filters": int(ll.size),
+            "rel_err": abs(lme - exact) / abs(exact),
+            "z": (lme - exact) / se if se > 0 else None,
+            "pf_mean": float(np.mean(ll)), "pf_sd": float(np.std(ll, ddof=1)) if ll.size > 1 else None}
 
 
 def peaks():
@@ -144,43 +196,52 @@ class ClockSampler:
 
 
 def cpu_baseline(nthreads: int, Tsample: int = 40, F: int | None = None):
-    """C restatement (oracle) on the host's cores, bounded sample of the workload."""
+    """C restatement (oracle) on the host's cores, bounded sample of the
+    workload: F seeds (one per thread) over the first Tsample observations."""
     from oracle import cora
+    from oracle.workloads import headline_lg
 
-    m = workload()
-    st = m.to_struct()
-    th = m.theta.to_array(m.canonical_param_names)
+    th, ys = headline_lg(T, seed=0)
     F = F or nthreads
     t0 = time.perf_counter()
-    cora.pfilter(1, 2, 2, np.repeat(th, F, 0), st.ys[:Tsample], J,
+    cora.pfilter(1, 2, 2, np.repeat(th[None], F, 0), ys[:Tsample], J,
                  seeds=np.arange(F, dtype=np.uint64), nthreads=nthreads)
     dt = time.perf_counter() - t0
     return F * J * Tsample / dt, dt, F, Tsample
 
 
 def run_reference(args):
+    """The reference arm: the C restatement on every host thread.  Each step
+    filters one seed per thread over the first REF_T_SAMPLE observations (a few
+    seconds of CPU work); ``ms_per_step`` is the time of that sample."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
-    vals = []
+    Ts = args.ref_t
+    times = []
     for i in range(args.warmup + args.steps):
-        v, dt, F, Ts = cpu_baseline(nthreads, Tsample=10, F=nthreads)
+        v, dt, F, _ = cpu_baseline(nthreads, Tsample=Ts, F=nthreads)
         if i >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
-    sample = f"{nthreads} of the 64 seeds x J={J} x first 10 of T={T} observations per step"
+            times.append(dt)
+    total = sum(times)
+    units = nthreads * J * Ts
+    value = units * len(times) / total
+    sample = (f"per step {nthreads} of the 64 seeds (one per thread) x J={J} x the first {Ts} of "
+              f"T={T} observations = {units:.3g} particle-steps")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": NSEED * J * T / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": total / len(times) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "LG 2-D pfilter, T=1000, J=262144, 64 seeds",
-                   "model": "LG", "global_batch": NSEED, "seq_len": T, "particles": J},
+        "config": headline_config(world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
                          "sample": sample,
-                         "note": "reference JAX CPU path unavailable (jax not installed); "
-                                 "C restatement of the same algorithm, all host threads"},
+                         "note": "the reference's JAX CPU path cannot run here (jax not installed); "
+                                 "C restatement of the path with this library's exact arithmetic "
+                                 "(fixed-point resampling CDF, polynomial exp / log), not the "
+                                 "reference's float32 running-sum CDF; all host threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -312,6 +373,14 @@ def run_ours(args):
         plain = {"value": plain_value, "unit": UNIT, "filters_timed": Fp,
                  "ratio_batched_over_plain": value / world / plain_value}
 
+    # ---- accuracy: the 64 log-likelihoods against the exact Kalman value ----
+    kalman_err = loglik_error(loglik, kalman_loglik(st.ys, LG_A, np.eye(2), LG_Q, LG_R, np.zeros(2)))
+
+    # ---- MOP-alpha value + gradient (the metric's second half) ------------
+    mop = None
+    if rank == 0 and not args.skip_mop:
+        mop = mop_block(args)
+
     # ---- CPU baseline (rank 0, N=1) ---------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -326,11 +395,8 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "LG 2-D pfilter, T=1000, J=262144, 64 seeds per GPU",
-                       "model": "LG", "global_batch": NSEED * world, "seq_len": T, "particles": J,
-                       "parallelism": f"replicas{world}", "path": "stream",
-                       "cuda_graph": bool(args.graph),
-                       "l2": "inputs larger than L2 (state 2x64x262144x12 B = 403 MB per step)"},
+            "config": headline_config(world),
+            "path": "stream", "cuda_graph": bool(args.graph),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "api": "pypomp_b200.functional.pfilter"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -344,7 +410,8 @@ def run_ours(args):
             "plain": plain,
             "clocks": clk.summary(),
             "gpu_launches": launches_per_step * args.steps,
-            "loglik_mean": float(np.mean(loglik)),
+            "loglik_err_vs_kalman": kalman_err,
+            "mop": mop,
         }
         print(json.dumps(line))
     if world > 1:
@@ -399,23 +466,30 @@ def run_c1(args):
     ms, clk = _timed(fn, args.steps, args.warmup, stream)
     reps = F.run_pfilter(st, np.repeat(th, 256, 0), np.arange(256, dtype=np.uint64), 1000, path="resident")
     ll = reps["loglik"]
+    err = loglik_error(ll, kalman_loglik(st.ys, LG_A, np.eye(2), LG_Q, LG_R, np.zeros(2)))
     _line(args, "LG 2-D pfilter, T=50, J=1000, one filter, resident path",
           1000 * 50 / (ms / 1e3), ms,
           {"e2e": {"value": 1000 * 50 / (ms / 1e3), "unit": UNIT, "api": "functional.run_pfilter",
                    "h2d_bytes_per_step": int(st.ys.nbytes + th.nbytes + 8), "d2h_bytes_per_step": 0},
-           "pf_loglik_mean_256_seeds": float(np.mean(ll)),
-           "pf_loglik_sd": float(np.std(ll)), "clocks": clk, "roofline": None,
+           "loglik_err_vs_kalman": err, "clocks": clk, "roofline": None,
            "note": "one CTA; latency bound, no HBM traffic to speak of"})
 
 
-def run_c3(args):
-    """SV MOP-alpha value + gradient: T=2000, J=65536, alpha=0.97, one parameter set."""
+def mop_block(args, steps=None, warmup=None):
+    """SV MOP-alpha value + gradient, T=2000, J=65536, alpha=0.97, one parameter
+    set: particle-steps/s over whole value+gradient calls (device-resident
+    inputs, one call = forward filter + adjoint sweep), per-kernel GB/s from
+    CUDA events around each launch (launched without the graph, which adds a
+    few per cent per launch), and the roofline of the whole call at the
+    algorithmic bytes of its kernels."""
     import torch
 
     import pypomp_b200 as pp
     from pypomp_b200 import _ffi
     from pypomp_b200.functional import MopCall
 
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     Jm, Tm = 65536, 2000
     m = pp.SV(T=Tm, key=0)
     st = m.to_struct()
@@ -424,8 +498,9 @@ def run_c3(args):
     if args.graph:
         call.d.flags |= _ffi.F_GRAPH
     stream = torch.cuda.current_stream()
-    ms, clk = _timed(lambda: call.forward(grad=True), args.steps, args.warmup, stream)
+    ms, clk = _timed(lambda: call.forward(grad=True), steps, warmup, stream)
     torch.cuda.synchronize()
+    res = {k: v.cpu().numpy() for k, v in call.out.items()}
     _ffi.profile_begin()
     call.forward(grad=True)
     prof = _ffi.profile_end()
@@ -434,23 +509,35 @@ def run_c3(args):
     # forward resample+propagate 24 + ancestor 4 + first-child offset 4; sums 4;
     # recompute 8 + 4 + 8; adjoint 8 (x) + 4 (anc) + 4 (offset) + 12 (adjoint in)
     # + 12 (adjoint out)
-    bytes_kind = {"resample_propagate": 32, "sum_lookback": 4, "mop_recompute": 20, "mop_adjoint": 40}
+    bytes_kind = {"resample_propagate": 32, "sum_lookback": 4, "mop_forward": 32, "mop_recompute": 20,
+                  "mop_adjoint": 40}
     peak, peak_kind = peaks()
     kern = {}
     for k, (tms, n) in prof.items():
-        if k in bytes_kind and n:
+        if n:
             avg = tms / n
-            per_launch_units = Jm
-            kern[k] = {"launches": n, "total_ms": tms, "avg_ms": avg,
-                       "GBps": bytes_kind[k] * per_launch_units / (avg / 1e3) / 1e9}
-    dom = max(kern, key=lambda k: kern[k]["total_ms"])
-    res = call.out
-    _line(args, "SV MOP-alpha value+grad, T=2000, J=65536, alpha=0.97", value, ms,
-          {"e2e": None, "clocks": clk, "kernels": kern,
-           "roofline": {"bound": "hbm", "achieved": kern[dom]["GBps"], "peak": peak, "unit": "GB/s",
-                        "frac": kern[dom]["GBps"] / peak, "traffic": None, "kernel": dom,
-                        "peak_source": peak_kind},
-           "value_out": float(res["value"][0]), "grad_out": res["grad"][0].tolist()})
+            e = {"launches": n, "total_ms": tms, "avg_ms": avg}
+            if k in bytes_kind:
+                e["GBps"] = bytes_kind[k] * Jm / (avg / 1e3) / 1e9
+            kern[k] = e
+    call_bytes = 92 * Jm * Tm
+    return {"workload": "SV MOP-alpha value+grad, T=2000, J=65536, alpha=0.97, one parameter set",
+            "value": value, "unit": UNIT, "ms_per_call": ms, "steps": steps, "warmup": warmup,
+            "cuda_graph": bool(args.graph), "kernels": kern, "clocks": clk,
+            "roofline": {"bound": "hbm", "achieved": call_bytes / (ms / 1e3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": call_bytes / (ms / 1e3) / 1e9 / peak,
+                         "algorithmic_bytes_per_particle_step": 92, "peak_source": peak_kind,
+                         "basis": "whole value+grad call"},
+            "value_out": float(res["value"][0]), "grad_out": res["grad"][0].tolist(),
+            "grad_finite": bool(np.all(np.isfinite(res["grad"])))}
+
+
+def run_c3(args):
+    """SV MOP-alpha value + gradient: T=2000, J=65536, alpha=0.97, one parameter set."""
+    b = mop_block(args)
+    _line(args, b["workload"], b["value"], b["ms_per_call"],
+          {"e2e": None, "clocks": b["clocks"], "kernels": b["kernels"], "roofline": b["roofline"],
+           "value_out": b["value_out"], "grad_out": b["grad_out"], "grad_finite": b["grad_finite"]})
 
 
 def run_c4(args):
@@ -544,6 +631,11 @@ def run_c5(args):
                       chunk_size=U)
         tr_ms, tr_wall = timed(lambda n: F.panel_train(st, s0, u0, Jp, Adam(), n, eta, 0.97,
                                                         np.array([4], np.uint64), chunk_size=U), args.steps)
+    # per unit: is the MOP gradient at the starting parameters finite?
+    est_all = np.stack([m_.spec.to_est(m_.theta.to_array(m_.canonical_param_names))[0]
+                        for m_ in units.values()])[None].astype(np.float32)
+    pm = F.panel_mop(st, est_all, Jp, 0.97, np.arange(U, dtype=np.uint64)[None] + 77, grad=True)
+    finite_u = np.all(np.isfinite(pm["grad"][0]), axis=-1)
     mif_rate = steps_units * args.steps / (mif_ms / 1e3)
     tr_rate = steps_units * args.steps / (tr_ms / 1e3)
     job_s = 100 * mif_ms / args.steps / 1e3 + 50 * tr_ms / args.steps / 1e3
@@ -552,7 +644,16 @@ def run_c5(args):
           {"e2e": {"value": mif_rate, "unit": UNIT, "api": "functional.panel_mif (host inputs)",
                    "h2d_bytes_per_step": int(sh.nbytes + un.nbytes + st.ys.nbytes), "d2h_bytes_per_step": 0},
            "train": {"value": tr_rate, "unit": UNIT, "ms_per_step": tr_ms / args.steps,
-                     "api": "functional.panel_train, chunk_size=U (one MOP call per step)"},
+                     "api": "functional.panel_train, chunk_size=U (one MOP call per step)",
+                     "grad_finite_units": int(finite_u.sum()), "units": U,
+                     "grad_finite_by_T_u": {"T_u<=150": int(finite_u[T_u <= 150].sum()),
+                                            "of": int((T_u <= 150).sum()),
+                                            "T_u>150": int(finite_u[T_u > 150].sum()),
+                                            "of_long": int((T_u > 150).sum())},
+                     "valid": bool(finite_u.all()),
+                     "note": "the speed of the MOP calls only: along chaotic Ricker trajectories "
+                             "(log r near 3.8) the pathwise MOP gradient overflows float32 on long "
+                             "series, and the update then propagates NaN as the reference's would"},
            "sum_T_u": int(T_u.sum()), "full_job_seconds_estimate": job_s,
            "wall_s": {"mif": mif_wall, "train": tr_wall}, "clocks": clk.summary(),
            "roofline": None,
@@ -716,6 +817,9 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-t", type=int, default=40)
+    ap.add_argument("--ref-t", type=int, default=50,
+                    help="observations per step of the reference arm's sample")
+    ap.add_argument("--skip-mop", action="store_true", help="leave the MOP value+grad block out")
     ap.add_argument("--profile-case", action="store_true",
                     help="run one small call of the same kernels (for ncu) and exit")
     ap.add_argument("--path", default="stream")

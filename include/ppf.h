@@ -251,6 +251,19 @@ int ppf_workspace_status(const void* workspace, void* stream);
 int ppf_profile_begin(void);
 int ppf_profile_end(double* ms, int* count, int n);
 
+/* Test hook for the bounded device-side waits (the decoupled-lookback spin in
+ * the weight-sum kernel and the bulk-copy barrier waits of the resampling
+ * kernel): set how many polls a wait makes before it gives up, for the calls
+ * that follow (polls < 0 restores the default, 2^22; larger values are
+ * clamped to it; 0 makes every such wait give up at its first check).  A wait
+ * that gives up sets the workspace's error word, so ppf_workspace_status
+ * reports PPF_ETIMEOUT and the call's outputs are invalid; a kernel whose
+ * copy wait gave up still drains that copy before it continues.  CUDA graphs
+ * cached by PPF_F_GRAPH keep the limit they were captured with.  Returns the
+ * previous limit.  Host-side setting, not thread-safe.  No counterpart in the
+ * reference (XLA has no device-side waits). */
+long long ppf_debug_set_wait_limit(long long polls);
+
 /* ppf_pfilter for callers that cannot allocate device memory.  No counterpart
  * in the reference: pypomp runs on JAX, whose runtime owns device memory.
  * Some callers of this library cannot hand it a workspace -- a host runtime
@@ -260,9 +273,13 @@ int ppf_profile_end(double* ms, int* count, int n);
  * ignored) on a scratch array of PPF_NOALLOC_SCRATCH_BYTES compiled into the
  * library, and allocates nothing.  A request whose workspace
  * (ppf_pfilter_workspace_bytes) exceeds that size returns PPF_ESCRATCH.  All
- * calls on a device share the array, so calls that overlap on the GPU race;
- * the first call on a device looks up the array's address and should come
- * before any stream capture; the call synchronises the stream. */
+ * calls on a device share the array, so calls that overlap on the GPU race.
+ * The first call on a device looks up the array's device address.  Every call
+ * is synchronous: it waits for `stream` and then reads the device-side status,
+ * so it returns PPF_EUNSUPPORTED, before doing any work, when `stream` is
+ * being captured into a CUDA graph.  PPF_F_GRAPH is ignored (a cached graph
+ * would need driver-side allocations); the launches go directly onto
+ * `stream`. */
 #define PPF_NOALLOC_SCRATCH_BYTES (16u << 20)
 int ppf_pfilter_noalloc(const ppf_pfilter_desc* d, void* stream);
 

@@ -186,7 +186,7 @@ def mop_surrogate(kind, dx, dy, theta_est, ys, J, alpha, anc, m0=None, *, seeds=
                 setattr(d, name, _p(a))
     d.flags = flags
     anc = np.ascontiguousarray(anc, dtype=np.int32)
-    m0_out = np.zeros((F, T, J), np.float32)
+    m0_out = np.zeros((F, T, J), np.float32) if m0 is None else None
     m0_in = None if m0 is None else np.ascontiguousarray(m0, dtype=np.float32)
     value = np.zeros(F, np.float64)
     rc = _L().ppfo_mop_surrogate(ctypes.byref(d), float(alpha), _p(anc), _p(m0_in), _p(m0_out), _p(value))

@@ -26,7 +26,10 @@ into injection arrays.
 The resampling CDF here is the reference's float32 running sum.  The CUDA path
 uses an exact fixed-point CDF instead (defined in ``include/ppf.h``); the C
 oracle (``oracle/ppf_oracle.c``) restates that definition for bit-exact
-comparisons, and tests report how often the two CDFs pick different ancestors.
+comparisons.  ``tests/test_oracle_cdf_mismatch.py`` measures how often the two
+pick different ancestors on the same weights (none of 1000, about 0.1 % of
+4096 and 10 % of 65536 children on its LG case, always a neighbouring parent)
+and how far whole runs then diverge.
 """
 
 from __future__ import annotations

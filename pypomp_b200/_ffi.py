@@ -51,6 +51,7 @@ EXPORTED = (
     "ppf_pfilter_noalloc",
     "ppf_simulate",
     "ppf_profile_begin",
+    "ppf_debug_set_wait_limit",
     "ppf_profile_end",
     "ppf_error_string",
     "ppf_version",
@@ -214,6 +215,8 @@ def _load():
     lib.ppf_simulate.restype = ctypes.c_int
     lib.ppf_workspace_status.argtypes = [_vp, _vp]
     lib.ppf_workspace_status.restype = ctypes.c_int
+    lib.ppf_debug_set_wait_limit.argtypes = [ctypes.c_longlong]
+    lib.ppf_debug_set_wait_limit.restype = ctypes.c_longlong
     lib.ppf_profile_begin.argtypes = []
     lib.ppf_profile_begin.restype = ctypes.c_int
     lib.ppf_profile_end.argtypes = [_vp, _vp, ctypes.c_int]

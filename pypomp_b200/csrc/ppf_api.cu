@@ -150,8 +150,12 @@ static int choose_tile(const ppf_model& m, int J, int F, int U, int inj, int req
   return kTileSmall;
 }
 
+// Polls before a bounded device-side wait gives up (ppf_debug_set_wait_limit).
+static long long g_spin_cap = kSpinCap;
+
 static int fill_args(const ppf_pfilter_desc* d, Args& a, int mode) {
   memset(&a, 0, sizeof(a));
+  a.spin_cap = g_spin_cap;
   a.model = d->model;
   a.J = d->J; a.F = d->F; a.T = d->T; a.U = d->U;
   a.flags = d->flags;
@@ -559,6 +563,12 @@ int ppf_workspace_status(const void* workspace, void* stream) {
   if (err & 1u) return PPF_ETIMEOUT;
   if (err) return PPF_EINTERNAL;
   return PPF_OK;
+}
+
+long long ppf_debug_set_wait_limit(long long polls) {
+  const long long prev = g_spin_cap;
+  g_spin_cap = polls < 0 ? kSpinCap : (polls > kSpinCap ? kSpinCap : polls);
+  return prev;
 }
 
 int ppf_profile_begin(void) {

@@ -19,6 +19,7 @@ constexpr uint64_t kStatusAgg = 1ull << 62;
 constexpr uint64_t kStatusIncl = 2ull << 62;
 constexpr uint64_t kValueMask = (1ull << 62) - 1;
 constexpr long long kSpinCap = 1ll << 22;          // bounded waits: then PPF_ETIMEOUT
+                                                   // (ppf_debug_set_wait_limit lowers it per call)
 
 // Per-filter, per-step accumulators (double-buffered by step parity).
 struct Acc {
@@ -81,9 +82,10 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-// Wait for phase `parity` of the barrier; false if the bounded wait gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long long i = 0; i < kSpinCap; ++i) {
+// Wait for phase `parity` of the barrier; false if the bounded wait gave up
+// after `cap` polls (cap 0: gives up at once).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long cap = kSpinCap) {
+  for (long long i = 0; i < cap; ++i) {
     uint32_t done;
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"

@@ -53,6 +53,7 @@ struct Args {
   float* W[2];            // [F][J] each
   unsigned char* consts;  // [F][512 B] per-filter model constants
   int tile, ntiles;
+  long long spin_cap;     // polls before a bounded device-side wait gives up
   size_t ctrl_bytes;      // leading workspace bytes zeroed per call
   // plain path
   uint64_t* pl_cdf;       // [J]

@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
         const int idx = pos - lane;
         uint64_t d = idx >= 0 ? ld_relaxed_u64(desc + idx) : kStatusIncl;
         while (__any_sync(0xffffffffu, (d >> 62) == 0ull)) {
-          if (++spins > kSpinCap) { timed_out = true; break; }
+          if (++spins > a.spin_cap) { timed_out = true; break; }
           if ((d >> 62) == 0ull) { __nanosleep(32); d = ld_relaxed_u64(desc + idx); }
         }
         if (timed_out) break;

@@ -19,10 +19,15 @@
 //    and fully writes the particle arrays before reading them;
 //  - the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (the host-side name is only a stand-in, not a device
-//    pointer); make that first call before any stream capture begins;
+//    pointer);
 //  - the call is synchronous: it waits for the stream, then reads the status
 //    word the kernels leave at the start of the scratch area, so a bounded
-//    device-side wait that gave up is reported as PPF_ETIMEOUT.
+//    device-side wait that gave up is reported as PPF_ETIMEOUT.  A stream
+//    wait cannot be recorded into a CUDA graph, so the call refuses to run
+//    (PPF_EUNSUPPORTED, before any work) while its stream is capturing;
+//  - PPF_F_GRAPH is ignored: replaying a cached graph would need a private
+//    stream and graph objects, which the driver allocates, so the launches
+//    always go directly onto the caller's stream.
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -61,6 +66,10 @@ int ppf_pfilter_noalloc(const ppf_pfilter_desc* d, void* stream) {
   const size_t need = ppf_pfilter_workspace_bytes(d);
   if (need == 0) return PPF_EINVAL;
   if (need > PPF_NOALLOC_SCRATCH_BYTES) return PPF_ESCRATCH;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return PPF_ECUDA;
+  if (cap != cudaStreamCaptureStatusNone) return PPF_EUNSUPPORTED;
   void* scratch = nullptr;
   const int rc = scratch_address(&scratch);
   if (rc != PPF_OK) return rc;
@@ -68,9 +77,9 @@ int ppf_pfilter_noalloc(const ppf_pfilter_desc* d, void* stream) {
   memcpy(&local, d, sizeof(local));
   local.workspace = scratch;
   local.ws_bytes = PPF_NOALLOC_SCRATCH_BYTES;
+  local.flags &= ~PPF_F_GRAPH;   // direct launches only: no driver-side graph objects
   const int run = ppf_pfilter(&local, stream);
   if (run != PPF_OK) return run;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   uint32_t status = 0;   // first word of the scratch: device-side error bits
   if (cudaMemcpyAsync(&status, scratch, sizeof(status), cudaMemcpyDeviceToHost, s) != cudaSuccess)
     return PPF_ECUDA;

@@ -195,8 +195,14 @@ __global__ void __launch_bounds__(TPB, RespropOccupancy<M>::B * (256 / TPB)) k_r
   const float base = (a.mode == MODE_MOP) ? 0.0f : a.base_rs;
   const int l0 = threadIdx.x * IT;
   __syncthreads();   // barrier init visible to all threads
+  // A wait that gives up marks the call failed (error bit 1, PPF_ETIMEOUT) and
+  // then still drains its own copy, so the CTA never leaves with a bulk copy
+  // in flight into its shared memory; what it computes is flagged invalid.
   bool ok = true;
-  if (bulk) ok = mbar_wait(&bar[0], 0);
+  if (bulk && !mbar_wait(&bar[0], 0, a.spin_cap)) {
+    ok = false;
+    mbar_wait(&bar[0], 0);
+  }
 
   // 1-2. parents: CDF and first-child offsets (or identity), staged states
   {
@@ -247,7 +253,10 @@ __global__ void __launch_bounds__(TPB, RespropOccupancy<M>::B * (256 / TPB)) k_r
     }
   }
   if (bulk) {
-    if (!mbar_wait(&bar[1], 0)) ok = false;
+    if (!mbar_wait(&bar[1], 0, a.spin_cap)) {
+      ok = false;
+      mbar_wait(&bar[1], 0);
+    }
   } else {
     for (int l = threadIdx.x; l < ntile; l += TPB)
 #pragma unroll

@@ -530,6 +530,22 @@ def mop_value_and_grad(struct: PompStruct, thetas_array, J: int, alpha: float, k
     return res["value"] * scale, res["grad"] * scale
 
 
+def _warn_nonfinite(grad, m: int) -> None:
+    """The reference applies a MOP gradient as it comes (its clip is
+    elementwise, ``train.py:115-116``, and lets NaN through), so a gradient
+    that overflowed float32 -- as pathwise derivatives along chaotic
+    trajectories do over long series -- turns the parameters into NaN.  Same
+    semantics here, but the caller is told."""
+    bad = ~np.isfinite(np.asarray(grad))
+    if bad.any():
+        import warnings
+
+        rows = np.unique(np.nonzero(bad.reshape(bad.shape[0], -1))[0]) if bad.ndim > 1 else [0]
+        warnings.warn(f"train iteration {m}: non-finite MOP gradient entries ({int(bad.sum())}) in "
+                      f"{len(rows)} parameter set(s); the update propagates them, as the reference does",
+                      RuntimeWarning, stacklevel=3)
+
+
 def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alpha: float, keys,
           alpha_cooling: float = 1.0, thresh: float = 0.0, n_monitors: int = 1):
     """MOP-alpha gradient training (``pypomp/functional/train.py:14-110`` /
@@ -605,6 +621,7 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
         hkeys = np.zeros(n, np.uint64)
         for i in range(n):
             chain[i], hkeys[i] = (int(v) for v in pprandom.split(chain[i]))
+        _warn_nonfinite(grad, m)
         if optimizer.clip_norm is not None:
             grad = np.clip(grad, -optimizer.clip_norm, optimizer.clip_norm)
         hess_fn = (lambda: mop_hessian_fd(struct, th, hkeys, J, alpha_m)) if optimizer.needs_hessian else None
@@ -1337,6 +1354,7 @@ def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optim
             grad_s = gp[:, :, :ns].sum(axis=1) * scale
             grad_u = gp[:, :, ns:] * scale * cs
             chunk_nll[:, c] = val.sum(axis=1) * scale * (Tn * U)
+            _warn_nonfinite(gp, m)
             if optimizer.clip_norm is not None:
                 grad_s = np.clip(grad_s, -optimizer.clip_norm, optimizer.clip_norm)
                 grad_u = np.clip(grad_u, -optimizer.clip_norm, optimizer.clip_norm)

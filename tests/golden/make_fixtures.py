@@ -3,7 +3,7 @@
 Run from the repository root (needs the reference checkout only to read its
 regression CSVs; the GPU tests read only the files written here):
 
-    python tests/golden/make_fixtures.py [/path/to/reference]
+    python tests/golden/make_fixtures.py /path/to/reference-checkout
 
 Writes
   ref_values.json  the reference's locked regression values, read from
@@ -150,4 +150,6 @@ def mif_cooling(nt, m, ntimes):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py /path/to/reference-checkout")
+    main(Path(sys.argv[1]))

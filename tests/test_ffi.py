@@ -80,3 +80,16 @@ def test_simulate_validation_without_gpu():
     assert _ffi.LIB.ppf_simulate(d, None) == _ffi.PPF_EINVAL      # null pointers
     d.model = _ffi.PpfModel(_ffi.MODEL_RICKER, 1, 1, 3, 0.0, 0)   # wrong parameter count
     assert _ffi.LIB.ppf_simulate(d, None) == _ffi.PPF_EINVAL
+
+
+def test_wait_limit_hook_is_host_only():
+    """ppf_debug_set_wait_limit only changes a host-side setting (no GPU work):
+    it returns the previous limit, restores the default for negative values
+    and clamps larger ones to it."""
+    from pypomp_b200 import _ffi
+
+    default = 1 << 22
+    assert _ffi.LIB.ppf_debug_set_wait_limit(5) == default
+    assert _ffi.LIB.ppf_debug_set_wait_limit(1 << 40) == 5
+    assert _ffi.LIB.ppf_debug_set_wait_limit(-1) == default
+    assert _ffi.LIB.ppf_debug_set_wait_limit(-1) == default

@@ -5,9 +5,12 @@ that owns the device memory pool, or plugin code that may not call the CUDA
 allocator -- so ppf_pfilter_noalloc runs the batched filter on a fixed scratch
 array compiled into the library.  This file checks, through the C ABI, that two
 calls in a row give the same results as the ordinary ppf_pfilter with a
-caller-provided workspace (the tolerance of the other parity tests), and that a
-request larger than the fixed scratch is refused with PPF_ESCRATCH before any
-GPU work.  It is collected last on purpose and also passes alone.
+caller-provided workspace (the tolerance of the other parity tests), also with
+PPF_F_GRAPH set (the flag is ignored: a cached graph would need driver-side
+allocations), that a request larger than the fixed scratch is refused with
+PPF_ESCRATCH before any GPU work, and that a call on a stream being captured
+into a CUDA graph is refused (the call waits for its stream, which a capture
+cannot record).  It is collected last on purpose and also passes alone.
 """
 
 import numpy as np
@@ -39,8 +42,8 @@ def _desc(torch, spec, ys, theta, seeds, J, T, path, flags=0):
     return d, keep
 
 
-@pytest.mark.parametrize("path", ["stream", "resident"])
-def test_noalloc_matches_workspace_entry_point(path):
+@pytest.mark.parametrize("path,graph", [("stream", False), ("resident", False), ("stream", True)])
+def test_noalloc_matches_workspace_entry_point(path, graph):
     import torch
 
     import pypomp_b200 as pp
@@ -63,7 +66,8 @@ def test_noalloc_matches_workspace_entry_point(path):
     want = {k: keep[k].cpu().numpy() for k in ("loglik", "cll", "anc")}
 
     for call in range(2):
-        d2, keep2 = _desc(torch, m.spec, st.ys, theta, seeds, J, T, _ffi.PATHS[path])
+        d2, keep2 = _desc(torch, m.spec, st.ys, theta, seeds, J, T, _ffi.PATHS[path],
+                          flags=_ffi.F_GRAPH if graph else 0)
         assert _ffi.LIB.ppf_pfilter_noalloc(d2, stream) == _ffi.PPF_OK
         got = {k: keep2[k].cpu().numpy() for k in ("loglik", "cll", "anc")}
         np.testing.assert_allclose(got["loglik"], want["loglik"], rtol=1e-12, err_msg=f"call {call}")
@@ -87,3 +91,30 @@ def test_noalloc_refuses_requests_beyond_its_scratch():
     stream = torch.cuda.current_stream().cuda_stream
     assert _ffi.LIB.ppf_pfilter_noalloc(d, stream) == _ffi.PPF_ESCRATCH
     assert "scratch" in _ffi.error_string(_ffi.PPF_ESCRATCH)
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    import torch
+
+    import pypomp_b200 as pp
+    from pypomp_b200 import _ffi
+    from tests.conftest import LG2_Q, LG2_R
+
+    m = pp.LG(T=5, Q=LG2_Q, R=LG2_R, key=4)
+    st = m.to_struct()
+    theta = m.theta.to_array(m.canonical_param_names).astype(np.float32)
+    d, keep = _desc(torch, m.spec, st.ys, theta, np.array([1], np.uint64), 1024, 5, _ffi.PATH_STREAM)
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        g.capture_begin()
+        try:
+            rc = _ffi.LIB.ppf_pfilter_noalloc(d, side.cuda_stream)
+            keep["loglik"].add_(0.0)      # something to capture
+        finally:
+            g.capture_end()
+    assert rc == _ffi.PPF_EUNSUPPORTED
+    # the stream and the library are usable afterwards
+    assert _ffi.LIB.ppf_pfilter_noalloc(d, torch.cuda.current_stream().cuda_stream) == _ffi.PPF_OK
+    del g
