@@ -85,6 +85,11 @@ typedef struct ppf_model {
 /* ppf_perfilter: use the streaming kernels even where the cluster-resident
  * path would be chosen (small swarms); for comparisons and tests */
 #define PPF_F_NO_CLUSTER (1u << 10)
+/* ppf_mop / ppf_mop_backward: use one launch per step even where the
+ * persistent form (the forward in one cooperative launch, the adjoint sweep in
+ * another, grid barriers between the steps) would be chosen; for comparisons
+ * and tests.  Both forms give the same forward results bit for bit. */
+#define PPF_F_NO_PERSIST (1u << 11)
 
 /* Execution paths; all produce bit-identical results. */
 enum {

@@ -26,6 +26,7 @@ static size_t carve(Args& a, int path, unsigned char* base) {
   const int dx = a.model.dx;
   a.err = reinterpret_cast<uint32_t*>(take(64));
   a.counter = reinterpret_cast<unsigned int*>(base ? base + 16 : nullptr);
+  a.gbar = reinterpret_cast<unsigned int*>(base ? base + 32 : nullptr);
   if (path == PPF_PATH_STREAM) {
     // a.tile is chosen before carving; the per-tile arrays are sized for the
     // smallest tile so that one workspace serves every tile configuration
@@ -222,6 +223,8 @@ static size_t carve_mop(Args& a, MopWork& w, const ppf_mop_desc* d, unsigned cha
   a.mop_M = reinterpret_cast<float*>(take(4 * F * T));
   a.mop_S = reinterpret_cast<double*>(take(8 * F * T));
   w.sb = reinterpret_cast<float*>(take(4 * F * L * dx * J));
+  w.sb2 = reinterpret_cast<float*>(take(4 * F * L * dx * J));
+  w.gpart = reinterpret_cast<double*>(take(8 * 64 * F * ((J + 255) / 256)));
   w.lx = reinterpret_cast<float*>(take(4 * 2 * F * dx * J));
   w.lw = reinterpret_cast<float*>(take(4 * 2 * F * J));
   w.gnat = reinterpret_cast<double*>(take(8 * F * 64));
@@ -247,7 +250,7 @@ static void mop_to_pfilter(const ppf_mop_desc* d, ppf_pfilter_desc* p) {
   p->model = d->model;
   p->J = d->J; p->F = d->F; p->T = d->T; p->U = d->U;
   p->path = PPF_PATH_STREAM;
-  p->flags = (d->flags & PPF_F_INJECT) | ((d->flags & PPF_F_NATURAL) ? 0u : PPF_F_EST);
+  p->flags = (d->flags & (PPF_F_INJECT | PPF_F_NO_PERSIST)) | ((d->flags & PPF_F_NATURAL) ? 0u : PPF_F_EST);
   p->thresh = 0.0f;
   p->theta = d->theta; p->ys = d->ys; p->ycon = d->ycon; p->unit = d->unit; p->T_u = d->T_u;
   p->seeds = d->seeds; p->inj_z0 = d->inj_z0; p->inj_z = d->inj_z; p->inj_u = d->inj_u;

@@ -97,6 +97,63 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
   return false;
 }
 
+// ---- grid-wide barrier for cooperative (co-resident) launches.  Three words
+// in the workspace's zeroed control block: arrivals, generation, abort.  The
+// last CTA to arrive resets the arrival count and advances the generation;
+// the others poll the generation.  Every poll loop is bounded: a CTA that
+// gives up sets error bit 1 (PPF_ETIMEOUT) and the abort word, so the other
+// CTAs stop at their next barrier instead of waiting in turn, and the kernel
+// ends.  The writes of every thread of every CTA before the barrier are
+// visible to every thread after it (CTA barrier, then a GPU-scope fence by the
+// arriving thread; acquire by the waiting thread, then a CTA barrier).
+struct GridBar {
+  unsigned int* count;
+  unsigned int* gen;
+  unsigned int* abort;
+  uint32_t* err;
+  unsigned int n;       // CTAs in the grid
+  long long cap;        // polls before giving up
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Returns false when the barrier gave up (this CTA's or another's wait).
+__device__ __forceinline__ bool grid_sync(const GridBar& g) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned int gen = ld_acquire_u32(g.gen);
+    __threadfence();
+    if (atomicAdd(g.count, 1u) == g.n - 1) {
+      atomicExch(g.count, 0u);
+      __threadfence();
+      st_release_u32(g.gen, gen + 1);
+    } else {
+      long long i = 0;
+      while (ld_acquire_u32(g.gen) == gen) {
+        if (++i > g.cap || ld_acquire_u32(g.abort) != 0u) { ok = 0; break; }
+        __nanosleep(32);
+      }
+    }
+    if (!ok) {
+      atomicOr(g.err, 1u);
+      atomicExch(g.abort, 1u);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 // The fixed-point weight q = rint(exp(w - M) * 2^40) (collapsed filters: 1),
 // in two halves: the float e = qweight_e(w, M, collapsed) and
 // q = qweight_from_e(e).  On a resampling step the streaming path's k_sum

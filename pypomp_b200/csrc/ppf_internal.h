@@ -44,6 +44,7 @@ struct Args {
   // workspace
   uint32_t* err;
   unsigned int* counter;  // [2]
+  unsigned int* gbar;     // [3] grid barrier: arrivals, generation, abort (zeroed per call)
   Acc* acc[2];            // [F] each
   uint64_t* desc[2];      // [F][ntiles] each
   uint64_t* excl;         // [F][ntiles]
@@ -103,6 +104,8 @@ struct MopWork {
   float* lx;      // [2][F][DX][J]
   float* lw;      // [2][F][J]
   float* sb;      // [F][ckpt_every][DX][J] recomputed states of one segment
+  float* sb2;     // second segment buffer (persistent adjoint: two segments in flight)
+  double* gpart;  // [F * ceil(J/256)][64] per-CTA gradient sums (persistent adjoint)
   double* gnat;   // [F][64] natural-scale gradient sums
   double* grad;   // out [F][P] estimation-scale gradient, or nullptr
   float alpha;

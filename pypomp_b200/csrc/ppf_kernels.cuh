@@ -405,21 +405,16 @@ __device__ __forceinline__ int if2_row_stride(int P) { return P | 1; }
 
 // Fixed-point sums of the weights of one tile, then the decoupled-lookback
 // prefix over the tiles of the filter (Merrill & Garland 2016).
+// The body for tile b of filter f at step t; k_sum takes (f, b) from a
+// dynamic tile counter, the persistent MOP kernel passes its own tile.  The
+// lookback needs every earlier tile of the filter to run at the same time or
+// before, which both launch forms guarantee.
 template <class M, int TPB, int IT>
-__global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
+__device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
-  __shared__ int s_v;
   __shared__ uint64_t s_red[TPB / 32];
   __shared__ double sd[TPB / 32];
-  if (threadIdx.x == 0) s_v = atomicAdd(a.counter + (t & 1), 1);
-  __syncthreads();
-  const int v = s_v;
-  if (v >= a.ntiles * a.F) {  // defensive: a stale counter must not index past the batch
-    if (threadIdx.x == 0) atomicOr(a.err, 4u);
-    return;
-  }
-  const int f = v / a.ntiles, b = v % a.ntiles;
   const int u = filter_unit(a, f);
   if (t >= filter_len(a, u)) return;
   const int p = t & 1;
@@ -554,6 +549,19 @@ __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
       if (threadIdx.x == 0) atomicAdd(&a.acc[p][f].fx[d], s);
     }
   }
+}
+
+template <class M, int TPB, int IT>
+__global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
+  __shared__ int s_v;
+  if (threadIdx.x == 0) s_v = atomicAdd(a.counter + (t & 1), 1);
+  __syncthreads();
+  const int v = s_v;
+  if (v >= a.ntiles * a.F) {  // defensive: a stale counter must not index past the batch
+    if (threadIdx.x == 0) atomicOr(a.err, 4u);
+    return;
+  }
+  sum_tile<M, TPB, IT>(a, t, v / a.ntiles, v % a.ntiles);
 }
 
 }  // namespace ppf

@@ -31,6 +31,7 @@
 #include "ppf_internal.h"
 #include "ppf_kernels.cuh"
 #include "ppf_models.cuh"
+#include "ppf_stream.cuh"
 
 namespace ppf {
 
@@ -242,8 +243,352 @@ __global__ void k_mop_chain(Args a, const double* gnat, double* grad) {
 }
 
 // ---------------------------------------------------------------------------
+// Persistent form: the whole forward in one cooperative launch and the whole
+// adjoint sweep in another, with grid barriers between the steps instead of
+// kernel boundaries.  For few filters of up to ~10^5 particles a step is a
+// few microseconds of work, and two launches per step (plus the adjoint's
+// two) cost more than the work; here the per-step cost is the barriers.
+//
+// Forward: CTA v owns tile (f, b) = (v / ntiles, v % ntiles) and runs the
+// streaming kernels' own tile bodies (init_tile, sum_tile, resprop_tile) in
+// sequence: the results are bit-identical to the per-step launches.
+//
+// Adjoint: the CTAs of filter f stride over its particles.  Segments are
+// swept from the last, as in mop_backward, but the recomputation of segment
+// s-1 runs in the same barrier intervals as the adjoint steps of segment s
+// (two segment buffers), so the sweep costs one barrier per step.  Each
+// thread sums its gradient terms in float over a segment, then the warp adds
+// them into per-warp float64 sums; the per-CTA totals are added in CTA order
+// by k_mop_chain_parts, so the gradient does not depend on scheduling.
+// ---------------------------------------------------------------------------
+
+struct MopBwdP {
+  float* sb[2];     // [F][L][DX][J] each: recomputed states of one segment
+  float* lx;        // [2][F][DX][J] adjoint of x^F by step parity
+  float* lw;        // [2][F][J]     adjoint of wF by step parity
+  double* gpart;    // [gridDim.x][kMaxNG] per-CTA natural-scale gradient sums
+  float alpha;
+  int nbf;          // CTAs per filter
+};
+
+template <class M, int N, bool INJ>
+__device__ __forceinline__ void own_normals(const Args& a, int f, int j, int s, float* z) {
+  if (N <= 0) return;
+  if (INJ) {
+    const float* src = (s == 0) ? a.inj_z0 + ((size_t)f * a.J + j) * N
+                                : a.inj_z + (((size_t)f * a.T + (s - 1)) * a.J + j) * N;
+#pragma unroll
+    for (int i = 0; i < N; ++i) z[i] = src[i];
+  } else {
+    pp_normals_own(a.seeds[f], (uint32_t)j, (uint32_t)s, PPF_TAG_PROCESS, N, z);
+  }
+}
+
+template <class M, int TPB, int IT, bool INJ>
+__global__ void __launch_bounds__(TPB) k_mop_fwd_persist(Args a, GridBar gb) {
+  const int f = blockIdx.x / a.ntiles, b = blockIdx.x % a.ntiles;
+  init_tile<M, TPB, INJ>(a, f, b);
+  if (!grid_sync(gb)) return;
+  for (int t = 0; t < a.T; ++t) {
+    sum_tile<M, TPB, IT>(a, t, f, b);
+    if (!grid_sync(gb)) return;
+    resprop_tile<M, TPB, IT, INJ, false>(a, t, f, b);
+    if (!grid_sync(gb)) return;
+  }
+}
+
+template <class M, int TPB, bool INJ>
+__global__ void __launch_bounds__(TPB) k_mop_bwd_persist(Args a, MopBwdP mb, GridBar gb) {
+  constexpr int DX = M::MAXDX, NG = M::NG, NW = TPB / 32;
+  constexpr int NZ = M::NZ > 0 ? M::NZ : 1, NZ0 = M::NZ0 > 0 ? M::NZ0 : 1;
+  __shared__ typename M::Consts c;
+  __shared__ double s_g[NW][NG];
+  const int f = blockIdx.x / mb.nbf, cb = blockIdx.x % mb.nbf;
+  const int u = filter_unit(a, f), Tf = filter_len(a, u);
+  const int J = a.J, T = a.T, L = a.ckpt_every;
+  load_consts<M>(a, f, c);
+  for (int i = threadIdx.x; i < NW * NG; i += TPB) (&s_g[0][0])[i] = 0.0;
+  __syncthreads();
+  const int stride = mb.nbf * TPB;
+  const int j0 = cb * TPB + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t sbf = (size_t)f * L * DX * J;
+  const float* ckf = a.mop_ckpt + (size_t)f * a.nseg * DX * J;
+  // Gradient terms: models with few parameters (SV, Ricker) add each step's
+  // float terms into float64 per thread, as the per-step kernels do across a
+  // block; the LG models (up to 27 entries) sum a segment's terms in float
+  // per thread before the float64 warp sums, to stay within registers.
+  constexpr bool GD = NG <= 8;
+  float gs[NG];
+  double gd[GD ? NG : 1];
+#pragma unroll
+  for (int i = 0; i < NG; ++i) gs[i] = 0.0f;
+#pragma unroll
+  for (int i = 0; i < (GD ? NG : 1); ++i) gd[i] = 0.0;
+  auto fold = [&]() {       // one particle-step's terms into the float64 sums
+    if (GD) {
+#pragma unroll
+      for (int i = 0; i < NG; ++i) {
+        gd[i] += (double)gs[i];
+        gs[i] = 0.0f;
+      }
+    }
+  };
+
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i < NG; ++i) {
+      const double v = warp_sum_f64(GD ? gd[GD ? i : 0] : (double)gs[i]);
+      if (lane == 0) s_g[warp][i] += v;
+      gs[i] = 0.0f;
+      if (GD) gd[GD ? i : 0] = 0.0;
+    }
+  };
+  // x^F_{t-1} for step t of segment seg: its checkpoint, or the buffer
+  auto xin_of = [&](int t, int seg, const float* sbuf) -> const float* {
+    const int t0 = seg * L;
+    return (t == t0) ? ckf + (size_t)seg * DX * J : sbuf + sbf + (size_t)(t - 1 - t0) * DX * J;
+  };
+  // x^F_t[k] = rproc(x^F_{t-1}[anc_t[k]]) with the parent's normals
+  auto recompute = [&](int t, int seg, float* sbuf) {
+    const float* xin = xin_of(t, seg, sbuf);
+    float* xo = sbuf + sbf + (size_t)(t - seg * L) * DX * J;
+    const int* anc = a.anc + ((size_t)f * T + t) * J;
+    for (int k = j0; k < J; k += stride) {
+      const int j = anc[k];
+      float x[DX];
+#pragma unroll
+      for (int d = 0; d < DX; ++d) x[d] = xin[d * J + j];
+      float z[NZ];
+      own_normals<M, M::NZ, INJ>(a, f, j, t + 1, z);
+      M::rproc(c, x, z);
+#pragma unroll
+      for (int d = 0; d < DX; ++d) xo[d * J + k] = x[d];
+    }
+  };
+  // the adjoint step of k_mop_bwd for this thread's particles
+  auto adjoint = [&](int t, int seg, const float* sbuf) {
+    const float* xin = xin_of(t, seg, sbuf);
+    Obs<M> ob;
+    ob.load(a, u, t);
+    const float Mt = a.mop_M[(size_t)f * T + t];
+    const double S1 = a.mop_S[(size_t)f * T + t];
+    const int* off = a.mop_off + ((size_t)f * T + t) * (J + 1);
+    const int pin = t & 1, pout = pin ^ 1;
+    const float* lxi = mb.lx + ((size_t)pin * a.F + f) * DX * J;
+    const float* lwi = mb.lw + ((size_t)pin * a.F + f) * J;
+    float* lxo = mb.lx + ((size_t)pout * a.F + f) * DX * J;
+    float* lwo = mb.lw + ((size_t)pout * a.F + f) * J;
+    for (int j = j0; j < J; j += stride) {
+      float x[DX];
+#pragma unroll
+      for (int d = 0; d < DX; ++d) x[d] = xin[d * J + j];
+      float z[NZ];
+      own_normals<M, M::NZ, INJ>(a, f, j, t + 1, z);
+      typename M::Keep kp;
+      const float m = M::fwd_keep(c, ob.y, ob.yc, x, z, kp);
+      float pi = 0.0f;
+      if (S1 > 0.0 && m == m) pi = (float)((double)pp_expf(m - Mt) / S1);
+      const int lo = off[j], hi = off[j + 1];
+      float lx[DX];
+#pragma unroll
+      for (int d = 0; d < DX; ++d) lx[d] = 0.0f;
+      float lw = 0.0f;
+      for (int k = lo; k < hi; ++k) {
+#pragma unroll
+        for (int d = 0; d < DX; ++d) lx[d] += lxi[d * J + k];
+        lw += lwi[k];
+      }
+      const float gl = -1.0f;
+      const float lm = lw + gl * pi;
+      const float lwP = lw + gl * (pi - 1.0f / (float)J);
+      if (m == m && m > -INFINITY) {
+        M::bwd(c, x, z, kp, lm, lx, gs);
+        fold();
+      } else {
+#pragma unroll
+        for (int d = 0; d < DX; ++d) lx[d] = 0.0f;
+      }
+#pragma unroll
+      for (int d = 0; d < DX; ++d) lxo[d * J + j] = lx[d];
+      lwo[j] = mb.alpha * lwP;
+    }
+  };
+
+  {   // recompute the last segment before its sweep
+    const int seg = a.nseg - 1, t0 = seg * L, t1 = min(t0 + L, T);
+    for (int t = t0; t < t1 - 1; ++t) {
+      if (t < Tf) recompute(t, seg, mb.sb[seg & 1]);
+      if (!grid_sync(gb)) return;
+    }
+  }
+  for (int seg = a.nseg - 1; seg >= 0; --seg) {
+    const int t0 = seg * L, t1 = min(t0 + L, T);
+    const int nb = t1 - t0, nr = seg > 0 ? L - 1 : 0;   // segment seg-1 is a full one
+    const int n = nb > nr ? nb : nr;
+    for (int i = 0; i < n; ++i) {
+      if (i < nb) {
+        const int t = t1 - 1 - i;
+        if (t < Tf) adjoint(t, seg, mb.sb[seg & 1]);
+      }
+      if (i < nr) {
+        const int t = (seg - 1) * L + i;
+        if (t < Tf) recompute(t, seg - 1, mb.sb[(seg - 1) & 1]);
+      }
+      if (!grid_sync(gb)) return;
+    }
+    flush();
+  }
+  {   // dtheta += (d rinit / dtheta)^T adjoint(x^F_{-1}) (the output of step 0 has parity 1)
+    const float* lx0 = mb.lx + ((size_t)1 * a.F + f) * DX * J;
+    for (int j = j0; j < J; j += stride) {
+      float z0[NZ0];
+      own_normals<M, M::NZ0, INJ>(a, f, j, 0, z0);
+      float l[DX];
+#pragma unroll
+      for (int d = 0; d < DX; ++d) l[d] = lx0[d * J + j];
+      M::bwd_init(c, z0, l, gs);
+      fold();
+    }
+    flush();
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < NG; i += TPB) {
+    double sum = 0.0;
+#pragma unroll 1
+    for (int w = 0; w < NW; ++w) sum += s_g[w][i];
+    mb.gpart[(size_t)blockIdx.x * kMaxNG + i] = sum;
+  }
+}
+
+// Natural-scale gradient sums of filter f (its CTAs' totals, in CTA order),
+// chained to the estimation scale as k_mop_chain does.
+template <class M>
+__global__ void k_mop_chain_parts(Args a, const double* gpart, int nbf, double* grad) {
+  __shared__ double gn[kMaxNG];
+  const int f = blockIdx.x;
+  for (int i = threadIdx.x; i < kMaxNG; i += blockDim.x) {
+    double sum = 0.0;
+    if (i < M::NG)
+      for (int c = 0; c < nbf; ++c) sum += gpart[((size_t)f * nbf + c) * kMaxNG + i];
+    gn[i] = sum;
+  }
+  __syncthreads();
+  const int P = a.model.n_params;
+  for (int p = threadIdx.x; p < P; p += blockDim.x)
+    grad[(size_t)f * P + p] = Chain<M>::map(a.model, a.theta + (size_t)f * P, gn, p, (a.flags & PPF_F_EST) != 0);
+}
+
+// ---------------------------------------------------------------------------
 // host orchestration
 // ---------------------------------------------------------------------------
+
+static int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      n = 0;
+  }
+  return n;
+}
+
+// CTAs of `kernel` that fit on the device at once (0 when unknown).
+template <class K>
+static int coresident(K kernel, int tpb, size_t smem) {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, tpb, smem) != cudaSuccess) return 0;
+  return per * num_sms();
+}
+
+static GridBar grid_bar(const Args& a, unsigned int n) {
+  GridBar g;
+  g.count = a.gbar;
+  g.gen = a.gbar + 1;
+  g.abort = a.gbar + 2;
+  g.err = a.err;
+  g.n = n;
+  g.cap = a.spin_cap;
+  return g;
+}
+
+template <class K, class... Args_>
+static int launch_coop(K kernel, int grid, int tpb, size_t smem, cudaStream_t s, Args_... args) {
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(tpb);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...) == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
+// The persistent forward with TILE = TPB * IT particles per CTA; PPF_EUNSUPPORTED
+// when the F * ntiles CTAs cannot all be resident at once.
+template <class M, int TPB, int IT, bool INJ>
+static int mop_forward_persist_t(Args& a, cudaStream_t s) {
+  constexpr int TILE = TPB * IT;
+  const size_t smem = sizeof(float) * M::MAXDX * TILE + sizeof(int) * (TILE + 4) + sizeof(float) * TILE;
+  auto kern = k_mop_fwd_persist<M, TPB, IT, INJ>;
+  const int ntiles = (a.J + TILE - 1) / TILE;
+  const long long grid = (long long)a.F * ntiles;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return PPF_ECUDA;
+  if (grid > coresident(kern, TPB, smem)) return PPF_EUNSUPPORTED;
+  a.tile = TILE;
+  a.ntiles = ntiles;
+  k_prep<M><<<(a.F + 127) / 128, 128, 0, s>>>(a);
+  PROF_BEGIN(KIND_MOP_FWD);
+  const int rc = launch_coop(kern, (int)grid, TPB, smem, s, a, grid_bar(a, (unsigned)grid));
+  PROF_END(KIND_MOP_FWD);
+  return rc;
+}
+
+template <class M, bool INJ>
+static int mop_backward_persist_t(Args& a, const MopWork& w, cudaStream_t s) {
+  constexpr int TPB = 256;
+  constexpr int DX = M::MAXDX;
+  auto kern = k_mop_bwd_persist<M, TPB, INJ>;
+  const int cap = coresident(kern, TPB, 0);
+  const int want = (a.J + TPB - 1) / TPB;
+  const int nbf = want < cap / a.F ? want : cap / a.F;
+  if (nbf < 1 || !w.sb2 || !w.gpart) return PPF_EUNSUPPORTED;
+  if (cudaMemsetAsync(w.lx, 0, sizeof(float) * 2ull * a.F * DX * a.J, s) != cudaSuccess) return PPF_ECUDA;
+  if (cudaMemsetAsync(w.lw, 0, sizeof(float) * 2ull * a.F * a.J, s) != cudaSuccess) return PPF_ECUDA;
+  MopBwdP mb;
+  memset(&mb, 0, sizeof(mb));
+  mb.sb[0] = w.sb;
+  mb.sb[1] = w.sb2;
+  mb.lx = w.lx;
+  mb.lw = w.lw;
+  mb.gpart = w.gpart;
+  mb.alpha = w.alpha;
+  mb.nbf = nbf;
+  const int grid = a.F * nbf;
+  PROF_BEGIN(KIND_MOP_BWD);
+  int rc = launch_coop(kern, grid, TPB, 0, s, a, mb, grid_bar(a, (unsigned)grid));
+  PROF_END(KIND_MOP_BWD);
+  if (rc) return rc;
+  k_mop_chain_parts<M><<<a.F, 64, 0, s>>>(a, w.gpart, nbf, w.grad);
+  return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
+// Persistent launches apply to few filters: the forward's tiles (256 or 512
+// particles) and the adjoint's CTAs must all fit on the device at once.
+template <class M, bool INJ>
+static int mop_forward_persist(Args& a, cudaStream_t s) {
+  const int rc = mop_forward_persist_t<M, 64, 4, INJ>(a, s);
+  if (rc != PPF_EUNSUPPORTED) return rc;
+  return mop_forward_persist_t<M, 128, 4, INJ>(a, s);
+}
+
+static bool want_persist(const Args& a) { return !(a.flags & PPF_F_NO_PERSIST) && a.gbar; }
 
 template <class M, bool INJ>
 int mop_backward(Args& a, const MopWork& w, cudaStream_t s) {
@@ -293,10 +638,23 @@ int mop_backward(Args& a, const MopWork& w, cudaStream_t s) {
 }
 
 template <class M>
+int run_mop_backward_model(Args& a, const MopWork& w, cudaStream_t s) {
+  const bool inj = (a.flags & PPF_F_INJECT) != 0;
+  if (want_persist(a)) {
+    const int rc = inj ? mop_backward_persist_t<M, true>(a, w, s) : mop_backward_persist_t<M, false>(a, w, s);
+    if (rc != PPF_EUNSUPPORTED) return rc;
+  }
+  return inj ? mop_backward<M, true>(a, w, s) : mop_backward<M, false>(a, w, s);
+}
+
+template <class M>
 int run_mop_model(Args& a, const MopWork& w, cudaStream_t s) {
-  int rc = run_stream_any(a, s);
+  const bool inj = (a.flags & PPF_F_INJECT) != 0;
+  int rc = PPF_EUNSUPPORTED;
+  if (want_persist(a)) rc = inj ? mop_forward_persist<M, true>(a, s) : mop_forward_persist<M, false>(a, s);
+  if (rc == PPF_EUNSUPPORTED) rc = run_stream_any(a, s);
   if (rc || !w.grad) return rc;
-  return (a.flags & PPF_F_INJECT) ? mop_backward<M, true>(a, w, s) : mop_backward<M, false>(a, w, s);
+  return run_mop_backward_model<M>(a, w, s);
 }
 
 int run_mop(Args& a, const MopWork& w, cudaStream_t s) {
@@ -315,10 +673,7 @@ int run_mop(Args& a, const MopWork& w, cudaStream_t s) {
   }
 }
 
-template <class M>
-int run_mop_backward_model(Args& a, const MopWork& w, cudaStream_t s) {
-  return (a.flags & PPF_F_INJECT) ? mop_backward<M, true>(a, w, s) : mop_backward<M, false>(a, w, s);
-}
+
 
 int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s) {
   switch (a.model.kind) {

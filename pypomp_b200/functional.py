@@ -399,7 +399,7 @@ class MopCall:
 
     def __init__(self, struct: PompStruct, theta_est, seeds_f, J: int, alpha: float, *, unit_f=None,
                  inject=None, ckpt_every: int = 0, save_ancestors: bool = False, natural: bool = False,
-                 graph: bool = False):
+                 graph: bool = False, persistent: bool = True):
         torch = _ffi.require_cuda()
         if J < 1:
             raise ValueError("J should be greater than 0.")
@@ -428,6 +428,8 @@ class MopCall:
             self.out["anc"] = torch.zeros(F, T, J, dtype=torch.int32, device=dev)
         inj = {}
         flags = (_ffi.F_NATURAL if natural else 0) | (_ffi.F_GRAPH if graph else 0)
+        if not persistent:
+            flags |= _ffi.F_NO_PERSIST
         if inject is not None:
             flags |= _ffi.F_INJECT
             for k in ("z0", "z", "u"):
@@ -492,11 +494,13 @@ class MopCall:
 
 def run_mop(struct: PompStruct, theta_est_f: np.ndarray, seeds_f: np.ndarray, J: int, alpha: float,
             *, grad: bool = True, unit_f=None, inject=None, ckpt_every: int = 0,
-            save_ancestors: bool = False, return_torch: bool = False):
+            save_ancestors: bool = False, return_torch: bool = False, persistent: bool = True):
     """One batched call of ``ppf_mop``: MOP-alpha value (negative log-likelihood,
-    summed over time) and, when ``grad``, its gradient on the estimation scale."""
+    summed over time) and, when ``grad``, its gradient on the estimation scale.
+    ``persistent=False`` keeps one launch per step where the library would use
+    its persistent form (same results; for comparisons)."""
     call = MopCall(struct, theta_est_f, seeds_f, J, alpha, unit_f=unit_f, inject=inject,
-                   ckpt_every=ckpt_every, save_ancestors=save_ancestors)
+                   ckpt_every=ckpt_every, save_ancestors=save_ancestors, persistent=persistent)
     out = dict(call.forward(grad=grad))
     if not grad:
         out.pop("grad")

@@ -142,3 +142,84 @@ def test_mop_gradient_finite_for_chaotic_ricker_with_zero_counts():
         th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(f32)
         got = F.run_mop(st, th, np.array([i], np.uint64), 8192, 0.97, grad=True)
         assert np.all(np.isfinite(got["value"])) and np.all(np.isfinite(got["grad"])), (logr, got["grad"])
+
+
+@pytest.mark.parametrize("alpha", [0.5, 0.97])
+@pytest.mark.parametrize("model", ["LG", "SV", "Ricker"])
+def test_persistent_form_equals_per_step_launches(model, alpha):
+    """The persistent MOP (forward and adjoint sweep as two cooperative
+    launches) against one launch per step: values and ancestors bit for bit;
+    the gradient to the float64 summation order of its terms."""
+    F = _F()
+    m, st, th, J = _case(model)
+    seeds = np.array([21, 22], np.uint64)
+    th2 = np.repeat(th, 2, axis=0)
+    th2[1, 0] += f32(0.02)
+    a = F.run_mop(st, th2, seeds, J, alpha, grad=True, save_ancestors=True, persistent=True)
+    b = F.run_mop(st, th2, seeds, J, alpha, grad=True, save_ancestors=True, persistent=False)
+    assert np.array_equal(a["anc"], b["anc"])
+    assert np.array_equal(a["value"], b["value"])
+    tol = 1e-9 if model in ("SV", "Ricker") else 1e-5
+    for f in range(2):
+        assert np.linalg.norm(a["grad"][f] - b["grad"][f]) <= tol * np.linalg.norm(b["grad"][f]), \
+            (a["grad"][f], b["grad"][f])
+
+
+def test_persistent_form_on_ragged_panel_units():
+    """Panel MOP with units of different lengths through the persistent form
+    (filters stop at their own T_u inside the launch) against per-step launches."""
+    import pypomp_b200 as pp
+    from pypomp_b200.functional import PompStruct
+
+    F = _F()
+    units = [pp.Ricker(T=T, r=6.0, key=30 + i) for i, T in enumerate((25, 40, 13))]
+    spec = units[0].spec
+    Tmax = 40
+    ys = np.zeros((3, Tmax, 1), f32)
+    for i, mm in enumerate(units):
+        y = mm.to_struct().ys
+        ys[i, :y.shape[0]] = y
+    st = PompStruct(spec=spec, ys=ys, times=np.arange(1, Tmax + 1.0), t0=0.0,
+                    T_u=np.array([25, 40, 13], np.int32))
+    th = np.stack([spec.to_est(mm.theta.to_array(mm.canonical_param_names))[0] for mm in units]).astype(f32)
+    seeds = np.array([5, 6, 7], np.uint64)
+    unit_f = np.arange(3, dtype=np.int32)
+    a = F.run_mop(st, th, seeds, 3000, 0.97, grad=True, unit_f=unit_f, persistent=True)
+    b = F.run_mop(st, th, seeds, 3000, 0.97, grad=True, unit_f=unit_f, persistent=False)
+    assert np.array_equal(a["value"], b["value"])
+    np.testing.assert_allclose(a["grad"], b["grad"], rtol=1e-9, atol=1e-12)
+
+
+def test_persistent_form_at_config_size_equals_per_step_launches():
+    """C3's shape (SV, T = 2000, J = 65536): the persistent form gives the
+    per-step launches' value bit for bit and their gradient to 1e-9."""
+    import pypomp_b200 as pp
+
+    F = _F()
+    m = pp.SV(T=2000, key=0)
+    st = m.to_struct()
+    th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(f32)
+    seeds = np.array([1], np.uint64)
+    a = F.run_mop(st, th, seeds, 65536, 0.97, grad=True, persistent=True)
+    b = F.run_mop(st, th, seeds, 65536, 0.97, grad=True, persistent=False)
+    assert np.array_equal(a["value"], b["value"])
+    np.testing.assert_allclose(a["grad"], b["grad"], rtol=1e-9)
+
+
+def test_persistent_form_replays_from_a_cuda_graph():
+    """PPF_F_GRAPH captures the persistent form's two cooperative launches once
+    and replays them: the replay equals a direct call."""
+    import pypomp_b200 as pp
+    from pypomp_b200.functional import MopCall
+
+    m = pp.SV(T=200, key=4)
+    st = m.to_struct()
+    th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(f32)
+    seeds = np.array([3], np.uint64)
+    direct = MopCall(st, th, seeds, 16384, 0.97)
+    want = {k: v.cpu().numpy() for k, v in direct.forward(grad=True).items()}
+    g = MopCall(st, th, seeds, 16384, 0.97, graph=True)
+    for _ in range(3):
+        got = {k: v.cpu().numpy() for k, v in g.forward(grad=True).items()}
+        assert np.array_equal(got["value"], want["value"])
+        np.testing.assert_allclose(got["grad"], want["grad"], rtol=1e-12)

@@ -81,3 +81,31 @@ def test_wait_limit_zero_times_out_promptly_then_recovers():
     want = cora.pfilter(1, 2, 2, th, st.ys, J, seeds=seeds, anc=True, nthreads=8)
     assert np.array_equal(keep["anc"].cpu().numpy(), want["anc"])
     np.testing.assert_allclose(keep["loglik"].cpu().numpy(), want["loglik"], rtol=1e-12)
+
+
+def test_persistent_mop_barriers_time_out_promptly_then_recover():
+    """The persistent MOP forward and adjoint wait at grid barriers; with the
+    limit at 0 every waiting CTA gives up at once, sets the abort word so the
+    others stop at their next barrier, and the call reports PPF_ETIMEOUT.  The
+    next call (the control words are cleared per call) is correct again."""
+    import pypomp_b200 as pp
+    from pypomp_b200 import _ffi
+    from pypomp_b200 import functional as F
+
+    m = pp.SV(T=300, key=2)
+    st = m.to_struct()
+    th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(f32)
+    seeds = np.array([9], np.uint64)
+    want = F.run_mop(st, th, seeds, 65536, 0.97, grad=True, persistent=False)
+    prev = _ffi.LIB.ppf_debug_set_wait_limit(0)
+    try:
+        t0 = time.perf_counter()
+        with pytest.raises(RuntimeError, match="timed out"):
+            F.run_mop(st, th, seeds, 65536, 0.97, grad=True, persistent=True)
+        dt = time.perf_counter() - t0
+    finally:
+        _ffi.LIB.ppf_debug_set_wait_limit(-1)
+    assert prev == 1 << 22 and dt < 10.0, dt
+    got = F.run_mop(st, th, seeds, 65536, 0.97, grad=True, persistent=True)
+    assert np.array_equal(got["value"], want["value"])
+    np.testing.assert_allclose(got["grad"], want["grad"], rtol=1e-9)
