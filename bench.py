@@ -505,25 +505,29 @@ def mop_block(args, steps=None, warmup=None):
     call.forward(grad=True)
     prof = _ffi.profile_end()
     value = Jm * Tm / (ms / 1e3)
-    # algorithmic bytes per particle-step of each MOP kernel (SV, dx = 2):
+    # algorithmic bytes per particle-step of each MOP kernel kind (SV, dx = 2):
     # forward resample+propagate 24 + ancestor 4 + first-child offset 4; sums 4;
     # recompute 8 + 4 + 8; adjoint 8 (x) + 4 (anc) + 4 (offset) + 12 (adjoint in)
-    # + 12 (adjoint out)
-    bytes_kind = {"resample_propagate": 32, "sum_lookback": 4, "mop_forward": 32, "mop_recompute": 20,
-                  "mop_adjoint": 40}
+    # + 12 (adjoint out).  The persistent form records its forward (sums and
+    # resample+propagate of every step) as one launch and its adjoint sweep
+    # (recompute and adjoint) as another.  Every kind touches each of the
+    # J x T particle-steps once, so its GB/s is bytes x J x T / its total time.
+    persistent = "mop_recompute" not in prof
+    bytes_kind = {"resample_propagate": 32, "sum_lookback": 4, "mop_forward": 36, "mop_recompute": 20,
+                  "mop_adjoint": 60 if persistent else 40}
     peak, peak_kind = peaks()
     kern = {}
     for k, (tms, n) in prof.items():
         if n:
-            avg = tms / n
-            e = {"launches": n, "total_ms": tms, "avg_ms": avg}
+            e = {"launches": n, "total_ms": tms, "avg_ms": tms / n}
             if k in bytes_kind:
-                e["GBps"] = bytes_kind[k] * Jm / (avg / 1e3) / 1e9
+                e["GBps"] = bytes_kind[k] * Jm * Tm / (tms / 1e3) / 1e9
             kern[k] = e
     call_bytes = 92 * Jm * Tm
     return {"workload": "SV MOP-alpha value+grad, T=2000, J=65536, alpha=0.97, one parameter set",
             "value": value, "unit": UNIT, "ms_per_call": ms, "steps": steps, "warmup": warmup,
-            "cuda_graph": bool(args.graph), "kernels": kern, "clocks": clk,
+            "cuda_graph": bool(args.graph), "form": "persistent" if persistent else "per-step launches",
+            "kernels": kern, "clocks": clk,
             "roofline": {"bound": "hbm", "achieved": call_bytes / (ms / 1e3) / 1e9, "peak": peak,
                          "unit": "GB/s", "frac": call_bytes / (ms / 1e3) / 1e9 / peak,
                          "algorithmic_bytes_per_particle_step": 92, "peak_source": peak_kind,
@@ -625,6 +629,9 @@ def run_c5(args):
         F.panel_mif(st, sh, un, rw, max(args.warmup, 1), Jp, np.array([1], np.uint64))
         mif_ms, mif_wall = timed(lambda n: F.panel_mif(st, sh, un, rw, n, Jp, np.array([2], np.uint64)),
                                  args.steps)
+        F.panel_mif(st, sh, un, rw, max(args.warmup, 1), Jp, np.array([1], np.uint64), mode="parallel")
+        par_ms, par_wall = timed(lambda n: F.panel_mif(st, sh, un, rw, n, Jp, np.array([2], np.uint64),
+                                                       mode="parallel"), args.steps)
         eta = LearningRate({n: 0.01 for n in pan.canonical_param_names})
         s0, u0 = pan.theta.shared_array(), pan.theta.unit_array(names)
         F.panel_train(st, s0, u0, Jp, Adam(), max(args.warmup, 1), eta, 0.97, np.array([3], np.uint64),
@@ -637,6 +644,7 @@ def run_c5(args):
     pm = F.panel_mop(st, est_all, Jp, 0.97, np.arange(U, dtype=np.uint64)[None] + 77, grad=True)
     finite_u = np.all(np.isfinite(pm["grad"][0]), axis=-1)
     mif_rate = steps_units * args.steps / (mif_ms / 1e3)
+    par_rate = steps_units * args.steps / (par_ms / 1e3)
     tr_rate = steps_units * args.steps / (tr_ms / 1e3)
     job_s = 100 * mif_ms / args.steps / 1e3 + 50 * tr_ms / args.steps / 1e3
     _line(args, "Ricker panel: 128 units, T_u in [50, 800], J=8192; IF2 then MOP train",
@@ -654,8 +662,13 @@ def run_c5(args):
                      "note": "the speed of the MOP calls only: along chaotic Ricker trajectories "
                              "(log r near 3.8) the pathwise MOP gradient overflows float32 on long "
                              "series, and the update then propagates NaN as the reference's would"},
+           "mif_parallel": {"value": par_rate, "unit": UNIT, "ms_per_iteration": par_ms / args.steps,
+                            "api": "functional.panel_mif(mode='parallel'): all 128 units in one batched "
+                                   "perturbed-filter call per iteration, shared swarm recombined "
+                                   "(not the reference's unit-by-unit semantics)"},
            "sum_T_u": int(T_u.sum()), "full_job_seconds_estimate": job_s,
-           "wall_s": {"mif": mif_wall, "train": tr_wall}, "clocks": clk.summary(),
+           "full_job_seconds_estimate_parallel": 100 * par_ms / args.steps / 1e3 + 50 * tr_ms / args.steps / 1e3,
+           "wall_s": {"mif": mif_wall, "mif_parallel": par_wall, "train": tr_wall}, "clocks": clk.summary(),
            "roofline": None,
            "note": "IF2 visits the units one after another (the shared swarm carries from unit to unit), "
                    "so each perturbed filter runs J=8192 particles = 4 tiles: launch- and latency-bound"})

@@ -409,7 +409,10 @@ __device__ __forceinline__ int if2_row_stride(int P) { return P | 1; }
 // dynamic tile counter, the persistent MOP kernel passes its own tile.  The
 // lookback needs every earlier tile of the filter to run at the same time or
 // before, which both launch forms guarantee.
-template <class M, int TPB, int IT>
+// LB = false (the persistent MOP forward, all tiles resident and a grid
+// barrier after this body): publish the tile total in desc[t & 1] and leave
+// the prefix to tile_prefix, instead of the lookback.
+template <class M, int TPB, int IT, bool LB = true>
 __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
@@ -488,7 +491,9 @@ __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
   // it (e, the run prefixes, excl and tot are read by the next kernel), so
   // strong relaxed accesses suffice; release / acquire would only add fences.
   uint64_t* desc = a.desc[p] + (size_t)f * a.ntiles;
-  if (threadIdx.x < 32) {
+  if (!LB) {
+    if (threadIdx.x == 0) desc[b] = btot;
+  } else if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     uint64_t excl = 0;
     if (b == 0) {
@@ -549,6 +554,28 @@ __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
       if (threadIdx.x == 0) atomicAdd(&a.acc[p][f].fx[d], s);
     }
   }
+}
+
+// After sum_tile<..., false> on every tile and a grid barrier: tile b's
+// exclusive prefix and the filter's total from the published tile totals
+// (every CTA of the filter writes the same total).
+__device__ __forceinline__ void tile_prefix(const Args& a, int t, int f, int b) {
+  if (threadIdx.x < 32) {
+    const uint64_t* sums = a.desc[t & 1] + (size_t)f * a.ntiles;
+    uint64_t before = 0, all = 0;
+    for (int i = threadIdx.x; i < a.ntiles; i += 32) {
+      const uint64_t v = sums[i];
+      all += v;
+      before += (i < b) ? v : 0ull;
+    }
+    before = warp_sum_u64(before);
+    all = warp_sum_u64(all);
+    if (threadIdx.x == 0) {
+      a.excl[(size_t)f * a.ntiles + b] = before;
+      a.tot[f] = all;
+    }
+  }
+  __syncthreads();
 }
 
 template <class M, int TPB, int IT>

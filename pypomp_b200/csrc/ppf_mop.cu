@@ -290,8 +290,9 @@ __global__ void __launch_bounds__(TPB) k_mop_fwd_persist(Args a, GridBar gb) {
   init_tile<M, TPB, INJ>(a, f, b);
   if (!grid_sync(gb)) return;
   for (int t = 0; t < a.T; ++t) {
-    sum_tile<M, TPB, IT>(a, t, f, b);
+    sum_tile<M, TPB, IT, false>(a, t, f, b);
     if (!grid_sync(gb)) return;
+    if (t < filter_len(a, filter_unit(a, f))) tile_prefix(a, t, f, b);
     resprop_tile<M, TPB, IT, INJ, false>(a, t, f, b);
     if (!grid_sync(gb)) return;
   }
@@ -314,11 +315,12 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_persist(Args a, MopBwdP mb, Gri
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const size_t sbf = (size_t)f * L * DX * J;
   const float* ckf = a.mop_ckpt + (size_t)f * a.nseg * DX * J;
-  // Gradient terms: models with few parameters (SV, Ricker) add each step's
-  // float terms into float64 per thread, as the per-step kernels do across a
-  // block; the LG models (up to 27 entries) sum a segment's terms in float
-  // per thread before the float64 warp sums, to stay within registers.
-  constexpr bool GD = NG <= 8;
+  // Gradient terms: each particle-step's float terms are added into float64
+  // per thread, as the per-step kernels add them across a block, for up to 32
+  // entries (SV, Ricker, LG up to dx = dy = 2); the larger LG models sum a
+  // segment's terms in float per thread before the float64 warp sums, to stay
+  // within registers.
+  constexpr bool GD = NG <= 32;
   float gs[NG];
   double gd[GD ? NG : 1];
 #pragma unroll
@@ -579,11 +581,18 @@ static int mop_backward_persist_t(Args& a, const MopWork& w, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
 
-// Persistent launches apply to few filters: the forward's tiles (256 or 512
-// particles) and the adjoint's CTAs must all fit on the device at once.
+// Persistent launches apply to few filters: the forward's tiles and the
+// adjoint's CTAs must all fit on the device at once.  The forward takes
+// 512-particle tiles when they need no more CTAs than there are SMs (one tile
+// per SM: fewer barrier arrivals and tile totals to add per step), else
+// 256-particle tiles.
 template <class M, bool INJ>
 static int mop_forward_persist(Args& a, cudaStream_t s) {
-  const int rc = mop_forward_persist_t<M, 64, 4, INJ>(a, s);
+  const long long t512 = (long long)a.F * ((a.J + 511) / 512);
+  int rc = PPF_EUNSUPPORTED;
+  if (t512 <= num_sms()) rc = mop_forward_persist_t<M, 128, 4, INJ>(a, s);
+  if (rc != PPF_EUNSUPPORTED) return rc;
+  rc = mop_forward_persist_t<M, 64, 4, INJ>(a, s);
   if (rc != PPF_EUNSUPPORTED) return rc;
   return mop_forward_persist_t<M, 128, 4, INJ>(a, s);
 }

@@ -1086,7 +1086,8 @@ def _perfilter_queued(st_u, unit_in, swarm, seeds_d, J, sig_d, sig0_d, cool_d, t
 
 
 def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, J: int, keys,
-              thresh: float = 0.0, n_monitors: int = 0, block: bool = True, *, inject=None):
+              thresh: float = 0.0, n_monitors: int = 0, block: bool = True, *, inject=None,
+              mode: str = "sequential"):
     """Panel iterated filtering (``pypomp/functional/mif.py:125-259``;
     ``_panel_mif_internal`` / ``_panel_mif_unit_scan_fn`` at
     ``pypomp/core/algorithms/panel_mif.py:17-247``).
@@ -1106,7 +1107,18 @@ def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, 
     unit_traces (n, M+1, U, nu+1), final shared swarm (n, J, ns), final unit
     swarm (n, J, U, nu)); column 0 of the traces is the log-likelihood
     (summed over units for the shared trace), the rest are swarm means.
+
+    ``mode="parallel"`` is not in the reference (see :func:`_panel_mif_parallel`):
+    every unit of every replicate is filtered in one batched call per
+    iteration, all from the iteration's shared swarm, and the units' shared
+    swarms are then combined.
     """
+    if mode == "parallel":
+        if inject is not None:
+            raise ValueError("mode='parallel' does not replay injected draws")
+        return _panel_mif_parallel(struct, shared_array, unit_array, rw_sd, M, J, keys, thresh, n_monitors)
+    if mode != "sequential":
+        raise ValueError("mode must be 'sequential' or 'parallel'")
     from . import random as pprandom
 
     torch = _ffi.require_cuda()
@@ -1257,6 +1269,119 @@ def panel_mif(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, 
         if u == 0:
             fs = nat[:, :, :ns]
     return shared_tr, unit_tr, fs, fu
+
+
+def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd, M: int, J: int, keys,
+                        thresh: float = 0.0, n_monitors: int = 0):
+    """Panel IF2 with the units filtered side by side -- a mode the reference
+    does not have (its unit scan carries the shared swarm from unit to unit,
+    ``pypomp/core/algorithms/panel_mif.py:119-123, 216-219``).
+
+    Iteration m, replicate r:
+
+    * one ``ppf_perfilter`` call filters all U units of all replicates
+      (n x U swarms, ragged series masked per unit), each from
+      [shared swarm S_r | unit u's swarm] with unit u's key (the sequential
+      mode's ``split(iteration key, U)[u]``) and cooling (its own length);
+    * unit u's unit-specific swarm becomes its filter's output, as in the
+      sequential mode with ``block=True`` (no reordering across units);
+    * the shared swarm is recombined from the units' outputs S'_{r,u}: per
+      shared parameter (estimation scale), the centre is the inverse-variance
+      weighted mean of the units' swarm means, sum_u mu_u / v_u / sum_u 1 / v_u
+      (the maximiser of the sum of the units' quadratic log-likelihood
+      approximations; a plain mean when no unit's swarm has spread), and
+      particle j is that centre plus the deviation of particle j of unit
+      (j mod U) from its unit's mean, so the swarm keeps the units' spread.
+
+    Without shared parameters the units never interact and each unit's swarm
+    is exactly what a single-unit IF2 iteration gives it.  The log-likelihood
+    columns are each unit's perturbed-filter log-likelihood (or, with
+    monitors, the mean of ``n_monitors`` filters at the unit's input swarm
+    mean, all units in one batched call).  Returns what :func:`panel_mif`
+    returns.
+    """
+    from . import random as pprandom
+
+    torch = _ffi.require_cuda()
+    spec = struct.spec
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sh = np.asarray(shared_array, dtype=np.float64)
+    un = np.asarray(unit_array, dtype=np.float64)
+    n = sh.shape[0]
+    ns, nu, U = sh.shape[2], un.shape[3], struct.U
+    if sh.shape[1] != J or un.shape[1] != J or un.shape[2] != U:
+        raise ValueError("shared_array must be (n_reps, J, n_shared) and unit_array (n_reps, J, U, n_spec)")
+    if M < 1:
+        raise ValueError("M must be greater than 0.")
+    perms = np.asarray(struct.permutations, dtype=np.int64)
+    if not np.all(perms == perms[0]):
+        raise ValueError("mode='parallel' needs the same parameter order in every unit")
+    perm, inv = perms[0], np.argsort(perms[0])
+    perm_t, inv_t = torch.tensor(perm, device=dev), torch.tensor(inv, device=dev)
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    sig_p, sig0_p = rw_sd.arrays(struct.param_names)
+    sig_u, sig0_u = sig_p[perm], sig0_p[perm]
+    panel0 = np.concatenate([sh[:, :, None, :].repeat(U, axis=2), un], axis=3)   # (n, J, U, Pp) natural
+    est0 = spec.to_est(panel0[..., perm])[..., inv]                               # panel order
+    S = torch.tensor(est0[:, :, 0, :ns].transpose(0, 2, 1).copy(), dtype=torch.float32, device=dev)
+    Us = torch.tensor(est0[:, :, :, ns:].transpose(0, 2, 3, 1).copy(), dtype=torch.float32, device=dev)
+    m_keys = np.stack([pprandom.split(k, M + 1)[1:] for k in keys])               # (n, M)
+    all_units = struct.all_units()
+    T_u = np.asarray(struct.T_u, dtype=np.int64)
+    Tmax = int(struct.ys.shape[1])
+    unit_f = np.tile(np.arange(U, dtype=np.int32), n)
+    jmod = torch.arange(J, device=dev) % U
+
+    def nat(s_est, u_est):        # (n, ns), (n, U, nu) estimation scale -> natural, panel order
+        panel = np.concatenate([np.repeat(s_est[:, None], U, axis=1), u_est], axis=2)
+        out = spec.from_est(panel[..., perm])[..., inv]
+        return out[:, 0, :ns], out[:, :, ns:]
+
+    shared_tr = np.full((n, M + 1, ns + 1), np.nan)
+    unit_tr = np.full((n, M + 1, U, nu + 1), np.nan)
+    s0, u0 = nat(S.mean(dim=2).cpu().numpy().astype(np.float64), Us.mean(dim=3).cpu().numpy().astype(np.float64))
+    shared_tr[:, 0, 1:], unit_tr[:, 0, :, 1:] = s0, u0
+    for it in range(M):
+        unit_keys = np.stack([pprandom.split(k, U) for k in m_keys[:, it]])       # (n, U)
+        cool = np.zeros((U, Tmax), np.float32)
+        for u in range(U):
+            cool[u, :T_u[u]] = [rw_sd.cooling_factor(i, it, int(T_u[u])) for i in range(int(T_u[u]))]
+        panel = torch.cat([S[:, None].expand(n, U, ns, J), Us], dim=2)           # (n, U, Pp, J)
+        swarm = panel.reshape(n * U, ns + nu, J).index_select(1, perm_t).contiguous()
+        res = run_perfilter(all_units, swarm, unit_keys.reshape(-1), J, sig_u, sig0_u, cool, cool[:, 0],
+                            thresh=thresh, unit_f=unit_f)
+        if n_monitors >= 1:
+            mean = swarm.mean(dim=2).cpu().numpy()                                # (n U, P) unit order
+            mon = np.stack([pprandom.split(k, n_monitors) for k in unit_keys.reshape(-1)])
+            pf = run_pfilter(all_units, np.repeat(mean, n_monitors, axis=0), mon.reshape(-1), J,
+                             thresh=thresh, est=True, unit_f=np.repeat(unit_f, n_monitors))
+            ll_units = pf["loglik"].reshape(n, U, n_monitors).mean(axis=2)
+        else:
+            ll_units = res["loglik"].cpu().numpy().reshape(n, U)
+        out = res["swarm"].index_select(1, inv_t).reshape(n, U, ns + nu, J)      # panel order
+        if nu > 0:
+            Us = out[:, :, ns:].contiguous()
+        if ns > 0:
+            su = out[:, :, :ns].double()                                          # (n, U, ns, J)
+            mu = su.mean(dim=3)
+            var = su.var(dim=3, unbiased=False)
+            w = torch.where(var > 0, 1.0 / var.clamp_min(1e-300), torch.zeros_like(var))
+            wsum = w.sum(dim=1)
+            centre = torch.where(wsum > 0, (w * mu).sum(dim=1) / wsum.clamp_min(1e-300), mu.mean(dim=1))
+            dev_j = su - mu[..., None]                                            # deviations from unit means
+            pick = dev_j.gather(1, jmod.view(1, 1, 1, J).expand(n, 1, ns, J)).squeeze(1)   # (n, ns, J)
+            S = (centre[..., None] + pick).float().contiguous()
+        s_mean, u_mean = nat(S.mean(dim=2).cpu().numpy().astype(np.float64),
+                             Us.mean(dim=3).cpu().numpy().astype(np.float64))
+        shared_tr[:, it + 1, 0] = ll_units.sum(axis=1)
+        shared_tr[:, it + 1, 1:] = s_mean
+        unit_tr[:, it + 1, :, 0] = ll_units
+        unit_tr[:, it + 1, :, 1:] = u_mean
+    s_fin = S.cpu().numpy().astype(np.float64).transpose(0, 2, 1)                 # (n, J, ns)
+    u_fin = Us.cpu().numpy().astype(np.float64).transpose(0, 3, 1, 2)             # (n, J, U, nu)
+    panel = np.concatenate([np.repeat(s_fin[:, :, None], U, axis=2), u_fin], axis=3)
+    natf = spec.from_est(panel[..., perm])[..., inv]
+    return shared_tr, unit_tr, natf[:, :, 0, :ns], natf[:, :, :, ns:]
 
 
 def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optimizer, M: int, eta,

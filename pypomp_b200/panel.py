@@ -383,8 +383,12 @@ class PanelPomp:
                                              time.time() - start, old_key))
 
     def mif(self, J: int, M: int, rw_sd, key=None, theta=None, thresh: float = 0.0, n_monitors: int = 0,
-            block: bool = True) -> None:
-        """Panel iterated filtering (``pypomp/panel/estimation_mixin.py:597-773``)."""
+            block: bool = True, mode: str = "sequential") -> None:
+        """Panel iterated filtering (``pypomp/panel/estimation_mixin.py:597-773``).
+
+        ``mode="parallel"`` (not in the reference) filters all units side by
+        side in one batched call per iteration and recombines the shared
+        swarm afterwards (``functional._panel_mif_parallel``)."""
         from . import functional as F
 
         start = time.time()
@@ -400,14 +404,16 @@ class PanelPomp:
         us = np.repeat(th.unit_array(names, un)[:, None, :, :], J, axis=1)
         key, old_key = self._update_fresh_key(key)
         keys = pprandom.split(key, n)
-        s_tr, u_tr, _, _ = F.panel_mif(self.to_struct(), sh, us, rw_sd, M, J, keys, thresh, n_monitors, block)
+        s_tr, u_tr, _, _ = F.panel_mif(self.to_struct(), sh, us, rw_sd, M, J, keys, thresh, n_monitors, block,
+                                       mode=mode)
         self.theta = PanelParameters.from_arrays(s_tr[:, -1, 1:], u_tr[:, -1, :, 1:], sn, un, names,
                                                  logLik_unit=u_tr[:, -1, :, 0])
         self.results_history.add(PanelResult(
             "mif", theta_for_result,
             {"shared_traces": s_tr, "unit_traces": u_tr, "unit_names": names, "shared_names": sn,
              "unit_param_names": un},
-            {"J": J, "M": M, "rw_sd": rw_sd, "thresh": thresh, "n_monitors": n_monitors, "block": block},
+            {"J": J, "M": M, "rw_sd": rw_sd, "thresh": thresh, "n_monitors": n_monitors, "block": block,
+             "mode": mode},
             time.time() - start, old_key))
 
     def train(self, J: int, M: int, eta, chunk_size: int = 1, optimizer=None, alpha: float = 0.97, key=None,

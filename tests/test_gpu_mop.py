@@ -159,7 +159,7 @@ def test_persistent_form_equals_per_step_launches(model, alpha):
     b = F.run_mop(st, th2, seeds, J, alpha, grad=True, save_ancestors=True, persistent=False)
     assert np.array_equal(a["anc"], b["anc"])
     assert np.array_equal(a["value"], b["value"])
-    tol = 1e-9 if model in ("SV", "Ricker") else 1e-5
+    tol = 1e-9
     for f in range(2):
         assert np.linalg.norm(a["grad"][f] - b["grad"][f]) <= tol * np.linalg.norm(b["grad"][f]), \
             (a["grad"][f], b["grad"][f])

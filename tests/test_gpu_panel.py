@@ -218,3 +218,90 @@ def test_panel_mif_queued_units_equal_separate_calls(block):
         assert np.array_equal(nat[:, :, ns:], u_fin[:, :, u])
         if u == 0:
             assert np.array_equal(nat[:, :, :ns], s_fin)
+
+
+def test_panel_mif_parallel_units_equal_single_unit_filters():
+    """mode='parallel' (not in the reference): all units of all replicates in
+    one batched perturbed-filter call per iteration.  Each unit's filter is
+    the single-unit filter from the iteration's swarms, bit for bit (the first
+    unit's also against the C oracle); the unit-specific swarms are those
+    filters' outputs, and the shared swarm follows the documented
+    recombination (inverse-variance weighted centre, deviations of unit
+    j mod U)."""
+    import torch
+
+    from pypomp_b200 import functional as F
+    from pypomp_b200 import random as pprandom
+    from pypomp_b200.optim import RWSigma
+
+    pan = _ricker_panel()
+    st = pan.to_struct()
+    names = pan.get_unit_names()
+    J, M = 1500, 2
+    rw = RWSigma({n: 0.03 for n in pan.canonical_param_names}).geometric_cooling(0.5)
+    sh = np.repeat(pan.theta.shared_array()[:, None, :], J, axis=1)
+    un = np.repeat(pan.theta.unit_array(names)[:, None], J, axis=1)
+    keys = np.array([23], np.uint64)
+    s_tr, u_tr, s_fin, u_fin = F.panel_mif(st, sh, un, rw, M, J, keys, mode="parallel")
+    spec, U = st.spec, st.U
+    perm = np.asarray(st.permutations)[0]
+    inv = np.argsort(perm)
+    ns, nu = sh.shape[2], un.shape[3]
+    sig_p, sig0_p = rw.arrays(st.param_names)
+    panel0 = np.concatenate([sh[:, :, None, :].repeat(U, axis=2), un], axis=3)
+    est = spec.to_est(panel0[..., perm])[..., inv]
+    S = est[0, :, 0, :ns].T.astype(f32)                       # (ns, J)
+    Us = est[0, :, :, ns:].transpose(1, 2, 0).astype(f32)     # (U, nu, J)
+    m_keys = pprandom.split(int(keys[0]), M + 1)[1:]
+    for it in range(M):
+        unit_keys = pprandom.split(int(m_keys[it]), U)
+        outs = []
+        for u in range(U):
+            st_u = st.unit(u)
+            T = st_u.ys.shape[0]
+            swarm = np.concatenate([S, Us[u]], axis=0)[perm]  # (P, J) unit order
+            cool = np.array([rw.cooling_factor(i, it, T) for i in range(T)], dtype=np.float32)
+            one = F.run_perfilter(st_u, torch.from_numpy(swarm[None].copy()).cuda(), unit_keys[u:u + 1], J,
+                                  sig_p[perm], sig0_p[perm], cool, cool[0])
+            assert one["loglik"].cpu().numpy()[0] == u_tr[0, it + 1, u, 0]
+            if it == 0 and u == 0:
+                want = cora.perfilter(spec.kind, 1, 1, swarm[None], st_u.ys, J, sig_p[perm].astype(f32),
+                                      sig0_p[perm].astype(f32), cool, cool[0], seeds=unit_keys[u:u + 1],
+                                      ycon=spec.ycon(st_u.ys))
+                assert np.array_equal(one["swarm"].cpu().numpy()[0], want["swarm"][0])
+            outs.append(one["swarm"].cpu().numpy()[0][inv])       # panel order (P, J)
+        outs = np.stack(outs)                                     # (U, P, J)
+        Us = outs[:, ns:].copy()
+        su = outs[:, :ns].astype(np.float64)
+        mu = su.mean(axis=2)
+        var = su.var(axis=2)
+        w = np.where(var > 0, 1.0 / np.where(var > 0, var, 1.0), 0.0)
+        centre = (w * mu).sum(axis=0) / w.sum(axis=0)
+        S = (centre[:, None] + (su - mu[..., None])[np.arange(J) % U, :, np.arange(J)].T).astype(f32)
+    s_e = S.T.astype(np.float64)                                  # (J, ns)
+    for u in range(U):
+        nat = spec.from_est(np.concatenate([s_e, Us[u].T.astype(np.float64)], axis=1)[:, perm])[:, inv]
+        assert np.array_equal(nat[:, ns:], u_fin[0, :, u])
+        if u == 0:
+            np.testing.assert_allclose(nat[:, :ns], s_fin[0], rtol=1e-6)
+
+
+def test_panel_mif_parallel_raises_the_panel_loglik():
+    """From a perturbed start, parallel-mode panel IF2 raises the summed unit
+    log-likelihood of the panel (PanelPomp.mif end to end, mode='parallel')."""
+    import pypomp_b200 as pp
+    from pypomp_b200.optim import RWSigma
+
+    units = {f"u{i}": pp.Ricker(T=60 + 10 * i, r=np.exp(3.0), sigma=0.3, phi=10.0, key=100 + i) for i in range(6)}
+    shared = pd.DataFrame({"shared": [0.6, 6.0]}, index=["sigma", "phi"])
+    spec = pd.DataFrame([[np.exp(2.6)] * 6, [7.0] * 6], index=["r", "N_0"], columns=list(units))
+    pan = pp.PanelPomp(units, pp.PanelParameters({"shared": shared, "unit_specific": spec}))
+    rw = RWSigma({"r": 0.05, "sigma": 0.05, "phi": 0.05, "N_0": 0.0}).geometric_cooling(0.5)
+    pan.pfilter(J=2000, key=1, reps=4)
+    before = pan.results()["shared logLik"].iloc[0]
+    pan.mif(J=2000, M=15, rw_sd=rw, key=2, mode="parallel")
+    tr = pan.traces()
+    assert np.all(np.isfinite(tr.loc[tr["unit"] == "shared", "logLik"].to_numpy()[1:]))
+    pan.pfilter(J=2000, key=3, reps=4)
+    after = pan.results()["shared logLik"].iloc[0]
+    assert after > before + 5.0, (before, after)
