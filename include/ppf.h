@@ -90,6 +90,15 @@ typedef struct ppf_model {
  * another, grid barriers between the steps) would be chosen; for comparisons
  * and tests.  Both forms give the same forward results bit for bit. */
 #define PPF_F_NO_PERSIST (1u << 11)
+/* ppf_pfilter, streaming path, Philox draws: the hardware approximations of
+ * the special-function units for the Box-Muller transform (log, sqrt, sin,
+ * cos) and for the resampling weights' exponential, and fused multiply-adds
+ * in the model arithmetic.  The fixed-point resampling CDF, the Philox
+ * counters and the float64 log-likelihood sums are unchanged.  Results are
+ * statistically equivalent to the exact arithmetic (log-weights of the same
+ * particles agree to ~1e-6 relative) but not bit-identical with the C oracle.
+ * Ignored with PPF_F_INJECT and on the other paths. */
+#define PPF_F_FAST (1u << 12)
 
 /* Execution paths; all produce bit-identical results. */
 enum {

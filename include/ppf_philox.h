@@ -71,6 +71,31 @@ PPF_HD void pp_boxmuller(uint32_t wa, uint32_t wb, float* z0, float* z1) {
   *z1 = rr * s;
 }
 
+#if defined(__CUDACC__)
+/* Box-Muller pair from the same two words with the SFU approximations
+ * (__log2f, rsqrtf, __sincosf; device only).  Used by the PPF_F_FAST kernels:
+ * close to pp_boxmuller (a few ulp) but not bit-identical, and there is no
+ * host counterpart.  sin / cos are taken at 2 pi (u2 - 1/2) in [-pi, pi),
+ * where the approximations hold their accuracy, and negated. */
+__device__ __forceinline__ void pp_boxmuller_fast(uint32_t wa, uint32_t wb, float* z0, float* z1) {
+  const float u1 = (float)((wa >> 8) + 1u) * 5.9604644775390625e-08f;
+  const float u2 = (float)(wb >> 8) * 5.9604644775390625e-08f;
+  const float t = -1.3862943611198906f * __log2f(u1);       /* -2 ln u1 */
+  const float rr = t > 0.0f ? t * rsqrtf(t) : 0.0f;
+  float s, c;
+  __sincosf(6.283185307179586f * (u2 - 0.5f), &s, &c);
+  *z0 = -rr * c;
+  *z1 = -rr * s;
+}
+
+__device__ __forceinline__ void pp_normal4_fast(uint64_t seed, uint32_t call, uint32_t s, uint32_t tag,
+                                                float* z4) {
+  const pp_u32x4 w = pp_philox4x32_10(call, s, tag, 0u, (uint32_t)seed, (uint32_t)(seed >> 32));
+  pp_boxmuller_fast(w.v[0], w.v[1], &z4[0], &z4[1]);
+  pp_boxmuller_fast(w.v[2], w.v[3], &z4[2], &z4[3]);
+}
+#endif
+
 /* Normal number i of the stream (step s, tag) of one filter:
  * element i % 4 of the four normals made from Philox(c0 = i / 4, s, tag, 0).
  * Particle k draws the n consecutive normals i = k n ... k n + n - 1, so a

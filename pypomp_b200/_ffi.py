@@ -32,6 +32,7 @@ F_EST = 1 << 7
 F_NATURAL = 1 << 8
 F_GRAPH = 1 << 9
 F_NO_PERSIST = 1 << 11
+F_FAST = 1 << 12
 F_NO_CLUSTER = 1 << 10
 
 PATH_AUTO, PATH_PLAIN, PATH_STREAM, PATH_RESIDENT, PATH_CLUSTER = 0, 1, 2, 3, 4

@@ -166,6 +166,14 @@ __device__ __forceinline__ float qweight_e(float w, float M, bool collapsed) {
   return pp_expq(w - M);     // equals pp_expf(w - M) wherever the quantised value can be >= 1
 }
 __device__ __forceinline__ uint64_t qweight_from_e(float e) { return __float2ull_rn(e * kQScale); }
+// qweight_e with the SFU exponential (PPF_F_FAST): e in (0, 1], not bit-identical.
+template <bool FAST>
+__device__ __forceinline__ float qweight_e_t(float w, float M, bool collapsed) {
+  if (!FAST) return qweight_e(w, M, collapsed);
+  if (collapsed) return 9.094947017729282e-13f;
+  if (w != w) return 0.0f;
+  return __expf(w - M);
+}
 __device__ __forceinline__ uint64_t qweight(float w, float M, bool collapsed) {
   return qweight_from_e(qweight_e(w, M, collapsed));
 }

@@ -112,6 +112,10 @@ struct MopWork {
 };
 
 int run_pfilter_path(Args& a, int path, cudaStream_t s);
+// the per-filter model constants (k_prep), dispatched by model
+int run_prep(Args& a, cudaStream_t s);
+// the streaming path with PPF_F_FAST (ppf_fast.cu, compiled with contraction)
+int run_stream_fast(Args& a, cudaStream_t s);
 int run_stream_any(Args& a, cudaStream_t s);   // stream path, any model
 // Stream-path tile configurations (particles per CTA = threads x items per
 // thread): the tile sets how many CTAs one step launches, F x ceil(J / tile).

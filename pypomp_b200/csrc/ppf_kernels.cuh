@@ -38,7 +38,7 @@ __device__ __forceinline__ void step_noise(const Args& a, int f, int j, int s, i
 // Normals of the group of 4 consecutive particles k0..k0+3 (k0 % 4 == 0) at
 // step s, N per particle: z[e*N + r].  Philox calls (k0 N)/4 ... + N-1 cover
 // the group exactly; positions past J read zeros in injection mode.
-template <int N, bool INJ>
+template <int N, bool INJ, bool FAST = false>
 __device__ __forceinline__ void group_noise(const Args& a, int f, int s, int k0, float* z) {
   if (N == 0) return;
   if (INJ) {
@@ -52,7 +52,10 @@ __device__ __forceinline__ void group_noise(const Args& a, int f, int s, int k0,
     const uint64_t seed = a.seeds[f];
     const uint32_t c0 = (uint32_t)(k0 / 4) * N;
 #pragma unroll
-    for (int c = 0; c < N; ++c) pp_normal4(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
+    for (int c = 0; c < N; ++c) {
+      if (FAST) pp_normal4_fast(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
+      else pp_normal4(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
+    }
   }
 }
 
@@ -69,7 +72,7 @@ struct ChildGroup {
 
 // Normals of the G consecutive particles k0..k0+G-1 (k0 % G == 0) at step s,
 // N per particle: z[e*N + r].  Philox calls (k0 N)/4 ... cover them exactly.
-template <int G, int N, bool INJ>
+template <int G, int N, bool INJ, bool FAST = false>
 __device__ __forceinline__ void group_noise_g(const Args& a, int f, int s, int k0, float* z) {
   if (N == 0) return;
   if (INJ) {
@@ -83,7 +86,10 @@ __device__ __forceinline__ void group_noise_g(const Args& a, int f, int s, int k
     const uint64_t seed = a.seeds[f];
     const uint32_t c0 = (uint32_t)k0 * N / 4;
 #pragma unroll
-    for (int c = 0; c < G * N / 4; ++c) pp_normal4(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
+    for (int c = 0; c < G * N / 4; ++c) {
+      if (FAST) pp_normal4_fast(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
+      else pp_normal4(seed, c0 + c, (uint32_t)s, PPF_TAG_PROCESS, z + 4 * c);
+    }
   }
 }
 
@@ -412,7 +418,7 @@ __device__ __forceinline__ int if2_row_stride(int P) { return P | 1; }
 // LB = false (the persistent MOP forward, all tiles resident and a grid
 // barrier after this body): publish the tile total in desc[t & 1] and leave
 // the prefix to tile_prefix, instead of the lookback.
-template <class M, int TPB, int IT, bool LB = true>
+template <class M, int TPB, int IT, bool LB = true, bool FAST = false>
 __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
@@ -450,7 +456,7 @@ __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
   }
 #pragma unroll
   for (int i = 0; i < IT; ++i) {
-    ev[i] = qweight_e(wv[i], Mx, collapsed);
+    ev[i] = qweight_e_t<FAST>(wv[i], Mx, collapsed);
     qs += (jb + i < J) ? qweight_from_e(ev[i]) : 0ull;
   }
   // a resampling step reads its parents' weights only through q: keep e in

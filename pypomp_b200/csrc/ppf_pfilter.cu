@@ -493,7 +493,30 @@ int run_stream_tiled(Args& a, cudaStream_t s) {
 
 template <class M>
 int run_stream(Args& a, cudaStream_t s) {
+  if ((a.flags & PPF_F_FAST) && !(a.flags & PPF_F_INJECT) && a.mode == MODE_PF) return run_stream_fast(a, s);
   return (a.flags & PPF_F_INJECT) ? run_stream_tiled<M, true>(a, s) : run_stream_tiled<M, false>(a, s);
+}
+
+template <class M>
+static int launch_prep(Args& a, cudaStream_t s) {
+  k_prep<M><<<(a.F + 127) / 128, 128, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
+}
+
+int run_prep(Args& a, cudaStream_t s) {
+  switch (a.model.kind) {
+    case PPF_MODEL_LG:
+      switch (a.model.dx) {
+        case 1: return a.model.dy == 1 ? launch_prep<LG<1, 1>>(a, s) : launch_prep<LG<1>>(a, s);
+        case 2: return a.model.dy == 2 ? launch_prep<LG<2, 2>>(a, s) : launch_prep<LG<2>>(a, s);
+        case 3: return a.model.dy == 3 ? launch_prep<LG<3, 3>>(a, s) : launch_prep<LG<3>>(a, s);
+        case 4: return a.model.dy == 4 ? launch_prep<LG<4, 4>>(a, s) : launch_prep<LG<4>>(a, s);
+        default: return PPF_EUNSUPPORTED;
+      }
+    case PPF_MODEL_SV: return launch_prep<SV>(a, s);
+    case PPF_MODEL_RICKER: return launch_prep<Ricker>(a, s);
+    default: return PPF_EINVAL;
+  }
 }
 
 template <class M>

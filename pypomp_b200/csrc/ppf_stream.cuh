@@ -11,7 +11,7 @@
 namespace ppf {
 
 // Initial states of tile b of filter f, propagated into observation 0.
-template <class M, int TPB, bool INJ>
+template <class M, int TPB, bool INJ, bool FAST = false>
 __device__ __forceinline__ void init_tile(const Args& a, int f, int b) {
   __shared__ typename M::Consts c;
   __shared__ unsigned int smk[2 * (TPB / 32)];
@@ -38,8 +38,8 @@ __device__ __forceinline__ void init_tile(const Args& a, int f, int b) {
   for (int k0 = j0 + 4 * threadIdx.x; k0 < j1; k0 += 4 * TPB) {
     float z0[4 * (M::NZ0 > 0 ? M::NZ0 : 1)];
     float z[4 * M::NZ];
-    group_noise<M::NZ0, INJ>(a, f, 0, k0, z0);
-    group_noise<M::NZ, INJ>(a, f, 1, k0, z);
+    group_noise<M::NZ0, INJ, FAST>(a, f, 0, k0, z0);
+    group_noise<M::NZ, INJ, FAST>(a, f, 1, k0, z);
     float xo[4][DX];
     float wo[4];
 #pragma unroll
@@ -102,7 +102,7 @@ struct RespropOccupancy {
 // The body for tile b of filter f at step t.  TMA: stage the tile's parent
 // rows with bulk copies (the streaming kernel) or plain loads (the persistent
 // MOP kernel, whose mbarriers would otherwise need a phase per step).
-template <class M, int TPB, int IT, bool INJ, bool TMA>
+template <class M, int TPB, int IT, bool INJ, bool TMA, bool FAST = false>
 __device__ __forceinline__ void resprop_tile(const Args& a, int t, int f, int b) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
@@ -275,7 +275,7 @@ __device__ __forceinline__ void resprop_tile(const Args& a, int t, int f, int b)
       if (k0 >= khi) break;
       const int lo = max(0, klo - k0), hi = min(G, khi - k0);   // valid e in [lo, hi)
       float z[G * M::NZ];
-      if (!last) group_noise_g<G, M::NZ, INJ>(a, f, t + 2, k0, z);
+      if (!last) group_noise_g<G, M::NZ, INJ, FAST>(a, f, t + 2, k0, z);
       float xo[G][DX];
       float wo[G];
 #pragma unroll

@@ -61,14 +61,16 @@ def _device_inputs(torch, struct: PompStruct, dev):
 def run_pfilter(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J: int, *,
                 thresh: float = 0.0, CLL=False, ESS=False, filter_mean=False,
                 prediction_mean=False, est=False, unit_f=None, path=None, inject=None,
-                save_ancestors=False, save_weights=False, return_torch=False):
+                save_ancestors=False, save_weights=False, return_torch=False, fast=False):
     """One batched call of ``ppf_pfilter`` over F filters.
 
     ``theta_f`` (F, P) parameters, ``seeds_f`` (F,) keys.  ``inject`` is an
     optional dict of host arrays ``z0`` (F,J,n0), ``z`` (F,T,J,nz), ``u``
     (F,T) that replaces the Philox draws.  ``path`` is "plain", "stream",
     "resident", "cluster", "stream@<tile>" (tile 2048, 512 or 256 particles
-    per CTA) or None (automatic).  Returns a dict of NumPy arrays.
+    per CTA) or None (automatic).  ``fast`` sets ``PPF_F_FAST`` (streaming
+    path, Philox draws: hardware special-function approximations, not
+    bit-identical with the oracle).  Returns a dict of NumPy arrays.
     """
     torch = _ffi.require_cuda()
     if J < 1:
@@ -89,6 +91,7 @@ def run_pfilter(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J:
     flags |= (_ffi.F_FMEAN if filter_mean else 0) | (_ffi.F_PMEAN if prediction_mean else 0)
     flags |= (_ffi.F_EST if est else 0)
     flags |= (_ffi.F_SAVE_ANC if save_ancestors else 0) | (_ffi.F_SAVE_W if save_weights else 0)
+    flags |= _ffi.F_FAST if fast else 0
     out = {"loglik": torch.zeros(F, dtype=torch.float64, device=dev)}
     f32 = dict(dtype=torch.float32, device=dev)
     if CLL:
@@ -174,13 +177,14 @@ def autotune(struct: PompStruct, theta_f: np.ndarray, seeds_f: np.ndarray, J: in
 
 def pfilter(struct: PompStruct, thetas_array, J: int, keys, thresh: float = 0.0,
             CLL: bool = False, ESS: bool = False, filter_mean: bool = False,
-            prediction_mean: bool = False, *, path=None) -> dict:
+            prediction_mean: bool = False, *, path=None, fast: bool = False) -> dict:
     """Bootstrap particle filter (``pypomp/functional/pfilter.py:11-90``).
 
     ``thetas_array`` (n_theta, P) natural scale; ``keys`` (n_theta, reps).
     Returns ``logLik`` (n_theta, reps) and, when requested, ``CLL``/``ESS``
     (n_theta, reps, T) and ``filter_mean``/``prediction_mean``
-    (n_theta, reps, T, dx).
+    (n_theta, reps, T, dx).  ``fast`` (not in the reference) uses the
+    ``PPF_F_FAST`` kernels on the streaming path.
     """
     thetas = np.atleast_2d(np.asarray(thetas_array, dtype=np.float32))
     keys = np.asarray(keys, dtype=np.uint64)
@@ -191,7 +195,7 @@ def pfilter(struct: PompStruct, thetas_array, J: int, keys, thresh: float = 0.0,
         raise ValueError("keys must have shape (n_theta, reps)")
     theta_f = np.repeat(thetas, reps, axis=0)
     res = run_pfilter(struct, theta_f, keys.reshape(-1), J, thresh=thresh, CLL=CLL, ESS=ESS,
-                      filter_mean=filter_mean, prediction_mean=prediction_mean, path=path)
+                      filter_mean=filter_mean, prediction_mean=prediction_mean, path=path, fast=fast)
     T = res.get("cll", res.get("ess", np.zeros((0, 0)))).shape[-1] if (CLL or ESS) else None
     out = {"logLik": res["loglik"].reshape(n, reps)}
     if CLL:

@@ -301,7 +301,9 @@ def test_panel_mif_parallel_raises_the_panel_loglik():
     before = pan.results()["shared logLik"].iloc[0]
     pan.mif(J=2000, M=15, rw_sd=rw, key=2, mode="parallel")
     tr = pan.traces()
-    assert np.all(np.isfinite(tr.loc[tr["unit"] == "shared", "logLik"].to_numpy()[1:]))
+    ll = tr.loc[(tr["unit"] == "shared") & (tr["method"] == "mif"), "logLik"].to_numpy()
+    assert ll.shape == (16,) and np.all(np.isfinite(ll[1:]))        # iteration 0 has no log-likelihood
+    assert ll[-1] > ll[1]
     pan.pfilter(J=2000, key=3, reps=4)
     after = pan.results()["shared logLik"].iloc[0]
     assert after > before + 5.0, (before, after)

@@ -300,3 +300,45 @@ def test_largest_swarm_bit_exact():
     got = F.run_pfilter(st, th, seeds, J, path="stream", save_ancestors=True)
     assert np.array_equal(got["anc"], want["anc"])
     np.testing.assert_allclose(got["loglik"], want["loglik"], rtol=1e-12)
+
+
+def test_fast_arithmetic_first_step_log_weights_close_to_exact(lg2d):
+    """PPF_F_FAST (hardware special functions, contraction): the first step's
+    log-weights of the same particles (same Philox words) agree with the exact
+    arithmetic within 1e-5 relative (1e-5 absolute near zero), and the
+    resampling ancestors stay sorted and in range."""
+    F = _F()
+    st = lg2d.to_struct()
+    st.ys = st.ys[:5]
+    th = np.repeat(lg2d.theta.to_array(lg2d.canonical_param_names), 3, axis=0).astype(f32)
+    seeds = np.array([3, 4, 5], np.uint64)
+    J = 65536
+    ex = F.run_pfilter(st, th, seeds, J, path="stream", save_weights=True)
+    fa = F.run_pfilter(st, th, seeds, J, path="stream", save_weights=True, save_ancestors=True, fast=True)
+    w_ex, w_fa = ex["logw"][:, 0], fa["logw"][:, 0]
+    assert np.all(np.isfinite(w_fa))
+    assert np.all(np.abs(w_fa - w_ex) <= 1e-5 * np.maximum(np.abs(w_ex), 1.0))
+    assert not np.array_equal(w_fa, w_ex)          # the fast kernels really ran
+    anc = fa["anc"]
+    assert np.all(np.diff(anc, axis=-1) >= 0) and anc.min() >= 0 and anc.max() < J
+
+
+def test_fast_arithmetic_loglik_against_kalman():
+    """LG 2-D, T = 300, J = 262144, 32 seeds with PPF_F_FAST: the log-mean-exp
+    of the log-likelihoods is within Monte Carlo error of the exact Kalman
+    value and within 1e-4 of it relative, as the exact arithmetic is."""
+    import pypomp_b200 as pp
+    from pypomp_b200.maths import logmeanexp, logmeanexp_se
+    from tests.conftest import LG2_Q, LG2_R
+
+    F = _F()
+    m = pp.LG(T=300, Q=LG2_Q, R=LG2_R, key=7)
+    st = m.to_struct()
+    th = np.repeat(m.theta.to_array(m.canonical_param_names), 32, axis=0).astype(f32)
+    A, C, Q, R, X0 = kalman.lg_matrices(th[0].astype(np.float64), 2, 2)
+    exact = kalman.kalman_loglik(st.ys, A, C, Q, R, X0)
+    for fast in (False, True):
+        ll = F.run_pfilter(st, th, np.arange(32, dtype=np.uint64) + 500, 262144, path="stream", fast=fast)["loglik"]
+        lme, se = logmeanexp(ll), logmeanexp_se(ll)
+        assert abs(lme - exact) <= 5 * se + 1e-3, (fast, lme, exact, se)
+        assert abs(lme - exact) / abs(exact) <= 1e-4, (fast, lme, exact)
