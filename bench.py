@@ -782,13 +782,54 @@ def run_pmcmc(args):
 def run_profile_case(args):
     """A small case of the same kernels for ncu captures: the headline model
     and J, 24 seeds (state 2 x 24 x 262144 x 12 B = 151 MB, larger than L2),
-    the first 12 observations, one call.  ``--config sim`` and ``--config c5``
-    give small cases of the simulation and cluster-path kernels."""
+    the first 12 observations, one call (``--fast``: the PPF_F_FAST kernels).
+    ``--config sim`` and ``--config c5`` give small cases of the simulation
+    and cluster-path kernels; ``c3`` the persistent MOP forward and adjoint
+    (SV, T = 200, J = 65536); ``c4`` the shared-memory-resident filter (64
+    Ricker filters, J = 16384, T = 50); ``plain`` the one-filter baseline
+    kernels (LG 2-D, J = 262144, T = 12); ``if2`` the streaming IF2 kernels
+    (128 Ricker filters, J = 8192, T = 50, as one iteration of the packed
+    panel IF2)."""
+    import math
+
     import torch
 
     from pypomp_b200 import functional as F
 
     import pypomp_b200 as pp
+
+    if args.config == "c3":
+        m = pp.SV(T=200, key=0)
+        th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(np.float32)
+        r = F.run_mop(m.to_struct(), th, np.array([1], np.uint64), 65536, 0.97, grad=True)
+        print("profile case MOP", r["value"], r["grad"])
+        return
+    if args.config == "c4":
+        m = pp.Ricker(T=50, key=0)
+        grid = np.array([[math.exp(a), b, 10.0, 7.0] for a in np.linspace(3.0, 4.6, 8)
+                         for b in np.linspace(0.05, 0.8, 8)], np.float32)
+        r = F.run_pfilter(m.to_struct(), grid, np.arange(64, dtype=np.uint64), 16384, path="resident")
+        print("profile case resident", r["loglik"][:2])
+        return
+    if args.config == "plain":
+        m = workload()
+        st = m.to_struct()
+        st.ys = st.ys[:12]
+        th = m.theta.to_array(m.canonical_param_names).astype(np.float32)
+        r = F.run_pfilter(st, th, np.array([3], np.uint64), J, path="plain")
+        print("profile case plain", r["loglik"])
+        return
+    if args.config == "if2":
+        m = pp.Ricker(T=50, key=0)
+        st = m.to_struct()
+        est = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(np.float32)
+        swarm = torch.from_numpy(np.ascontiguousarray(np.repeat(est[:, :, None], 8192, axis=2).repeat(128, 0))).cuda()
+        sig = np.full(4, 0.02, np.float32)
+        r = F.run_perfilter(st, swarm, np.arange(128, dtype=np.uint64), 8192, sig, sig, np.full(50, 0.5, np.float32),
+                            0.5, stream_only=True)
+        torch.cuda.synchronize()
+        print("profile case IF2", float(r["loglik"][0]))
+        return
 
     if args.config == "sim":
         # k_simulate: LG 2-D, one parameter set x 65536 replicates x T = 200
@@ -818,7 +859,7 @@ def run_profile_case(args):
     st = m.to_struct()
     st.ys = st.ys[:12]
     th = np.repeat(m.theta.to_array(m.canonical_param_names), 24, axis=0).astype(np.float32)
-    out = F.run_pfilter(st, th, np.arange(24, dtype=np.uint64), J, path=args.path)
+    out = F.run_pfilter(st, th, np.arange(24, dtype=np.uint64), J, path=args.path, fast=args.fast)
     torch.cuda.synchronize()
     print("profile case logLik", out["loglik"][:2])
 
@@ -844,7 +885,7 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="stream-path tile (0 = automatic)")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch the step loop directly instead of replaying it as a CUDA graph")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "sim", "pmcmc"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "sim", "pmcmc", "plain", "if2"],
                     help="c2 (default) is the headline line; c1/c3/c4 print their own lines")
     args = ap.parse_args()
     if args.config != "c2" and args.impl == "ours" and not args.profile_case:

@@ -103,9 +103,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
 // the others poll the generation.  Every poll loop is bounded: a CTA that
 // gives up sets error bit 1 (PPF_ETIMEOUT) and the abort word, so the other
 // CTAs stop at their next barrier instead of waiting in turn, and the kernel
-// ends.  The writes of every thread of every CTA before the barrier are
-// visible to every thread after it (CTA barrier, then a GPU-scope fence by the
-// arriving thread; acquire by the waiting thread, then a CTA barrier).
+// ends.  Ordering: the CTA barrier orders every thread's writes before thread
+// 0's acquire-release add of its arrival; the last arrival's add acquires
+// all earlier ones and its release of the new generation is acquired by the
+// waiting threads, and a CTA barrier then orders every thread's reads after
+// it -- no sequentially consistent fence is needed.
 struct GridBar {
   unsigned int* count;
   unsigned int* gen;
@@ -120,8 +122,23 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_u32(unsigned int* p, unsigned int v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// acquire + release: the last CTA to arrive also acquires the earlier
+// arrivals' writes (their release-adds form one release sequence on `count`).
+__device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int* p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
 }
 
 // Returns false when the barrier gave up (this CTA's or another's wait).
@@ -130,24 +147,21 @@ __device__ __forceinline__ bool grid_sync(const GridBar& g) {
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned int gen = ld_acquire_u32(g.gen);
-    __threadfence();
-    if (atomicAdd(g.count, 1u) == g.n - 1) {
-      atomicExch(g.count, 0u);
-      __threadfence();
+    const unsigned int gen = ld_relaxed_u32(g.gen);   // cannot advance before this CTA arrives
+    if (atom_add_acq_rel_u32(g.count, 1u) == g.n - 1) {
+      st_relaxed_u32(g.count, 0u);
       st_release_u32(g.gen, gen + 1);
     } else {
       long long i = 0;
       while (ld_acquire_u32(g.gen) == gen) {
-        if (++i > g.cap || ld_acquire_u32(g.abort) != 0u) { ok = 0; break; }
-        __nanosleep(32);
+        if (++i > g.cap || ld_relaxed_u32(g.abort) != 0u) { ok = 0; break; }
+        __nanosleep(20);
       }
     }
     if (!ok) {
       atomicOr(g.err, 1u);
       atomicExch(g.abort, 1u);
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();
