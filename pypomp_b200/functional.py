@@ -473,6 +473,15 @@ class MopCall:
         seeds_d.copy_(torch.from_numpy(np.asarray(seeds_f, dtype=np.uint64).view(np.int64).reshape(-1).copy()))
         self.forward_done = False
 
+    def launch(self, grad: bool, err_acc) -> None:
+        """``ppf_mop`` queued on the stream without waiting; the workspace's
+        status word is OR-ed into the device flag ``err_acc`` (int32)."""
+        d = self.d
+        d.grad = _ffi.ptr(self.out["grad"]) if grad else 0
+        _ffi.check(_ffi.LIB.ppf_mop(d, self._stream()), "ppf_mop")
+        err_acc.bitwise_or_(self.ws[:4].view(self.torch.int32))
+        self.forward_done = True
+
     def forward(self, grad: bool = False) -> dict:
         d = self.d
         d.grad = _ffi.ptr(self.out["grad"]) if grad else 0
@@ -555,7 +564,7 @@ def _warn_nonfinite(grad, m: int) -> None:
 
 
 def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alpha: float, keys,
-          alpha_cooling: float = 1.0, thresh: float = 0.0, n_monitors: int = 1):
+          alpha_cooling: float = 1.0, thresh: float = 0.0, n_monitors: int = 1, *, device_loop: bool = True):
     """MOP-alpha gradient training (``pypomp/functional/train.py:14-110`` /
     ``_train_internal``, ``train.py:38-180``).
 
@@ -575,6 +584,10 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
     differences of its gradient under the iteration's Hessian key (common
     random numbers), all 2P perturbed gradients of all parameter sets in one
     batched launch (:func:`mop_hessian_fd`).
+
+    SGD and Adam without line search and with at most one monitor run the
+    loop on the device side (:func:`_train_device`); ``device_loop=False``
+    keeps the host loop (same results).
     """
     from . import random as pprandom
     from .optim import LearningRate, cosine_alpha
@@ -585,6 +598,8 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
         raise ValueError("Line search requires at least one monitor")
     if not isinstance(optimizer, (SGD, Adam, FullMatrixAdam, Newton, WeightedNewton, BFGS)):
         raise ValueError(f"Optimizer '{optimizer.__class__.__name__}' not supported")
+    if device_loop and type(optimizer) in (SGD, Adam) and not optimizer.ls and n_monitors <= 1 and M > 0:
+        return _train_device(struct, thetas_array, J, optimizer, M, eta, alpha, keys, alpha_cooling, n_monitors)
     th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float64)).copy()
     n, P = th.shape
     keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
@@ -644,6 +659,79 @@ def train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alph
             th = th + eta_arr[m] * direction
         traces[:, m + 1] = th
     return nll, traces
+
+
+def _train_device(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alpha: float, keys,
+                  alpha_cooling: float, n_monitors: int):
+    """:func:`train` for SGD / Adam without line search and with at most one
+    monitor, with the loop on the device side: the parameters, optimiser
+    state, learning rates, keys and traces stay in device memory, each
+    iteration's MOP value + gradient (one ``ppf_mop`` call, its launch
+    sequence replayed from a CUDA graph when alpha is constant), clipping and
+    update are queued on the stream, and the host synchronises once at the
+    end.  The keys come from the same splits as the host loop and every update
+    is the same float64 arithmetic, so the results are the host loop's."""
+    from . import random as pprandom
+    from .optim import LearningRate, cosine_alpha
+
+    torch = _ffi.require_cuda()
+    th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float64)).copy()
+    n, P = th.shape
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    if keys.shape[0] != n:
+        raise ValueError("keys must have one key per parameter set")
+    names = list(struct.spec.param_names)
+    eta_arr = eta.to_array(names, M) if isinstance(eta, LearningRate) else np.broadcast_to(
+        np.asarray(eta, dtype=np.float64), (max(M, 1), P))
+    T = np.asarray(struct.ys).shape[-2]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    # the key chain of the host loop: per iteration one split for the MOP key,
+    # one for the (unused) Hessian key
+    chain = [int(k) for k in keys]
+    subs = np.zeros((M, n), np.uint64)
+    for m in range(M):
+        for i in range(n):
+            chain[i], subs[m, i] = (int(v) for v in pprandom.split(chain[i]))
+            chain[i], _ = (int(v) for v in pprandom.split(chain[i]))
+    alphas = [1.0 - (1.0 - alpha) * cosine_alpha(m, M, alpha_cooling) for m in range(M)]
+    reuse = len(set(alphas)) == 1
+    th_d = torch.tensor(th, dtype=torch.float64, device=dev)
+    subs_d = torch.from_numpy(subs.view(np.int64)).to(dev)
+    eta_d = torch.tensor(np.ascontiguousarray(eta_arr[:M]), dtype=torch.float64, device=dev)
+    nll_d = torch.full((n, M + 1), float("nan"), dtype=torch.float64, device=dev)
+    tr_d = torch.zeros(n, M + 1, P, dtype=torch.float64, device=dev)
+    tr_d[:, 0] = th_d
+    bad = torch.zeros(1, dtype=torch.int64, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    call = MopCall(struct, th.astype(np.float32), subs[0], J, alphas[0], graph=reuse)
+    th32_d, seeds_d = call.keep[0], call.keep[4]
+    state = optimizer.init_state_device(th_d) if hasattr(optimizer, "init_state_device") else ()
+    for m in range(M):
+        th32_d.copy_(th_d)
+        seeds_d.copy_(subs_d[m])
+        call.d.alpha = float(alphas[m])
+        call.launch(True, err)
+        grad = call.out["grad"] / T
+        if n_monitors == 1:
+            nll_d[:, m + 1] = call.out["value"]
+        bad += (~torch.isfinite(grad)).sum()
+        if optimizer.clip_norm is not None:
+            grad = grad.clamp(-optimizer.clip_norm, optimizer.clip_norm)
+        direction, state = optimizer.step_device(grad, state, m)
+        if optimizer.scale:
+            direction = direction / (direction * direction).sum(dim=-1, keepdim=True).sqrt()
+        th_d = th_d + eta_d[m] * direction
+        tr_d[:, m + 1] = th_d
+    e = int(err.item())
+    if e:
+        _ffi.check(_ffi.PPF_ETIMEOUT if e & 1 else _ffi.PPF_EINTERNAL, "ppf_mop")
+    nbad = int(bad.item())
+    if nbad:
+        import warnings
+
+        warnings.warn(f"train: {nbad} non-finite MOP gradient entries over {M} iterations; the updates "
+                      "propagate them, as the reference does", RuntimeWarning, stacklevel=3)
+    return nll_d.cpu().numpy(), tr_d.cpu().numpy()
 
 
 def mop_hessian_fd(struct: PompStruct, theta_est, keys, J: int, alpha: float, h: float = 1e-2):
@@ -806,7 +894,7 @@ class PerfilterCall:
     persistent buffers alone save 5-8 % against separate calls."""
 
     def __init__(self, struct: PompStruct, swarm, J: int, rw_sig, rw_sig0, *, thresh: float = 0.0,
-                 graph: bool = False):
+                 graph: bool = False, unit_f=None):
         torch = _ffi.require_cuda()
         self.torch = torch
         dev = torch.device("cuda", torch.cuda.current_device())
@@ -824,8 +912,9 @@ class PerfilterCall:
         self.cool = torch.zeros(U, T, **f32d)
         self.cool0 = torch.zeros(U, **f32d)
         self.ll = torch.zeros(F, dtype=torch.float64, device=dev)
+        unit_d = None if unit_f is None else torch.from_numpy(np.asarray(unit_f, dtype=np.int32)).to(dev)
         self.keep = [ys_d, ycon_d, Tu_d, torch.tensor(np.asarray(rw_sig, np.float32), **f32d),
-                     torch.tensor(np.asarray(rw_sig0, np.float32), **f32d)]
+                     torch.tensor(np.asarray(rw_sig0, np.float32), **f32d), unit_d]
         self.descs = []
         self.ws = None
         for i in (0, 1):
@@ -838,6 +927,7 @@ class PerfilterCall:
             d.rw_sig, d.rw_sig0 = _ffi.ptr(self.keep[3]), _ffi.ptr(self.keep[4])
             d.cool, d.cool0 = _ffi.ptr(self.cool), _ffi.ptr(self.cool0)
             d.ys, d.ycon, d.T_u = _ffi.ptr(ys_d), _ffi.ptr(ycon_d), _ffi.ptr(Tu_d)
+            d.unit = _ffi.ptr(unit_d)
             d.seeds, d.loglik = _ffi.ptr(self.seeds), _ffi.ptr(self.ll)
             if self.ws is None:
                 self.ws = torch.empty(max(int(_ffi.LIB.ppf_perfilter_workspace_bytes(d)), 256),
@@ -851,6 +941,19 @@ class PerfilterCall:
     def swarm(self):
         """The current swarm (F, P, J), estimation scale."""
         return self.swarms[self.cur]
+
+    def run_device(self, seeds_d, cool_d, err_acc) -> None:
+        """One iteration from device-resident keys (F,) int64 and cooling
+        factors (U, T): the copies and the launch are queued on the stream and
+        the host does not wait; the workspace's status word is OR-ed into the
+        device flag ``err_acc`` (int32) for one check after the loop."""
+        self.seeds.copy_(seeds_d)
+        self.cool.copy_(cool_d)
+        self.cool0.copy_(cool_d[:, 0])
+        d = self.descs[self.cur]
+        _ffi.check(_ffi.LIB.ppf_perfilter(d, self.stream), "ppf_perfilter")
+        err_acc.bitwise_or_(self.ws[:4].view(self.torch.int32))
+        self.cur ^= 1
 
     def __call__(self, seeds_f, cool, cool0) -> np.ndarray:
         torch = self.torch
@@ -867,7 +970,7 @@ class PerfilterCall:
 
 
 def mif(struct: PompStruct, thetas_array, rw_sd, M: int, J: int, keys, thresh: float = 0.0,
-        n_monitors: int = 0, *, inject=None):
+        n_monitors: int = 0, *, inject=None, device_loop: bool = True):
     """Iterated filtering 2 (``pypomp/functional/mif.py:15-122``,
     ``_mif_internal`` / ``_mif_scan_body`` at ``pypomp/core/algorithms/mif.py:16-85``).
 
@@ -886,6 +989,9 @@ def mif(struct: PompStruct, thetas_array, rw_sd, M: int, J: int, keys, thresh: f
     leading replicate axis) and ``"monitors"`` (a list of ``z0``/``z``/``u``
     dicts, leading replicate axis).  Returns ``(logliks (n_reps, M), traces
     (n_reps, M+1, P), final swarm (n_reps, J, P))``, natural scale.
+    Without monitors or injected draws the loop runs on the device side
+    (:func:`_mif_device`); ``device_loop=False`` keeps the host loop (same
+    results).
     """
     from . import random as pprandom
 
@@ -909,6 +1015,8 @@ def mif(struct: PompStruct, thetas_array, rw_sd, M: int, J: int, keys, thresh: f
     m_keys = np.stack([pprandom.split(k, M + 1)[1:] for k in keys]) if M > 0 else np.zeros((n, 0), np.uint64)
     means = [swarm.mean(dim=2)]
     logliks = np.zeros((n, M))
+    if device_loop and inject is None and n_monitors < 1 and M > 0:
+        return _mif_device(struct, swarm, rw_sd, rw_sig, rw_sig0, M, J, m_keys, T, thresh)
     # without injected draws the iterations share one set of device buffers
     call = PerfilterCall(struct, swarm, J, rw_sig, rw_sig0, thresh=thresh) if inject is None and M > 0 else None
     for it in range(M):
@@ -939,6 +1047,51 @@ def mif(struct: PompStruct, thetas_array, rw_sd, M: int, J: int, keys, thresh: f
     traces = torch.stack(means, dim=1).cpu().numpy()                       # (n, M+1, P) est
     traces = spec.from_est(traces.reshape(-1, len(names))).reshape(traces.shape)
     final = swarm.cpu().numpy().transpose(0, 2, 1)
+    final = spec.from_est(final.reshape(-1, len(names))).reshape(final.shape)
+    return logliks, traces, final
+
+
+def _cooling_table(rw_sd, M: int, T_u, width: int | None = None) -> np.ndarray:
+    """(M, U, width) cooling factors of every iteration, unit and step (zero
+    past a unit's length; width defaults to max T_u)."""
+    T_u = np.atleast_1d(np.asarray(T_u, dtype=np.int64))
+    out = np.zeros((M, T_u.size, int(width or T_u.max())), np.float32)
+    for m in range(M):
+        for u, Tu in enumerate(T_u):
+            out[m, u, :Tu] = [rw_sd.cooling_factor(i, m, int(Tu)) for i in range(int(Tu))]
+    return out
+
+
+def _mif_device(struct, swarm, rw_sd, rw_sig, rw_sig0, M, J, m_keys, T, thresh):
+    """The IF2 iterations of :func:`mif` (no monitors, no injected draws) with
+    the loop on the device side: the cooling factors of all M iterations and
+    all iteration keys are uploaded once, every iteration's launch, swarm
+    means and log-likelihoods are queued on the stream without a host wait,
+    and one synchronisation at the end reads the traces and the status.
+    Same kernels and inputs as the host loop, so the same results bit for bit."""
+    torch = _ffi.require_cuda()
+    spec = struct.spec
+    names = list(spec.param_names)
+    dev = swarm.device
+    n = swarm.shape[0]
+    call = PerfilterCall(struct, swarm, J, rw_sig, rw_sig0, thresh=thresh)
+    cool_d = torch.from_numpy(_cooling_table(rw_sd, M, [T])).to(dev)                 # (M, 1, T)
+    keys_d = torch.from_numpy(np.ascontiguousarray(m_keys.T).view(np.int64)).to(dev)  # (M, n)
+    ll_d = torch.zeros(M, n, dtype=torch.float64, device=dev)
+    means_d = torch.zeros(M + 1, n, spec.n_params, dtype=torch.float32, device=dev)
+    means_d[0] = swarm.mean(dim=2)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    for it in range(M):
+        call.run_device(keys_d[it], cool_d[it], err)
+        ll_d[it].copy_(call.ll)
+        means_d[it + 1] = call.swarm.mean(dim=2)
+    e = int(err.item())
+    if e:
+        _ffi.check(_ffi.PPF_ETIMEOUT if e & 1 else _ffi.PPF_EINTERNAL, "ppf_perfilter")
+    logliks = ll_d.T.cpu().numpy()
+    traces = means_d.transpose(0, 1).cpu().numpy()
+    traces = spec.from_est(traces.reshape(-1, len(names))).reshape(traces.shape)
+    final = call.swarm.cpu().numpy().transpose(0, 2, 1)
     final = spec.from_est(final.reshape(-1, len(names))).reshape(final.shape)
     return logliks, traces, final
 
@@ -1341,46 +1494,60 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
         out = spec.from_est(panel[..., perm])[..., inv]
         return out[:, 0, :ns], out[:, :, ns:]
 
-    shared_tr = np.full((n, M + 1, ns + 1), np.nan)
-    unit_tr = np.full((n, M + 1, U, nu + 1), np.nan)
-    s0, u0 = nat(S.mean(dim=2).cpu().numpy().astype(np.float64), Us.mean(dim=3).cpu().numpy().astype(np.float64))
-    shared_tr[:, 0, 1:], unit_tr[:, 0, :, 1:] = s0, u0
+    # device-side loop: the keys and cooling factors of all iterations are
+    # uploaded once, the swarms stay in one PerfilterCall's buffers, and
+    # without monitors nothing waits for the host until the end
+    unit_keys_all = np.stack([np.stack([pprandom.split(k, U) for k in m_keys[:, it]]) for it in range(M)])
+    keys_d = torch.from_numpy(np.ascontiguousarray(unit_keys_all.reshape(M, n * U)).view(np.int64)).to(dev)
+    cool_d = torch.from_numpy(_cooling_table(rw_sd, M, T_u, Tmax)).to(dev)               # (M, U, Tmax)
+    panel = torch.cat([S[:, None].expand(n, U, ns, J), Us], dim=2)
+    call = PerfilterCall(all_units, panel.reshape(n * U, ns + nu, J).index_select(1, perm_t), J, sig_u, sig0_u,
+                         thresh=thresh, unit_f=unit_f)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    ll_d = torch.zeros(M, n, U, dtype=torch.float64, device=dev)
+    smeans = torch.zeros(M + 1, n, ns, dtype=torch.float64, device=dev)
+    umeans = torch.zeros(M + 1, n, U, nu, dtype=torch.float64, device=dev)
+    smeans[0], umeans[0] = S.mean(dim=2).double(), Us.mean(dim=3).double()
     for it in range(M):
-        unit_keys = np.stack([pprandom.split(k, U) for k in m_keys[:, it]])       # (n, U)
-        cool = np.zeros((U, Tmax), np.float32)
-        for u in range(U):
-            cool[u, :T_u[u]] = [rw_sd.cooling_factor(i, it, int(T_u[u])) for i in range(int(T_u[u]))]
-        panel = torch.cat([S[:, None].expand(n, U, ns, J), Us], dim=2)           # (n, U, Pp, J)
-        swarm = panel.reshape(n * U, ns + nu, J).index_select(1, perm_t).contiguous()
-        res = run_perfilter(all_units, swarm, unit_keys.reshape(-1), J, sig_u, sig0_u, cool, cool[:, 0],
-                            thresh=thresh, unit_f=unit_f)
+        if it > 0:
+            panel = torch.cat([S[:, None].expand(n, U, ns, J), Us], dim=2)
+            call.swarm.copy_(panel.reshape(n * U, ns + nu, J).index_select(1, perm_t))
         if n_monitors >= 1:
-            mean = swarm.mean(dim=2).cpu().numpy()                                # (n U, P) unit order
-            mon = np.stack([pprandom.split(k, n_monitors) for k in unit_keys.reshape(-1)])
+            mean = call.swarm.mean(dim=2).cpu().numpy()                              # (n U, P) unit order
+            mon = np.stack([pprandom.split(k, n_monitors) for k in unit_keys_all[it].reshape(-1)])
             pf = run_pfilter(all_units, np.repeat(mean, n_monitors, axis=0), mon.reshape(-1), J,
                              thresh=thresh, est=True, unit_f=np.repeat(unit_f, n_monitors))
-            ll_units = pf["loglik"].reshape(n, U, n_monitors).mean(axis=2)
-        else:
-            ll_units = res["loglik"].cpu().numpy().reshape(n, U)
-        out = res["swarm"].index_select(1, inv_t).reshape(n, U, ns + nu, J)      # panel order
+            ll_d[it] = torch.from_numpy(pf["loglik"].reshape(n, U, n_monitors).mean(axis=2)).to(dev)
+        call.run_device(keys_d[it], cool_d[it], err)
+        if n_monitors < 1:
+            ll_d[it] = call.ll.view(n, U)
+        out = call.swarm.index_select(1, inv_t).reshape(n, U, ns + nu, J)            # panel order
         if nu > 0:
             Us = out[:, :, ns:].contiguous()
         if ns > 0:
-            su = out[:, :, :ns].double()                                          # (n, U, ns, J)
+            su = out[:, :, :ns].double()                                              # (n, U, ns, J)
             mu = su.mean(dim=3)
             var = su.var(dim=3, unbiased=False)
             w = torch.where(var > 0, 1.0 / var.clamp_min(1e-300), torch.zeros_like(var))
             wsum = w.sum(dim=1)
             centre = torch.where(wsum > 0, (w * mu).sum(dim=1) / wsum.clamp_min(1e-300), mu.mean(dim=1))
-            dev_j = su - mu[..., None]                                            # deviations from unit means
+            dev_j = su - mu[..., None]                                                # deviations from unit means
             pick = dev_j.gather(1, jmod.view(1, 1, 1, J).expand(n, 1, ns, J)).squeeze(1)   # (n, ns, J)
             S = (centre[..., None] + pick).float().contiguous()
-        s_mean, u_mean = nat(S.mean(dim=2).cpu().numpy().astype(np.float64),
-                             Us.mean(dim=3).cpu().numpy().astype(np.float64))
-        shared_tr[:, it + 1, 0] = ll_units.sum(axis=1)
-        shared_tr[:, it + 1, 1:] = s_mean
-        unit_tr[:, it + 1, :, 0] = ll_units
-        unit_tr[:, it + 1, :, 1:] = u_mean
+        smeans[it + 1], umeans[it + 1] = S.mean(dim=2).double(), Us.mean(dim=3).double()
+    e = int(err.item())
+    if e:
+        _ffi.check(_ffi.PPF_ETIMEOUT if e & 1 else _ffi.PPF_EINTERNAL, "ppf_perfilter")
+    shared_tr = np.full((n, M + 1, ns + 1), np.nan)
+    unit_tr = np.full((n, M + 1, U, nu + 1), np.nan)
+    sm, um = smeans.cpu().numpy(), umeans.cpu().numpy()
+    ll_units = ll_d.cpu().numpy()                                                     # (M, n, U)
+    for it in range(M + 1):
+        s_mean, u_mean = nat(sm[it], um[it])
+        shared_tr[:, it, 1:], unit_tr[:, it, :, 1:] = s_mean, u_mean
+        if it > 0:
+            shared_tr[:, it, 0] = ll_units[it - 1].sum(axis=1)
+            unit_tr[:, it, :, 0] = ll_units[it - 1]
     s_fin = S.cpu().numpy().astype(np.float64).transpose(0, 2, 1)                 # (n, J, ns)
     u_fin = Us.cpu().numpy().astype(np.float64).transpose(0, 3, 1, 2)             # (n, J, U, nu)
     panel = np.concatenate([np.repeat(s_fin[:, :, None], U, axis=2), u_fin], axis=3)

@@ -56,6 +56,10 @@ class SGD(Optimizer):
     def step(self, grad, state, step_num, compute_hessian_fn=None, eta_i=None):
         return -np.asarray(grad, dtype=np.float64), ()
 
+    def step_device(self, grad, state, step_num):
+        """``step`` on float64 torch tensors (device-side training loop)."""
+        return -grad, ()
+
 
 @dataclass(frozen=True)
 class Adam(Optimizer):
@@ -75,6 +79,19 @@ class Adam(Optimizer):
         m_hat = m_new / (1 - self.beta1 ** (step_num + 1))
         v_hat = v_new / (1 - self.beta2 ** (step_num + 1))
         return -m_hat / (np.sqrt(v_hat) + self.epsilon), (m_new, v_new)
+
+    def init_state_device(self, theta):
+        return (theta.new_zeros(theta.shape), theta.new_zeros(theta.shape))
+
+    def step_device(self, grad, state, step_num):
+        """``step`` on float64 torch tensors, operation for operation (the
+        same IEEE float64 results as the NumPy form)."""
+        m, v = state
+        m_new = self.beta1 * m + (1 - self.beta1) * grad
+        v_new = self.beta2 * v + (1 - self.beta2) * (grad * grad)
+        m_hat = m_new / (1 - self.beta1 ** (step_num + 1))
+        v_hat = v_new / (1 - self.beta2 ** (step_num + 1))
+        return -m_hat / (v_hat.sqrt() + self.epsilon), (m_new, v_new)
 
 
 def _rows(a):

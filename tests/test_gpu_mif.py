@@ -236,3 +236,23 @@ def test_mif_graph_replay_equals_per_iteration_calls(J):
         cool = np.array([rw.cooling_factor(i, it, 30) for i in range(30)], dtype=np.float32)
         assert np.array_equal(call(m_keys[:, it], cool, cool[0]), ll[:, it])
     assert np.array_equal(call.swarm.cpu().numpy(), swarm.cpu().numpy())
+
+
+def test_mif_device_loop_equals_host_loop():
+    """The device-side IF2 loop (cooling factors and keys uploaded once, no
+    host wait per iteration) gives the host loop's traces, log-likelihoods and
+    final swarm bit for bit."""
+    import pypomp_b200 as pp
+    from pypomp_b200 import functional as F
+    from pypomp_b200.optim import RWSigma
+
+    m = pp.Ricker(T=60, key=5)
+    st = m.to_struct()
+    th = np.repeat(m.theta.to_array(m.canonical_param_names)[:, None, :], 3000, axis=1)
+    th = np.repeat(th, 2, axis=0)
+    rw = RWSigma({n: 0.03 for n in m.canonical_param_names}).geometric_cooling(0.5)
+    keys = np.array([4, 5], np.uint64)
+    a = F.mif(st, th, rw, 4, 3000, keys, device_loop=True)
+    b = F.mif(st, th, rw, 4, 3000, keys, device_loop=False)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)

@@ -172,3 +172,25 @@ def test_train_reused_mop_call_equals_fresh_calls():
             chain[i] = int(pprandom.split(chain[i])[0])
         th = th + rate * (-res["grad"] / 40)
         assert np.array_equal(th, tr[:, step + 1])
+
+
+@pytest.mark.parametrize("opt_name,alpha_cooling", [("Adam", 1.0), ("SGD", 0.5)])
+def test_train_device_loop_equals_host_loop(opt_name, alpha_cooling):
+    """The device-side training loop (parameters, optimiser state and traces in
+    device memory, one synchronisation at the end) gives the host loop's
+    negative log-likelihoods and parameter traces bit for bit, with a
+    constant alpha (graph replay) and with cosine-cooled alpha."""
+    import pypomp_b200 as pp
+    from pypomp_b200 import functional as F
+    from pypomp_b200 import optim
+
+    m = pp.SV(T=80, key=3)
+    st = m.to_struct()
+    est = np.repeat(m.spec.to_est(m.theta.to_array(m.canonical_param_names)), 2, axis=0)
+    opt = optim.Adam(clip_norm=5.0) if opt_name == "Adam" else optim.SGD()
+    eta = optim.LearningRate({n: 0.01 for n in m.canonical_param_names})
+    keys = np.array([8, 9], np.uint64)
+    a = F.train(st, est, 4096, opt, 5, eta, 0.97, keys, alpha_cooling=alpha_cooling, device_loop=True)
+    b = F.train(st, est, 4096, opt, 5, eta, 0.97, keys, alpha_cooling=alpha_cooling, device_loop=False)
+    assert np.array_equal(a[0], b[0], equal_nan=True)
+    assert np.array_equal(a[1], b[1])
