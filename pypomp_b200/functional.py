@@ -703,6 +703,7 @@ def _train_device(struct: PompStruct, thetas_array, J: int, optimizer, M: int, e
     tr_d[:, 0] = th_d
     bad = torch.zeros(1, dtype=torch.int64, device=dev)
     err = torch.zeros(1, dtype=torch.int32, device=dev)
+    T_d = torch.tensor(float(T), dtype=torch.float64, device=dev)
     call = MopCall(struct, th.astype(np.float32), subs[0], J, alphas[0], graph=reuse)
     th32_d, seeds_d = call.keep[0], call.keep[4]
     state = optimizer.init_state_device(th_d) if hasattr(optimizer, "init_state_device") else ()
@@ -711,7 +712,7 @@ def _train_device(struct: PompStruct, thetas_array, J: int, optimizer, M: int, e
         seeds_d.copy_(subs_d[m])
         call.d.alpha = float(alphas[m])
         call.launch(True, err)
-        grad = call.out["grad"] / T
+        grad = call.out["grad"] / T_d     # a device divisor: true division, as on the host
         if n_monitors == 1:
             nll_d[:, m + 1] = call.out["value"]
         bad += (~torch.isfinite(grad)).sum()

@@ -89,8 +89,10 @@ class Adam(Optimizer):
         m, v = state
         m_new = self.beta1 * m + (1 - self.beta1) * grad
         v_new = self.beta2 * v + (1 - self.beta2) * (grad * grad)
-        m_hat = m_new / (1 - self.beta1 ** (step_num + 1))
-        v_hat = v_new / (1 - self.beta2 ** (step_num + 1))
+        # divisors as device tensors: torch turns division by a host scalar
+        # into multiplication by its reciprocal, which can differ in the last bit
+        m_hat = m_new / grad.new_full((), 1 - self.beta1 ** (step_num + 1))
+        v_hat = v_new / grad.new_full((), 1 - self.beta2 ** (step_num + 1))
         return -m_hat / (v_hat.sqrt() + self.epsilon), (m_new, v_new)
 
 
