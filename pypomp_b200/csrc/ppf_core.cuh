@@ -168,6 +168,34 @@ __device__ __forceinline__ bool grid_sync(const GridBar& g) {
   return s_ok != 0;
 }
 
+// Counting form: every CTA adds 1 to `count` (release) per barrier and waits
+// (acquire) until it reaches epoch * n for its own barrier number `epoch`
+// (1, 2, ...; the count starts at 0 and only grows).  No CTA resets or
+// advances anything, so a barrier costs one fire-and-forget add and the
+// polls: one round trip less than the arrival-then-generation form.  The same
+// bounded wait, error and abort words as grid_sync.
+__device__ __forceinline__ bool grid_sync_count(const GridBar& g, unsigned int epoch) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.count) : "memory");
+    const unsigned int target = epoch * g.n;
+    long long i = 0;
+    while ((int)(ld_acquire_u32(g.count) - target) < 0) {
+      if (++i > g.cap || ld_relaxed_u32(g.abort) != 0u) { ok = 0; break; }
+      __nanosleep(20);
+    }
+    if (!ok) {
+      atomicOr(g.err, 1u);
+      atomicExch(g.abort, 1u);
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 // The fixed-point weight q = rint(exp(w - M) * 2^40) (collapsed filters: 1),
 // in two halves: the float e = qweight_e(w, M, collapsed) and
 // q = qweight_from_e(e).  On a resampling step the streaming path's k_sum

@@ -45,6 +45,8 @@ struct Args {
   uint32_t* err;
   unsigned int* counter;  // [2]
   unsigned int* gbar;     // [3] grid barrier: arrivals, generation, abort (zeroed per call)
+  uint64_t* slotw;        // [7][kMaxGridSlots] per-CTA step words of the grid-resident MOP
+                          // forward and per-filter arrival counters (zeroed by its launch)
   Acc* acc[2];            // [F] each
   uint64_t* desc[2];      // [F][ntiles] each
   uint64_t* excl;         // [F][ntiles]
@@ -123,6 +125,8 @@ constexpr int kTileLarge = 2048;   // 256 threads x 8
 constexpr int kTileMid = 512;      // 128 threads x 4
 constexpr int kTileSmall = 256;    // 64 threads x 4
 constexpr int kNumSMs = 148;
+// CTAs of a grid-resident launch that publish per-step words (8 per SM)
+constexpr int kMaxGridSlots = 8 * kNumSMs;
 
 int run_mop(Args& a, const MopWork& w, cudaStream_t s);
 int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s);

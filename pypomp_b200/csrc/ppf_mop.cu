@@ -298,6 +298,327 @@ __global__ void __launch_bounds__(TPB) k_mop_fwd_persist(Args a, GridBar gb) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Grid-resident MOP forward: one cooperative launch for the whole time loop,
+// C CTAs per filter, CTA c owning particles [c JC, (c+1) JC) (the structure
+// of the cluster kernel, ppf_cluster.cu, at grid scope).  CTAs of one filter
+// exchange their per-step numbers through tagged words in global memory
+// instead of grid barriers: each CTA publishes one word per quantity and step
+// (tag = step + 1 in the top 12 bits), and a reader's bounded poll of the C
+// words of its filter is both the exchange and the wait.  Per observation t:
+//   A. read the max / min / NaN words of the weights produced for t (the
+//      release that published them also publishes those children's states and
+//      weights), load the CTA's slice of parents from global memory into shared
+//      memory (at t = 0 the initial states are already there), form their
+//      fixed-point weights, block-scan them and publish the slice total;
+//   B. read the C slice totals: this slice's exclusive prefix and the filter
+//      total; first-child offsets of the slice's parents; one child per thread
+//      at a time: rproc + dmeas, the child's state and weight written to global
+//      memory, its ancestor, the first-child offsets and checkpoints kept for
+//      the adjoint; then publish the max / min / NaN of the weights produced.
+// Arithmetic, Philox counters and the order of the float64 log-likelihood sum
+// are the streaming kernels', so results are bit-identical to them.  Words
+// are double-buffered by step parity: a CTA can be at most one phase ahead of
+// any other CTA of its filter, so a word is never overwritten before every
+// reader has seen it (the argument is spelled out at the poll sites).
+// ---------------------------------------------------------------------------
+
+constexpr int kGridTagShift = 52;
+constexpr int kGridMaxC = 256;          // CTAs per filter (8 words per polling lane)
+
+__device__ __forceinline__ uint64_t grid_word(int tag, uint64_t v) {
+  return ((uint64_t)((unsigned)tag & 0xfffu) << kGridTagShift) | v;
+}
+
+// Warp 0: wait until the filter's arrival counter `cnt` reaches `target`
+// (every CTA of the filter adds 1 with release semantics after writing its
+// word for the step), then read the C words w[0..C) once and combine them with
+// fn(r, value) (lane-strided, r the CTA rank).  One lane polls the counter
+// (acquire), so the polling traffic is one word per CTA rather than C; the
+// warp barrier then orders the other lanes' reads after that acquire.  The
+// wait is bounded: the lane gives up after spin_cap polls or when another CTA
+// aborted, and sets the error and abort words.  A word without the expected
+// tag means the exchange protocol was violated (error bit 4).  Returns false
+// (to all of warp 0) on either failure.
+template <class Fn>
+__device__ __forceinline__ bool grid_exchange(const uint64_t* w, unsigned int* cnt, unsigned int target,
+                                              int C, int tag, const Args& a, Fn fn) {
+  const int lane = threadIdx.x & 31;
+  unsigned int* abortw = a.gbar + 2;
+  int ok = 1;
+  if (lane == 0) {
+    long long spins = 0;
+    while (ld_acquire_u32(cnt) < target) {
+      if (++spins > a.spin_cap || ld_relaxed_u32(abortw) != 0u) {
+        ok = 0;
+        atomicOr(a.err, 1u);
+        atomicExch(abortw, 1u);
+        break;
+      }
+      __nanosleep(20);
+    }
+  }
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  if (!ok) return false;
+  const uint64_t want = (uint64_t)((unsigned)tag & 0xfffu);
+  const uint64_t vm = (1ull << kGridTagShift) - 1;
+  bool good = true;
+  for (int r = lane; r < C; r += 32) {
+    const uint64_t v = ld_relaxed_u64(w + r);
+    good &= (v >> kGridTagShift) == want;
+    fn(r, v & vm);
+  }
+  if (!__all_sync(0xffffffffu, good)) {
+    if (lane == 0) {
+      atomicOr(a.err, 4u);
+      atomicExch(abortw, 1u);
+    }
+    return false;
+  }
+  return true;
+}
+
+// Arrival: after the CTA barrier that orders every thread's writes, thread 0
+// adds 1 to the counter with release semantics.
+__device__ __forceinline__ void grid_arrive(unsigned int* cnt) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+}
+
+template <class M, int TPB, bool INJ>
+__global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) {
+  constexpr int DX = M::MAXDX;
+  constexpr int NW = TPB / 32;
+  extern __shared__ __align__(16) float smf[];
+  __shared__ typename M::Consts csh;
+  __shared__ uint64_t s_scan[NW + 1];
+  __shared__ unsigned int smk[3 * NW];
+  __shared__ unsigned int s_key[3];      // max key, min key, NaN of the filter's weights
+  __shared__ uint64_t s_sum[2];          // exclusive prefix of this slice, filter total
+  __shared__ int s_ok;
+
+  const int f = blockIdx.x / C, c = blockIdx.x % C;
+  const int u = filter_unit(a, f);
+  const int Tf = filter_len(a, u);
+  const int J = a.J, T = a.T, L = a.ckpt_every;
+  const int base = c * JC;
+  const int nc = max(0, min(JC, J - base));
+  const int G = gridDim.x;
+  uint64_t* maxw[2] = {a.slotw, a.slotw + G};
+  uint64_t* minw[2] = {a.slotw + 2 * G, a.slotw + 3 * G};
+  uint64_t* sumw[2] = {a.slotw + 4 * G, a.slotw + 5 * G};
+  // arrival counters of the filter's key and sum words (monotone over steps)
+  unsigned int* cnt_key = reinterpret_cast<unsigned int*>(a.slotw + 6 * G) + 2 * f;
+  unsigned int* cnt_sum = cnt_key + 1;
+  const int fw = f * C;                  // first word of this filter
+  // with no resampling threshold (MOP: always resample) the min key is not needed
+  const bool need_min = a.logthresh != -INFINITY;
+  float* Xs = smf;                       // [DX][JC] parents of the current step
+  float* Ws = Xs + DX * JC;              // [JC]
+  int* st = reinterpret_cast<int*>(Ws + JC);   // [JC + 4] first-child offsets
+  const int ITC = (JC + TPB - 1) / TPB;  // parents per thread (contiguous)
+  const int l0 = threadIdx.x * ITC;
+  const int l1 = min(l0 + ITC, nc);
+
+  load_consts<M>(a, f, csh);
+  __syncthreads();
+  const typename M::Consts cr = csh;
+
+  // block max / min / NaN of the weights this CTA produced, published for
+  // step `tag - 1` after every thread's stores (release)
+  auto publish_keys = [&](unsigned int mx, unsigned int mn, unsigned int nn, int par, int tag) {
+    mx = warp_max_u32(mx);
+    mn = warp_min_u32(mn);
+    nn = __any_sync(0xffffffffu, nn != 0u) ? 1u : 0u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { smk[warp] = mx; smk[NW + warp] = mn; smk[2 * NW + warp] = nn; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned int A = 0u, B = 0xffffffffu, O = 0u;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) { A = max(A, smk[w]); B = min(B, smk[NW + w]); O |= smk[2 * NW + w]; }
+      if (need_min) st_relaxed_u64(minw[par] + blockIdx.x, grid_word(tag, (uint64_t)B));
+      st_relaxed_u64(maxw[par] + blockIdx.x, grid_word(tag, ((uint64_t)O << 32) | A));
+      grid_arrive(cnt_key);
+    }
+  };
+
+  // ---- initial states into shared memory, propagated into observation 0
+  {
+    Obs<M> ob;
+    ob.load(a, u, 0);
+    float* logw0 = a.logw ? a.logw + (size_t)f * T * J : nullptr;
+    unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
+    for (int l = threadIdx.x; l < nc; l += TPB) {
+      const int k = base + l;
+      float x[DX];
+      float z0[M::NZ0 > 0 ? M::NZ0 : 1];
+      step_noise<M>(a, f, k, 0, M::NZ0, z0);
+      M::rinit(cr, z0, x);
+      if (a.mop_ckpt)
+#pragma unroll
+        for (int d = 0; d < DX; ++d) a.mop_ckpt[((size_t)f * a.nseg * DX + d) * J + k] = x[d];
+      float z[M::NZ > 0 ? M::NZ : 1];
+      step_noise<M>(a, f, k, 1, M::NZ, z);
+      const float w = 0.0f + step1<M>(cr, ob, x, z);
+#pragma unroll
+      for (int d = 0; d < DX; ++d) Xs[d * JC + l] = x[d];
+      Ws[l] = w;
+      accum_maxmin(w, mx, mn, nn);
+      if (logw0) logw0[k] = w;
+    }
+    publish_keys(mx, mn, nn, 0, 1);
+  }
+
+  double ll_acc = 0.0;
+  for (int t = 0; t < Tf; ++t) {
+    const int pc = t & 1, pn = pc ^ 1;
+    const bool last = (t == Tf - 1);
+    Obs<M> ob;
+    if (!last) ob.load(a, u, t + 1);
+
+    // A. The keys of step t's weights: every CTA's key word (tag t+1) was
+    //    written at the end of step t-1 before its arrival, so the key counter
+    //    reaching (t+1) C means all are there (a CTA's arrival for step t+1
+    //    comes after step t's sum exchange, which needs every CTA's step-t
+    //    arrival).  A CTA overwrites its word (tag t+3) only at the end of
+    //    step t+1, after step t+1's sum exchange, which every CTA of the
+    //    filter reaches only after reading this word.
+    if (threadIdx.x < 32) {
+      unsigned int A = 0u, B = 0xffffffffu, O = 0u;
+      bool ok = grid_exchange(maxw[pc] + fw, cnt_key, (unsigned)(t + 1) * (unsigned)C, C, t + 1, a,
+                              [&](int, uint64_t v) {
+                                A = max(A, (unsigned int)v);
+                                O |= (unsigned int)(v >> 32);
+                              });
+      if (ok && need_min)
+        ok = grid_exchange(minw[pc] + fw, cnt_key, (unsigned)(t + 1) * (unsigned)C, C, t + 1, a,
+                           [&](int, uint64_t v) { B = min(B, (unsigned int)v); });
+      A = warp_max_u32(A);
+      B = warp_min_u32(B);
+      O = __any_sync(0xffffffffu, O != 0u) ? 1u : 0u;
+      if (threadIdx.x == 0) { s_key[0] = A; s_key[1] = need_min ? B : A; s_key[2] = O; s_ok = ok ? 1 : 0; }
+    }
+    // the systematic draw of step t does not depend on the exchange
+    const uint32_t u32 = resample_u32(a, f, t);
+    __syncthreads();
+    if (!s_ok) return;
+    Acc acc;
+    memset(&acc, 0, sizeof(acc));
+    acc.maxkey = s_key[0];
+    acc.minkey = s_key[1];   // (= max key when unused: decide_resample then depends on NaN only)
+    acc.nan = s_key[2];
+    const bool nanf = acc.nan != 0;
+    const float Mx = keyf(acc.maxkey);
+    const bool collapsed = !nanf && Mx == -INFINITY;
+    const bool qc = nanf || Mx == -INFINITY;
+    // parents of step t >= 1 were written to global memory by whichever CTAs
+    // drew them; the release / acquire above made them visible
+    if (t > 0) {
+      const float* Xg = a.X[pc] + (size_t)f * DX * J + base;
+      const float* Wg = a.W[pc] + (size_t)f * J + base;
+      for (int l = threadIdx.x; l < nc; l += TPB) {
+#pragma unroll
+        for (int d = 0; d < DX; ++d) Xs[d * JC + l] = Xg[(size_t)d * J + l];
+        Ws[l] = Wg[l];
+      }
+      __syncthreads();
+    }
+    uint64_t qs = 0;
+    for (int l = l0; l < l1; ++l) qs += qweight(Ws[l], Mx, qc);
+    uint64_t btot;
+    const uint64_t tex = block_excl_scan_u64_1b<TPB>(qs, s_scan, btot);
+    // sum words of step t (tag t+1) overwrite those of step t-2: their readers
+    // finished step t-2's sum exchange before their step t-1 key arrival,
+    // which this CTA has waited for
+    if (threadIdx.x == 0) {
+      st_relaxed_u64(sumw[pc] + blockIdx.x, grid_word(t + 1, btot));
+      grid_arrive(cnt_sum);
+    }
+
+    // B. slice prefix and filter total
+    if (threadIdx.x < 32) {
+      uint64_t E = 0, tot = 0;
+      const bool ok = grid_exchange(sumw[pc] + fw, cnt_sum, (unsigned)(t + 1) * (unsigned)C, C, t + 1, a,
+                                    [&](int r, uint64_t v) {
+                                      tot += v;
+                                      E += (r < c) ? v : 0ull;
+                                    });
+      E = warp_sum_u64(E);
+      tot = warp_sum_u64(tot);
+      if (threadIdx.x == 0) { s_sum[0] = E; s_sum[1] = tot; s_ok = ok ? 1 : 0; }
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    const uint64_t E = s_sum[0], tot = s_sum[1];
+    const bool rs = decide_resample(a, acc);
+    float lt32 = 0.0f;
+    if (rs) {
+      const Offsets o = make_offsets(tot, u32, J);
+      if (l0 < nc) {
+        OffWalk wk = offwalk_init(o, E + tex);
+        st[l0] = wk.k;
+        for (int l = l0; l < l1; ++l) {
+          const int kn = offwalk_add(o, wk, qweight(Ws[l], Mx, qc));
+          if (l + 1 < l1 || l + 1 == nc) st[l + 1] = kn;
+        }
+      }
+    } else {
+      if (nanf) lt32 = __int_as_float(0x7fc00000);
+      else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
+      for (int l = l0; l < l1; ++l) st[l] = base + l;
+      if (l0 < nc && l1 == nc) st[nc] = base + nc;
+    }
+    __syncthreads();
+    if (a.mop_off) {
+      int* off = a.mop_off + ((size_t)f * T + t) * (J + 1) + base;
+      for (int l = threadIdx.x; l <= nc; l += TPB)
+        if (l < nc || base + nc == J) off[l] = st[l];
+    }
+    float* ckpt = nullptr;
+    if (a.mop_ckpt && (t + 1) % L == 0 && (t + 1) / L < a.nseg)
+      ckpt = a.mop_ckpt + ((size_t)f * a.nseg + (t + 1) / L) * DX * J;
+    unsigned int mx = 0u, mn = 0xffffffffu, nn = 0u;
+    if (nc > 0) {
+      const int klo = st[0], khi = st[nc];
+      const float nwc = -pp_logf((float)J);
+      int* anc = a.anc ? a.anc + ((size_t)f * T + t) * J : nullptr;
+      float* logw = (a.logw && !last) ? a.logw + ((size_t)f * T + t + 1) * J : nullptr;
+      float* Xn = a.X[pn] + (size_t)f * DX * J;
+      float* Wn = a.W[pn] + (size_t)f * J;
+#pragma unroll 1
+      for (int k = klo + (int)threadIdx.x; k < khi; k += TPB) {
+        const int l = find_parent(st, nc, k);
+        if (anc) anc[k] = base + l;
+        float x[DX];
+#pragma unroll
+        for (int d = 0; d < DX; ++d) x[d] = Xs[d * JC + l];
+        if (ckpt)
+#pragma unroll
+          for (int d = 0; d < DX; ++d) ckpt[(size_t)d * J + k] = x[d];
+        if (last) continue;
+        float z[M::NZ > 0 ? M::NZ : 1];
+        step_noise<M>(a, f, k, t + 2, M::NZ, z);
+        const float wb = rs ? 0.0f : (collapsed ? nwc : Ws[l] - lt32);
+        const float w = wb + step1<M>(cr, ob, x, z);
+        accum_maxmin(w, mx, mn, nn);
+#pragma unroll
+        for (int d = 0; d < DX; ++d) Xn[(size_t)d * J + k] = x[d];
+        Wn[k] = w;
+        if (logw) logw[k] = w;
+      }
+    }
+    // keys of step t+1's weights (tag t+2) overwrite those of step t-1, whose
+    // readers all finished step t-1's key poll before publishing the step t
+    // sums this CTA has read
+    if (!last) publish_keys(mx, mn, nn, pn, t + 2);
+    // the step's log-likelihood term and saved per-step numbers, by a thread
+    // outside warp 0 once the keys are out (off the exchange's critical path)
+    if (c == 0 && threadIdx.x == TPB - 32) finalize_step(a, f, t, acc, tot, &ll_acc);
+    __syncthreads();   // Xs / Ws / st are rewritten by the next step
+  }
+  if (c == 0 && threadIdx.x == TPB - 32) a.loglik[f] = ll_acc;
+}
+
 template <class M, int TPB, bool INJ>
 __global__ void __launch_bounds__(TPB) k_mop_bwd_persist(Args a, MopBwdP mb, GridBar gb) {
   constexpr int DX = M::MAXDX, NG = M::NG, NW = TPB / 32;
@@ -463,6 +784,207 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_persist(Args a, MopBwdP mb, Gri
   }
 }
 
+// The persistent adjoint with a split-phase barrier, for launches where every
+// thread owns one particle j (CTAs x threads >= J).  The iterations are those
+// of k_mop_bwd_persist in the same order (recompute of the last segment, then
+// per segment the backward steps interleaved with the recomputation of the
+// segment before), decoded from one flat index, so every float64 gradient sum
+// is formed in the same order and the results are identical.  Between
+// iterations a CTA arrives at the counting barrier right after its stores,
+// then does the next iteration's work that reads nothing written by other
+// CTAs in the current one -- the forward quantities of its backward step
+// (state, normals, log-density, pi, first-child offsets) and its
+// recomputation's ancestor and normals -- and only then waits.  What remains
+// after the wait is the children's adjoint sums and the parent gather.
+template <class M, int TPB, bool INJ>
+__global__ void __launch_bounds__(TPB) k_mop_bwd_split(Args a, MopBwdP mb, GridBar gb) {
+  constexpr int DX = M::MAXDX, NG = M::NG, NW = TPB / 32;
+  constexpr int NZ = M::NZ > 0 ? M::NZ : 1, NZ0 = M::NZ0 > 0 ? M::NZ0 : 1;
+  __shared__ typename M::Consts c;
+  __shared__ double s_g[NW][NG];
+  __shared__ int s_ok;
+  const int f = blockIdx.x / mb.nbf, cb = blockIdx.x % mb.nbf;
+  const int u = filter_unit(a, f), Tf = filter_len(a, u);
+  const int J = a.J, T = a.T, L = a.ckpt_every, nseg = a.nseg;
+  load_consts<M>(a, f, c);
+  for (int i = threadIdx.x; i < NW * NG; i += TPB) (&s_g[0][0])[i] = 0.0;
+  __syncthreads();
+  const int j = cb * TPB + threadIdx.x;
+  const bool act = j < J;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t sbf = (size_t)f * L * DX * J;
+  const float* ckf = a.mop_ckpt + (size_t)f * nseg * DX * J;
+  constexpr bool GD = NG <= 32;
+  float gs[NG];
+  double gd[GD ? NG : 1];
+#pragma unroll
+  for (int i = 0; i < NG; ++i) gs[i] = 0.0f;
+#pragma unroll
+  for (int i = 0; i < (GD ? NG : 1); ++i) gd[i] = 0.0;
+  auto fold = [&]() {
+    if (GD) {
+#pragma unroll
+      for (int i = 0; i < NG; ++i) {
+        gd[i] += (double)gs[i];
+        gs[i] = 0.0f;
+      }
+    }
+  };
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i < NG; ++i) {
+      const double v = warp_sum_f64(GD ? gd[GD ? i : 0] : (double)gs[i]);
+      if (lane == 0) s_g[warp][i] += v;
+      gs[i] = 0.0f;
+      if (GD) gd[GD ? i : 0] = 0.0;
+    }
+  };
+  auto xin_of = [&](int t, int seg) -> const float* {
+    const int t0 = seg * L;
+    return (t == t0) ? ckf + (size_t)seg * DX * J : mb.sb[seg & 1] + sbf + (size_t)(t - 1 - t0) * DX * J;
+  };
+  // iteration q: backward step ta of segment sa (or -1), recomputation of
+  // step tr of segment sr (or -1), and whether segment sa's sums are flushed
+  const int nb_last = T - (nseg - 1) * L;
+  const int n0 = nb_last > 1 ? nb_last - 1 : 0;
+  const int n_last = max(nb_last, nseg > 1 ? L - 1 : 0);
+  const int Q = n0 + n_last + (nseg - 1) * L;
+  auto sched = [&](int q, int& ta, int& sa, int& tr, int& sr, bool& fl) {
+    ta = -1; tr = -1; sa = 0; sr = 0; fl = false;
+    if (q < n0) { tr = (nseg - 1) * L + q; sr = nseg - 1; return; }
+    int qq = q - n0, seg, i, n;
+    if (qq < n_last) { seg = nseg - 1; i = qq; n = n_last; }
+    else { qq -= n_last; seg = nseg - 2 - qq / L; i = qq % L; n = L; }
+    const int t0 = seg * L, t1 = min(t0 + L, T);
+    const int nb = t1 - t0, nr = seg > 0 ? L - 1 : 0;
+    if (i < nb) { ta = t1 - 1 - i; sa = seg; }
+    if (i < nr) { tr = (seg - 1) * L + i; sr = seg - 1; }
+    fl = (i == n - 1);
+  };
+  // work of iteration q that reads only the forward's saves and this
+  // thread's own earlier writes
+  float px[DX], pz[NZ], pm = 0.0f, ppi = 0.0f, rz[NZ];
+  int plo = 0, phi = 0, rj = 0;
+  typename M::Keep kp;
+  auto prefetch = [&](int q) {
+    int ta, sa, tr, sr;
+    bool fl;
+    sched(q, ta, sa, tr, sr, fl);
+    if (act && ta >= 0 && ta < Tf) {
+      const float* xin = xin_of(ta, sa);
+#pragma unroll
+      for (int d = 0; d < DX; ++d) px[d] = xin[(size_t)d * J + j];
+      own_normals<M, M::NZ, INJ>(a, f, j, ta + 1, pz);
+      Obs<M> ob;
+      ob.load(a, u, ta);
+      pm = M::fwd_keep(c, ob.y, ob.yc, px, pz, kp);
+      const float Mt = a.mop_M[(size_t)f * T + ta];
+      const double S1 = a.mop_S[(size_t)f * T + ta];
+      ppi = 0.0f;
+      if (S1 > 0.0 && pm == pm) ppi = (float)((double)pp_expf(pm - Mt) / S1);
+      const int* off = a.mop_off + ((size_t)f * T + ta) * (J + 1);
+      plo = off[j];
+      phi = off[j + 1];
+    }
+    if (act && tr >= 0 && tr < Tf) {
+      rj = a.anc[((size_t)f * T + tr) * J + j];
+      own_normals<M, M::NZ, INJ>(a, f, rj, tr + 1, rz);
+    }
+  };
+  auto wait = [&](unsigned int epoch) -> bool {
+    if (threadIdx.x == 0) {
+      int ok = 1;
+      const unsigned int target = epoch * gb.n;
+      long long i = 0;
+      while ((int)(ld_acquire_u32(gb.count) - target) < 0) {
+        if (++i > gb.cap || ld_relaxed_u32(gb.abort) != 0u) { ok = 0; break; }
+        __nanosleep(20);
+      }
+      if (!ok) {
+        atomicOr(gb.err, 1u);
+        atomicExch(gb.abort, 1u);
+      }
+      s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+  };
+
+  prefetch(0);
+  for (int q = 0; q < Q; ++q) {
+    if (q > 0 && !wait((unsigned)q)) return;
+    int ta, sa, tr, sr;
+    bool fl;
+    sched(q, ta, sa, tr, sr, fl);
+    if (act && ta >= 0 && ta < Tf) {
+      const int pin = ta & 1, pout = pin ^ 1;
+      const float* lxi = mb.lx + ((size_t)pin * a.F + f) * DX * J;
+      const float* lwi = mb.lw + ((size_t)pin * a.F + f) * J;
+      float lx[DX];
+#pragma unroll
+      for (int d = 0; d < DX; ++d) lx[d] = 0.0f;
+      float lw = 0.0f;
+      for (int k = plo; k < phi; ++k) {
+#pragma unroll
+        for (int d = 0; d < DX; ++d) lx[d] += lxi[(size_t)d * J + k];
+        lw += lwi[k];
+      }
+      const float gl = -1.0f;
+      const float lm = lw + gl * ppi;
+      const float lwP = lw + gl * (ppi - 1.0f / (float)J);
+      if (pm == pm && pm > -INFINITY) {
+        M::bwd(c, px, pz, kp, lm, lx, gs);
+        fold();
+      } else {
+#pragma unroll
+        for (int d = 0; d < DX; ++d) lx[d] = 0.0f;
+      }
+      float* lxo = mb.lx + ((size_t)pout * a.F + f) * DX * J;
+      float* lwo = mb.lw + ((size_t)pout * a.F + f) * J;
+#pragma unroll
+      for (int d = 0; d < DX; ++d) lxo[(size_t)d * J + j] = lx[d];
+      lwo[j] = mb.alpha * lwP;
+    }
+    if (act && tr >= 0 && tr < Tf) {
+      const float* xin = xin_of(tr, sr);
+      float* xo = mb.sb[sr & 1] + sbf + (size_t)(tr - sr * L) * DX * J;
+      float x[DX];
+#pragma unroll
+      for (int d = 0; d < DX; ++d) x[d] = xin[(size_t)d * J + rj];
+      M::rproc(c, x, rz);
+#pragma unroll
+      for (int d = 0; d < DX; ++d) xo[(size_t)d * J + j] = x[d];
+    }
+    if (fl) flush();
+    if (q + 1 < Q) {
+      __syncthreads();   // every thread's stores before the arrival (release)
+      if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(gb.count) : "memory");
+      prefetch(q + 1);
+    }
+  }
+  {   // dtheta += (d rinit / dtheta)^T adjoint(x^F_{-1}): this thread's own
+      // adjoint of step 0 (parity 1), written above
+    if (act) {
+      const float* lx0 = mb.lx + ((size_t)1 * a.F + f) * DX * J;
+      float z0[NZ0];
+      own_normals<M, M::NZ0, INJ>(a, f, j, 0, z0);
+      float l[DX];
+#pragma unroll
+      for (int d = 0; d < DX; ++d) l[d] = lx0[(size_t)d * J + j];
+      M::bwd_init(c, z0, l, gs);
+      fold();
+    }
+    flush();
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < NG; i += TPB) {
+    double sum = 0.0;
+#pragma unroll 1
+    for (int w = 0; w < NW; ++w) sum += s_g[w][i];
+    mb.gpart[(size_t)blockIdx.x * kMaxNG + i] = sum;
+  }
+}
+
 // Natural-scale gradient sums of filter f (its CTAs' totals, in CTA order),
 // chained to the estimation scale as k_mop_chain does.
 template <class M>
@@ -557,10 +1079,16 @@ static int mop_backward_persist_t(Args& a, const MopWork& w, cudaStream_t s) {
   constexpr int TPB = 256;
   constexpr int DX = M::MAXDX;
   auto kern = k_mop_bwd_persist<M, TPB, INJ>;
-  const int cap = coresident(kern, TPB, 0);
+  auto kern_split = k_mop_bwd_split<M, TPB, INJ>;
   const int want = (a.J + TPB - 1) / TPB;
+  // one particle per thread: the split-phase form, when all its CTAs fit
+  const bool split = (long long)a.F * want <= coresident(kern_split, TPB, 0);
+  const int cap = split ? a.F * want : coresident(kern, TPB, 0);
   const int nbf = want < cap / a.F ? want : cap / a.F;
   if (nbf < 1 || !w.sb2 || !w.gpart) return PPF_EUNSUPPORTED;
+  // the counting barrier's arrivals start from zero (with the generation and
+  // abort words of the other form)
+  if (cudaMemsetAsync(a.gbar, 0, 3 * sizeof(unsigned int), s) != cudaSuccess) return PPF_ECUDA;
   if (cudaMemsetAsync(w.lx, 0, sizeof(float) * 2ull * a.F * DX * a.J, s) != cudaSuccess) return PPF_ECUDA;
   if (cudaMemsetAsync(w.lw, 0, sizeof(float) * 2ull * a.F * a.J, s) != cudaSuccess) return PPF_ECUDA;
   MopBwdP mb;
@@ -574,20 +1102,59 @@ static int mop_backward_persist_t(Args& a, const MopWork& w, cudaStream_t s) {
   mb.nbf = nbf;
   const int grid = a.F * nbf;
   PROF_BEGIN(KIND_MOP_BWD);
-  int rc = launch_coop(kern, grid, TPB, 0, s, a, mb, grid_bar(a, (unsigned)grid));
+  int rc = split ? launch_coop(kern_split, grid, TPB, 0, s, a, mb, grid_bar(a, (unsigned)grid))
+               : launch_coop(kern, grid, TPB, 0, s, a, mb, grid_bar(a, (unsigned)grid));
   PROF_END(KIND_MOP_BWD);
   if (rc) return rc;
   k_mop_chain_parts<M><<<a.F, 64, 0, s>>>(a, w.gpart, nbf, w.grad);
   return cudaGetLastError() == cudaSuccess ? PPF_OK : PPF_ECUDA;
 }
 
-// Persistent launches apply to few filters: the forward's tiles and the
-// adjoint's CTAs must all fit on the device at once.  The forward takes
+// The grid-resident forward: C CTAs of 512 threads per filter, as many as fit
+// on the device at once (up to kGridMaxC per filter, at least 128 particles per
+// CTA), each CTA's slice at most 2048 particles.  PPF_EUNSUPPORTED when the
+// shape does not fit (the caller then takes the per-step kernels).
+template <class M, bool INJ>
+static int mop_forward_grid(Args& a, cudaStream_t s) {
+  constexpr int TPB = 512;
+  constexpr int kMaxJC = 2048;
+  if (!a.slotw || (a.flags & (PPF_F_ESS | PPF_F_FMEAN | PPF_F_PMEAN))) return PPF_EUNSUPPORTED;
+  auto kern = k_mop_fwd_grid<M, TPB, INJ>;
+  auto smem_of = [](int jc) { return sizeof(float) * (M::MAXDX + 1) * jc + sizeof(int) * (jc + 4); };
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(kMaxJC)) !=
+      cudaSuccess)
+    return PPF_ECUDA;
+  const int cap = coresident(kern, TPB, smem_of(kMaxJC));
+  int C = cap / a.F;
+  C = C < kGridMaxC ? C : kGridMaxC;
+  const int cmax = (a.J + 127) / 128;
+  C = C < cmax ? C : cmax;
+  if (C < 1 || (long long)a.F * C > kMaxGridSlots) return PPF_EUNSUPPORTED;
+  const int JC = (((a.J + C - 1) / C) + 3) & ~3;
+  if (JC > kMaxJC) return PPF_EUNSUPPORTED;
+  C = (a.J + JC - 1) / JC;
+  const int grid = a.F * C;
+  // the step words and, after them, two arrival counters per filter
+  if (cudaMemsetAsync(a.slotw, 0, sizeof(uint64_t) * (6 * (size_t)grid + a.F), s) != cudaSuccess) return PPF_ECUDA;
+  k_prep<M><<<(a.F + 127) / 128, 128, 0, s>>>(a);
+  PROF_BEGIN(KIND_MOP_FWD);
+  const int rc = launch_coop(kern, grid, TPB, smem_of(JC), s, a, C, JC);
+  PROF_END(KIND_MOP_FWD);
+  return rc;
+}
+
+// Persistent launches apply to few filters: the forward's CTAs and the
+// adjoint's must all fit on the device at once.  The grid-resident forward
+// comes first; failing that, the tiled form with grid barriers takes
 // 512-particle tiles when they need no more CTAs than there are SMs (one tile
 // per SM: fewer barrier arrivals and tile totals to add per step), else
 // 256-particle tiles.
 template <class M, bool INJ>
 static int mop_forward_persist(Args& a, cudaStream_t s) {
+  {
+    const int rc = mop_forward_grid<M, INJ>(a, s);
+    if (rc != PPF_EUNSUPPORTED) return rc;
+  }
   const long long t512 = (long long)a.F * ((a.J + 511) / 512);
   int rc = PPF_EUNSUPPORTED;
   if (t512 <= num_sms()) rc = mop_forward_persist_t<M, 128, 4, INJ>(a, s);
