@@ -228,7 +228,7 @@ static size_t carve_mop(Args& a, MopWork& w, const ppf_mop_desc* d, unsigned cha
   w.lx = reinterpret_cast<float*>(take(4 * 2 * F * dx * J));
   w.lw = reinterpret_cast<float*>(take(4 * 2 * F * J));
   w.gnat = reinterpret_cast<double*>(take(8 * F * 64));
-  a.slotw = reinterpret_cast<uint64_t*>(take(8ull * 7 * kMaxGridSlots));
+  a.slotw = reinterpret_cast<uint64_t*>(take(8ull * 6 * kInboxWords));
   return off;
 }
 

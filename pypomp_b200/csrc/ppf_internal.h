@@ -45,7 +45,7 @@ struct Args {
   uint32_t* err;
   unsigned int* counter;  // [2]
   unsigned int* gbar;     // [3] grid barrier: arrivals, generation, abort (zeroed per call)
-  uint64_t* slotw;        // [7][kMaxGridSlots] per-CTA step words of the grid-resident MOP
+  uint64_t* slotw;        // [6][kInboxWords] per-CTA step inboxes of the grid-resident MOP
                           // forward and per-filter arrival counters (zeroed by its launch)
   Acc* acc[2];            // [F] each
   uint64_t* desc[2];      // [F][ntiles] each
@@ -127,6 +127,9 @@ constexpr int kTileSmall = 256;    // 64 threads x 4
 constexpr int kNumSMs = 148;
 // CTAs of a grid-resident launch that publish per-step words (8 per SM)
 constexpr int kMaxGridSlots = 8 * kNumSMs;
+// words of one inbox array of the grid-resident MOP forward: F x C x C for F
+// filters of C CTAs (C = 148 for one filter on one CTA per SM)
+constexpr int kInboxWords = 32768;
 
 int run_mop(Args& a, const MopWork& w, cudaStream_t s);
 int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s);

@@ -330,64 +330,70 @@ __device__ __forceinline__ uint64_t grid_word(int tag, uint64_t v) {
   return ((uint64_t)((unsigned)tag & 0xfffu) << kGridTagShift) | v;
 }
 
-// Warp 0: wait until the filter's arrival counter `cnt` reaches `target`
-// (every CTA of the filter adds 1 with release semantics after writing its
-// word for the step), then read the C words w[0..C) once and combine them with
-// fn(r, value) (lane-strided, r the CTA rank).  One lane polls the counter
-// (acquire), so the polling traffic is one word per CTA rather than C; the
-// warp barrier then orders the other lanes' reads after that acquire.  The
-// wait is bounded: the lane gives up after spin_cap polls or when another CTA
-// aborted, and sets the error and abort words.  A word without the expected
-// tag means the exchange protocol was violated (error bit 4).  Returns false
-// (to all of warp 0) on either failure.
+// Warp 0: read the C words of this CTA's inbox w[0..C) (word r is written by
+// CTA r of the filter, and no other CTA reads this inbox), re-reading each
+// word until it carries the step's tag (lane r polls words r, r + 32, ...),
+// then combine the values with fn(r, value).  A word seen with its tag is not
+// read again: no writer reuses its slot before this CTA has moved on (the
+// argument is at the call sites).  The polls are relaxed; the acquire fence
+// after the last one orders the CTA's later reads after every writer's
+// release of its word (the CTA barrier that follows extends this to the
+// other warps).  The wait is bounded: after spin_cap rounds, or when another
+// CTA aborted, lane 0 sets the error and abort words and all of warp 0
+// returns false.
 template <class Fn>
-__device__ __forceinline__ bool grid_exchange(const uint64_t* w, unsigned int* cnt, unsigned int target,
-                                              int C, int tag, const Args& a, Fn fn) {
+__device__ __forceinline__ bool grid_gather(const uint64_t* w, int C, int tag, const Args& a, Fn fn) {
+  constexpr int PER = kGridMaxC / 32;
   const int lane = threadIdx.x & 31;
   unsigned int* abortw = a.gbar + 2;
-  int ok = 1;
-  if (lane == 0) {
-    long long spins = 0;
-    while (ld_acquire_u32(cnt) < target) {
-      if (++spins > a.spin_cap || ld_relaxed_u32(abortw) != 0u) {
-        ok = 0;
-        atomicOr(a.err, 1u);
-        atomicExch(abortw, 1u);
-        break;
-      }
-      __nanosleep(20);
-    }
-  }
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  if (!ok) return false;
   const uint64_t want = (uint64_t)((unsigned)tag & 0xfffu);
   const uint64_t vm = (1ull << kGridTagShift) - 1;
-  bool good = true;
-  for (int r = lane; r < C; r += 32) {
-    const uint64_t v = ld_relaxed_u64(w + r);
-    good &= (v >> kGridTagShift) == want;
-    fn(r, v & vm);
+  uint64_t v[PER];
+  unsigned int need = 0u;   // bit i: word lane + 32 i not yet seen with the tag
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    v[i] = 0ull;
+    if (lane + 32 * i < C) need |= 1u << i;
   }
-  if (!__all_sync(0xffffffffu, good)) {
-    if (lane == 0) {
-      atomicOr(a.err, 4u);
-      atomicExch(abortw, 1u);
+  long long spins = 0;
+  for (;;) {
+    // all of a round's loads are issued before any of them is examined, so a
+    // round costs one memory round trip, not one per word
+    const unsigned int nd = need;
+    uint64_t r[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i)
+      if (nd & (1u << i)) r[i] = ld_relaxed_u64(w + lane + 32 * i);
+#pragma unroll
+    for (int i = 0; i < PER; ++i)
+      if (nd & (1u << i)) {
+        v[i] = r[i];
+        if ((r[i] >> kGridTagShift) == want) need &= ~(1u << i);
+      }
+    if (!__any_sync(0xffffffffu, need != 0u)) break;
+    int stop = 0;
+    if (lane == 0) stop = (++spins > a.spin_cap) || ld_relaxed_u32(abortw) != 0u;
+    stop = __shfl_sync(0xffffffffu, stop, 0);
+    if (stop) {
+      if (lane == 0) {
+        atomicOr(a.err, 1u);
+        atomicExch(abortw, 1u);
+      }
+      return false;
     }
-    return false;
   }
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < PER; ++i)
+    if (lane + 32 * i < C) fn(lane + 32 * i, v[i] & vm);
   return true;
-}
-
-// Arrival: after the CTA barrier that orders every thread's writes, thread 0
-// adds 1 to the counter with release semantics.
-__device__ __forceinline__ void grid_arrive(unsigned int* cnt) {
-  asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
 }
 
 template <class M, int TPB, bool INJ>
 __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) {
   constexpr int DX = M::MAXDX;
   constexpr int NW = TPB / 32;
+  constexpr int ITM = 4;                 // parents per thread at most (JC <= 4 TPB)
   extern __shared__ __align__(16) float smf[];
   __shared__ typename M::Consts csh;
   __shared__ uint64_t s_scan[NW + 1];
@@ -402,20 +408,22 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
   const int J = a.J, T = a.T, L = a.ckpt_every;
   const int base = c * JC;
   const int nc = max(0, min(JC, J - base));
-  const int G = gridDim.x;
-  uint64_t* maxw[2] = {a.slotw, a.slotw + G};
-  uint64_t* minw[2] = {a.slotw + 2 * G, a.slotw + 3 * G};
-  uint64_t* sumw[2] = {a.slotw + 4 * G, a.slotw + 5 * G};
-  // arrival counters of the filter's key and sum words (monotone over steps)
-  unsigned int* cnt_key = reinterpret_cast<unsigned int*>(a.slotw + 6 * G) + 2 * f;
-  unsigned int* cnt_sum = cnt_key + 1;
-  const int fw = f * C;                  // first word of this filter
+  // Inboxes: per quantity (max, min, sum) and step parity, an array of
+  // [F][C readers][C writers] words.  A CTA pushes its word into every inbox
+  // of its filter and polls only its own, so the polling of one CTA does not
+  // contend with that of the others.
+  const size_t box = (size_t)gridDim.x * C;
+  uint64_t* maxw[2] = {a.slotw, a.slotw + box};
+  uint64_t* minw[2] = {a.slotw + 2 * box, a.slotw + 3 * box};
+  uint64_t* sumw[2] = {a.slotw + 4 * box, a.slotw + 5 * box};
+  const size_t fin = (size_t)f * C * C;  // this filter's inboxes
+  const size_t mine = fin + (size_t)c * C;   // this CTA's inbox
   // with no resampling threshold (MOP: always resample) the min key is not needed
   const bool need_min = a.logthresh != -INFINITY;
   float* Xs = smf;                       // [DX][JC] parents of the current step
   float* Ws = Xs + DX * JC;              // [JC]
   int* st = reinterpret_cast<int*>(Ws + JC);   // [JC + 4] first-child offsets
-  const int ITC = (JC + TPB - 1) / TPB;  // parents per thread (contiguous)
+  const int ITC = (JC + TPB - 1) / TPB;  // parents per thread (contiguous), <= ITM
   const int l0 = threadIdx.x * ITC;
   const int l1 = min(l0 + ITC, nc);
 
@@ -424,7 +432,8 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
   const typename M::Consts cr = csh;
 
   // block max / min / NaN of the weights this CTA produced, published for
-  // step `tag - 1` after every thread's stores (release)
+  // step `tag - 1` after every thread's stores: the release store of the max
+  // word publishes the children's states and weights with it
   auto publish_keys = [&](unsigned int mx, unsigned int mn, unsigned int nn, int par, int tag) {
     mx = warp_max_u32(mx);
     mn = warp_min_u32(mn);
@@ -432,13 +441,16 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) { smk[warp] = mx; smk[NW + warp] = mn; smk[2 * NW + warp] = nn; }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    // thread r (r < C) combines the warps' numbers and pushes the word to CTA
+    // r's inbox; each release store publishes the CTA's children with it
+    // (every thread's stores precede the barrier above)
+    for (int r = threadIdx.x; r < C; r += TPB) {
       unsigned int A = 0u, B = 0xffffffffu, O = 0u;
 #pragma unroll
       for (int w = 0; w < NW; ++w) { A = max(A, smk[w]); B = min(B, smk[NW + w]); O |= smk[2 * NW + w]; }
-      if (need_min) st_relaxed_u64(minw[par] + blockIdx.x, grid_word(tag, (uint64_t)B));
-      st_relaxed_u64(maxw[par] + blockIdx.x, grid_word(tag, ((uint64_t)O << 32) | A));
-      grid_arrive(cnt_key);
+      const size_t slot = fin + (size_t)r * C + c;
+      if (need_min) st_relaxed_u64(minw[par] + slot, grid_word(tag, (uint64_t)B));
+      st_release_u64(maxw[par] + slot, grid_word(tag, ((uint64_t)O << 32) | A));
     }
   };
 
@@ -476,23 +488,18 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
     Obs<M> ob;
     if (!last) ob.load(a, u, t + 1);
 
-    // A. The keys of step t's weights: every CTA's key word (tag t+1) was
-    //    written at the end of step t-1 before its arrival, so the key counter
-    //    reaching (t+1) C means all are there (a CTA's arrival for step t+1
-    //    comes after step t's sum exchange, which needs every CTA's step-t
-    //    arrival).  A CTA overwrites its word (tag t+3) only at the end of
-    //    step t+1, after step t+1's sum exchange, which every CTA of the
-    //    filter reaches only after reading this word.
+    // A. The keys of step t's weights (tag t+1), written at the end of step
+    //    t-1.  A CTA overwrites its key word (tag t+3) only at the end of step
+    //    t+1, after gathering the step t+1 key words, which every CTA of the
+    //    filter releases only after its own gather here.
     if (threadIdx.x < 32) {
       unsigned int A = 0u, B = 0xffffffffu, O = 0u;
-      bool ok = grid_exchange(maxw[pc] + fw, cnt_key, (unsigned)(t + 1) * (unsigned)C, C, t + 1, a,
-                              [&](int, uint64_t v) {
-                                A = max(A, (unsigned int)v);
-                                O |= (unsigned int)(v >> 32);
-                              });
+      bool ok = grid_gather(maxw[pc] + mine, C, t + 1, a, [&](int, uint64_t v) {
+        A = max(A, (unsigned int)v);
+        O |= (unsigned int)(v >> 32);
+      });
       if (ok && need_min)
-        ok = grid_exchange(minw[pc] + fw, cnt_key, (unsigned)(t + 1) * (unsigned)C, C, t + 1, a,
-                           [&](int, uint64_t v) { B = min(B, (unsigned int)v); });
+        ok = grid_gather(minw[pc] + mine, C, t + 1, a, [&](int, uint64_t v) { B = min(B, (unsigned int)v); });
       A = warp_max_u32(A);
       B = warp_min_u32(B);
       O = __any_sync(0xffffffffu, O != 0u) ? 1u : 0u;
@@ -512,37 +519,48 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
     const bool collapsed = !nanf && Mx == -INFINITY;
     const bool qc = nanf || Mx == -INFINITY;
     // parents of step t >= 1 were written to global memory by whichever CTAs
-    // drew them; the release / acquire above made them visible
+    // drew them (visible after the gather's acquire and the barrier): states
+    // into shared memory for the children, each thread's own weights straight
+    // into registers (and shared memory, for steps without resampling).  At
+    // t = 0 they are already in shared memory.
+    float wv[ITM];
     if (t > 0) {
       const float* Xg = a.X[pc] + (size_t)f * DX * J + base;
       const float* Wg = a.W[pc] + (size_t)f * J + base;
-      for (int l = threadIdx.x; l < nc; l += TPB) {
+#pragma unroll
+      for (int i = 0; i < ITM; ++i) wv[i] = (l0 + i < l1) ? Wg[l0 + i] : 0.0f;
+      for (int l = threadIdx.x; l < nc; l += TPB)
 #pragma unroll
         for (int d = 0; d < DX; ++d) Xs[d * JC + l] = Xg[(size_t)d * J + l];
-        Ws[l] = Wg[l];
-      }
-      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < ITM; ++i)
+        if (l0 + i < l1) Ws[l0 + i] = wv[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < ITM; ++i) wv[i] = (l0 + i < l1) ? Ws[l0 + i] : 0.0f;
     }
+    uint64_t q[ITM];
     uint64_t qs = 0;
-    for (int l = l0; l < l1; ++l) qs += qweight(Ws[l], Mx, qc);
+#pragma unroll
+    for (int i = 0; i < ITM; ++i) {
+      q[i] = (l0 + i < l1) ? qweight(wv[i], Mx, qc) : 0ull;
+      qs += q[i];
+    }
     uint64_t btot;
     const uint64_t tex = block_excl_scan_u64_1b<TPB>(qs, s_scan, btot);
     // sum words of step t (tag t+1) overwrite those of step t-2: their readers
-    // finished step t-2's sum exchange before their step t-1 key arrival,
-    // which this CTA has waited for
-    if (threadIdx.x == 0) {
-      st_relaxed_u64(sumw[pc] + blockIdx.x, grid_word(t + 1, btot));
-      grid_arrive(cnt_sum);
-    }
+    // gathered them before releasing their step t key words, which this CTA
+    // has gathered (the words carry values only, so the store is relaxed)
+    for (int r = threadIdx.x; r < C; r += TPB)
+      st_relaxed_u64(sumw[pc] + fin + (size_t)r * C + c, grid_word(t + 1, btot));
 
     // B. slice prefix and filter total
     if (threadIdx.x < 32) {
       uint64_t E = 0, tot = 0;
-      const bool ok = grid_exchange(sumw[pc] + fw, cnt_sum, (unsigned)(t + 1) * (unsigned)C, C, t + 1, a,
-                                    [&](int r, uint64_t v) {
-                                      tot += v;
-                                      E += (r < c) ? v : 0ull;
-                                    });
+      const bool ok = grid_gather(sumw[pc] + mine, C, t + 1, a, [&](int r, uint64_t v) {
+        tot += v;
+        E += (r < c) ? v : 0ull;
+      });
       E = warp_sum_u64(E);
       tot = warp_sum_u64(tot);
       if (threadIdx.x == 0) { s_sum[0] = E; s_sum[1] = tot; s_ok = ok ? 1 : 0; }
@@ -557,9 +575,11 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
       if (l0 < nc) {
         OffWalk wk = offwalk_init(o, E + tex);
         st[l0] = wk.k;
-        for (int l = l0; l < l1; ++l) {
-          const int kn = offwalk_add(o, wk, qweight(Ws[l], Mx, qc));
-          if (l + 1 < l1 || l + 1 == nc) st[l + 1] = kn;
+#pragma unroll
+        for (int i = 0; i < ITM; ++i) {
+          if (l0 + i >= l1) break;
+          const int kn = offwalk_add(o, wk, q[i]);
+          if (l0 + i + 1 < l1 || l0 + i + 1 == nc) st[l0 + i + 1] = kn;
         }
       }
     } else {
@@ -607,14 +627,14 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
         if (logw) logw[k] = w;
       }
     }
-    // keys of step t+1's weights (tag t+2) overwrite those of step t-1, whose
-    // readers all finished step t-1's key poll before publishing the step t
-    // sums this CTA has read
+    // keys of step t+1's weights (tag t+2) overwrite those of step t-1 (see A)
     if (!last) publish_keys(mx, mn, nn, pn, t + 2);
     // the step's log-likelihood term and saved per-step numbers, by a thread
     // outside warp 0 once the keys are out (off the exchange's critical path)
     if (c == 0 && threadIdx.x == TPB - 32) finalize_step(a, f, t, acc, tot, &ll_acc);
-    __syncthreads();   // Xs / Ws / st are rewritten by the next step
+    // No barrier here: shared memory is next written after the barrier that
+    // follows the next key gather, which every thread reaches only after its
+    // reads of this step (publish_keys' barrier orders smk).
   }
   if (c == 0 && threadIdx.x == TPB - 32) a.loglik[f] = ll_acc;
 }
@@ -1134,8 +1154,9 @@ static int mop_forward_grid(Args& a, cudaStream_t s) {
   if (JC > kMaxJC) return PPF_EUNSUPPORTED;
   C = (a.J + JC - 1) / JC;
   const int grid = a.F * C;
-  // the step words and, after them, two arrival counters per filter
-  if (cudaMemsetAsync(a.slotw, 0, sizeof(uint64_t) * (6 * (size_t)grid + a.F), s) != cudaSuccess) return PPF_ECUDA;
+  // the inboxes (tag 0: not yet written)
+  if ((long long)grid * C > kInboxWords) return PPF_EUNSUPPORTED;
+  if (cudaMemsetAsync(a.slotw, 0, sizeof(uint64_t) * 6 * (size_t)grid * C, s) != cudaSuccess) return PPF_ECUDA;
   k_prep<M><<<(a.F + 127) / 128, 128, 0, s>>>(a);
   PROF_BEGIN(KIND_MOP_FWD);
   const int rc = launch_coop(kern, grid, TPB, smem_of(JC), s, a, C, JC);
