@@ -99,6 +99,14 @@ typedef struct ppf_model {
  * particles agree to ~1e-6 relative) but not bit-identical with the C oracle.
  * Ignored with PPF_F_INJECT and on the other paths. */
 #define PPF_F_FAST (1u << 12)
+/* ppf_mop / ppf_mop_backward: the DPOP objective instead of MOP-alpha
+ * (pypomp/core/algorithms/dpop.py:34-243).  State component
+ * process_weight_index of the predicted particles holds the transition
+ * log-weight accumulated over the interval, and enters the carried weights
+ * as pw - stop_gradient(pw) (dpop.py:203-209).  Its value is zero, so the
+ * objective's value is MOP-alpha's; the gradient gains the adjoint of the
+ * carried weight times d pw / d theta along each lineage. */
+#define PPF_F_DPOP (1u << 13)
 
 /* Execution paths; all produce bit-identical results. */
 enum {
@@ -158,7 +166,7 @@ typedef struct ppf_pfilter_desc {
 typedef struct ppf_mop_desc {
   ppf_model model;
   int32_t J, F, T, U;
-  uint32_t flags;         /* PPF_F_INJECT, PPF_F_NATURAL */
+  uint32_t flags;         /* PPF_F_INJECT, PPF_F_NATURAL, PPF_F_GRAPH, PPF_F_DPOP */
   float alpha;            /* MOP discount in [0, 1] */
   int32_t ckpt_every;     /* 0 = ceil(sqrt(T)) */
   const float* theta;     /* [F][P] estimation scale */
@@ -175,6 +183,7 @@ typedef struct ppf_mop_desc {
   int32_t* anc;           /* optional out [F][T][J] resampling ancestors */
   void* workspace;
   size_t ws_bytes;
+  int32_t process_weight_index;   /* with PPF_F_DPOP: state component in [0, dx) */
 } ppf_mop_desc;
 
 size_t ppf_mop_workspace_bytes(const ppf_mop_desc* d);

@@ -52,6 +52,9 @@ def lib():
     L.ppfo_pfilter.restype = ctypes.c_int
     L.ppfo_mop_surrogate.argtypes = [ctypes.POINTER(_Desc), ctypes.c_float, _vp, _vp, _vp, _vp]
     L.ppfo_mop_surrogate.restype = ctypes.c_int
+    L.ppfo_dpop_surrogate.argtypes = [ctypes.POINTER(_Desc), ctypes.c_float, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
+                                      _vp]
+    L.ppfo_dpop_surrogate.restype = ctypes.c_int
     L.ppfo_perfilter.argtypes = [ctypes.POINTER(_IF2Desc), ctypes.c_int]
     L.ppfo_perfilter.restype = ctypes.c_int
     L.ppfo_expf.argtypes = [ctypes.c_float]
@@ -152,11 +155,14 @@ def pfilter(kind, dx, dy, theta_f, ys, J, *, seeds=None, ycon=None, unit=None, T
 
 
 def mop_surrogate(kind, dx, dy, theta_est, ys, J, alpha, anc, m0=None, *, seeds=None,
-                  ycon=None, dt=0.0, inject=None, natural=False):
+                  ycon=None, dt=0.0, inject=None, natural=False, pwi=None, p0=None):
     """MOP-alpha surrogate value (frozen ancestry, frozen stop_gradient(m)).
 
     ``anc`` (F,T,J) ancestors; ``m0`` (F,T,J) or None to record it.  Returns
-    ``(value (F,), m0 (F,T,J))``."""
+    ``(value (F,), m0 (F,T,J))``.  With ``pwi`` (a state component) it is the
+    DPOP surrogate: the predicted state's component ``pwi`` enters the carried
+    weights as ``pw - p0`` (``p0`` (F,T,J) frozen, or None to record it), and
+    the return is ``(value, m0, p0)``."""
     theta_est = np.ascontiguousarray(np.atleast_2d(theta_est), dtype=np.float32)
     F, P = theta_est.shape
     ys = np.ascontiguousarray(ys, dtype=np.float32)
@@ -189,10 +195,18 @@ def mop_surrogate(kind, dx, dy, theta_est, ys, J, alpha, anc, m0=None, *, seeds=
     m0_out = np.zeros((F, T, J), np.float32) if m0 is None else None
     m0_in = None if m0 is None else np.ascontiguousarray(m0, dtype=np.float32)
     value = np.zeros(F, np.float64)
-    rc = _L().ppfo_mop_surrogate(ctypes.byref(d), float(alpha), _p(anc), _p(m0_in), _p(m0_out), _p(value))
+    if pwi is None:
+        rc = _L().ppfo_mop_surrogate(ctypes.byref(d), float(alpha), _p(anc), _p(m0_in), _p(m0_out), _p(value))
+    else:
+        p0_out = np.zeros((F, T, J), np.float32) if p0 is None else None
+        p0_in = None if p0 is None else np.ascontiguousarray(p0, dtype=np.float32)
+        rc = _L().ppfo_dpop_surrogate(ctypes.byref(d), float(alpha), int(pwi), _p(anc), _p(m0_in), _p(m0_out),
+                                      _p(p0_in), _p(p0_out), _p(value))
     if rc != 0:
         raise RuntimeError(f"oracle returned {rc}")
     del keep
+    if pwi is not None:
+        return value, (m0_out if m0 is None else m0_in), (p0_out if p0 is None else p0_in)
     return value, (m0_out if m0 is None else m0_in)
 
 

@@ -384,8 +384,14 @@ static double lse(const double* v, int n) {
   return mx + log(s);
 }
 
-int ppfo_mop_surrogate(const ppf_pfilter_desc* d, float alpha, const int* anc, const float* m0_in,
-                       float* m0_out, double* value) {
+/* DPOP adds, per step, the predicted state's component pwi as
+ * pw - stop_gradient(pw) to the carried weights (dpop.py:203-209):
+ *   wP = alpha wF + pw - p0
+ * with p0[F][T][J] the frozen pw (p0_in, or recorded into p0_out).  pwi < 0
+ * is MOP-alpha. */
+static int surrogate_impl(const ppf_pfilter_desc* d, float alpha, int pwi, const int* anc,
+                          const float* m0_in, float* m0_out, const float* p0_in, float* p0_out,
+                          double* value) {
   const int J = d->J, dx = d->model.dx, T = d->T;
   for (int f = 0; f < d->F; ++f) {
     const int u = d->unit ? d->unit[f] : 0;
@@ -406,12 +412,18 @@ int ppfo_mop_surrogate(const ppf_pfilter_desc* d, float alpha, const int* anc, c
     }
     double ll = 0.0;
     for (int t = 0; t < T; ++t) {
+      const size_t row = ((size_t)f * T + t) * J;
       for (int j = 0; j < J; ++j) {
         wP[j] = (double)alpha * wF[j];
         float xj[4];
         for (int k = 0; k < dx; ++k) xj[k] = x[k * J + j];
         m[j] = propagate(d, &c, f, u, j, t, xj);
         for (int k = 0; k < dx; ++k) xp[k * J + j] = xj[k];
+        if (pwi >= 0) {
+          const float pw = xj[pwi];
+          if (!p0_in && p0_out) p0_out[row + j] = pw;
+          wP[j] += (double)pw - (double)(p0_in ? p0_in[row + j] : pw);
+        }
         v[j] = wP[j] + (double)m[j];
       }
       const double a1 = lse(v, J), a2 = lse(wP, J);
@@ -430,6 +442,18 @@ int ppfo_mop_surrogate(const ppf_pfilter_desc* d, float alpha, const int* anc, c
     free(x); free(xp); free(wF); free(wP); free(v); free(m);
   }
   return PPF_OK;
+}
+
+int ppfo_mop_surrogate(const ppf_pfilter_desc* d, float alpha, const int* anc, const float* m0_in,
+                       float* m0_out, double* value) {
+  return surrogate_impl(d, alpha, -1, anc, m0_in, m0_out, NULL, NULL, value);
+}
+
+int ppfo_dpop_surrogate(const ppf_pfilter_desc* d, float alpha, int pwi, const int* anc,
+                        const float* m0_in, float* m0_out, const float* p0_in, float* p0_out,
+                        double* value) {
+  if (pwi < 0 || pwi >= d->model.dx) return PPF_EINVAL;
+  return surrogate_impl(d, alpha, pwi, anc, m0_in, m0_out, p0_in, p0_out, value);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -33,6 +33,7 @@ F_NATURAL = 1 << 8
 F_GRAPH = 1 << 9
 F_NO_PERSIST = 1 << 11
 F_FAST = 1 << 12
+F_DPOP = 1 << 13
 F_NO_CLUSTER = 1 << 10
 
 PATH_AUTO, PATH_PLAIN, PATH_STREAM, PATH_RESIDENT, PATH_CLUSTER = 0, 1, 2, 3, 4
@@ -129,6 +130,7 @@ class MopDesc(ctypes.Structure):
         ("anc", _vp),
         ("workspace", _vp),
         ("ws_bytes", ctypes.c_size_t),
+        ("process_weight_index", ctypes.c_int32),
     ]
 
 

@@ -156,6 +156,7 @@ static long long g_spin_cap = kSpinCap;
 
 static int fill_args(const ppf_pfilter_desc* d, Args& a, int mode) {
   memset(&a, 0, sizeof(a));
+  a.pwi = -1;
   a.spin_cap = g_spin_cap;
   a.model = d->model;
   a.J = d->J; a.F = d->F; a.T = d->T; a.U = d->U;
@@ -243,6 +244,8 @@ static int validate_mop(const ppf_mop_desc* d) {
   if ((d->flags & PPF_F_INJECT) && d->model.kind == PPF_MODEL_LG && !d->inj_z0) return PPF_EINVAL;
   if (d->model.kind == PPF_MODEL_RICKER && !d->ycon) return PPF_EINVAL;
   if (!(d->alpha >= 0.0f && d->alpha <= 1.0f)) return PPF_EINVAL;
+  if ((d->flags & PPF_F_DPOP) && (d->process_weight_index < 0 || d->process_weight_index >= d->model.dx))
+    return PPF_EINVAL;
   return PPF_OK;
 }
 
@@ -429,6 +432,7 @@ int ppf_mop(const ppf_mop_desc* d, void* stream) {
   Args a;
   fill_args(&p, a, MODE_MOP);
   a.flags |= PPF_F_SAVE_ANC;
+  a.pwi = (d->flags & PPF_F_DPOP) ? d->process_weight_index : -1;
   MopWork w;
   memset(&w, 0, sizeof(w));
   const size_t need = carve_mop(a, w, d, nullptr);
@@ -492,6 +496,7 @@ int ppf_mop_backward(const ppf_mop_desc* d, const double* dvalue, void* stream) 
   Args a;
   fill_args(&p, a, MODE_MOP);
   a.flags |= PPF_F_SAVE_ANC;
+  a.pwi = (d->flags & PPF_F_DPOP) ? d->process_weight_index : -1;
   MopWork w;
   memset(&w, 0, sizeof(w));
   const size_t need = carve_mop(a, w, d, nullptr);

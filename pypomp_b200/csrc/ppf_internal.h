@@ -22,6 +22,7 @@ struct Args {
   int J, F, T, U;
   uint32_t flags;
   int mode;
+  int pwi;          // DPOP: state component of the transition log-weight; -1 for MOP
   float thresh, logthresh;
   float base_init;  // log(1/J): the reference's initial log-weight (pfilter.py:35)
   float base_rs;    // -log(J): the log-weight after resampling (helpers.py:88-90)
@@ -46,7 +47,7 @@ struct Args {
   unsigned int* counter;  // [2]
   unsigned int* gbar;     // [3] grid barrier: arrivals, generation, abort (zeroed per call)
   uint64_t* slotw;        // [6][kInboxWords] per-CTA step inboxes of the grid-resident MOP
-                          // forward and per-filter arrival counters (zeroed by its launch)
+                          // forward (zeroed by its launch)
   Acc* acc[2];            // [F] each
   uint64_t* desc[2];      // [F][ntiles] each
   uint64_t* excl;         // [F][ntiles]

@@ -21,7 +21,9 @@
 //   lx(x^P) = Lx_j + lm dm/dx ; dtheta += lm dm/dtheta + lx dx^P/dtheta
 //   adjoint of x^F_{t-1}[j] = (dx^P/dx)^T lx ; of wF_{t-1}[j] = alpha lwP
 // and finally dtheta += (d rinit / dtheta)^T adjoint(x^F_{-1}).  The sums over
-// children read the stored offsets, so they are deterministic.
+// children read the stored offsets, so they are deterministic.  DPOP
+// (PPF_F_DPOP) has the same forward; its adjoint adds lwP to lx[pwi] before
+// the model step (the transition log-weight rides on the carried weight).
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -60,6 +62,17 @@ __device__ __forceinline__ void particle_normals(const Args& a, int f, int j, in
   } else {
     pp_normals(a.seeds[f], (uint32_t)j, (uint32_t)s, PPF_TAG_PROCESS, n, z);
   }
+}
+
+// DPOP (dpop.py:203-209): the predicted state's component pwi is added to the
+// carried weights as pw - stop_gradient(pw), so its adjoint is the carried
+// weight's, lwP.  Added to the state adjoint before the model's backward step
+// takes it through rproc; a no-op for MOP (pwi < 0).
+template <int DX>
+__device__ __forceinline__ void add_process_weight(float* lx, int pwi, float lwP) {
+#pragma unroll
+  for (int d = 0; d < DX; ++d)
+    if (d == pwi) lx[d] += lwP;
 }
 
 // x^F_t[k] = rproc(x^F_{t-1}[anc_t[k]]) with the parent's noise.
@@ -144,8 +157,10 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd(Args a, MopBwd mb, int t) {
     const float gl = -1.0f;                       // d(-sum ll)/d ll_t
     const float lm = lw + gl * pi;
     const float lwP = lw + gl * (pi - 1.0f / (float)J);
-    if (m == m && m > -INFINITY) M::bwd(cr, x, z, kp, lm, lx, g);
-    else {
+    if (m == m && m > -INFINITY) {
+      add_process_weight<DX>(lx, a.pwi, lwP);
+      M::bwd(cr, x, z, kp, lm, lx, g);
+    } else {
 #pragma unroll
       for (int d = 0; d < DX; ++d) lx[d] = 0.0f;
     }
@@ -746,6 +761,7 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_persist(Args a, MopBwdP mb, Gri
       const float lm = lw + gl * pi;
       const float lwP = lw + gl * (pi - 1.0f / (float)J);
       if (m == m && m > -INFINITY) {
+        add_process_weight<DX>(lx, a.pwi, lwP);
         M::bwd(c, x, z, kp, lm, lx, gs);
         fold();
       } else {
@@ -953,6 +969,7 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_split(Args a, MopBwdP mb, GridB
       const float lm = lw + gl * ppi;
       const float lwP = lw + gl * (ppi - 1.0f / (float)J);
       if (pm == pm && pm > -INFINITY) {
+        add_process_weight<DX>(lx, a.pwi, lwP);
         M::bwd(c, px, pz, kp, lm, lx, gs);
         fold();
       } else {

@@ -403,7 +403,7 @@ class MopCall:
 
     def __init__(self, struct: PompStruct, theta_est, seeds_f, J: int, alpha: float, *, unit_f=None,
                  inject=None, ckpt_every: int = 0, save_ancestors: bool = False, natural: bool = False,
-                 graph: bool = False, persistent: bool = True):
+                 graph: bool = False, persistent: bool = True, process_weight_index: int | None = None):
         torch = _ffi.require_cuda()
         if J < 1:
             raise ValueError("J should be greater than 0.")
@@ -434,6 +434,12 @@ class MopCall:
         flags = (_ffi.F_NATURAL if natural else 0) | (_ffi.F_GRAPH if graph else 0)
         if not persistent:
             flags |= _ffi.F_NO_PERSIST
+        pwi = -1
+        if process_weight_index is not None:
+            pwi = int(process_weight_index)
+            if not 0 <= pwi < spec.dx:
+                raise ValueError(f"process_weight_index must be a state index in [0, {spec.dx})")
+            flags |= _ffi.F_DPOP
         if inject is not None:
             flags |= _ffi.F_INJECT
             for k in ("z0", "z", "u"):
@@ -449,6 +455,7 @@ class MopCall:
         d.unit, d.T_u, d.seeds = _ffi.ptr(unit_d), _ffi.ptr(Tu_d), _ffi.ptr(seeds_d)
         d.inj_z0, d.inj_z, d.inj_u = _ffi.ptr(inj.get("z0")), _ffi.ptr(inj.get("z")), _ffi.ptr(inj.get("u"))
         d.value, d.anc = _ffi.ptr(self.out["value"]), _ffi.ptr(self.out.get("anc"))
+        d.process_weight_index = pwi
         nbytes = _ffi.LIB.ppf_mop_workspace_bytes(d)
         self.ws = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
         d.workspace, d.ws_bytes = _ffi.ptr(self.ws), self.ws.numel()
@@ -507,13 +514,18 @@ class MopCall:
 
 def run_mop(struct: PompStruct, theta_est_f: np.ndarray, seeds_f: np.ndarray, J: int, alpha: float,
             *, grad: bool = True, unit_f=None, inject=None, ckpt_every: int = 0,
-            save_ancestors: bool = False, return_torch: bool = False, persistent: bool = True):
+            save_ancestors: bool = False, return_torch: bool = False, persistent: bool = True,
+            process_weight_index: int | None = None):
     """One batched call of ``ppf_mop``: MOP-alpha value (negative log-likelihood,
     summed over time) and, when ``grad``, its gradient on the estimation scale.
     ``persistent=False`` keeps one launch per step where the library would use
-    its persistent form (same results; for comparisons)."""
+    its persistent form (same results; for comparisons).  With
+    ``process_weight_index`` the objective is DPOP's (``PPF_F_DPOP``): same
+    value, gradient with the transition log-weight held in that state
+    component."""
     call = MopCall(struct, theta_est_f, seeds_f, J, alpha, unit_f=unit_f, inject=inject,
-                   ckpt_every=ckpt_every, save_ancestors=save_ancestors, persistent=persistent)
+                   ckpt_every=ckpt_every, save_ancestors=save_ancestors, persistent=persistent,
+                   process_weight_index=process_weight_index)
     out = dict(call.forward(grad=grad))
     if not grad:
         out.pop("grad")
@@ -545,6 +557,117 @@ def mop_value_and_grad(struct: PompStruct, thetas_array, J: int, alpha: float, k
     T = np.asarray(struct.ys).shape[-2]
     scale = 1.0 / T if mean else 1.0
     return res["value"] * scale, res["grad"] * scale
+
+
+def dpop(struct: PompStruct, thetas_array, J: int, alpha: float, process_weight_index: int,
+         keys) -> np.ndarray:
+    """DPOP negative log-likelihood (``pypomp/functional/dpop.py:13-90`` ->
+    ``_dpop_internal``, ``pypomp/core/algorithms/dpop.py:34-134``).
+
+    ``thetas_array`` (n, P) on the estimation scale, ``keys`` (n,).  DPOP adds
+    the transition log-weight held in state component ``process_weight_index``
+    to the carried weights as ``pw - stop_gradient(pw)``: its value is zero,
+    so the objective's value equals MOP-alpha's with the same draws; only its
+    gradient differs (:func:`dpop_value_and_grad`).  Experimental in the
+    reference, which warns; so does this function."""
+    import warnings
+
+    warnings.warn("dpop is experimental and its API and behavior are subject to change.",
+                  category=FutureWarning, stacklevel=2)
+    th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float32))
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    if keys.shape[0] != th.shape[0]:
+        raise ValueError("keys must have one key per parameter set")
+    return run_mop(struct, th, keys, J, alpha, grad=False, process_weight_index=process_weight_index)["value"]
+
+
+def dpop_value_and_grad(struct: PompStruct, thetas_array, J: int, alpha: float, process_weight_index: int,
+                        keys, mean: bool = True):
+    """Value and gradient of the (mean) DPOP objective, the
+    ``jax.value_and_grad(_dpop_internal_mean)`` of
+    ``pypomp/core/algorithms/train_dpop.py:130-146``: one ``ppf_mop`` call with
+    ``PPF_F_DPOP`` (forward and adjoint) for all n parameter sets."""
+    th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float32))
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    res = run_mop(struct, th, keys, J, alpha, grad=True, process_weight_index=process_weight_index)
+    T = np.asarray(struct.ys).shape[-2]
+    scale = 1.0 / T if mean else 1.0
+    return res["value"] * scale, res["grad"] * scale
+
+
+def dpop_train(struct: PompStruct, thetas_array, J: int, optimizer, M: int, eta, alpha: float,
+               process_weight_index: int, keys, alpha_cooling: float = 1.0, thresh: float = 0.0,
+               n_monitors: int = 1):
+    """DPOP gradient training (``pypomp/functional/dpop.py:93-185`` ->
+    ``_dpop_train_internal``, ``pypomp/core/algorithms/train_dpop.py:118-227``).
+
+    ``thetas_array`` (n, P) on the estimation scale, ``keys`` (n,).  Iteration
+    m splits the key, cools alpha (cosine, ``alpha_cooling``), takes the mean
+    DPOP objective's value and gradient in one batched ``ppf_mop`` call,
+    replaces NaN gradient entries by 0, clips elementwise (``clip_norm``),
+    takes the optimiser's step (scaled to unit norm with ``scale``) and moves
+    ``theta += eta[m] * direction``.  After the M steps one more split gives
+    the key of the final objective at the last parameters.  Returns
+    ``(neg_logliks (n, M+1), thetas (n, M+1, P))``: entry m < M is the total
+    negative DPOP log-likelihood at the parameters before step m, entry M the
+    one at the final parameters.  ``thresh`` and ``n_monitors`` are accepted
+    for the reference's signature and, as there, unused.  First-order
+    optimisers only (the reference's scan passes no Hessian)."""
+    import warnings
+
+    from . import random as pprandom
+    from .optim import LearningRate, cosine_alpha
+
+    warnings.warn("dpop_train is experimental and its API and behavior are subject to change.",
+                  category=FutureWarning, stacklevel=2)
+    if getattr(optimizer, "needs_hessian", False):
+        raise ValueError(f"Optimizer '{optimizer.__class__.__name__}' needs a Hessian; dpop_train "
+                         "supports first-order optimizers")
+    th = np.atleast_2d(np.asarray(thetas_array, dtype=np.float64)).copy()
+    n, P = th.shape
+    keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
+    if keys.shape[0] != n:
+        raise ValueError("keys must have one key per parameter set")
+    names = list(struct.spec.param_names)
+    eta_arr = eta.to_array(names, M) if isinstance(eta, LearningRate) else np.broadcast_to(
+        np.asarray(eta, dtype=np.float64), (max(M, 1), P))
+    T = np.asarray(struct.ys).shape[-2]
+    state = optimizer.init_state(th)
+    nll = np.zeros((n, M + 1))
+    traces = np.zeros((n, M + 1, P))
+    traces[:, 0] = th
+    chain = [int(k) for k in keys]
+
+    def split_all():
+        subs = np.zeros(n, np.uint64)
+        for i in range(n):
+            chain[i], subs[i] = (int(v) for v in pprandom.split(chain[i]))
+        return subs
+
+    alphas = [1.0 - (1.0 - alpha) * cosine_alpha(m, M, alpha_cooling) for m in range(M + 1)]
+    reuse = len(set(alphas)) == 1
+    call = None
+    for m in range(M):
+        subs = split_all()
+        if reuse and call is not None:
+            call.update(th.astype(np.float32), subs)
+        else:
+            call = MopCall(struct, th.astype(np.float32), subs, J, alphas[m], graph=reuse,
+                           process_weight_index=process_weight_index)
+        res = {k: v.cpu().numpy() for k, v in call.forward(grad=True).items()}
+        nll[:, m] = res["value"]
+        grad = np.where(np.isnan(res["grad"]), 0.0, res["grad"] / T)
+        if optimizer.clip_norm is not None:
+            grad = np.clip(grad, -optimizer.clip_norm, optimizer.clip_norm)
+        direction, state = optimizer.step(grad, state, m, eta_i=eta_arr[m])
+        if optimizer.scale:
+            direction = direction / np.maximum(np.linalg.norm(direction, axis=-1, keepdims=True), 1e-8)
+        th = th + eta_arr[m] * direction
+        traces[:, m + 1] = th
+    subs = split_all()
+    nll[:, M] = run_mop(struct, th.astype(np.float32), subs, J, alphas[M], grad=False,
+                        process_weight_index=process_weight_index)["value"]
+    return nll, traces
 
 
 def _warn_nonfinite(grad, m: int) -> None:
@@ -1557,7 +1680,8 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
 
 
 def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optimizer, M: int, eta,
-                alpha: float, keys, alpha_cooling: float = 1.0, chunk_size: int = 1, *, inject=None):
+                alpha: float, keys, alpha_cooling: float = 1.0, chunk_size: int = 1, *, inject=None,
+                process_weight_index: int | None = None):
     """Panel MOP-alpha gradient training (``pypomp/functional/train.py:112-190``;
     ``_panel_train_internal`` / ``_chunk_scan_step`` at
     ``pypomp/core/algorithms/train.py:191-413``).
@@ -1573,13 +1697,25 @@ def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optim
     (neg_logliks (n, M+1), shared (n, M+1, ns), unit (n, M+1, U, nu)),
     natural scale, NaN first log-likelihood.  ``inject[m][c]`` optionally
     replays external draws for chunk c of iteration m.
+
+    With ``process_weight_index`` it is the panel DPOP training of
+    ``_panel_dpop_train_internal`` (``pypomp/core/algorithms/train_panel_dpop.py:152-322``):
+    the chunks' values and gradients are DPOP's (``PPF_F_DPOP``), gradients
+    are not clipped, SGD and Adam only, and the first log-likelihood entry is
+    the summed DPOP objective of all units at the initial parameters under
+    iteration 0's keys and the uncooled alpha (``train_panel_dpop.py:295-316``).
     """
     from . import random as pprandom
     from .optim import SGD, Adam, FullMatrixAdam, LearningRate, cosine_alpha
 
+    dpop_mode = process_weight_index is not None
+    if dpop_mode and inject is not None:
+        raise ValueError("panel DPOP training does not replay injected draws")
     # as _panel_train_internal (train.py:191-200): these three only; `ls` is not used by panel train
-    if not isinstance(optimizer, (SGD, Adam, FullMatrixAdam)):
-        raise ValueError(f"Optimizer '{optimizer.__class__.__name__}' not supported for panel train")
+    allowed = (SGD, Adam) if dpop_mode else (SGD, Adam, FullMatrixAdam)
+    if not isinstance(optimizer, allowed):
+        what = "panel dpop_train" if dpop_mode else "panel train"
+        raise ValueError(f"Optimizer '{optimizer.__class__.__name__}' not supported for {what}")
     spec = struct.spec
     U, Tn = struct.U, struct.ys.shape[1]
     cs = max(1, int(chunk_size))
@@ -1641,11 +1777,12 @@ def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optim
                 res = {k: v.cpu().numpy() for k, v in calls[c].forward(grad=True).items()}
             elif reuse:
                 calls[c] = MopCall(all_units, th32, ks, J, alpha_m, unit_f=np.tile(units.astype(np.int32), n),
-                                   graph=True)
+                                   graph=True, process_weight_index=process_weight_index)
                 res = {k: v.cpu().numpy() for k, v in calls[c].forward(grad=True).items()}
             else:
                 res = run_mop(all_units, th32, ks, J, alpha_m, grad=True,
-                              unit_f=np.tile(units.astype(np.int32), n), inject=inj)
+                              unit_f=np.tile(units.astype(np.int32), n), inject=inj,
+                              process_weight_index=process_weight_index)
             val = res["value"].reshape(n, cs)
             g = res["grad"].reshape(n, cs, -1)
             gp = np.zeros((n, cs, ns + nu))
@@ -1656,7 +1793,7 @@ def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optim
             grad_u = gp[:, :, ns:] * scale * cs
             chunk_nll[:, c] = val.sum(axis=1) * scale * (Tn * U)
             _warn_nonfinite(gp, m)
-            if optimizer.clip_norm is not None:
+            if optimizer.clip_norm is not None and not dpop_mode:
                 grad_s = np.clip(grad_s, -optimizer.clip_norm, optimizer.clip_norm)
                 grad_u = np.clip(grad_u, -optimizer.clip_norm, optimizer.clip_norm)
             d_s, st_s = optimizer.step(grad_s, st_s, gstep)
@@ -1672,4 +1809,27 @@ def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optim
             gstep += 1
         nll[:, m + 1] = chunk_nll.mean(axis=1)
         hist_s[:, m + 1], hist_u[:, m + 1] = from_est_blocks(s_est, u_est)
+    if dpop_mode:
+        s0, u0 = to_est_blocks(sh, un)
+        units = np.arange(U)
+        th0 = _panel_thetas(s0, u0, perms).reshape(n * U, -1).astype(np.float32)
+        v0 = run_mop(all_units, th0, keys[:, 0, :].reshape(-1), J, alpha, grad=False,
+                     unit_f=np.tile(units.astype(np.int32), n), process_weight_index=process_weight_index)["value"]
+        nll[:, 0] = v0.reshape(n, U).sum(axis=1)
     return nll, hist_s, hist_u
+
+
+def panel_dpop_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optimizer, M: int, eta,
+                     alpha: float, process_weight_index: int, keys, alpha_cooling: float = 1.0,
+                     chunk_size: int = 1):
+    """Panel DPOP gradient training (``_panel_dpop_train_internal``,
+    ``pypomp/core/algorithms/train_panel_dpop.py:152-322``, behind
+    ``PanelPomp._dpop_train``): :func:`panel_train`'s chunk loop on the DPOP
+    objective.  Returns ``(neg_logliks (n, M+1), shared (n, M+1, ns),
+    unit (n, M+1, U, nu))``, natural scale."""
+    import warnings
+
+    warnings.warn("dpop_train is experimental and its API and behavior are subject to change.",
+                  category=FutureWarning, stacklevel=2)
+    return panel_train(struct, shared_array, unit_array, J, optimizer, M, eta, alpha, keys, alpha_cooling,
+                       chunk_size, process_weight_index=int(process_weight_index))

@@ -447,6 +447,64 @@ class PanelPomp:
              "alpha_cooling": alpha_cooling, "optimizer": optimizer},
             time.time() - start, old_key))
 
+    def _dpop_train(self, J: int, M: int, eta, chunk_size: int = 1, optimizer=None, alpha: float = 0.97,
+                    alpha_cooling: float = 1.0, process_weight_state: str | None = None, key=None,
+                    theta=None) -> None:
+        """Panel DPOP training (``pypomp/panel/estimation_mixin.py:995-1180``,
+        experimental there too): :meth:`train`'s chunked loop on the DPOP
+        objective with the transition log-weight in state component
+        ``process_weight_state``.  A ``chunk_size`` that does not divide the
+        number of units is lowered to the largest divisor below it, with a
+        warning, as the reference does."""
+        import warnings
+
+        from . import functional as F
+        from .optim import Adam
+
+        warnings.warn("dpop_train is experimental and its API and behavior are subject to change.",
+                      category=FutureWarning, stacklevel=2)
+        start = time.time()
+        optimizer = optimizer or Adam()
+        th = self._theta_in(theta)
+        theta_for_result = deepcopy(th)
+        n = th.num_replicates()
+        key, old_key = self._update_fresh_key(key)
+        if J < 1:
+            raise ValueError("J should be greater than 0.")
+        if M < 1:
+            raise ValueError("M should be greater than 0.")
+        names = self.get_unit_names()
+        U = len(names)
+        cs = min(max(int(chunk_size), 1), U)
+        if U % cs:
+            orig = cs
+            cs = max(d for d in range(cs, 0, -1) if U % d == 0)
+            warnings.warn("chunk_size does not divide the number of units; "
+                          f"using chunk_size={cs} instead of {orig}.", UserWarning, stacklevel=2)
+        if process_weight_state is None:
+            raise ValueError(
+                "dpop_train requires a process-weight state. Please provide `process_weight_state` as the "
+                "name of the state variable that accumulates the transition log-weight (e.g. 'logw').")
+        statenames = list(self.unit_objects[names[0]].statenames)
+        if process_weight_state not in statenames:
+            raise ValueError(f"process_weight_state '{process_weight_state}' not found in statenames: "
+                             f"{statenames}")
+        pwi = statenames.index(process_weight_state)
+        sn, un = self.canonical_shared_param_names, self.canonical_unit_param_names
+        keys = pprandom.split(key, n * M * U).reshape(n, M, U)
+        nll, hs, hu = F.panel_train(self.to_struct(), th.shared_array(sn), th.unit_array(names, un), J,
+                                    optimizer, M, eta, alpha, keys, alpha_cooling, cs, process_weight_index=pwi)
+        s_tr = np.concatenate([-nll[:, :, None], hs], axis=2)
+        u_tr = np.concatenate([np.full(hu.shape[:3] + (1,), np.nan), hu], axis=3)
+        self.theta = PanelParameters.from_arrays(hs[:, -1], hu[:, -1], sn, un, names)
+        self.results_history.add(PanelResult(
+            "dpop_train", theta_for_result,
+            {"shared_traces": s_tr, "unit_traces": u_tr, "unit_names": names, "shared_names": sn,
+             "unit_param_names": un},
+            {"J": J, "M": M, "eta": eta, "alpha": alpha, "chunk_size": cs, "alpha_cooling": alpha_cooling,
+             "optimizer": optimizer, "process_weight_state": process_weight_state},
+            time.time() - start, old_key))
+
     # -- analysis ------------------------------------------------------------
     def time(self) -> pd.DataFrame:
         return self.results_history.time()

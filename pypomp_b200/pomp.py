@@ -378,6 +378,54 @@ class Pomp:
                     "alpha_cooling": alpha_cooling, "optimizer": optimizer},
             execution_time=(time.time() - start) if track_time else None, key=old_key))
 
+    def _dpop_train(self, J: int, M: int, eta, optimizer=None, alpha: float = 0.8, alpha_cooling: float = 1.0,
+                    process_weight_state: str | None = None, key=None, theta=None,
+                    track_time: bool = True) -> None:
+        """DPOP gradient training (``pypomp/core/estimation_mixin.py:637-820``,
+        experimental there too).  ``process_weight_state`` names the state
+        component that holds the transition log-weight of an interval.  Sets
+        ``self.theta`` to the final parameters with the final objective as
+        ``logLik`` and records a ``dpop_train`` result with the traces."""
+        import warnings
+
+        from . import functional as F
+        from .optim import Adam, LearningRate
+
+        warnings.warn("dpop_train is experimental and its API and behavior are subject to change.",
+                      category=FutureWarning, stacklevel=2)
+        start = time.time()
+        optimizer = optimizer or Adam()
+        theta_in = deepcopy(self._prepare_theta_input(theta))
+        theta_for_results = deepcopy(theta_in)
+        n = theta_in.num_replicates()
+        if J < 1:
+            raise ValueError("J should be greater than 0")
+        if not isinstance(eta, LearningRate):
+            raise TypeError("eta must be a LearningRate object")
+        if process_weight_state is None:
+            raise ValueError(
+                "dpop_train requires a process-weight state. Please provide `process_weight_state` as the "
+                "name of the state variable that accumulates the transition log-weight (e.g. 'logw').")
+        if process_weight_state not in self.statenames:
+            raise ValueError(f"State '{process_weight_state}' not found in statenames {self.statenames}")
+        pwi = self.statenames.index(process_weight_state)
+        new_key, old_key = self._update_fresh_key(key)
+        keys = pprandom.split(new_key, n)
+        th_est = self.spec.to_est(theta_in.to_array(self.canonical_param_names))
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", FutureWarning)
+            nll, traces = F.dpop_train(self.to_struct(), th_est, J, optimizer, M, eta, alpha, pwi, keys,
+                                       alpha_cooling)
+        nat = self.spec.from_est(traces.reshape(-1, traces.shape[-1])).reshape(traces.shape)
+        self.theta = PompParameters.from_array(nat[:, -1, :], self.canonical_param_names)
+        self.theta.logLik = -nll[:, -1]
+        self.results_history.add(Result(
+            method="dpop_train", theta=theta_for_results,
+            payload={"logLiks": -nll, "traces": nat, "param_names": self.canonical_param_names},
+            config={"J": J, "M": M, "eta": eta, "alpha": alpha, "alpha_cooling": alpha_cooling,
+                    "optimizer": optimizer, "process_weight_state": process_weight_state},
+            execution_time=(time.time() - start) if track_time else None, key=old_key))
+
     # -- analysis ------------------------------------------------------------
     def pmcmc(self, J: int, M: int, proposal, dprior=None, key=None, theta=None, thresh: float = 0.0,
               track_time: bool = True) -> None:

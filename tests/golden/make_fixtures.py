@@ -64,6 +64,8 @@ def main(ref_root: Path):
         "mif": _read_csv(reg / "test_mif_regression" / "test_mif_regression.csv"),
         "mif_full_trace": _read_csv(reg / "test_mif_regression" / "test_mif_full_trace_regression.csv"),
         "train": _read_csv(reg / "test_train_regression" / "test_train_regression.csv"),
+        "dpop": _read_csv(reg / "test_dpop_regression" / "test_dpop_regression.csv"),
+        "dpop_train": _read_csv(reg / "test_dpop_train_regression" / "test_dpop_train_regression.csv"),
         "panel_pfilter": _read_csv(reg / "test_panel_pfilter_regression" / "test_panel_pfilter_regression.csv"),
         "panel_mif": _read_csv(reg / "test_panel_mif_regression" / "test_panel_mif_regression.csv"),
         "panel_train": _read_csv(reg / "test_panel_train_regression" / "test_panel_train_regression.csv"),

@@ -93,3 +93,26 @@ def test_wait_limit_hook_is_host_only():
     assert _ffi.LIB.ppf_debug_set_wait_limit(1 << 40) == 5
     assert _ffi.LIB.ppf_debug_set_wait_limit(-1) == default
     assert _ffi.LIB.ppf_debug_set_wait_limit(-1) == default
+
+
+def test_dpop_descriptor_validation_without_gpu():
+    """ppf_mop with PPF_F_DPOP refuses a process-weight index outside the
+    state before touching the device; the descriptor carries the index after
+    the workspace fields, as include/ppf.h declares it."""
+    import ctypes
+
+    from pypomp_b200 import _ffi
+
+    assert _ffi.MopDesc.process_weight_index.offset == _ffi.MopDesc.ws_bytes.offset + ctypes.sizeof(ctypes.c_size_t)
+    d = _ffi.MopDesc()
+    d.model = _ffi.PpfModel(_ffi.MODEL_LG, 2, 2, 16, 0.0, 0)
+    d.J, d.F, d.T, d.U = 100, 1, 5, 1
+    d.alpha = 0.5
+    buf = (ctypes.c_float * 64)()
+    d.theta = d.ys = d.value = ctypes.addressof(buf)
+    d.seeds = ctypes.addressof(buf)
+    d.flags = _ffi.F_DPOP
+    for bad in (-1, 2, 7):
+        d.process_weight_index = bad
+        assert _ffi.LIB.ppf_mop(d, None) == _ffi.PPF_EINVAL
+        assert _ffi.LIB.ppf_mop_backward(d, None, None) == _ffi.PPF_EINVAL

@@ -62,6 +62,36 @@ def test_refpath_reproduces_mop_fixture(ref_values, ref_lg1d):
     assert _close(float(v), ref_values["mop"]["mop"][0], ref_values["tolerance"])
 
 
+
+def test_refpath_reproduces_dpop_fixture(ref_values, ref_lg1d):
+    """DPOP's forward is MOP's (the transition log-weight enters the carried
+    weights as pw - stop_gradient(pw), value 0; same key tree,
+    ``pypomp/core/algorithms/dpop.py:85-134``), so the MOP restatement
+    reproduces the locked DPOP value (alpha = 0.5, process_weight_index = 0)."""
+    k = jr.split(jr.key(20260811), 1)[0]
+    v = rp.mop("LG", ref_lg1d["theta"], ref_lg1d["ys"], 12, 0.5, rp.JaxKeyNoise(k, 12, 1, 1))
+    assert _close(float(v), ref_values["dpop"]["dpop"][0], ref_values["tolerance"])
+
+
+def test_dpop_surrogate_value_equals_mop_surrogate():
+    """At the base parameters the frozen DPOP surrogate of the C oracle has the
+    MOP surrogate's value, and its recorded pw are the predicted states'
+    component pwi."""
+    import pypomp_b200 as pp
+
+    m = pp.LG(T=8, key=5)
+    st, spec = m.to_struct(), m.spec
+    th = spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(np.float32)
+    seeds = np.array([2], np.uint64)
+    J = 300
+    w = cora.pfilter(spec.kind, spec.dx, spec.dy, th, st.ys, J, seeds=seeds, est=True, mop=True, anc=True)
+    v_mop, m0 = cora.mop_surrogate(spec.kind, spec.dx, spec.dy, th, st.ys, J, 0.5, w["anc"], seeds=seeds)
+    for pwi in range(spec.dx):
+        v_dp, m0_dp, p0 = cora.mop_surrogate(spec.kind, spec.dx, spec.dy, th, st.ys, J, 0.5, w["anc"],
+                                             seeds=seeds, pwi=pwi)
+        assert v_dp[0] == v_mop[0]
+        assert np.array_equal(m0_dp, m0) and p0.shape == m0.shape and np.all(np.isfinite(p0))
+
 def test_recorded_streams_replay_identically(ref_lg1d):
     # the committed injection arrays are the draws of the key tree above
     res = rp.pfilter("LG", ref_lg1d["theta"], ref_lg1d["ys"], 12,
