@@ -377,6 +377,46 @@ def run_ours(args):
     # ---- accuracy: the 64 log-likelihoods against the exact Kalman value ----
     kalman_err = loglik_error(loglik, kalman_loglik(st.ys, LG_A, np.eye(2), LG_Q, LG_R, np.zeros(2)))
 
+    # ---- the same workload with PPF_F_FAST (SFU special functions) --------
+    fast = None
+    if rank == 0 and not args.fast and not args.skip_fast:
+        import ctypes
+
+        dfa = _ffi.PfilterDesc()
+        ctypes.memmove(ctypes.addressof(dfa), bytes(d), ctypes.sizeof(d))
+        dfa.flags = d.flags | _ffi.F_FAST
+        llf = torch.zeros(NSEED, dtype=torch.float64, device=dev)
+        dfa.loglik = _ffi.ptr(llf)
+
+        def step_fast():
+            _ffi.check(_ffi.LIB.ppf_pfilter(dfa, stream.cuda_stream), "ppf_pfilter (fast)")
+
+        for _ in range(args.warmup):
+            step_fast()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as fclk:
+            f0.record(stream)
+            for _ in range(args.steps):
+                step_fast()
+            f1.record(stream)
+            torch.cuda.synchronize()
+        fms = f0.elapsed_time(f1) / args.steps
+        _ffi.profile_begin()
+        step_fast()
+        fprof = _ffi.profile_end()
+        f_rp = fprof["resample_propagate"][0] / fprof["resample_propagate"][1]
+        f_ach = RESPROP_BYTES * J * NSEED / (f_rp / 1e3) / 1e9
+        fast = {"arithmetic": "fast (PPF_F_FAST: SFU Box-Muller and weight exponential, contraction)",
+                "value": NSEED * J * T / (fms / 1e3), "unit": UNIT, "ms_per_step": fms,
+                "roofline": {"kernel": "k_resprop_fast", "avg_launch_ms": f_rp, "achieved": f_ach,
+                             "peak": peak, "unit": "GB/s", "frac": f_ach / peak},
+                "sum_kernel_avg_ms": fprof["sum_lookback"][0] / fprof["sum_lookback"][1],
+                "clocks": fclk.summary(),
+                "loglik_err_vs_kalman": loglik_error(llf.cpu().numpy(), kalman_err["kalman"])}
+        if plain is not None:
+            fast["ratio_over_plain"] = fast["value"] / plain["value"]
+
     # ---- MOP-alpha value + gradient (the metric's second half) ------------
     mop = None
     if rank == 0 and not args.skip_mop:
@@ -413,6 +453,7 @@ def run_ours(args):
             "clocks": clk.summary(),
             "gpu_launches": launches_per_step * args.steps,
             "loglik_err_vs_kalman": kalman_err,
+            "fast": fast,
             "mop": mop,
         }
         print(json.dumps(line))
@@ -571,12 +612,20 @@ def run_c4(args):
     best = min(res, key=lambda k: res[k][0])
     ms, clk = res[best]
     value = Fg * Jr * Tr / (ms / 1e3)
+    # the plain one-filter-at-a-time kernels on two of the grid points (the
+    # same results, one filter after the other)
+    Fp = 2
+    pms, _ = _timed(lambda: F.run_pfilter(st, grid[:Fp], seeds[:Fp], Jr, path="plain", return_torch=True),
+                    1, 1, stream)
+    plain_value = Fp * Jr * Tr / (pms / 1e3)
     _line(args, "Ricker 32x32 (log r, sigma) grid x J=16384, T=500", value, ms,
           {"e2e": {"value": value, "unit": UNIT, "api": "functional.run_pfilter (host inputs)",
                    "h2d_bytes_per_step": int(grid.nbytes + st.ys.nbytes + seeds.nbytes),
                    "d2h_bytes_per_step": 0},
            "clocks": clk, "path": best,
            "paths_ms": {k: v[0] for k, v in res.items()},
+           "plain": {"value": plain_value, "unit": UNIT, "filters_timed": Fp,
+                     "ratio_batched_over_plain": value / plain_value},
            "roofline": {"bound": "issue", "achieved": None, "peak": None, "unit": None, "frac": None,
                         "traffic": None,
                         "note": "resident path keeps each swarm in shared memory for all T: "
@@ -876,6 +925,7 @@ def main():
     ap.add_argument("--ref-t", type=int, default=50,
                     help="observations per step of the reference arm's sample")
     ap.add_argument("--skip-mop", action="store_true", help="leave the MOP value+grad block out")
+    ap.add_argument("--skip-fast", action="store_true", help="leave the PPF_F_FAST block out")
     ap.add_argument("--fast", action="store_true",
                     help="PPF_F_FAST kernels (hardware special functions; statistically, not bitwise, "
                          "equal to the exact arithmetic)")

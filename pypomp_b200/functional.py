@@ -1180,9 +1180,12 @@ def _cooling_table(rw_sd, M: int, T_u, width: int | None = None) -> np.ndarray:
     past a unit's length; width defaults to max T_u)."""
     T_u = np.atleast_1d(np.asarray(T_u, dtype=np.int64))
     out = np.zeros((M, T_u.size, int(width or T_u.max())), np.float32)
-    for m in range(M):
-        for u, Tu in enumerate(T_u):
-            out[m, u, :Tu] = [rw_sd.cooling_factor(i, m, int(Tu)) for i in range(int(Tu))]
+    rows = {}                      # units of equal length share their rows
+    for u, Tu in enumerate(T_u):
+        Tu = int(Tu)
+        if Tu not in rows:
+            rows[Tu] = np.array([rw_sd.cooling_factors(Tu, m) for m in range(M)], dtype=np.float32)
+        out[:, u, :Tu] = rows[Tu]
     return out
 
 
@@ -1603,7 +1606,14 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
     sig_p, sig0_p = rw_sd.arrays(struct.param_names)
     sig_u, sig0_u = sig_p[perm], sig0_p[perm]
     panel0 = np.concatenate([sh[:, :, None, :].repeat(U, axis=2), un], axis=3)   # (n, J, U, Pp) natural
-    est0 = spec.to_est(panel0[..., perm])[..., inv]                               # panel order
+    # the transforms act column by column: panel column j is canonical
+    # parameter inv[j], so apply that parameter's transform to it directly (no
+    # gathers of the J x U swarm)
+    import dataclasses
+
+    pspec = dataclasses.replace(spec, est_log=tuple(j for j in range(len(inv)) if inv[j] in spec.est_log),
+                                est_atanh=tuple(j for j in range(len(inv)) if inv[j] in spec.est_atanh))
+    est0 = pspec.to_est(panel0)                                                   # panel order
     S = torch.tensor(est0[:, :, 0, :ns].transpose(0, 2, 1).copy(), dtype=torch.float32, device=dev)
     Us = torch.tensor(est0[:, :, :, ns:].transpose(0, 2, 3, 1).copy(), dtype=torch.float32, device=dev)
     m_keys = np.stack([pprandom.split(k, M + 1)[1:] for k in keys])               # (n, M)
@@ -1615,7 +1625,7 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
 
     def nat(s_est, u_est):        # (n, ns), (n, U, nu) estimation scale -> natural, panel order
         panel = np.concatenate([np.repeat(s_est[:, None], U, axis=1), u_est], axis=2)
-        out = spec.from_est(panel[..., perm])[..., inv]
+        out = pspec.from_est(panel)
         return out[:, 0, :ns], out[:, :, ns:]
 
     # device-side loop: the keys and cooling factors of all iterations are
@@ -1675,7 +1685,7 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
     s_fin = S.cpu().numpy().astype(np.float64).transpose(0, 2, 1)                 # (n, J, ns)
     u_fin = Us.cpu().numpy().astype(np.float64).transpose(0, 3, 1, 2)             # (n, J, U, nu)
     panel = np.concatenate([np.repeat(s_fin[:, :, None], U, axis=2), u_fin], axis=3)
-    natf = spec.from_est(panel[..., perm])[..., inv]
+    natf = pspec.from_est(panel)
     return shared_tr, unit_tr, natf[:, :, 0, :ns], natf[:, :, :, ns:]
 
 

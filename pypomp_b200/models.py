@@ -49,25 +49,25 @@ class ModelSpec:
     def ffi_model(self) -> _ffi.PpfModel:
         return _ffi.PpfModel(self.kind, self.dx, self.dy, self.n_params, float(self.dt), 0)
 
-    def to_est(self, theta: np.ndarray) -> np.ndarray:
+    def _apply(self, theta, f_log, f_atanh) -> np.ndarray:
         t = np.array(theta, dtype=np.float64, copy=True)
         if self.natural:
             return t
-        if self.est_log:
-            t[..., list(self.est_log)] = np.log(t[..., list(self.est_log)])
-        if self.est_atanh:
-            t[..., list(self.est_atanh)] = np.arctanh(t[..., list(self.est_atanh)])
+        P = t.shape[-1]
+        for cols, f in ((self.est_log, f_log), (self.est_atanh, f_atanh)):
+            if not cols:
+                continue
+            if sorted(cols) == list(range(P)):
+                t = f(t)                          # every column: one contiguous pass
+            else:
+                t[..., list(cols)] = f(t[..., list(cols)])
         return t
 
+    def to_est(self, theta: np.ndarray) -> np.ndarray:
+        return self._apply(theta, np.log, np.arctanh)
+
     def from_est(self, theta: np.ndarray) -> np.ndarray:
-        t = np.array(theta, dtype=np.float64, copy=True)
-        if self.natural:
-            return t
-        if self.est_log:
-            t[..., list(self.est_log)] = np.exp(t[..., list(self.est_log)])
-        if self.est_atanh:
-            t[..., list(self.est_atanh)] = np.tanh(t[..., list(self.est_atanh)])
-        return t
+        return self._apply(theta, np.exp, np.tanh)
 
     def log_det_jac_from_est(self, theta_est: np.ndarray) -> np.ndarray:
         """log |det d from_est / d theta_est| (the change of variables a prior on

@@ -381,6 +381,14 @@ class RWSigma:
             return float(self._custom(nt, m, ntimes))
         return 1.0
 
+    def cooling_factors(self, ntimes: int, m: int) -> list:
+        """``cooling_factor(nt, m, ntimes)`` for nt = 0 .. ntimes-1, the same
+        float64 arithmetic with the loop-invariant parts taken out."""
+        if self.cooling_type == "geometric":
+            base = self.a ** (1.0 / 50.0)
+            return [base ** (nt / ntimes + m) for nt in range(ntimes)]
+        return [self.cooling_factor(nt, m, ntimes) for nt in range(ntimes)]
+
     def arrays(self, canonical_names: Sequence[str]):
         """(sigmas for per-step perturbation, sigmas for t0 only) in canonical order."""
         names = list(canonical_names)
