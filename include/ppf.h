@@ -54,8 +54,8 @@ enum { PPF_MODEL_LG = 1, PPF_MODEL_SV = 2, PPF_MODEL_RICKER = 3 };
 
 typedef struct ppf_model {
   int32_t kind;     /* PPF_MODEL_* */
-  int32_t dx;       /* state dimension (LG 1..4, SV 2, Ricker 1) */
-  int32_t dy;       /* observation dimension (LG 1..4, SV 1, Ricker 1) */
+  int32_t dx;       /* state dimension (LG 1..9, SV 2, Ricker 1) */
+  int32_t dy;       /* observation dimension (LG 1..9, SV 1, Ricker 1) */
   int32_t n_params; /* P, the canonical parameter count */
   float dt;         /* SV time step (1/252); ignored by the other models */
   int32_t reserved;

@@ -39,13 +39,19 @@
 
 typedef unsigned __int128 u128;
 
+/* LG dimensions up to 9 (pypomp/models/linear_gaussian.py:48 MAX_DIM): matrix
+ * row stride, and the largest parameter count (LG 9 x 9: 81 + 81 + 45 + 45 + 9). */
+#define LGS 9
+#define MAXP 261
+
 /* ------------------------------------------------------------------------ */
 /* Models (same formulas and operation order as the CUDA device code)       */
 /* ------------------------------------------------------------------------ */
 
 typedef struct {
   int kind, dx, dy;
-  float A[16], C[16], LQ[16], L[16], Linv[4], X0[4], c0, LR[16];  /* LG */
+  float A[LGS * LGS], C[LGS * LGS], LQ[LGS * LGS], L[LGS * LGS], Linv[LGS], X0[LGS], c0,
+        LR[LGS * LGS];  /* LG, row stride LGS */
   float kappa, theta, xi, rho, mu, v0, dt, sqdt, mudt, rhoc, svc0, kdt, xsq; /* SV */
   float r, sigma, phi, N0;                                         /* Ricker */
 } consts_t;
@@ -64,40 +70,40 @@ static void prepare(consts_t* c, const float* th, const ppf_model* m, int est) {
     int p = 0;
     float* LR = c->LR;
     for (int i = 0; i < dx; ++i)
-      for (int k = 0; k < dx; ++k) c->A[i * 4 + k] = th[p++];
+      for (int k = 0; k < dx; ++k) c->A[i * LGS + k] = th[p++];
     for (int i = 0; i < dy; ++i)
-      for (int k = 0; k < dx; ++k) c->C[i * 4 + k] = th[p++];
+      for (int k = 0; k < dx; ++k) c->C[i * LGS + k] = th[p++];
     for (int i = 0; i < dx; ++i)
       for (int k = 0; k <= i; ++k) {
         float v = th[p++];
         if (est && i == k) v = pp_expf(v);
-        c->LQ[i * 4 + k] = v;
+        c->LQ[i * LGS + k] = v;
       }
     for (int i = 0; i < dy; ++i)
       for (int k = 0; k <= i; ++k) {
         float v = th[p++];
         if (est && i == k) v = pp_expf(v);
-        LR[i * 4 + k] = v;
+        LR[i * LGS + k] = v;
       }
     for (int i = 0; i < dx; ++i) c->X0[i] = th[p++];
-    float R[16] = {0};
+    float R[LGS * LGS] = {0};
     for (int i = 0; i < dy; ++i)
       for (int k = 0; k <= i; ++k) {
         float s = 0.0f;
-        for (int l = 0; l <= k; ++l) s = s + LR[i * 4 + l] * LR[k * 4 + l];
-        R[i * 4 + k] = s;
+        for (int l = 0; l <= k; ++l) s = s + LR[i * LGS + l] * LR[k * LGS + l];
+        R[i * LGS + k] = s;
       }
     for (int i = 0; i < dy; ++i)
       for (int k = 0; k <= i; ++k) {
-        float s = R[i * 4 + k];
-        for (int l = 0; l < k; ++l) s = s - c->L[i * 4 + l] * c->L[k * 4 + l];
-        if (i == k) c->L[i * 4 + i] = sqrtf(s);
-        else c->L[i * 4 + k] = s / c->L[k * 4 + k];
+        float s = R[i * LGS + k];
+        for (int l = 0; l < k; ++l) s = s - c->L[i * LGS + l] * c->L[k * LGS + l];
+        if (i == k) c->L[i * LGS + i] = sqrtf(s);
+        else c->L[i * LGS + k] = s / c->L[k * LGS + k];
       }
     float c0 = -0.5f * (float)dy * LOG2PI_F;
     for (int i = 0; i < dy; ++i) {
-      c->Linv[i] = 1.0f / c->L[i * 4 + i];
-      c0 = c0 - pp_logf(c->L[i * 4 + i]);
+      c->Linv[i] = 1.0f / c->L[i * LGS + i];
+      c0 = c0 - pp_logf(c->L[i * LGS + i]);
     }
     c->c0 = c0;
   } else if (m->kind == PPF_MODEL_SV) {
@@ -129,7 +135,7 @@ static void rinit(const consts_t* c, const float* z, float* x) {
   if (c->kind == PPF_MODEL_LG) {
     for (int i = 0; i < c->dx; ++i) {
       float acc = c->X0[i];
-      for (int k = 0; k <= i; ++k) acc = fmaf(c->LQ[i * 4 + k], z[k], acc);
+      for (int k = 0; k <= i; ++k) acc = fmaf(c->LQ[i * LGS + k], z[k], acc);
       x[i] = acc;
     }
   } else if (c->kind == PPF_MODEL_SV) {
@@ -142,11 +148,11 @@ static void rinit(const consts_t* c, const float* z, float* x) {
 
 static void rproc(const consts_t* c, float* x, const float* z) {
   if (c->kind == PPF_MODEL_LG) {
-    float y[4];
+    float y[LGS];
     for (int i = 0; i < c->dx; ++i) {
       float acc = 0.0f;
-      for (int k = 0; k < c->dx; ++k) acc = fmaf(c->A[i * 4 + k], x[k], acc);
-      for (int k = 0; k <= i; ++k) acc = fmaf(c->LQ[i * 4 + k], z[k], acc);
+      for (int k = 0; k < c->dx; ++k) acc = fmaf(c->A[i * LGS + k], x[k], acc);
+      for (int k = 0; k <= i; ++k) acc = fmaf(c->LQ[i * LGS + k], z[k], acc);
       y[i] = acc;
     }
     for (int i = 0; i < c->dx; ++i) x[i] = y[i];
@@ -166,13 +172,13 @@ static void rproc(const consts_t* c, float* x, const float* z) {
 
 static float dmeas(const consts_t* c, const float* y, float ycon, const float* x) {
   if (c->kind == PPF_MODEL_LG) {
-    float s[4];
+    float s[LGS];
     float q = 0.0f;
     for (int i = 0; i < c->dy; ++i) {
       float a = 0.0f;
-      for (int k = 0; k < c->dx; ++k) a = fmaf(c->C[i * 4 + k], x[k], a);
+      for (int k = 0; k < c->dx; ++k) a = fmaf(c->C[i * LGS + k], x[k], a);
       float r = y[i] - a;
-      for (int l = 0; l < i; ++l) r = fmaf(-c->L[i * 4 + l], s[l], r);
+      for (int l = 0; l < i; ++l) r = fmaf(-c->L[i * LGS + l], s[l], r);
       s[i] = r * c->Linv[i];
       q = fmaf(s[i], s[i], q);
     }
@@ -213,7 +219,7 @@ static uint32_t uniform32(const ppf_pfilter_desc* d, int f, int t) {
 }
 
 static float propagate(const ppf_pfilter_desc* d, const consts_t* c, int f, int u, int j, int t, float* x) {
-  float z[4];
+  float z[LGS];
   noise(d, f, j, t + 1, n_step(c), z);
   rproc(c, x, z);
   const float* y = d->ys + ((size_t)u * d->T + t) * d->model.dy;
@@ -239,7 +245,7 @@ static void run_filter(const ppf_pfilter_desc* d, int f, int mop) {
   uint64_t* C = (uint64_t*)malloc(sizeof(uint64_t) * J);
   int* par = (int*)malloc(sizeof(int) * J);
   for (int j = 0; j < J; ++j) {
-    float z[4], xj[4];
+    float z[LGS], xj[LGS];
     noise(d, f, j, 0, n_init(&c), z);
     rinit(&c, z, xj);
     const float m = propagate(d, &c, f, u, j, 0, xj);
@@ -260,7 +266,7 @@ static void run_filter(const ppf_pfilter_desc* d, int f, int mop) {
     const int collapsed = !nanf && Mx == -INFINITY;
     const int qc = nanf || Mx == -INFINITY;
     uint64_t tot = 0;
-    double s2 = 0.0, fx[4] = {0, 0, 0, 0}, px[4] = {0, 0, 0, 0};
+    double s2 = 0.0, fx[LGS] = {0}, px[LGS] = {0};
     for (int j = 0; j < J; ++j) {
       uint64_t q;
       double e;
@@ -322,7 +328,7 @@ static void run_filter(const ppf_pfilter_desc* d, int f, int mop) {
       else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
     }
     for (int k = 0; k < J; ++k) {
-      float xk[4];
+      float xk[LGS];
       for (int q = 0; q < dx; ++q) xk[q] = x[q * J + par[k]];
       float b;
       if (rs) b = mop ? 0.0f : base_rs;
@@ -404,7 +410,7 @@ static int surrogate_impl(const ppf_pfilter_desc* d, float alpha, int pwi, const
     double* v = (double*)malloc(sizeof(double) * J);
     float* m = (float*)malloc(sizeof(float) * J);
     for (int j = 0; j < J; ++j) {
-      float z[4], xj[4];
+      float z[LGS], xj[LGS];
       noise(d, f, j, 0, n_init(&c), z);
       rinit(&c, z, xj);
       for (int k = 0; k < dx; ++k) x[k * J + j] = xj[k];
@@ -415,7 +421,7 @@ static int surrogate_impl(const ppf_pfilter_desc* d, float alpha, int pwi, const
       const size_t row = ((size_t)f * T + t) * J;
       for (int j = 0; j < J; ++j) {
         wP[j] = (double)alpha * wF[j];
-        float xj[4];
+        float xj[LGS];
         for (int k = 0; k < dx; ++k) xj[k] = x[k * J + j];
         m[j] = propagate(d, &c, f, u, j, t, xj);
         for (int k = 0; k < dx; ++k) xp[k * J + j] = xj[k];
@@ -498,12 +504,12 @@ static float if2_measure(float m) {
 static float if2_step(const ppf_perfilter_desc* d, int f, int u, int j, int t, int s, float cool,
                       float* th, float* x) {
   const int P = d->model.n_params;
-  float zp[64];
+  float zp[MAXP];
   if2_perturb_noise(d, f, j, s, P, zp);
   for (int p = 0; p < P; ++p) th[p] = th[p] + (cool * d->rw_sig[p]) * zp[p];
   consts_t c;
   prepare(&c, th, &d->model, !(d->flags & PPF_F_NATURAL));
-  float z[4];
+  float z[LGS];
   if2_noise(d, f, j, s, n_step(&c), z);
   rproc(&c, x, z);
   const float* y = d->ys + ((size_t)u * d->T + t) * d->model.dy;
@@ -529,7 +535,7 @@ static void run_perfilter(const ppf_perfilter_desc* d, int f) {
   int* par = (int*)malloc(sizeof(int) * J);
   const float* S = d->swarm_in + (size_t)f * P * J;
   for (int j = 0; j < J; ++j) {
-    float tj[64], zp[64], z[4], xj[4];
+    float tj[MAXP], zp[MAXP], z[LGS], xj[LGS];
     for (int p = 0; p < P; ++p) tj[p] = S[(size_t)p * J + j];
     if2_perturb_noise(d, f, j, 0, P, zp);
     for (int p = 0; p < P; ++p) tj[p] = tj[p] + (d->cool0[u] * d->rw_sig0[p]) * zp[p];
@@ -598,7 +604,7 @@ static void run_perfilter(const ppf_perfilter_desc* d, int f) {
       else if (!collapsed) lt32 = Mx + pp_logf((float)tot * 9.094947017729282e-13f);
     }
     for (int k = 0; k < J; ++k) {
-      float xk[4], tk[64];
+      float xk[LGS], tk[MAXP];
       for (int q = 0; q < dx; ++q) xk[q] = x[q * J + par[k]];
       for (int p = 0; p < P; ++p) tk[p] = th[(size_t)p * J + par[k]];
       float b;
@@ -630,7 +636,7 @@ static void* if2_worker(void* arg) {
 
 /* Runs the F perturbed filters of `d` (all pointers HOST memory). */
 int ppfo_perfilter(const ppf_perfilter_desc* d, int nthreads) {
-  if (!d || d->J < 1 || d->F < 1 || d->T < 1 || d->model.n_params > 64) return PPF_EINVAL;
+  if (!d || d->J < 1 || d->F < 1 || d->T < 1 || d->model.n_params > MAXP) return PPF_EINVAL;
   if (nthreads <= 1 || d->F == 1) {
     for (int f = 0; f < d->F; ++f) run_perfilter(d, f);
     return PPF_OK;
@@ -655,12 +661,12 @@ int ppfo_perfilter(const ppf_perfilter_desc* d, int nthreads) {
  * Ricker: Poisson(phi N)). */
 static void rmeas(const consts_t* c, const float* x, uint64_t seed, uint32_t k, uint32_t s, float* y) {
   if (c->kind == PPF_MODEL_LG) {
-    float w[4];
+    float w[LGS];
     pp_normals(seed, k, s, PPF_TAG_MEASURE, c->dy, w);
     for (int i = 0; i < c->dy; ++i) {
       float a = 0.0f;
-      for (int q = 0; q < c->dx; ++q) a = fmaf(c->C[i * 4 + q], x[q], a);
-      for (int l = 0; l <= i; ++l) a = fmaf(c->LR[i * 4 + l], w[l], a);
+      for (int q = 0; q < c->dx; ++q) a = fmaf(c->C[i * LGS + q], x[q], a);
+      for (int l = 0; l <= i; ++l) a = fmaf(c->LR[i * LGS + l], w[l], a);
       y[i] = a;
     }
   } else if (c->kind == PPF_MODEL_SV) {
@@ -688,7 +694,7 @@ int ppfo_simulate(const ppf_simulate_desc* d) {
     for (int k = 0; k < d->nsim; ++k) {
       float* X = d->X + ((size_t)f * d->nsim + k) * (size_t)(d->T + 1) * dx;
       float* Y = d->Y ? d->Y + ((size_t)f * d->nsim + k) * (size_t)d->T * dy : NULL;
-      float x[4], z[4];
+      float x[LGS], z[LGS];
       const int n0 = n_init(&c), n1 = n_step(&c);
       if (n0 > 0) pp_normals(seed, (uint32_t)k, 0u, PPF_TAG_PROCESS, n0, z);
       rinit(&c, z, x);

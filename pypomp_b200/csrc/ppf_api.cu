@@ -38,7 +38,7 @@ static size_t carve(Args& a, int path, unsigned char* base) {
     a.excl = reinterpret_cast<uint64_t*>(take(8ull * a.F * nt_alloc));
     a.tot = reinterpret_cast<uint64_t*>(take(8ull * a.F));
     a.ctrl_bytes = off;
-    a.consts = take(512ull * a.F);
+    a.consts = take((lg_wide(a.model) ? 2048ull : 512ull) * a.F);
     // per-thread run prefixes: ntiles x threads per tile, the largest over the tile configurations
     const size_t J = (size_t)a.J;
     const size_t nrun = std::max({(J + kTileLarge - 1) / kTileLarge * 256, (J + kTileMid - 1) / kTileMid * 128,
@@ -77,7 +77,7 @@ static int n_params_of(const ppf_model& m) {
 static int check_model(const ppf_model& m) {
   switch (m.kind) {
     case PPF_MODEL_LG:
-      if (m.dx < 1 || m.dx > 4 || m.dy < 1 || m.dy > 4) return PPF_EUNSUPPORTED;
+      if (m.dx < 1 || m.dx > 9 || m.dy < 1 || m.dy > 9) return PPF_EINVAL;   // linear_gaussian.py:48 MAX_DIM
       break;
     case PPF_MODEL_SV:
       if (m.dx != 2 || m.dy != 1 || !(m.dt > 0.0f)) return PPF_EINVAL;
@@ -95,6 +95,8 @@ static int choose_path(const ppf_pfilter_desc* d) {
   if (d->path != PPF_PATH_AUTO) return d->path;
   Args a{};
   a.J = d->J; a.F = d->F; a.flags = d->flags; a.model = d->model; a.mode = MODE_PF;
+  // the wide LG streams only
+  if (lg_wide(d->model)) return PPF_PATH_STREAM;
   // swarm fits one CTA's shared memory: keep it on chip for the whole loop
   const bool resident = resident_smem_bytes(a) <= kResidentSmemMax && d->J <= 16384;
   if (resident && d->F >= kNumSMs) return PPF_PATH_RESIDENT;
@@ -141,6 +143,7 @@ static void tune_store(const ppf_model& m, int J, int F, int U, int inj, int til
 }
 
 static int choose_tile(const ppf_model& m, int J, int F, int U, int inj, int requested) {
+  if (lg_wide(m)) return kTileSmall;   // the wide LG has one tile configuration
   if (requested == kTileLarge || requested == kTileMid || requested == kTileSmall) return requested;
   const int tuned = tune_lookup(m, J, F, U, inj);
   if (tuned) return tuned;
@@ -225,10 +228,10 @@ static size_t carve_mop(Args& a, MopWork& w, const ppf_mop_desc* d, unsigned cha
   a.mop_S = reinterpret_cast<double*>(take(8 * F * T));
   w.sb = reinterpret_cast<float*>(take(4 * F * L * dx * J));
   w.sb2 = reinterpret_cast<float*>(take(4 * F * L * dx * J));
-  w.gpart = reinterpret_cast<double*>(take(8 * 64 * F * ((J + 255) / 256)));
+  w.gpart = reinterpret_cast<double*>(take(8 * kMaxNG * F * ((J + 255) / 256)));
   w.lx = reinterpret_cast<float*>(take(4 * 2 * F * dx * J));
   w.lw = reinterpret_cast<float*>(take(4 * 2 * F * J));
-  w.gnat = reinterpret_cast<double*>(take(8 * F * 64));
+  w.gnat = reinterpret_cast<double*>(take(8 * F * kMaxNG));
   a.slotw = reinterpret_cast<uint64_t*>(take(8ull * 6 * kInboxWords));
   return off;
 }

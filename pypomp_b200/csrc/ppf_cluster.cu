@@ -208,8 +208,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     acc.nan = 0u;
     acc.pad = 0u;
     acc.s2 = 0.0;
-    acc.pad2 = 0.0;
-    for (int d = 0; d < 4; ++d) { acc.fx[d] = 0.0; acc.px[d] = 0.0; }
+    for (int d = 0; d < kMaxDim; ++d) { acc.fx[d] = 0.0; acc.px[d] = 0.0; }
     for (int r = 0; r < NC; ++r) {
       acc.maxkey = max(acc.maxkey, slots[r].maxkey);
       acc.minkey = min(acc.minkey, slots[r].minkey);
@@ -499,14 +498,9 @@ static bool fits_m(const Args& a) {
 template <bool IF2>
 static bool fits_any(const Args& a) {
   switch (a.model.kind) {
-    case PPF_MODEL_LG:
-      switch (a.model.dx) {
-        case 1: return a.model.dy == 1 ? fits_m<LG<1, 1>, IF2>(a) : fits_m<LG<1>, IF2>(a);
-        case 2: return a.model.dy == 2 ? fits_m<LG<2, 2>, IF2>(a) : fits_m<LG<2>, IF2>(a);
-        case 3: return a.model.dy == 3 ? fits_m<LG<3, 3>, IF2>(a) : fits_m<LG<3>, IF2>(a);
-        case 4: return a.model.dy == 4 ? fits_m<LG<4, 4>, IF2>(a) : fits_m<LG<4>, IF2>(a);
-        default: return false;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<bool>(a.model, false, false,
+                           [&](auto tg) { return fits_m<typename decltype(tg)::type, IF2>(a); });
     case PPF_MODEL_SV: return fits_m<SV, IF2>(a);
     case PPF_MODEL_RICKER: return fits_m<Ricker, IF2>(a);
     default: return false;
@@ -516,14 +510,9 @@ static bool fits_any(const Args& a) {
 template <bool IF2>
 static int run_any(Args& a, cudaStream_t s) {
   switch (a.model.kind) {
-    case PPF_MODEL_LG:
-      switch (a.model.dx) {
-        case 1: return a.model.dy == 1 ? run_cluster_m<LG<1, 1>, IF2>(a, s) : run_cluster_m<LG<1>, IF2>(a, s);
-        case 2: return a.model.dy == 2 ? run_cluster_m<LG<2, 2>, IF2>(a, s) : run_cluster_m<LG<2>, IF2>(a, s);
-        case 3: return a.model.dy == 3 ? run_cluster_m<LG<3, 3>, IF2>(a, s) : run_cluster_m<LG<3>, IF2>(a, s);
-        case 4: return a.model.dy == 4 ? run_cluster_m<LG<4, 4>, IF2>(a, s) : run_cluster_m<LG<4>, IF2>(a, s);
-        default: return PPF_EUNSUPPORTED;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<int>(a.model, false, PPF_EUNSUPPORTED,
+                          [&](auto tg) { return run_cluster_m<typename decltype(tg)::type, IF2>(a, s); });
     case PPF_MODEL_SV: return run_cluster_m<SV, IF2>(a, s);
     case PPF_MODEL_RICKER: return run_cluster_m<Ricker, IF2>(a, s);
     default: return PPF_EINVAL;

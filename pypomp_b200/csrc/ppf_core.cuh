@@ -22,14 +22,14 @@ constexpr long long kSpinCap = 1ll << 22;          // bounded waits: then PPF_ET
                                                    // (ppf_debug_set_wait_limit lowers it per call)
 
 // Per-filter, per-step accumulators (double-buffered by step parity).
+constexpr int kMaxDim = 9;                          // largest state dimension (LG 9 x 9)
 struct Acc {
   unsigned int maxkey, minkey, nan, pad;
-  double s2;        // sum e^2 (ESS)
-  double fx[4];     // sum x e (filter mean)
-  double px[4];     // sum x (prediction mean)
-  double pad2;
+  double s2;              // sum e^2 (ESS)
+  double fx[kMaxDim];     // sum x e (filter mean)
+  double px[kMaxDim];     // sum x (prediction mean)
 };
-static_assert(sizeof(Acc) == 96, "Acc layout");
+static_assert(sizeof(Acc) == 168, "Acc layout");
 
 __device__ __forceinline__ unsigned int fkey(float f) {
   const unsigned int b = __float_as_uint(f);

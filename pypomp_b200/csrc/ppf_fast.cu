@@ -84,14 +84,9 @@ static int run_fast_m(Args& a, cudaStream_t s) {
 
 int run_stream_fast(Args& a, cudaStream_t s) {
   switch (a.model.kind) {
-    case PPF_MODEL_LG:
-      switch (a.model.dx) {
-        case 1: return a.model.dy == 1 ? run_fast_m<LG<1, 1>>(a, s) : run_fast_m<LG<1>>(a, s);
-        case 2: return a.model.dy == 2 ? run_fast_m<LG<2, 2>>(a, s) : run_fast_m<LG<2>>(a, s);
-        case 3: return a.model.dy == 3 ? run_fast_m<LG<3, 3>>(a, s) : run_fast_m<LG<3>>(a, s);
-        case 4: return a.model.dy == 4 ? run_fast_m<LG<4, 4>>(a, s) : run_fast_m<LG<4>>(a, s);
-        default: return PPF_EUNSUPPORTED;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<int>(a.model, false, PPF_EUNSUPPORTED,
+                          [&](auto tg) { return run_fast_m<typename decltype(tg)::type>(a, s); });
     case PPF_MODEL_SV: return run_fast_m<SV>(a, s);
     case PPF_MODEL_RICKER: return run_fast_m<Ricker>(a, s);
     default: return PPF_EINVAL;

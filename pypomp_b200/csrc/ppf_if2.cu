@@ -242,7 +242,14 @@ int run_if2_tiled(Args& a, cudaStream_t s) {
 
 template <class M>
 int run_if2_m(Args& a, cudaStream_t s) {
-  return (a.flags & PPF_F_INJECT) ? run_if2_tiled<M, true>(a, s) : run_if2_tiled<M, false>(a, s);
+  if constexpr (M::WIDE) {
+    // the wide LG: Philox draws, 256-particle tiles (the per-thread parameter
+    // rows of up to 261 entries fit shared memory only with 64 threads)
+    if (a.flags & PPF_F_INJECT) return PPF_EUNSUPPORTED;
+    return a.tile == kTileSmall ? run_if2_t<M, 64, 4, false>(a, s) : PPF_EINTERNAL;
+  } else {
+    return (a.flags & PPF_F_INJECT) ? run_if2_tiled<M, true>(a, s) : run_if2_tiled<M, false>(a, s);
+  }
 }
 
 int run_if2(Args& a, cudaStream_t s) {
@@ -259,14 +266,9 @@ int run_if2(Args& a, cudaStream_t s) {
     if (rc != PPF_EUNSUPPORTED) return rc;
   }
   switch (a.model.kind) {
-    case PPF_MODEL_LG:
-      switch (a.model.dx) {
-        case 1: return a.model.dy == 1 ? run_if2_m<LG<1, 1>>(a, s) : run_if2_m<LG<1>>(a, s);
-        case 2: return a.model.dy == 2 ? run_if2_m<LG<2, 2>>(a, s) : run_if2_m<LG<2>>(a, s);
-        case 3: return a.model.dy == 3 ? run_if2_m<LG<3, 3>>(a, s) : run_if2_m<LG<3>>(a, s);
-        case 4: return a.model.dy == 4 ? run_if2_m<LG<4, 4>>(a, s) : run_if2_m<LG<4>>(a, s);
-        default: return PPF_EUNSUPPORTED;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<int>(a.model, true, PPF_EUNSUPPORTED,
+                          [&](auto tg) { return run_if2_m<typename decltype(tg)::type>(a, s); });
     case PPF_MODEL_SV: return run_if2_m<SV>(a, s);
     case PPF_MODEL_RICKER: return run_if2_m<Ricker>(a, s);
     default: return PPF_EINVAL;

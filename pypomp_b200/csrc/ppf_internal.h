@@ -126,6 +126,11 @@ constexpr int kTileLarge = 2048;   // 256 threads x 8
 constexpr int kTileMid = 512;      // 128 threads x 4
 constexpr int kTileSmall = 256;    // 64 threads x 4
 constexpr int kNumSMs = 148;
+// the wide LG instantiations (dx or dy above 4, up to 9)
+inline bool lg_wide(const ppf_model& m) { return m.kind == PPF_MODEL_LG && (m.dx > 4 || m.dy > 4); }
+// natural-scale gradient entries per filter in the MOP workspace: the padded
+// layout of the largest model, LG 9 x 9 (81 + 81 + 45 + 45 + 9 = 261)
+constexpr int kMaxNG = 264;
 // CTAs of a grid-resident launch that publish per-step words (8 per SM)
 constexpr int kMaxGridSlots = 8 * kNumSMs;
 // words of one inbox array of the grid-resident MOP forward: F x C x C for F

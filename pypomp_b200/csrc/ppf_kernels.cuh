@@ -287,22 +287,22 @@ __device__ __forceinline__ int find_parent(const int* st, int n, int k) {
 
 // Per-filter model constants, computed once per call (Cholesky factors, log
 // determinants, transformed parameters) and copied by every block.
-constexpr int kConstStride = 512;   // bytes per filter in the workspace
-
+// Bytes per filter in the workspace: M::CONST_BYTES (512, or 2048 for the
+// wide LG); the workspace reserves const_bytes(model) per filter.
 template <class M>
 __global__ void k_prep(Args a) {
-  static_assert(sizeof(typename M::Consts) <= kConstStride, "Consts stride");
+  static_assert(sizeof(typename M::Consts) <= M::CONST_BYTES, "Consts stride");
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= a.F) return;
   typename M::Consts c;
   M::prepare(c, a.theta + (size_t)f * a.model.n_params, a.model, (a.flags & PPF_F_EST) != 0);
-  *reinterpret_cast<typename M::Consts*>(a.consts + (size_t)f * kConstStride) = c;
+  *reinterpret_cast<typename M::Consts*>(a.consts + (size_t)f * M::CONST_BYTES) = c;
 }
 
 template <class M>
 __device__ __forceinline__ void load_consts(const Args& a, int f, typename M::Consts& c) {
   constexpr int NW = (sizeof(typename M::Consts) + 3) / 4;
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(a.consts + (size_t)f * kConstStride);
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(a.consts + (size_t)f * M::CONST_BYTES);
   uint32_t* dst = reinterpret_cast<uint32_t*>(&c);
   for (int i = threadIdx.x; i < NW; i += blockDim.x) dst[i] = src[i];
 }
@@ -432,7 +432,7 @@ __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
     Acc* nx = a.acc[p ^ 1] + f;
     nx->maxkey = 0u; nx->minkey = 0xffffffffu; nx->nan = 0u;
     nx->s2 = 0.0;
-    for (int d = 0; d < 4; ++d) { nx->fx[d] = 0.0; nx->px[d] = 0.0; }
+    for (int d = 0; d < kMaxDim; ++d) { nx->fx[d] = 0.0; nx->px[d] = 0.0; }
   }
   const bool nanf = acc.nan != 0;
   const float Mx = keyf(acc.maxkey);

@@ -23,27 +23,32 @@
 namespace ppf {
 
 // ---------------------------------------------------------------------------
-// Linear Gaussian (dx, dy <= 4).  Parameter order as LG's canonical names:
-// A (row-major dx*dx), C (row-major dy*dx), lower triangle of chol(Q)
-// row-major, lower triangle of chol(R) row-major, X0 (dx).
+// Linear Gaussian (dx, dy <= 9, pypomp/models/linear_gaussian.py:48 MAX_DIM).
+// Parameter order as LG's canonical names: A (row-major dx*dx), C (row-major
+// dy*dx), lower triangle of chol(Q) row-major, lower triangle of chol(R)
+// row-major, X0 (dx).
 // ---------------------------------------------------------------------------
 // DYS > 0 fixes the observation dimension at compile time (the dispatch uses
-// it for dy == dx): the measurement loops become static and the model
-// constants stay in registers.  DYS == 0 reads dy (<= 4) at run time.
-template <int DX, int DYS = 0>
+// it for dy == dx <= 4): the measurement loops become static and the model
+// constants stay in registers.  DYS == 0 reads dy (<= MDY) at run time.  The
+// matrices are stored with row stride S: 4 for the models up to 4 x 4, 9 for
+// the wide ones (dx or dy above 4), whose constant block is 2 KB.
+template <int DX, int DYS = 0, int MDY = 4>
 struct LG {
   static constexpr int kind = PPF_MODEL_LG;
   static constexpr int MAXDX = DX;     // state dimension, fixed per instantiation
   static constexpr int NZ = DX;        // process normals per particle-step
   static constexpr int NZ0 = DX;       // initial-state normals per particle
-  static constexpr int MAXDY = DYS > 0 ? DYS : 4;
-  static constexpr int MAXP = DYS > 0 ? DX * DX + DYS * DX + DX * (DX + 1) / 2 + DYS * (DYS + 1) / 2 + DX
-                                      : DX * DX + 4 * DX + DX * (DX + 1) / 2 + 10 + DX;  // dy <= 4
+  static constexpr int MAXDY = DYS > 0 ? DYS : MDY;
+  static constexpr bool WIDE = (DX > 4 || MAXDY > 4);
+  static constexpr int S = WIDE ? 9 : 4;                      // row stride of the matrices
+  static constexpr int CONST_BYTES = WIDE ? 2048 : 512;       // workspace bytes per filter
+  static constexpr int MAXP = DX * DX + MAXDY * DX + DX * (DX + 1) / 2 + MAXDY * (MAXDY + 1) / 2 + DX;
   struct Consts {
     int dx, dy;
-    float A[16], C[16], LQ[16], L[16], Linv[4], X0[4];
+    float A[S * S], C[S * S], LQ[S * S], L[S * S], Linv[S], X0[S];
     float c0;
-    float LR[16];   // the parameter factor of R, as rmeas draws with it
+    float LR[S * S];   // the parameter factor of R, as rmeas draws with it
   };
   __device__ static __forceinline__ int ndy(const Consts& c) { return DYS > 0 ? DYS : c.dy; }
   __device__ static void prepare(Consts& c, const float* th, const ppf_model& m, bool est) {
@@ -51,43 +56,43 @@ struct LG {
     c.dx = dx; c.dy = dy;
     int p = 0;
     for (int i = 0; i < dx; ++i)
-      for (int k = 0; k < dx; ++k) c.A[i * 4 + k] = th[p++];
+      for (int k = 0; k < dx; ++k) c.A[i * S + k] = th[p++];
     for (int i = 0; i < dy; ++i)
-      for (int k = 0; k < dx; ++k) c.C[i * 4 + k] = th[p++];
+      for (int k = 0; k < dx; ++k) c.C[i * S + k] = th[p++];
     float* LR = c.LR;
-    for (int i = 0; i < 16; ++i) { c.LQ[i] = 0.0f; LR[i] = 0.0f; c.L[i] = 0.0f; }
+    for (int i = 0; i < S * S; ++i) { c.LQ[i] = 0.0f; LR[i] = 0.0f; c.L[i] = 0.0f; }
     for (int i = 0; i < dx; ++i)
       for (int k = 0; k <= i; ++k) {
         float v = th[p++];
         if (est && i == k) v = pp_expf(v);
-        c.LQ[i * 4 + k] = v;
+        c.LQ[i * S + k] = v;
       }
     for (int i = 0; i < dy; ++i)
       for (int k = 0; k <= i; ++k) {
         float v = th[p++];
         if (est && i == k) v = pp_expf(v);
-        LR[i * 4 + k] = v;
+        LR[i * S + k] = v;
       }
     for (int i = 0; i < dx; ++i) c.X0[i] = th[p++];
     // R = LR LR^T, then its Cholesky factor (as multivariate_normal.logpdf does).
-    float R[16];
+    float R[S * S];
     for (int i = 0; i < dy; ++i)
       for (int k = 0; k <= i; ++k) {
         float s = 0.0f;
-        for (int l = 0; l <= k; ++l) s = s + LR[i * 4 + l] * LR[k * 4 + l];
-        R[i * 4 + k] = s;
+        for (int l = 0; l <= k; ++l) s = s + LR[i * S + l] * LR[k * S + l];
+        R[i * S + k] = s;
       }
     for (int i = 0; i < dy; ++i)
       for (int k = 0; k <= i; ++k) {
-        float s = R[i * 4 + k];
-        for (int l = 0; l < k; ++l) s = s - c.L[i * 4 + l] * c.L[k * 4 + l];
-        if (i == k) c.L[i * 4 + i] = sqrtf(s);
-        else c.L[i * 4 + k] = s / c.L[k * 4 + k];
+        float s = R[i * S + k];
+        for (int l = 0; l < k; ++l) s = s - c.L[i * S + l] * c.L[k * S + l];
+        if (i == k) c.L[i * S + i] = sqrtf(s);
+        else c.L[i * S + k] = s / c.L[k * S + k];
       }
     float c0 = -0.5f * (float)dy * PPF_LOG2PI_F;
     for (int i = 0; i < dy; ++i) {
-      c.Linv[i] = 1.0f / c.L[i * 4 + i];
-      c0 = c0 - pp_logf(c.L[i * 4 + i]);
+      c.Linv[i] = 1.0f / c.L[i * S + i];
+      c0 = c0 - pp_logf(c.L[i * S + i]);
     }
     c.c0 = c0;
   }
@@ -97,7 +102,7 @@ struct LG {
     for (int i = 0; i < DX; ++i) {
       float acc = c.X0[i];
 #pragma unroll
-      for (int k = 0; k <= i; ++k) acc = pp_fma(c.LQ[i * 4 + k], z[k], acc);
+      for (int k = 0; k <= i; ++k) acc = pp_fma(c.LQ[i * S + k], z[k], acc);
       x[i] = acc;
     }
   }
@@ -108,9 +113,9 @@ struct LG {
     for (int i = 0; i < DX; ++i) {
       float acc = 0.0f;
 #pragma unroll
-      for (int k = 0; k < DX; ++k) acc = pp_fma(c.A[i * 4 + k], x[k], acc);
+      for (int k = 0; k < DX; ++k) acc = pp_fma(c.A[i * S + k], x[k], acc);
 #pragma unroll
-      for (int k = 0; k <= i; ++k) acc = pp_fma(c.LQ[i * 4 + k], z[k], acc);
+      for (int k = 0; k <= i; ++k) acc = pp_fma(c.LQ[i * S + k], z[k], acc);
       y[i] = acc;
     }
 #pragma unroll
@@ -125,10 +130,10 @@ struct LG {
       if (i < ndy(c)) {
         float a = 0.0f;
 #pragma unroll
-        for (int k = 0; k < DX; ++k) a = pp_fma(c.C[i * 4 + k], x[k], a);
+        for (int k = 0; k < DX; ++k) a = pp_fma(c.C[i * S + k], x[k], a);
         float r = y[i] - a;
 #pragma unroll
-        for (int l = 0; l < i; ++l) r = pp_fma(-c.L[i * 4 + l], s[l], r);
+        for (int l = 0; l < i; ++l) r = pp_fma(-c.L[i * S + l], s[l], r);
         s[i] = r * c.Linv[i];
         q = pp_fma(s[i], s[i], q);
       }
@@ -145,9 +150,9 @@ struct LG {
       if (i < ndy(c)) {
         float a = 0.0f;
 #pragma unroll
-        for (int q = 0; q < DX; ++q) a = pp_fma(c.C[i * 4 + q], x[q], a);
+        for (int q = 0; q < DX; ++q) a = pp_fma(c.C[i * S + q], x[q], a);
 #pragma unroll
-        for (int l = 0; l <= i; ++l) a = pp_fma(c.LR[i * 4 + l], w[l], a);
+        for (int l = 0; l <= i; ++l) a = pp_fma(c.LR[i * S + l], w[l], a);
         y[i] = a;
       }
     }
@@ -160,10 +165,11 @@ struct LG {
   }
 
   // ---- adjoint (MOP-alpha gradient).  Natural-scale gradient in a padded
-  // layout with static indices: A[DX*DX] | C[4*DX] | LQ tril(DX) | LR tril(4)
-  // | X0[DX]; the host maps it to the canonical order.
+  // layout with static indices: A[DX*DX] | C[MAXDY*DX] | LQ tril(DX) |
+  // LR tril(MAXDY) | X0[DX]; the host maps it to the canonical order.
   static constexpr int NQ = DX * (DX + 1) / 2;
-  static constexpr int GA = 0, GC = DX * DX, GQ = GC + 4 * DX, GR = GQ + NQ, GX0 = GR + 10;
+  static constexpr int GA = 0, GC = DX * DX, GQ = GC + MAXDY * DX, GR = GQ + NQ,
+                       GX0 = GR + MAXDY * (MAXDY + 1) / 2;
   static constexpr int NG = GX0 + DX;
   struct Keep {
     float xP[DX];
@@ -181,10 +187,10 @@ struct LG {
       if (i < ndy(c)) {
         float a = 0.0f;
 #pragma unroll
-        for (int kk = 0; kk < DX; ++kk) a = pp_fma(c.C[i * 4 + kk], k.xP[kk], a);
+        for (int kk = 0; kk < DX; ++kk) a = pp_fma(c.C[i * S + kk], k.xP[kk], a);
         float r = y[i] - a;
 #pragma unroll
-        for (int l = 0; l < i; ++l) r = pp_fma(-c.L[i * 4 + l], k.s[l], r);
+        for (int l = 0; l < i; ++l) r = pp_fma(-c.L[i * S + l], k.s[l], r);
         k.s[i] = r * c.Linv[i];
         q = pp_fma(k.s[i], k.s[i], q);
       }
@@ -203,7 +209,7 @@ struct LG {
         float r = k.s[i];
 #pragma unroll
         for (int l = i + 1; l < MAXDY; ++l)
-          if (l < ndy(c)) r = r - c.L[l * 4 + i] * v[l];
+          if (l < ndy(c)) r = r - c.L[l * S + i] * v[l];
         v[i] = r * c.Linv[i];
       }
     }
@@ -213,7 +219,7 @@ struct LG {
       float a = lx[kk];
 #pragma unroll
       for (int i = 0; i < MAXDY; ++i)
-        if (i < ndy(c)) a = a + lm * c.C[i * 4 + kk] * v[i];
+        if (i < ndy(c)) a = a + lm * c.C[i * S + kk] * v[i];
       lxP[kk] = a;
     }
 #pragma unroll
@@ -236,7 +242,7 @@ struct LG {
     for (int kk = 0; kk < DX; ++kk) {
       float a = 0.0f;
 #pragma unroll
-      for (int i = 0; i < DX; ++i) a = a + c.A[i * 4 + kk] * lxP[i];
+      for (int i = 0; i < DX; ++i) a = a + c.A[i * S + kk] * lxP[i];
       lx[kk] = a;
     }
   }
@@ -268,6 +274,8 @@ struct SV {
   static constexpr int NZ = 1;
   static constexpr int NZ0 = 0;
   static constexpr int MAXDY = 1;
+  static constexpr bool WIDE = false;
+  static constexpr int CONST_BYTES = 512;
   static constexpr int MAXP = 6;
   struct Consts {
     int dx, dy;
@@ -383,6 +391,8 @@ struct Ricker {
   static constexpr int NZ = 1;
   static constexpr int NZ0 = 0;
   static constexpr int MAXDY = 1;
+  static constexpr bool WIDE = false;
+  static constexpr int CONST_BYTES = 512;
   static constexpr int MAXP = 4;
   struct Consts {
     int dx, dy;
@@ -457,5 +467,43 @@ struct Ricker {
     g[3] += lx0[0];
   }
 };
+
+// ---------------------------------------------------------------------------
+// Model dispatch for LG: fn(Tag<M>{}) with M the instantiation for the
+// model's dimensions -- compile-time dy for dx == dy <= 4, run-time dy <= 4
+// otherwise up to 4 x 4, and the wide model (stride 9, run-time dy <= 9)
+// when dx or dy is above 4.  Returns `none` when no instantiation applies
+// (dimensions out of range, or a wide model where `wide` is false).
+// ---------------------------------------------------------------------------
+template <class M>
+struct Tag {
+  using type = M;
+};
+
+template <class R, class Fn>
+R with_lg(const ppf_model& m, bool wide, R none, Fn&& fn) {
+  if (m.dx <= 4 && m.dy <= 4) {
+    switch (m.dx) {
+      case 1: return m.dy == 1 ? fn(Tag<LG<1, 1>>{}) : fn(Tag<LG<1>>{});
+      case 2: return m.dy == 2 ? fn(Tag<LG<2, 2>>{}) : fn(Tag<LG<2>>{});
+      case 3: return m.dy == 3 ? fn(Tag<LG<3, 3>>{}) : fn(Tag<LG<3>>{});
+      case 4: return m.dy == 4 ? fn(Tag<LG<4, 4>>{}) : fn(Tag<LG<4>>{});
+      default: return none;
+    }
+  }
+  if (!wide || m.dy < 1 || m.dy > 9) return none;
+  switch (m.dx) {
+    case 1: return fn(Tag<LG<1, 0, 9>>{});
+    case 2: return fn(Tag<LG<2, 0, 9>>{});
+    case 3: return fn(Tag<LG<3, 0, 9>>{});
+    case 4: return fn(Tag<LG<4, 0, 9>>{});
+    case 5: return fn(Tag<LG<5, 0, 9>>{});
+    case 6: return fn(Tag<LG<6, 0, 9>>{});
+    case 7: return fn(Tag<LG<7, 0, 9>>{});
+    case 8: return fn(Tag<LG<8, 0, 9>>{});
+    case 9: return fn(Tag<LG<9, 0, 9>>{});
+    default: return none;
+  }
+}
 
 }  // namespace ppf

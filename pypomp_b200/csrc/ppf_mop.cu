@@ -37,7 +37,7 @@
 
 namespace ppf {
 
-constexpr int kMaxNG = 64;
+
 
 struct MopBwd {
   const float* xin;    // x^F_{t-1} of filter 0: [DX][J], filter stride xin_fs
@@ -203,30 +203,31 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_init(Args a, MopBwd mb) {
 template <class M>
 struct Chain;
 
-template <int DX, int DYS>
-struct Chain<LG<DX, DYS>> {
+template <int DX, int DYS, int MDY>
+struct Chain<LG<DX, DYS, MDY>> {
+  using L = LG<DX, DYS, MDY>;
   __device__ static double map(const ppf_model& m, const float* th, const double* gn, int p, bool est) {
     const int dy = m.dy;
     const int nA = DX * DX, nC = dy * DX, nQ = DX * (DX + 1) / 2, nR = dy * (dy + 1) / 2;
-    if (p < nA) return gn[LG<DX, DYS>::GA + p];
+    if (p < nA) return gn[L::GA + p];
     p -= nA;
-    if (p < nC) return gn[LG<DX, DYS>::GC + p];
+    if (p < nC) return gn[L::GC + p];
     p -= nC;
     if (p < nQ) {
-      double v = gn[LG<DX, DYS>::GQ + p];
+      double v = gn[L::GQ + p];
       for (int i = 0; i < DX; ++i)
         if (est && p == i * (i + 1) / 2 + i) v *= (double)pp_expf(th[nA + nC + p]);
       return v;
     }
     p -= nQ;
     if (p < nR) {
-      double v = gn[LG<DX, DYS>::GR + p];
+      double v = gn[L::GR + p];
       for (int i = 0; i < dy; ++i)
         if (est && p == i * (i + 1) / 2 + i) v *= (double)pp_expf(th[nA + nC + nQ + p]);
       return v;
     }
     p -= nR;
-    return gn[LG<DX, DYS>::GX0 + p];
+    return gn[L::GX0 + p];
   }
 };
 template <>
@@ -1254,18 +1255,26 @@ int mop_backward(Args& a, const MopWork& w, cudaStream_t s) {
 template <class M>
 int run_mop_backward_model(Args& a, const MopWork& w, cudaStream_t s) {
   const bool inj = (a.flags & PPF_F_INJECT) != 0;
-  if (want_persist(a)) {
-    const int rc = inj ? mop_backward_persist_t<M, true>(a, w, s) : mop_backward_persist_t<M, false>(a, w, s);
-    if (rc != PPF_EUNSUPPORTED) return rc;
+  if constexpr (M::WIDE) {
+    // the wide LG: per-step adjoint launches, Philox draws
+    if (inj) return PPF_EUNSUPPORTED;
+    return mop_backward<M, false>(a, w, s);
+  } else {
+    if (want_persist(a)) {
+      const int rc = inj ? mop_backward_persist_t<M, true>(a, w, s) : mop_backward_persist_t<M, false>(a, w, s);
+      if (rc != PPF_EUNSUPPORTED) return rc;
+    }
+    return inj ? mop_backward<M, true>(a, w, s) : mop_backward<M, false>(a, w, s);
   }
-  return inj ? mop_backward<M, true>(a, w, s) : mop_backward<M, false>(a, w, s);
 }
 
 template <class M>
 int run_mop_model(Args& a, const MopWork& w, cudaStream_t s) {
   const bool inj = (a.flags & PPF_F_INJECT) != 0;
   int rc = PPF_EUNSUPPORTED;
-  if (want_persist(a)) rc = inj ? mop_forward_persist<M, true>(a, s) : mop_forward_persist<M, false>(a, s);
+  if constexpr (!M::WIDE) {
+    if (want_persist(a)) rc = inj ? mop_forward_persist<M, true>(a, s) : mop_forward_persist<M, false>(a, s);
+  }
   if (rc == PPF_EUNSUPPORTED) rc = run_stream_any(a, s);
   if (rc || !w.grad) return rc;
   return run_mop_backward_model<M>(a, w, s);
@@ -1273,14 +1282,9 @@ int run_mop_model(Args& a, const MopWork& w, cudaStream_t s) {
 
 int run_mop(Args& a, const MopWork& w, cudaStream_t s) {
   switch (a.model.kind) {
-    case PPF_MODEL_LG:
-      switch (a.model.dx) {
-        case 1: return a.model.dy == 1 ? run_mop_model<LG<1, 1>>(a, w, s) : run_mop_model<LG<1>>(a, w, s);
-        case 2: return a.model.dy == 2 ? run_mop_model<LG<2, 2>>(a, w, s) : run_mop_model<LG<2>>(a, w, s);
-        case 3: return a.model.dy == 3 ? run_mop_model<LG<3, 3>>(a, w, s) : run_mop_model<LG<3>>(a, w, s);
-        case 4: return a.model.dy == 4 ? run_mop_model<LG<4, 4>>(a, w, s) : run_mop_model<LG<4>>(a, w, s);
-        default: return PPF_EUNSUPPORTED;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<int>(a.model, true, PPF_EUNSUPPORTED,
+                          [&](auto tg) { return run_mop_model<typename decltype(tg)::type>(a, w, s); });
     case PPF_MODEL_SV: return run_mop_model<SV>(a, w, s);
     case PPF_MODEL_RICKER: return run_mop_model<Ricker>(a, w, s);
     default: return PPF_EINVAL;
@@ -1291,14 +1295,10 @@ int run_mop(Args& a, const MopWork& w, cudaStream_t s) {
 
 int run_mop_backward(Args& a, const MopWork& w, cudaStream_t s) {
   switch (a.model.kind) {
-    case PPF_MODEL_LG:
-      switch (a.model.dx) {
-        case 1: return a.model.dy == 1 ? run_mop_backward_model<LG<1, 1>>(a, w, s) : run_mop_backward_model<LG<1>>(a, w, s);
-        case 2: return a.model.dy == 2 ? run_mop_backward_model<LG<2, 2>>(a, w, s) : run_mop_backward_model<LG<2>>(a, w, s);
-        case 3: return a.model.dy == 3 ? run_mop_backward_model<LG<3, 3>>(a, w, s) : run_mop_backward_model<LG<3>>(a, w, s);
-        case 4: return a.model.dy == 4 ? run_mop_backward_model<LG<4, 4>>(a, w, s) : run_mop_backward_model<LG<4>>(a, w, s);
-        default: return PPF_EUNSUPPORTED;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<int>(a.model, true, PPF_EUNSUPPORTED, [&](auto tg) {
+        return run_mop_backward_model<typename decltype(tg)::type>(a, w, s);
+      });
     case PPF_MODEL_SV: return run_mop_backward_model<SV>(a, w, s);
     case PPF_MODEL_RICKER: return run_mop_backward_model<Ricker>(a, w, s);
     default: return PPF_EINVAL;

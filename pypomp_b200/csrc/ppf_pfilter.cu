@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     nn = __syncthreads_or(nn);
     if (threadIdx.x == 0) {
       s_acc.maxkey = mx; s_acc.minkey = mn; s_acc.nan = nn; s_acc.s2 = 0.0;
-      for (int d = 0; d < 4; ++d) { s_acc.fx[d] = 0.0; s_acc.px[d] = 0.0; }
+      for (int d = 0; d < kMaxDim; ++d) { s_acc.fx[d] = 0.0; s_acc.px[d] = 0.0; }
     }
     __syncthreads();
     const bool nanf = s_acc.nan != 0;
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
 
 __device__ __forceinline__ void reset_acc(Acc* acc) {
   acc->maxkey = 0u; acc->minkey = 0xffffffffu; acc->nan = 0u; acc->s2 = 0.0;
-  for (int d = 0; d < 4; ++d) { acc->fx[d] = 0.0; acc->px[d] = 0.0; }
+  for (int d = 0; d < kMaxDim; ++d) { acc->fx[d] = 0.0; acc->px[d] = 0.0; }
 }
 __global__ void k_reset_acc(Acc* acc) { reset_acc(acc); }
 
@@ -493,8 +493,15 @@ int run_stream_tiled(Args& a, cudaStream_t s) {
 
 template <class M>
 int run_stream(Args& a, cudaStream_t s) {
-  if ((a.flags & PPF_F_FAST) && !(a.flags & PPF_F_INJECT) && a.mode == MODE_PF) return run_stream_fast(a, s);
-  return (a.flags & PPF_F_INJECT) ? run_stream_tiled<M, true>(a, s) : run_stream_tiled<M, false>(a, s);
+  if constexpr (M::WIDE) {
+    // the wide LG (dx or dy above 4): exact arithmetic, Philox draws, the
+    // 256-particle tiles (register-heavy particles, small CTAs)
+    if (a.flags & PPF_F_INJECT) return PPF_EUNSUPPORTED;
+    return a.tile == kTileSmall ? run_stream_t<M, 64, 4, false>(a, s) : PPF_EINTERNAL;
+  } else {
+    if ((a.flags & PPF_F_FAST) && !(a.flags & PPF_F_INJECT) && a.mode == MODE_PF) return run_stream_fast(a, s);
+    return (a.flags & PPF_F_INJECT) ? run_stream_tiled<M, true>(a, s) : run_stream_tiled<M, false>(a, s);
+  }
 }
 
 template <class M>
@@ -505,14 +512,9 @@ static int launch_prep(Args& a, cudaStream_t s) {
 
 int run_prep(Args& a, cudaStream_t s) {
   switch (a.model.kind) {
-    case PPF_MODEL_LG:
-      switch (a.model.dx) {
-        case 1: return a.model.dy == 1 ? launch_prep<LG<1, 1>>(a, s) : launch_prep<LG<1>>(a, s);
-        case 2: return a.model.dy == 2 ? launch_prep<LG<2, 2>>(a, s) : launch_prep<LG<2>>(a, s);
-        case 3: return a.model.dy == 3 ? launch_prep<LG<3, 3>>(a, s) : launch_prep<LG<3>>(a, s);
-        case 4: return a.model.dy == 4 ? launch_prep<LG<4, 4>>(a, s) : launch_prep<LG<4>>(a, s);
-        default: return PPF_EUNSUPPORTED;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<int>(a.model, true, PPF_EUNSUPPORTED,
+                          [&](auto tg) { return launch_prep<typename decltype(tg)::type>(a, s); });
     case PPF_MODEL_SV: return launch_prep<SV>(a, s);
     case PPF_MODEL_RICKER: return launch_prep<Ricker>(a, s);
     default: return PPF_EINVAL;
@@ -585,7 +587,9 @@ int dispatch_model(Args& a, int path, cudaStream_t s) {
   switch (path) {
     case PPF_PATH_PLAIN: return run_plain<M>(a, s);
     case PPF_PATH_STREAM: return run_stream<M>(a, s);
-    case PPF_PATH_RESIDENT: return run_resident<M>(a, s);
+    case PPF_PATH_RESIDENT:
+      if constexpr (M::WIDE) return PPF_EUNSUPPORTED;   // the wide LG streams only
+      else return run_resident<M>(a, s);
     default: return PPF_EINVAL;
   }
 }
@@ -593,14 +597,9 @@ int dispatch_model(Args& a, int path, cudaStream_t s) {
 int run_pfilter_path(Args& a, int path, cudaStream_t s) {
   if (path == PPF_PATH_CLUSTER) return run_cluster(a, false, s);
   switch (a.model.kind) {
-    case PPF_MODEL_LG:
-      switch (a.model.dx) {
-        case 1: return a.model.dy == 1 ? dispatch_model<LG<1, 1>>(a, path, s) : dispatch_model<LG<1>>(a, path, s);
-        case 2: return a.model.dy == 2 ? dispatch_model<LG<2, 2>>(a, path, s) : dispatch_model<LG<2>>(a, path, s);
-        case 3: return a.model.dy == 3 ? dispatch_model<LG<3, 3>>(a, path, s) : dispatch_model<LG<3>>(a, path, s);
-        case 4: return a.model.dy == 4 ? dispatch_model<LG<4, 4>>(a, path, s) : dispatch_model<LG<4>>(a, path, s);
-        default: return PPF_EUNSUPPORTED;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<int>(a.model, true, PPF_EUNSUPPORTED,
+                          [&](auto tg) { return dispatch_model<typename decltype(tg)::type>(a, path, s); });
     case PPF_MODEL_SV: return dispatch_model<SV>(a, path, s);
     case PPF_MODEL_RICKER: return dispatch_model<Ricker>(a, path, s);
     default: return PPF_EINVAL;

@@ -55,7 +55,9 @@ __device__ __forceinline__ void flush_rows(float* g, size_t gstride, const float
 template <class M>
 __global__ void __launch_bounds__(kSimTPB) k_simulate(SimArgs s) {
   constexpr int DX = M::MAXDX, DYM = M::MAXDY;
-  constexpr int XS = kSimChunk * DX + 1, YS = kSimChunk * DYM + 1;   // odd row strides
+  // time points staged per flush: fewer for the wide LG, whose rows are long
+  constexpr int CH = M::WIDE ? 2 : kSimChunk;
+  constexpr int XS = CH * DX + 1, YS = CH * DYM + 1;   // odd row strides
   __shared__ typename M::Consts cs;
   __shared__ float xs[kSimTPB * XS];
   __shared__ float ys[kSimTPB * YS];
@@ -94,7 +96,7 @@ __global__ void __launch_bounds__(kSimTPB) k_simulate(SimArgs s) {
 #pragma unroll
       for (int d = 0; d < DX; ++d) xs[threadIdx.x * XS + slot * DX + d] = x[d];
     }
-    if (slot == kSimChunk - 1 || tau == s.T) {
+    if (slot == CH - 1 || tau == s.T) {
       __syncthreads();
       // states of time points tb..tau, one contiguous run per replicate
       flush_rows(Xf + (size_t)tb * DX, (size_t)(s.T + 1) * DX, xs, XS, (tau - tb + 1) * DX, nlive);
@@ -130,14 +132,9 @@ int run_simulate(const ppf_simulate_desc* d, cudaStream_t st) {
   s.X = d->X;
   s.Y = d->Y;
   switch (d->model.kind) {
-    case PPF_MODEL_LG:
-      switch (d->model.dx) {
-        case 1: return d->model.dy == 1 ? launch_simulate<LG<1, 1>>(s, st) : launch_simulate<LG<1>>(s, st);
-        case 2: return d->model.dy == 2 ? launch_simulate<LG<2, 2>>(s, st) : launch_simulate<LG<2>>(s, st);
-        case 3: return d->model.dy == 3 ? launch_simulate<LG<3, 3>>(s, st) : launch_simulate<LG<3>>(s, st);
-        case 4: return d->model.dy == 4 ? launch_simulate<LG<4, 4>>(s, st) : launch_simulate<LG<4>>(s, st);
-        default: return PPF_EINVAL;
-      }
+        case PPF_MODEL_LG:
+      return with_lg<int>(d->model, true, PPF_EINVAL,
+                          [&](auto tg) { return launch_simulate<typename decltype(tg)::type>(s, st); });
     case PPF_MODEL_SV: return launch_simulate<SV>(s, st);
     case PPF_MODEL_RICKER: return launch_simulate<Ricker>(s, st);
     default: return PPF_EINVAL;

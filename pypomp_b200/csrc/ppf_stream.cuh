@@ -96,7 +96,7 @@ __device__ __forceinline__ void init_tile(const Args& a, int f, int b) {
 // (80 registers; the SV kernel spills at 64).
 template <class M>
 struct RespropOccupancy {
-  static constexpr int B = (M::MAXDX == 1 || (M::MAXDX == 2 && M::NZ == 2)) ? 4 : 3;
+  static constexpr int B = M::WIDE ? 1 : (M::MAXDX == 1 || (M::MAXDX == 2 && M::NZ == 2)) ? 4 : 3;
 };
 
 // The body for tile b of filter f at step t.  TMA: stage the tile's parent

@@ -25,7 +25,8 @@ import pandas as pd
 from . import _ffi
 from .pomp import Pomp
 
-MAX_DIM = 4
+#: Largest LG state or observation dimension (pypomp/models/linear_gaussian.py:48).
+MAX_DIM = 9
 
 
 @dataclass(frozen=True)
@@ -218,7 +219,9 @@ def LG(T: int = 4, A=None, C=None, Q=None, R=None, X0=None, key=None, ys=None) -
         if d < 1:
             raise ValueError(f"The {kind} dimension must be at least 1, but is {d}.")
         if d > MAX_DIM:
-            raise ValueError(f"LG supports dimensions up to {MAX_DIM} here, but the {kind} dimension is {d}.")
+            raise ValueError(
+                f"LG supports dimensions up to {MAX_DIM}, but the {kind} dimension is "
+                f"{d}. Above {MAX_DIM} the 'A11' style parameter names are ambiguous.")
     A_ = _default_A(dx) if A is None else np.asarray(A, float)
     C_ = np.eye(dy, dx) if C is None else np.asarray(C, float)
     Q_ = _default_cov(dx, 1.0, 0.02) / 100 if Q is None else np.asarray(Q, float)

@@ -231,3 +231,23 @@ def test_weight_quantiser_exp_equals_expf():
         assert q1 == q2, (x, e1, e2)
         if x >= -32.0:
             assert e1 == e2, (x, e1, e2)
+
+
+@pytest.mark.parametrize("dx,dy", [(6, 7), (9, 9), (2, 5)])
+def test_c_oracle_wide_lg_against_kalman(dx, dy):
+    """The C oracle's LG above 4 x 4 (up to the reference's MAX_DIM = 9,
+    ``pypomp/models/linear_gaussian.py:48``): log-mean-exp of 8 filters within
+    5 standard errors of the exact FP64 Kalman log-likelihood."""
+    import pypomp_b200 as pp
+    from pypomp_b200.maths import logmeanexp, logmeanexp_se
+
+    m = pp.LG(T=15, A=0.9 * np.eye(dx), C=np.eye(dy, dx) + 0.1, Q=np.eye(dx) * 0.05,
+              R=np.eye(dy) * 0.2 + 0.02, key=5)
+    st = m.to_struct()
+    th = m.theta.to_array(m.canonical_param_names).astype(np.float32)
+    r = cora.pfilter(m.spec.kind, dx, dy, np.repeat(th, 8, 0), st.ys, 20000, seeds=np.arange(8, dtype=np.uint64),
+                     nthreads=8)
+    A, C, Q, R, X0 = kalman.lg_matrices(th[0].astype(np.float64), dx, dy)
+    exact = kalman.kalman_loglik(st.ys, A, C, Q, R, X0)
+    lme, se = logmeanexp(r["loglik"]), logmeanexp_se(r["loglik"])
+    assert abs(lme - exact) <= 5 * se, (lme, exact, se)
