@@ -321,7 +321,7 @@ def run_ours(args):
     step()
     prof = _ffi.profile_end()
     rp_ms, rp_n = prof["resample_propagate"]
-    sum_ms, sum_n = prof["sum_lookback"]
+    sum_ms, sum_n = prof["weight_sum"]
     peak, peak_kind = peaks()
     rp_avg = rp_ms / rp_n
     achieved = RESPROP_BYTES * J * NSEED / (rp_avg / 1e3) / 1e9
@@ -411,7 +411,7 @@ def run_ours(args):
                 "value": NSEED * J * T / (fms / 1e3), "unit": UNIT, "ms_per_step": fms,
                 "roofline": {"kernel": "k_resprop_fast", "avg_launch_ms": f_rp, "achieved": f_ach,
                              "peak": peak, "unit": "GB/s", "frac": f_ach / peak},
-                "sum_kernel_avg_ms": fprof["sum_lookback"][0] / fprof["sum_lookback"][1],
+                "sum_kernel_avg_ms": fprof["weight_sum"][0] / fprof["weight_sum"][1],
                 "clocks": fclk.summary(),
                 "loglik_err_vs_kalman": loglik_error(llf.cpu().numpy(), kalman_err["kalman"])}
         if plain is not None:
@@ -556,7 +556,7 @@ def mop_block(args, steps=None, warmup=None):
     # (recompute and adjoint) as another.  Every kind touches each of the
     # J x T particle-steps once, so its GB/s is bytes x J x T / its total time.
     persistent = "mop_recompute" not in prof
-    bytes_kind = {"resample_propagate": 32, "sum_lookback": 4, "mop_forward": 36, "mop_recompute": 20,
+    bytes_kind = {"resample_propagate": 32, "weight_sum": 4, "mop_forward": 36, "mop_recompute": 20,
                   "mop_adjoint": 60 if persistent else 40}
     peak, peak_kind = peaks()
     kern = {}

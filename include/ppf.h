@@ -268,15 +268,15 @@ int ppf_workspace_status(const void* workspace, void* stream);
  * recorded on the launch stream around each kernel (host-side bookkeeping
  * only).  ppf_profile_end synchronises and writes, for each kernel kind k < n,
  * the summed milliseconds ms[k] and launch count count[k].  Kinds: 0 init,
- * 1 weight-sum + lookback, 2 resample + propagate, 3 resident filter,
+ * 1 weight-sum (tile totals and the filter's tile prefixes), 2 resample + propagate, 3 resident filter,
  * 4 plain-path step (four kernels), 5..8 MOP forward / recompute / adjoint /
  * IF2, 9 cluster filter, 10 simulation.  Not reentrant. */
 int ppf_profile_begin(void);
 int ppf_profile_end(double* ms, int* count, int n);
 
-/* Test hook for the bounded device-side waits (the decoupled-lookback spin in
- * the weight-sum kernel and the bulk-copy barrier waits of the resampling
- * kernel): set how many polls a wait makes before it gives up, for the calls
+/* Test hook for the bounded device-side waits (the bulk-copy barrier waits of
+ * the resampling kernel, the exchanges and grid barriers of the persistent
+ * MOP kernels): set how many polls a wait makes before it gives up, for the calls
  * that follow (polls < 0 restores the default, 2^22; larger values are
  * clamped to it; 0 makes every such wait give up at its first check).  A wait
  * that gives up sets the workspace's error word, so ppf_workspace_status

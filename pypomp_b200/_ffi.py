@@ -236,7 +236,7 @@ LIB = _load()
 LIB_PATH = str(_LIB_PATH)
 
 
-KIND_NAMES = ("init", "sum_lookback", "resample_propagate", "resident", "plain_step",
+KIND_NAMES = ("init", "weight_sum", "resample_propagate", "resident", "plain_step",
               "mop_forward", "mop_recompute", "mop_adjoint", "if2", "cluster", "simulate")
 
 

@@ -37,6 +37,7 @@ static size_t carve(Args& a, int path, unsigned char* base) {
     for (int i = 0; i < 2; ++i) a.desc[i] = reinterpret_cast<uint64_t*>(take(8ull * a.F * nt_alloc));
     a.excl = reinterpret_cast<uint64_t*>(take(8ull * a.F * nt_alloc));
     a.tot = reinterpret_cast<uint64_t*>(take(8ull * a.F));
+    for (int i = 0; i < 2; ++i) a.fdone[i] = reinterpret_cast<unsigned int*>(take(4ull * a.F));
     a.ctrl_bytes = off;
     a.consts = take((lg_wide(a.model) ? 2048ull : 512ull) * a.F);
     // per-thread run prefixes: ntiles x threads per tile, the largest over the tile configurations

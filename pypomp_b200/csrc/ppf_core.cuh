@@ -15,9 +15,6 @@ typedef unsigned __int128 u128;
 
 constexpr float kQScale = 1099511627776.0f;        // 2^40, fixed-point weight scale
 constexpr double kLn2 = 0.69314718055994530942;
-constexpr uint64_t kStatusAgg = 1ull << 62;
-constexpr uint64_t kStatusIncl = 2ull << 62;
-constexpr uint64_t kValueMask = (1ull << 62) - 1;
 constexpr long long kSpinCap = 1ll << 22;          // bounded waits: then PPF_ETIMEOUT
                                                    // (ppf_debug_set_wait_limit lowers it per call)
 

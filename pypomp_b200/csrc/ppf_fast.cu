@@ -31,14 +31,7 @@ __global__ void __launch_bounds__(TPB) k_init_fast(Args a) {
 
 template <class M, int TPB, int IT>
 __global__ void __launch_bounds__(TPB) k_sum_fast(Args a, int t) {
-  __shared__ int s_v;
-  if (threadIdx.x == 0) s_v = atomicAdd(a.counter + (t & 1), 1);
-  __syncthreads();
-  const int v = s_v;
-  if (v >= a.ntiles * a.F) {
-    if (threadIdx.x == 0) atomicOr(a.err, 4u);
-    return;
-  }
+  const int v = blockIdx.x;
   sum_tile<M, TPB, IT, true, true>(a, t, v / a.ntiles, v % a.ntiles);
 }
 

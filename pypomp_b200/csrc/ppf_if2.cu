@@ -99,6 +99,7 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
   if (threadIdx.x == 0) {
     a.desc[p2 ^ 1][(size_t)f * a.ntiles + b] = 0ull;
     if (b == 0 && f == 0) a.counter[p2 ^ 1] = 0;
+    if (b == 0) a.fdone[p2 ^ 1][f] = 0u;   // the next step's tile count
   }
   if (t >= Tf) return;
   const Acc acc = a.acc[p2][f];

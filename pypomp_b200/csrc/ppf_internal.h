@@ -52,6 +52,7 @@ struct Args {
   uint64_t* desc[2];      // [F][ntiles] each
   uint64_t* excl;         // [F][ntiles]
   uint64_t* tot;          // [F]
+  unsigned int* fdone[2]; // [F] each: tiles of the filter whose total is out (k_sum)
   uint64_t* runpre;       // [F][ntiles][TPB] exclusive prefix of each thread's run of q in its tile
   float* X[2];            // [F][dx][J] each
   float* W[2];            // [F][J] each

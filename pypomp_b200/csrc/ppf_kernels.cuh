@@ -409,16 +409,17 @@ __device__ __forceinline__ void perturb_row(const Args& a, int f, int k, int s, 
 // owns row r, stride P | 1 (odd, so a warp's rows fall in distinct banks).
 __device__ __forceinline__ int if2_row_stride(int P) { return P | 1; }
 
-// Fixed-point sums of the weights of one tile, then the decoupled-lookback
-// prefix over the tiles of the filter (Merrill & Garland 2016).
-// The body for tile b of filter f at step t; k_sum takes (f, b) from a
-// dynamic tile counter, the persistent MOP kernel passes its own tile.  The
-// lookback needs every earlier tile of the filter to run at the same time or
-// before, which both launch forms guarantee.
-// LB = false (the persistent MOP forward, all tiles resident and a grid
-// barrier after this body): publish the tile total in desc[t & 1] and leave
-// the prefix to tile_prefix, instead of the lookback.
-template <class M, int TPB, int IT, bool LB = true, bool FAST = false>
+// Fixed-point sums of the weights of one tile, published as the tile's total
+// in desc[t & 1].  The body for tile b of filter f at step t.
+// SCAN = true (k_sum, one launch per step): each tile publishes its total and
+// counts itself done (a fence, then an atomic on the filter's counter); the
+// tile that finds every other tile of its filter already done forms all the
+// filter's exclusive tile prefixes and its total (excl, tot) for the next
+// kernel.  No tile waits on another, and the prefixes are exact integer sums,
+// so they do not depend on which tile finishes last.
+// SCAN = false (the persistent MOP forward, all tiles resident and a grid
+// barrier after this body): the prefix is left to tile_prefix.
+template <class M, int TPB, int IT, bool SCAN = true, bool FAST = false>
 __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
   constexpr int TILE = TPB * IT;
   constexpr int DX = M::MAXDX;
@@ -492,46 +493,33 @@ __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
     }
     if (rs) a.runpre[((size_t)f * a.ntiles + b) * TPB + threadIdx.x] = before + inc - qs;
   }
-  // Decoupled lookback.  Each descriptor word packs its status (2 bits) with the
-  // value, written by one 64-bit store, and nothing else is published through
-  // it (e, the run prefixes, excl and tot are read by the next kernel), so
-  // strong relaxed accesses suffice; release / acquire would only add fences.
   uint64_t* desc = a.desc[p] + (size_t)f * a.ntiles;
-  if (!LB) {
-    if (threadIdx.x == 0) desc[b] = btot;
-  } else if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    uint64_t excl = 0;
-    if (b == 0) {
-      if (lane == 0) st_relaxed_u64(desc, kStatusIncl | btot);
-    } else {
-      if (lane == 0) st_relaxed_u64(desc + b, kStatusAgg | btot);
-      int pos = b - 1;
-      long long spins = 0;
-      bool timed_out = false;
-      while (true) {
-        const int idx = pos - lane;
-        uint64_t d = idx >= 0 ? ld_relaxed_u64(desc + idx) : kStatusIncl;
-        while (__any_sync(0xffffffffu, (d >> 62) == 0ull)) {
-          if (++spins > a.spin_cap) { timed_out = true; break; }
-          if ((d >> 62) == 0ull) { __nanosleep(32); d = ld_relaxed_u64(desc + idx); }
-        }
-        if (timed_out) break;
-        const unsigned int inc = __ballot_sync(0xffffffffu, (d >> 62) == 2ull);
-        if (inc) {
-          const int first = __ffs(inc) - 1;
-          excl += warp_sum_u64(lane <= first ? (d & kValueMask) : 0ull);
-          break;
-        }
-        excl += warp_sum_u64(d & kValueMask);
-        pos -= 32;
-      }
-      if (timed_out && lane == 0) atomicOr(a.err, 1u);
-      if (lane == 0) st_relaxed_u64(desc + b, kStatusIncl | (excl + btot));
+  if (threadIdx.x == 0) desc[b] = btot;
+  if (SCAN) {
+    __shared__ int s_last;
+    __shared__ uint64_t s_scan2[TPB / 32 + 1];
+    if (threadIdx.x == 0) {
+      __threadfence();   // the total is visible before the count that reveals it
+      s_last = atomicAdd(a.fdone[p] + f, 1u) == (unsigned int)(a.ntiles - 1);
     }
-    if (lane == 0) {
-      a.excl[(size_t)f * a.ntiles + b] = excl;
-      if (b == a.ntiles - 1) a.tot[f] = excl + btot;
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      // every thread sums a run of consecutive tile totals; one block scan of
+      // the runs, then each tile's exclusive prefix along the run
+      const int nt = a.ntiles;
+      const int per = (nt + TPB - 1) / TPB;
+      const int i0 = min(nt, (int)threadIdx.x * per), i1 = min(nt, i0 + per);
+      uint64_t run = 0;
+      for (int i = i0; i < i1; ++i) run += __ldcg(reinterpret_cast<const unsigned long long*>(desc + i));
+      uint64_t all;
+      uint64_t pre = block_excl_scan_u64_1b<TPB>(run, s_scan2, all);
+      uint64_t* ex = a.excl + (size_t)f * nt;
+      for (int i = i0; i < i1; ++i) {
+        ex[i] = pre;
+        pre += __ldcg(reinterpret_cast<const unsigned long long*>(desc + i));
+      }
+      if (threadIdx.x == 0) a.tot[f] = all;
     }
   }
   if (a.flags & PPF_F_ESS) {
@@ -584,17 +572,12 @@ __device__ __forceinline__ void tile_prefix(const Args& a, int t, int f, int b) 
   __syncthreads();
 }
 
+// One CTA per tile: fixed-point weights, e in place, run prefixes and the
+// tile total; the filter's last tile forms the tile prefixes (sum_tile).
 template <class M, int TPB, int IT>
 __global__ void __launch_bounds__(TPB) k_sum(Args a, int t) {
-  __shared__ int s_v;
-  if (threadIdx.x == 0) s_v = atomicAdd(a.counter + (t & 1), 1);
-  __syncthreads();
-  const int v = s_v;
-  if (v >= a.ntiles * a.F) {  // defensive: a stale counter must not index past the batch
-    if (threadIdx.x == 0) atomicOr(a.err, 4u);
-    return;
-  }
-  sum_tile<M, TPB, IT>(a, t, v / a.ntiles, v % a.ntiles);
+  const int v = blockIdx.x;
+  sum_tile<M, TPB, IT, true>(a, t, v / a.ntiles, v % a.ntiles);
 }
 
 }  // namespace ppf

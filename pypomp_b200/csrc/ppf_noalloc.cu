@@ -15,7 +15,7 @@
 //    the GPU (different streams, or different host threads) race and corrupt
 //    each other -- serialise them;
 //  - the array keeps the previous call's contents; ppf_pfilter clears the part
-//    that must start at zero (counters, accumulators, lookback descriptors)
+//    that must start at zero (counters, accumulators, tile totals)
 //    and fully writes the particle arrays before reading them;
 //  - the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (the host-side name is only a stand-in, not a device

@@ -8,8 +8,8 @@
 //
 //  STREAM   (large J): particle state in HBM, structure of arrays
 //           X[F][dx][J], W[F][J], two kernels per observation:
-//             k_sum      fixed-point weights, block sums, single-pass
-//                        decoupled-lookback prefix over the tiles of a filter
+//             k_sum      fixed-point weights, tile totals; the filter's last
+//                        tile to finish forms every tile's exclusive prefix
 //             k_resprop  tile CDF, closed-form systematic offsets per parent,
 //                        child expansion by a max-scan in shared memory, and
 //                        the NEXT step's rproc + dmeas fused for each child

@@ -121,11 +121,12 @@ __device__ __forceinline__ void resprop_tile(const Args& a, int t, int f, int b)
   const int u = filter_unit(a, f);
   const int Tf = filter_len(a, u);
   const int p = t & 1;
-  // reset the next step's lookback descriptors and tile counter (before any
-  // early exit: finished filters of a ragged panel still own these slots)
+  // reset the next step's tile-total slot and done-count (before any early
+  // exit: finished filters of a ragged panel still own these slots)
   if (threadIdx.x == 0) {
     a.desc[p ^ 1][(size_t)f * a.ntiles + b] = 0ull;
     if (b == 0 && f == 0) a.counter[p ^ 1] = 0;
+    if (b == 0) a.fdone[p ^ 1][f] = 0u;   // the next step's tile count
   }
   if (t >= Tf) return;
   const Acc acc = a.acc[p][f];

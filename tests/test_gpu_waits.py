@@ -1,8 +1,8 @@
 """Bounded device-side waits give up with PPF_ETIMEOUT and leave the context usable.
 
-The weight-sum kernel's decoupled lookback spins on its predecessors' tile
-descriptors, and the resampling kernel waits on the bulk copies of its parent
-rows; each wait is bounded.  ``ppf_debug_set_wait_limit(0)`` makes every such
+The resampling kernel waits on the bulk copies of its parent rows, and the
+persistent MOP kernels wait on each other's per-step words and at grid
+barriers; each wait is bounded.  ``ppf_debug_set_wait_limit(0)`` makes every such
 wait give up at its first check, on a many-tile case (8 filters x 128 tiles
 of 2048 particles).  The call must come back promptly with PPF_ETIMEOUT from
 ``ppf_workspace_status``, and, with the limit restored, the next call on the
