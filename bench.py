@@ -447,7 +447,10 @@ def run_ours(args):
                          "algorithmic_bytes_per_particle": RESPROP_BYTES,
                          "avg_launch_ms": rp_avg, "peak_source": peak_kind,
                          "sum_kernel_avg_ms": sum_avg,
-                         "step_bytes_per_particle_step": RESPROP_BYTES + SUM_BYTES},
+                         "step_bytes_per_particle_step": RESPROP_BYTES + SUM_BYTES,
+                         "kernel_timing": "CUDA events around each launch of one extra step run "
+                                          "without the graph; the two kernels' averages add up "
+                                          "to a few per cent more than the graph-replayed step"},
             "cpu_baseline": cpu,
             "plain": plain,
             "clocks": clk.summary(),
