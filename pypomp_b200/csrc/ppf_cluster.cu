@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     acc.nan = 0u;
     acc.pad = 0u;
     acc.s2 = 0.0;
-    for (int d = 0; d < kMaxDim; ++d) { acc.fx[d] = 0.0; acc.px[d] = 0.0; }
+    for (int d = 0; d < M::MAXDX; ++d) { acc.fx[d] = 0.0; acc.px[d] = 0.0; }   // the model's dimensions only
     for (int r = 0; r < NC; ++r) {
       acc.maxkey = max(acc.maxkey, slots[r].maxkey);
       acc.minkey = min(acc.minkey, slots[r].minkey);

@@ -525,8 +525,9 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
     const uint32_t u32 = resample_u32(a, f, t);
     __syncthreads();
     if (!s_ok) return;
-    Acc acc;
-    memset(&acc, 0, sizeof(acc));
+    Acc acc;                 // the fields this kernel's flags read (no ESS / means here)
+    acc.pad = 0u;
+    acc.s2 = 0.0;
     acc.maxkey = s_key[0];
     acc.minkey = s_key[1];   // (= max key when unused: decide_resample then depends on NaN only)
     acc.nan = s_key[2];

@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     nn = __syncthreads_or(nn);
     if (threadIdx.x == 0) {
       s_acc.maxkey = mx; s_acc.minkey = mn; s_acc.nan = nn; s_acc.s2 = 0.0;
-      for (int d = 0; d < kMaxDim; ++d) { s_acc.fx[d] = 0.0; s_acc.px[d] = 0.0; }
+      for (int d = 0; d < DX; ++d) { s_acc.fx[d] = 0.0; s_acc.px[d] = 0.0; }
     }
     __syncthreads();
     const bool nanf = s_acc.nan != 0;
