@@ -841,7 +841,9 @@ def run_profile_case(args):
     Ricker filters, J = 16384, T = 50); ``plain`` the one-filter baseline
     kernels (LG 2-D, J = 262144, T = 12); ``if2`` the streaming IF2 kernels
     (128 Ricker filters, J = 8192, T = 50, as one iteration of the packed
-    panel IF2)."""
+    panel IF2); ``mopsteps`` the per-step MOP kernels (8 LG 2-D filters,
+    J = 131072, T = 20, persistent forms off); ``wide`` the wide LG's streaming
+    kernels (4 LG 9 x 9 filters, J = 262144, T = 6)."""
     import math
 
     import torch
@@ -855,6 +857,18 @@ def run_profile_case(args):
         th = m.spec.to_est(m.theta.to_array(m.canonical_param_names)).astype(np.float32)
         r = F.run_mop(m.to_struct(), th, np.array([1], np.uint64), 65536, 0.97, grad=True)
         print("profile case MOP", r["value"], r["grad"])
+        return
+    if args.config == "mopsteps":
+        m = pp.LG(T=20, Q=LG_Q, R=LG_R, key=0)
+        th = m.spec.to_est(np.repeat(m.theta.to_array(m.canonical_param_names), 8, axis=0)).astype(np.float32)
+        r = F.run_mop(m.to_struct(), th, np.arange(8, dtype=np.uint64), 131072, 0.97, grad=True, persistent=False)
+        print("profile case MOP per-step", r["value"][:2])
+        return
+    if args.config == "wide":
+        m = pp.LG(T=6, A=0.9 * np.eye(9), C=np.eye(9) + 0.1, Q=np.eye(9) * 0.05, R=np.eye(9) * 0.2 + 0.02, key=0)
+        th = np.repeat(m.theta.to_array(m.canonical_param_names), 4, axis=0).astype(np.float32)
+        r = F.run_pfilter(m.to_struct(), th, np.arange(4, dtype=np.uint64), 262144, path="stream")
+        print("profile case wide LG", r["loglik"][:2])
         return
     if args.config == "c4":
         m = pp.Ricker(T=50, key=0)
@@ -938,9 +952,13 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="stream-path tile (0 = automatic)")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch the step loop directly instead of replaying it as a CUDA graph")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "sim", "pmcmc", "plain", "if2"],
-                    help="c2 (default) is the headline line; c1/c3/c4 print their own lines")
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "sim", "pmcmc", "plain", "if2", "mopsteps",
+                                                   "wide"],
+                    help="c2 (default) is the headline line; c1/c3/c4/c5/sim/pmcmc print their own lines; "
+                         "plain, if2, mopsteps and wide are --profile-case cases")
     args = ap.parse_args()
+    if args.config in ("plain", "if2", "mopsteps", "wide") and not args.profile_case:
+        ap.error(f"--config {args.config} is a --profile-case case")
     if args.config != "c2" and args.impl == "ours" and not args.profile_case:
         {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "sim": run_sim, "pmcmc": run_pmcmc}[args.config](args)
         return
