@@ -222,10 +222,17 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     // fixed-point weights of the slice: totals and this thread's prefix
     uint64_t qs = 0;
     double s2 = 0.0, fx[DX], px[DX];
+    // the first QC fixed-point weights stay in registers for the offsets below
+    constexpr int QC = 4;
+    uint64_t qk[QC];
 #pragma unroll
     for (int d = 0; d < DX; ++d) { fx[d] = 0.0; px[d] = 0.0; }
     for (int l = l0; l < l1; ++l) {
-      qs += qweight(Wc[l], Mx, qc);
+      const uint64_t q = qweight(Wc[l], Mx, qc);
+#pragma unroll
+      for (int i = 0; i < QC; ++i)
+        if (l - l0 == i) qk[i] = q;
+      qs += q;
       if (want_sums) {
         const double e = qc ? 1.0 : (double)pp_expf(Wc[l] - Mx);
         s2 += e * e;
@@ -278,7 +285,12 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
         OffWalk wk = offwalk_init(o, E + tex);
         st[l0] = wk.k;
         for (int l = l0; l < l1; ++l) {
-          const int kn = offwalk_add(o, wk, qweight(Wc[l], Mx, qc));
+          uint64_t q = 0;
+#pragma unroll
+          for (int i = 0; i < QC; ++i)
+            if (l - l0 == i) q = qk[i];
+          if (l - l0 >= QC) q = qweight(Wc[l], Mx, qc);
+          const int kn = offwalk_add(o, wk, q);
           if (l + 1 < l1 || l + 1 == nc) st[l + 1] = kn;
         }
       }

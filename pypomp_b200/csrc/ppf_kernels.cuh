@@ -189,16 +189,21 @@ __device__ __forceinline__ void accum_maxmin(float w, unsigned int& mx, unsigned
 // chi = floor(u32 tot / 2^32) (derivation in ppf_core.cuh, nchild).
 struct Offsets {
   uint64_t tot, chi;
-  double inv, chi_d;   // J / tot and chi / tot, for the first guess
+  double inv, chi_d;   // about J / tot and chi / tot, for the first guess
   int J;
 };
 
+// The guess needs no division: 1 / tot from the correctly rounded float
+// reciprocal of (float)tot has a relative error below 2^-22, so
+// C * J / tot - chi / tot (at most J <= 2^21) is off by less than 1/2 and
+// nchild_fast's exact comparisons settle the answer within one step.
 __device__ __forceinline__ Offsets make_offsets(uint64_t tot, uint32_t u32, int J) {
   Offsets o;
   o.tot = tot;
   o.chi = __umul64hi((uint64_t)u32 << 32, tot);   // (u32 * tot) >> 32
-  o.inv = (double)J / (double)tot;
-  o.chi_d = (double)o.chi / (double)tot;
+  const double r = (double)__frcp_rn((float)tot);
+  o.inv = (double)J * r;
+  o.chi_d = (double)o.chi * r;
   o.J = J;
   return o;
 }
@@ -210,10 +215,9 @@ __device__ __forceinline__ void mul64(uint64_t a, uint64_t b, uint64_t& hi, uint
 }
 
 // nchild(C) = #{ k in [0,J) : k tot + chi < C J } = #{ k : k tot < D },
-// D = C J - chi.  The double-precision guess ceil(D / tot) is within one of
-// the answer (its relative error is ~1e-16 on a value below 2^21), so one
-// exact 128-bit comparison on each side settles it; a bounded loop covers the
-// impossible case defensively.
+// D = C J - chi.  The guess ceil(C inv - chi_d) is within one of the answer
+// (make_offsets), so one exact 128-bit comparison on each side settles it; a
+// bounded loop covers the impossible case defensively.
 __device__ __forceinline__ bool lt128(uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl) {
   return (ah < bh) | ((ah == bh) & (al < bl));
 }
