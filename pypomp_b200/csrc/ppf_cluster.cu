@@ -55,6 +55,15 @@ struct Slot {
   double s2, fx[4], px[4];                // ESS / mean sums of c's slice (pushed to CTA 0 only)
 };
 
+// What finalize_step reads of one step, kept by CTA 0 until the flush.
+constexpr int kRecSteps = 32;
+template <int DX>
+struct StepRec {
+  unsigned int maxkey, nan;
+  double s2, fx[DX], px[DX];
+  unsigned long long tot;
+};
+
 // Dynamic shared memory of one CTA, in 4-byte words: X[2][DX][JC], W[2][JC],
 // (IF2) TH[2][P][JC], st[JC + 4], (IF2) per-thread parameter rows [TPB][P|1].
 template <class M, bool IF2>
@@ -109,6 +118,8 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
   __shared__ uint64_t s_scan[TPB / 32 + 1];
   __shared__ unsigned int smk[3 * (TPB / 32)];
   __shared__ double sd[TPB / 32];
+  __shared__ StepRec<DX> s_rec[kRecSteps];     // CTA 0: the steps not yet added to the log-likelihood
+  __shared__ double s_rll[kRecSteps];
 
   const int NC = (int)cl.num_blocks();
   const int c = (int)cl.block_rank();
@@ -273,7 +284,14 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
           acc.s2 += slots[r].s2;
           for (int d = 0; d < DX; ++d) { acc.fx[d] += slots[r].fx[d]; acc.px[d] += slots[r].px[d]; }
         }
-      finalize_step(a, f, t, acc, tot, &ll_acc);
+      // the step's log-likelihood term is formed later (flush below): its
+      // float64 log would otherwise hold CTA 0, and so the cluster, every step
+      StepRec<DX>& rec = s_rec[t % kRecSteps];
+      rec.maxkey = acc.maxkey;
+      rec.nan = acc.nan;
+      rec.s2 = acc.s2;
+      for (int d = 0; d < DX; ++d) { rec.fx[d] = acc.fx[d]; rec.px[d] = acc.px[d]; }
+      rec.tot = tot;
     }
     const bool rs = decide_resample(a, acc);
 
@@ -388,6 +406,29 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     }
     if (!last) push_maxmin<TPB>(cl, slots, c, NC, mx, mn, nn, smk);
     cl.sync();   // children and slots visible to their owners; nobody leaves while others write to it
+    // every kRecSteps steps (and after the last) CTA 0 forms the buffered
+    // steps' terms in parallel and adds them in step order, as one thread
+    // adding each step's term in turn would
+    if (c == 0 && ((t + 1) % kRecSteps == 0 || t == Tf - 1)) {
+      const int n = t % kRecSteps + 1, tb = t + 1 - n;
+      __syncthreads();
+      if ((int)threadIdx.x < n) {
+        const StepRec<DX>& rec = s_rec[threadIdx.x];
+        Acc ra;
+        ra.maxkey = rec.maxkey;
+        ra.minkey = rec.maxkey;
+        ra.nan = rec.nan;
+        ra.pad = 0u;
+        ra.s2 = rec.s2;
+        for (int d = 0; d < DX; ++d) { ra.fx[d] = rec.fx[d]; ra.px[d] = rec.px[d]; }
+        double v = 0.0;
+        finalize_step(a, f, tb + (int)threadIdx.x, ra, rec.tot, &v);
+        s_rll[threadIdx.x] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0)
+        for (int i = 0; i < n; ++i) ll_acc += s_rll[i];
+    }
   }
   if (c == 0 && threadIdx.x == 0) a.loglik[f] = ll_acc;
 }

@@ -108,7 +108,7 @@ def test_wide_lg_mop_gradient_vs_finite_differences(dx, dy):
     assert err <= 1e-3, (err, g, fd)
 
 
-@pytest.mark.parametrize("dx,dy", [(1, 5), (5, 5)])
+@pytest.mark.parametrize("dx,dy", [(1, 5), (5, 5), (9, 9)])
 def test_wide_lg_perfilter_bit_exact(dx, dy):
     from pypomp_b200 import functional as F
 
