@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(TPB) k_if2_resprop(Args a, int t) {
     if (b == 0) a.fdone[p2 ^ 1][f] = 0u;   // the next step's tile count
   }
   if (t >= Tf) return;
-  const Acc acc = a.acc[p2][f];
+  const Acc& acc = a.acc[p2][f];   // read in place (a copy would sit in local memory)
   const uint64_t tot = a.tot[f];
   if (b == 0 && threadIdx.x == 0) finalize_step(a, f, t, acc, tot, a.loglik + f);
   const bool last = (t == Tf - 1);

@@ -432,7 +432,7 @@ __device__ __forceinline__ void sum_tile(const Args& a, int t, int f, int b) {
   const int u = filter_unit(a, f);
   if (t >= filter_len(a, u)) return;
   const int p = t & 1;
-  const Acc acc = a.acc[p][f];
+  const Acc& acc = a.acc[p][f];   // read in place (a copy would sit in local memory)
   if (b == 0 && threadIdx.x == 0) {
     Acc* nx = a.acc[p ^ 1] + f;
     nx->maxkey = 0u; nx->minkey = 0xffffffffu; nx->nan = 0u;

@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(TPB) kp_scan1(Args a, int f, int t) {
   __shared__ double sd[TPB / 32];
   if (t >= filter_len(a, filter_unit(a, f))) return;
   const int p = t & 1;
-  const Acc acc = *a.acc[p];
+  const Acc& acc = *a.acc[p];
   const float Mx = keyf(acc.maxkey);
   const bool qc = acc.nan != 0 || Mx == -INFINITY;
   const int j = blockIdx.x * TPB + threadIdx.x;
@@ -397,7 +397,7 @@ template <int TPB>
 __global__ void __launch_bounds__(TPB) kp_anc(Args a, int f, int t) {
   if (t >= filter_len(a, filter_unit(a, f))) return;
   const int p = t & 1;
-  const Acc acc = *a.acc[p];
+  const Acc& acc = *a.acc[p];
   const uint64_t tot = a.tot[0];
   const int k = blockIdx.x * TPB + threadIdx.x;
   const bool rs = decide_resample(a, acc);

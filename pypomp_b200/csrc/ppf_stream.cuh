@@ -129,7 +129,7 @@ __device__ __forceinline__ void resprop_tile(const Args& a, int t, int f, int b)
     if (b == 0) a.fdone[p ^ 1][f] = 0u;   // the next step's tile count
   }
   if (t >= Tf) return;
-  const Acc acc = a.acc[p][f];
+  const Acc& acc = a.acc[p][f];   // read in place (a copy would sit in local memory)
   const uint64_t tot = a.tot[f];
   if (b == 0 && threadIdx.x == 0) finalize_step(a, f, t, acc, tot, a.loglik + f);
   const bool last = (t == Tf - 1);
