@@ -160,12 +160,17 @@ __device__ __forceinline__ void finalize_step(const Args& a, int f, int t, const
     else e = (float)(S1 * S1 / acc.s2);
     a.ess[(size_t)f * a.T + t] = e;
   }
+  // static indices into acc (bounded by dx at run time), so a caller's local
+  // record can stay in registers
   const int dx = a.model.dx;
   if ((a.flags & PPF_F_FMEAN) && a.fmean)
-    for (int d = 0; d < dx; ++d)
-      a.fmean[((size_t)f * a.T + t) * dx + d] = (float)(collapsed ? acc.px[d] / a.J : acc.fx[d] / S1);
+#pragma unroll
+    for (int d = 0; d < kMaxDim; ++d)
+      if (d < dx) a.fmean[((size_t)f * a.T + t) * dx + d] = (float)(collapsed ? acc.px[d] / a.J : acc.fx[d] / S1);
   if ((a.flags & PPF_F_PMEAN) && a.pmean)
-    for (int d = 0; d < dx; ++d) a.pmean[((size_t)f * a.T + t) * dx + d] = (float)(acc.px[d] / a.J);
+#pragma unroll
+    for (int d = 0; d < kMaxDim; ++d)
+      if (d < dx) a.pmean[((size_t)f * a.T + t) * dx + d] = (float)(acc.px[d] / a.J);
 }
 
 __device__ __forceinline__ bool decide_resample(const Args& a, const Acc& acc) {
