@@ -61,9 +61,9 @@ LG_A = np.array([[math.cos(0.2), -math.sin(0.2)], [math.sin(0.2), math.cos(0.2)]
 RESPROP_BYTES = 24
 SUM_BYTES = 4
 # DRAM traffic of one k_resprop launch per particle, from an ncu capture of a
-# 24-seed case (dram__bytes_read.sum + dram__bytes_write.sum = 150.0 MB for
+# 24-seed case (dram__bytes_read.sum + dram__bytes_write.sum = 109.1 MB for
 # 6.29 M particles); traffic is proportional to the particles processed
-RESPROP_TRAFFIC_PER_PARTICLE = 23.85
+RESPROP_TRAFFIC_PER_PARTICLE = 17.35
 # DRAM traffic of one k_simulate launch per trajectory-step, from an ncu capture
 # of LG 2-D, 1 parameter set x 65536 replicates x T = 200 (188.0 MB written +
 # 37.0 MB read for 13.1 M trajectory-steps); the writes and the partial-sector
