@@ -1175,17 +1175,29 @@ def mif(struct: PompStruct, thetas_array, rw_sd, M: int, J: int, keys, thresh: f
     return logliks, traces, final
 
 
+def _cooling_rows(rw_sd, m: int, T_u, width: int | None = None, out=None) -> np.ndarray:
+    """(U, width) cooling factors of iteration m for every unit and step (zero
+    past a unit's length; width defaults to max T_u), written into ``out``
+    when given."""
+    T_u = np.atleast_1d(np.asarray(T_u, dtype=np.int64))
+    if out is None:
+        out = np.empty((T_u.size, int(width or T_u.max())), np.float32)
+    out.fill(0.0)
+    rows = {}                      # units of equal length share their rows
+    for u, Tu in enumerate(T_u.tolist()):
+        if Tu not in rows:
+            rows[Tu] = np.array(rw_sd.cooling_factors(Tu, m), dtype=np.float32)
+        out[u, :Tu] = rows[Tu]
+    return out
+
+
 def _cooling_table(rw_sd, M: int, T_u, width: int | None = None) -> np.ndarray:
     """(M, U, width) cooling factors of every iteration, unit and step (zero
     past a unit's length; width defaults to max T_u)."""
     T_u = np.atleast_1d(np.asarray(T_u, dtype=np.int64))
     out = np.zeros((M, T_u.size, int(width or T_u.max())), np.float32)
-    rows = {}                      # units of equal length share their rows
-    for u, Tu in enumerate(T_u):
-        Tu = int(Tu)
-        if Tu not in rows:
-            rows[Tu] = np.array([rw_sd.cooling_factors(Tu, m) for m in range(M)], dtype=np.float32)
-        out[:, u, :Tu] = rows[Tu]
+    for m in range(M):
+        _cooling_rows(rw_sd, m, T_u, out=out[m])
     return out
 
 
@@ -1605,17 +1617,22 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
     keys = np.asarray(keys, dtype=np.uint64).reshape(-1)
     sig_p, sig0_p = rw_sd.arrays(struct.param_names)
     sig_u, sig0_u = sig_p[perm], sig0_p[perm]
-    panel0 = np.concatenate([sh[:, :, None, :].repeat(U, axis=2), un], axis=3)   # (n, J, U, Pp) natural
     # the transforms act column by column: panel column j is canonical
     # parameter inv[j], so apply that parameter's transform to it directly (no
-    # gathers of the J x U swarm)
+    # gathers of the J x U swarm); the shared block (n, J, ns) and the unit
+    # block (n, J, U, nu) are transformed apart (the shared columns are not
+    # repeated per unit) and transposed on the device
     import dataclasses
 
-    pspec = dataclasses.replace(spec, est_log=tuple(j for j in range(len(inv)) if inv[j] in spec.est_log),
-                                est_atanh=tuple(j for j in range(len(inv)) if inv[j] in spec.est_atanh))
-    est0 = pspec.to_est(panel0)                                                   # panel order
-    S = torch.tensor(est0[:, :, 0, :ns].transpose(0, 2, 1).copy(), dtype=torch.float32, device=dev)
-    Us = torch.tensor(est0[:, :, :, ns:].transpose(0, 2, 3, 1).copy(), dtype=torch.float32, device=dev)
+    def colspec(cols):
+        cols = list(cols)
+        return dataclasses.replace(spec, est_log=tuple(i for i, j in enumerate(cols) if inv[j] in spec.est_log),
+                                   est_atanh=tuple(i for i, j in enumerate(cols) if inv[j] in spec.est_atanh))
+
+    pspec = colspec(range(ns + nu))
+    sspec, uspec = colspec(range(ns)), colspec(range(ns, ns + nu))
+    S = torch.from_numpy(sspec.to_est(np.ascontiguousarray(sh))).to(dev).float().permute(0, 2, 1).contiguous()
+    Us = torch.from_numpy(uspec.to_est(np.ascontiguousarray(un))).to(dev).float().permute(0, 2, 3, 1).contiguous()
     m_keys = np.stack([pprandom.split(k, M + 1)[1:] for k in keys])               # (n, M)
     all_units = struct.all_units()
     T_u = np.asarray(struct.T_u, dtype=np.int64)
@@ -1628,12 +1645,17 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
         out = pspec.from_est(panel)
         return out[:, 0, :ns], out[:, :, ns:]
 
-    # device-side loop: the keys and cooling factors of all iterations are
-    # uploaded once, the swarms stay in one PerfilterCall's buffers, and
-    # without monitors nothing waits for the host until the end
+    # device-side loop: the keys of all iterations are uploaded once, the
+    # swarms stay in one PerfilterCall's buffers, and without monitors nothing
+    # waits for the GPU until the end.  Each iteration's cooling factors are
+    # formed on the host while the previous iterations run, in a ring of two
+    # pinned buffers (a buffer is refilled once its copy two iterations back
+    # has run)
     unit_keys_all = np.stack([np.stack([pprandom.split(k, U) for k in m_keys[:, it]]) for it in range(M)])
     keys_d = torch.from_numpy(np.ascontiguousarray(unit_keys_all.reshape(M, n * U)).view(np.int64)).to(dev)
-    cool_d = torch.from_numpy(_cooling_table(rw_sd, M, T_u, Tmax)).to(dev)               # (M, U, Tmax)
+    cool_h = [torch.empty((U, Tmax), dtype=torch.float32).pin_memory() for _ in range(2)]
+    cool_ev = [None, None]
+    cool_d = torch.empty((M, U, Tmax), dtype=torch.float32, device=dev)
     panel = torch.cat([S[:, None].expand(n, U, ns, J), Us], dim=2)
     call = PerfilterCall(all_units, panel.reshape(n * U, ns + nu, J).index_select(1, perm_t), J, sig_u, sig0_u,
                          thresh=thresh, unit_f=unit_f)
@@ -1643,6 +1665,13 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
     umeans = torch.zeros(M + 1, n, U, nu, dtype=torch.float64, device=dev)
     smeans[0], umeans[0] = S.mean(dim=2).double(), Us.mean(dim=3).double()
     for it in range(M):
+        r = it & 1
+        if cool_ev[r] is not None:
+            cool_ev[r].synchronize()
+        _cooling_rows(rw_sd, it, T_u, Tmax, out=cool_h[r].numpy())
+        cool_d[it].copy_(cool_h[r], non_blocking=True)
+        cool_ev[r] = torch.cuda.Event()
+        cool_ev[r].record()
         if it > 0:
             panel = torch.cat([S[:, None].expand(n, U, ns, J), Us], dim=2)
             call.swarm.copy_(panel.reshape(n * U, ns + nu, J).index_select(1, perm_t))
@@ -1682,11 +1711,9 @@ def _panel_mif_parallel(struct: PanelPompStruct, shared_array, unit_array, rw_sd
         if it > 0:
             shared_tr[:, it, 0] = ll_units[it - 1].sum(axis=1)
             unit_tr[:, it, :, 0] = ll_units[it - 1]
-    s_fin = S.cpu().numpy().astype(np.float64).transpose(0, 2, 1)                 # (n, J, ns)
-    u_fin = Us.cpu().numpy().astype(np.float64).transpose(0, 3, 1, 2)             # (n, J, U, nu)
-    panel = np.concatenate([np.repeat(s_fin[:, :, None], U, axis=2), u_fin], axis=3)
-    natf = pspec.from_est(panel)
-    return shared_tr, unit_tr, natf[:, :, 0, :ns], natf[:, :, :, ns:]
+    s_fin = sspec.from_est(S.permute(0, 2, 1).contiguous().double().cpu().numpy())        # (n, J, ns)
+    u_fin = uspec.from_est(Us.permute(0, 3, 1, 2).contiguous().double().cpu().numpy())    # (n, J, U, nu)
+    return shared_tr, unit_tr, s_fin, u_fin
 
 
 def panel_train(struct: PanelPompStruct, shared_array, unit_array, J: int, optimizer, M: int, eta,

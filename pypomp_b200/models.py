@@ -88,8 +88,13 @@ class ModelSpec:
     def ycon(self, ys: np.ndarray) -> np.ndarray | None:
         """Per-observation constant of dmeas (Ricker: log y!), else None."""
         if self.kind == _ffi.MODEL_RICKER:
+            # counts repeat: lgamma once per distinct finite value (0 where missing)
             y = np.asarray(ys, dtype=np.float64)[..., 0]
-            return np.vectorize(lambda v: math.lgamma(v + 1.0) if np.isfinite(v) else 0.0)(y).astype(np.float32)
+            out = np.zeros(y.shape, np.float64)
+            fin = np.isfinite(y)
+            vals, inv = np.unique(y[fin], return_inverse=True)
+            out[fin] = np.array([math.lgamma(v + 1.0) for v in vals.tolist()], np.float64)[inv]
+            return out.astype(np.float32)
         return None
 
 
