@@ -838,7 +838,8 @@ def run_profile_case(args):
     ``--config sim`` and ``--config c5`` give small cases of the simulation
     and cluster-path kernels; ``c3`` the persistent MOP forward and adjoint
     (SV, T = 200, J = 65536); ``c4`` the shared-memory-resident filter (64
-    Ricker filters, J = 16384, T = 50); ``plain`` the one-filter baseline
+    Ricker filters, J = 16384, T = 50; ``--path stream`` for the streaming
+    kernels on the same filters); ``plain`` the one-filter baseline
     kernels (LG 2-D, J = 262144, T = 12); ``if2`` the streaming IF2 kernels
     (128 Ricker filters, J = 8192, T = 50, as one iteration of the packed
     panel IF2); ``mopsteps`` the per-step MOP kernels (8 LG 2-D filters,
@@ -874,8 +875,9 @@ def run_profile_case(args):
         m = pp.Ricker(T=50, key=0)
         grid = np.array([[math.exp(a), b, 10.0, 7.0] for a in np.linspace(3.0, 4.6, 8)
                          for b in np.linspace(0.05, 0.8, 8)], np.float32)
-        r = F.run_pfilter(m.to_struct(), grid, np.arange(64, dtype=np.uint64), 16384, path="resident")
-        print("profile case resident", r["loglik"][:2])
+        path = args.path or "resident"
+        r = F.run_pfilter(m.to_struct(), grid, np.arange(64, dtype=np.uint64), 16384, path=path)
+        print("profile case", path, r["loglik"][:2])
         return
     if args.config == "plain":
         m = workload()
@@ -925,7 +927,7 @@ def run_profile_case(args):
     st = m.to_struct()
     st.ys = st.ys[:12]
     th = np.repeat(m.theta.to_array(m.canonical_param_names), 24, axis=0).astype(np.float32)
-    out = F.run_pfilter(st, th, np.arange(24, dtype=np.uint64), J, path=args.path, fast=args.fast)
+    out = F.run_pfilter(st, th, np.arange(24, dtype=np.uint64), J, path=args.path or "stream", fast=args.fast)
     torch.cuda.synchronize()
     print("profile case logLik", out["loglik"][:2])
 
@@ -948,7 +950,8 @@ def main():
                          "equal to the exact arithmetic)")
     ap.add_argument("--profile-case", action="store_true",
                     help="run one small call of the same kernels (for ncu) and exit")
-    ap.add_argument("--path", default="stream")
+    ap.add_argument("--path", default=None,
+                    help="filter path of a --profile-case (default: stream; resident for c4)")
     ap.add_argument("--tile", type=int, default=0, help="stream-path tile (0 = automatic)")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch the step loop directly instead of replaying it as a CUDA graph")

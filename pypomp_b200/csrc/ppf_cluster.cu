@@ -300,7 +300,8 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
     if (rs) {
       const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
       if (l0 < nc) {
-        OffWalk wk = offwalk_init(o, E + tex);
+        uint64_t C = E + tex;
+        OffWalk wk = offwalk_init(o, C);
         st[l0] = wk.k;
         for (int l = l0; l < l1; ++l) {
           uint64_t q = 0;
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(TPB, 1) k_cluster(Args a, int JC) {
           for (int i = 0; i < QC; ++i)
             if (l - l0 == i) q = qk[i];
           if (l - l0 >= QC) q = qweight(Wc[l], Mx, qc);
-          const int kn = offwalk_add(o, wk, q);
+          const int kn = offwalk_add_c(o, wk, C, q);
           if (l + 1 < l1 || l + 1 == nc) st[l + 1] = kn;
         }
       }

@@ -250,19 +250,24 @@ __device__ __forceinline__ int nchild_fast(const Offsets& o, uint64_t C) {
 
 // Incremental form for consecutive parents: with P = k tot + chi and
 // D = C J, a parent of weight q moves D by q J (< 2^62) and its children are
-// the points P < D passed while advancing k.  No floating point, no division.
+// the points P < D passed while advancing k.  No floating point, no division
+// for the usual parent of a few children.
 struct OffWalk {
   uint64_t Dh, Dl, Ph, Pl;
   int k;
 };
 
-__device__ __forceinline__ OffWalk offwalk_init(const Offsets& o, uint64_t C) {
-  OffWalk w;
-  w.k = nchild_fast(o, C);
-  mul64(C, (uint64_t)o.J, w.Dh, w.Dl);
-  mul64((uint64_t)w.k, o.tot, w.Ph, w.Pl);
+__device__ __forceinline__ void offwalk_set_k(const Offsets& o, OffWalk& w, int k) {
+  w.k = k;
+  mul64((uint64_t)k, o.tot, w.Ph, w.Pl);
   w.Pl += o.chi;
   w.Ph += (w.Pl < o.chi);
+}
+
+__device__ __forceinline__ OffWalk offwalk_init(const Offsets& o, uint64_t C) {
+  OffWalk w;
+  mul64(C, (uint64_t)o.J, w.Dh, w.Dl);
+  offwalk_set_k(o, w, nchild_fast(o, C));
   return w;
 }
 
@@ -277,6 +282,49 @@ __device__ __forceinline__ int offwalk_add(const Offsets& o, OffWalk& w, uint64_
     ++w.k;
   }
   return w.k;
+}
+
+// The points are tot apart, so a parent with q J <= n tot has at most n
+// children.  offwalk_add walks them point by point: cheap for the usual parent
+// of a few children, but a parent that takes much of the swarm under
+// degenerate weights would cost its thread one step per child while the rest
+// of the CTA waits.  The callers therefore take the closed form (nchild_fast,
+// the same exact count, about as costly as 16 steps) for runs or parents that
+// hold more than about 64 expected children:
+//   * runs of parents held in registers test the run first (run_has_heavy,
+//     run_has_heavy_e) and then either walk (the usual case, the same code as
+//     without the test) or evaluate every offset in closed form;
+//   * loops over parents in shared or global memory call offwalk_add_c,
+//     which keeps the cumulative weight C (D = C J) and jumps per parent.
+// Both forms are exact, so the threshold only picks the faster one.
+__device__ __forceinline__ bool heavy_parent(const Offsets& o, uint64_t q) {
+  return ((q * (uint64_t)o.J) >> 6) > o.tot;
+}
+template <int N>
+__device__ __forceinline__ bool run_has_heavy(const Offsets& o, const uint64_t (&q)[N]) {
+  uint64_t m = 0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) m = q[i] > m ? q[i] : m;
+  return heavy_parent(o, m);
+}
+// The same test on the float weights e = q 2^-40 (an estimate is enough).
+template <int N>
+__device__ __forceinline__ bool run_has_heavy_e(const float (&e)[N], uint64_t tot, int J) {
+  float m = 0.0f;
+#pragma unroll
+  for (int i = 0; i < N; ++i) m = fmaxf(m, e[i]);
+  return m * (float)J > (float)tot * (64.0f / 1099511627776.0f);
+}
+__device__ __forceinline__ int offwalk_add_c(const Offsets& o, OffWalk& w, uint64_t& C, uint64_t q) {
+  C += q;
+  if (heavy_parent(o, q)) {
+    const uint64_t add = q * (uint64_t)o.J;
+    w.Dl += add;
+    w.Dh += (w.Dl < add);
+    offwalk_set_k(o, w, nchild_fast(o, C));
+    return w.k;
+  }
+  return offwalk_add(o, w, q);
 }
 
 // Parent (tile-local index) of child k: the last l in [0, n) with st[l] <= k.

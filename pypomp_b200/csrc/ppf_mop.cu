@@ -589,13 +589,23 @@ __global__ void __launch_bounds__(TPB, 1) k_mop_fwd_grid(Args a, int C, int JC) 
     float lt32 = 0.0f;
     if (rs) {
       const Offsets o = make_offsets(tot, u32, J);
-      if (l0 < nc) {
+      if (l0 < nc && !run_has_heavy(o, q)) {
         OffWalk wk = offwalk_init(o, E + tex);
         st[l0] = wk.k;
 #pragma unroll
         for (int i = 0; i < ITM; ++i) {
           if (l0 + i >= l1) break;
           const int kn = offwalk_add(o, wk, q[i]);
+          if (l0 + i + 1 < l1 || l0 + i + 1 == nc) st[l0 + i + 1] = kn;
+        }
+      } else if (l0 < nc) {
+        uint64_t C = E + tex;   // a heavy parent in the run: closed form throughout
+        st[l0] = nchild_fast(o, C);
+#pragma unroll
+        for (int i = 0; i < ITM; ++i) {
+          if (l0 + i >= l1) break;
+          C += q[i];
+          const int kn = nchild_fast(o, C);
           if (l0 + i + 1 < l1 || l0 + i + 1 == nc) st[l0 + i + 1] = kn;
         }
       }

@@ -167,10 +167,11 @@ __global__ void __launch_bounds__(TPB, 1) k_resident(Args a) {
     if (rs) {
       const Offsets o = make_offsets(tot, resample_u32(a, f, t), J);
       if (l0 < l1) {
-        OffWalk wk = offwalk_init(o, tex);
+        uint64_t C = tex;
+        OffWalk wk = offwalk_init(o, C);
         for (int j = l0; j < l1; ++j) {
           st[j] = wk.k;
-          offwalk_add(o, wk, qweight(ws[j], Mx, qc));
+          offwalk_add_c(o, wk, C, qweight(ws[j], Mx, qc));
         }
       }
     } else {

@@ -208,13 +208,23 @@ __device__ __forceinline__ void resprop_tile(const Args& a, int t, int f, int b)
       for (int i = 0; i < IT; ++i) q[i] = (l0 + i < ntile) ? qweight_from_e(wv[i]) : 0ull;   // k_sum left e
       // the exclusive prefix of this thread's run within the tile, from k_sum
       const uint64_t tex = a.runpre[((size_t)f * a.ntiles + b) * TPB + threadIdx.x];
-      if (l0 < ntile) {
+      if (l0 < ntile && !run_has_heavy_e(wv, tot, J)) {
         OffWalk wk = offwalk_init(o, E + tex);
         st[l0] = wk.k;
 #pragma unroll
         for (int i = 0; i < IT; ++i) {
           if (l0 + i >= ntile) break;
           const int kn = offwalk_add(o, wk, q[i]);
+          if (i + 1 < IT || l0 + i + 1 == ntile) st[l0 + i + 1] = kn;
+        }
+      } else if (l0 < ntile) {
+        uint64_t C = E + tex;   // a heavy parent in the run: closed form throughout
+        st[l0] = nchild_fast(o, C);
+#pragma unroll
+        for (int i = 0; i < IT; ++i) {
+          if (l0 + i >= ntile) break;
+          C += q[i];
+          const int kn = nchild_fast(o, C);
           if (i + 1 < IT || l0 + i + 1 == ntile) st[l0 + i + 1] = kn;
         }
       }
