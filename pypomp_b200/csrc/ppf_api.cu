@@ -98,8 +98,11 @@ static int choose_path(const ppf_pfilter_desc* d) {
   a.J = d->J; a.F = d->F; a.flags = d->flags; a.model = d->model; a.mode = MODE_PF;
   // the wide LG streams only
   if (lg_wide(d->model)) return PPF_PATH_STREAM;
-  // swarm fits one CTA's shared memory: keep it on chip for the whole loop
-  const bool resident = resident_smem_bytes(a) <= kResidentSmemMax && d->J <= 16384;
+  // swarm fits one CTA's shared memory: keep it on chip for the whole loop.
+  // Up to J = 8192: at J = 16384 (1024 Ricker filters) the streaming kernels
+  // take 179 ms against the resident kernel's 259 ms (one 512-thread CTA per
+  // SM holds such a swarm, too few warps to hide its latencies)
+  const bool resident = resident_smem_bytes(a) <= kResidentSmemMax && d->J <= 8192;
   if (resident && d->F >= kNumSMs) return PPF_PATH_RESIDENT;
   // few filters of a few thousand particles or more: the streaming kernels
   // would leave most SMs idle; a cluster per filter keeps the swarm on chip
