@@ -149,6 +149,9 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd(Args a, MopBwd mb, int t) {
     float lw = 0.0f;
     const float* lxi = mb.lx_in + (size_t)f * DX * J;
     const float* lwi = mb.lw_in + (size_t)f * J;
+    // a parent of many children (degenerate weights): several loads in flight,
+    // the sums still taken in child order
+#pragma unroll 4
     for (int k = lo; k < hi; ++k) {
 #pragma unroll
       for (int d = 0; d < DX; ++d) lx[d] += lxi[d * J + k];
@@ -764,6 +767,9 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_persist(Args a, MopBwdP mb, Gri
 #pragma unroll
       for (int d = 0; d < DX; ++d) lx[d] = 0.0f;
       float lw = 0.0f;
+      // a parent of many children (degenerate weights): several loads in flight,
+      // the sums still taken in child order
+#pragma unroll 4
       for (int k = lo; k < hi; ++k) {
 #pragma unroll
         for (int d = 0; d < DX; ++d) lx[d] += lxi[d * J + k];
@@ -972,6 +978,9 @@ __global__ void __launch_bounds__(TPB) k_mop_bwd_split(Args a, MopBwdP mb, GridB
 #pragma unroll
       for (int d = 0; d < DX; ++d) lx[d] = 0.0f;
       float lw = 0.0f;
+      // a parent of many children (degenerate weights): several loads in flight,
+      // the sums still taken in child order
+#pragma unroll 4
       for (int k = plo; k < phi; ++k) {
 #pragma unroll
         for (int d = 0; d < DX; ++d) lx[d] += lxi[(size_t)d * J + k];
